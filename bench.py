@@ -1,0 +1,318 @@
+#!/usr/bin/env python
+"""Throughput of the B1 bilinear fan-beam projector pair (forward + adjoint).
+
+Workload: 512 x 512 image at 0.5 mm of a seeded random-ellipse phantom,
+720 views over [0, 2 pi), 736 bins at 1.0 mm, source-isocentre 595 mm,
+source-detector 1085.6 mm.  One step = one forward projection and one back
+projection (A x, A^T y).  Metric: fwd+adj voxel-view updates per second,
+2 * nx * ny * np per step, summed over all ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`--impl reference` times the reference's CPU path for this operator (its
+sparse system matrix applied with scipy CSR SpMV, as
+python/operators/operators.py:31-49 does) on a bounded sample of views.
+Each rank of a multi-GPU run projects its own phantom (independent replicas,
+weak scaling); there is no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NX = NY = 512
+DX = DY = 0.5
+NP, NU, DU = 720, 736, 1.0
+LSD, LSO = 1085.6, 595.0
+ANGLES = 2 * np.pi * np.arange(NP) / NP
+METRIC = "fwd+adj voxel-view updates/s (B1 fan beam)"
+UNIT = "voxel-view updates/s"
+CONFIG = {
+    "workload": "B1 bilinear fan-beam forward + adjoint, 512x512 @0.5mm, 720 views over 2pi, 736 bins @1mm, "
+                "SOD 595 mm, SDD 1085.6 mm, seeded 10-ellipse phantom",
+    "nx": NX, "ny": NY, "views": NP, "bins": NU,
+    "l2": "flushed between steps (256 MiB write outside the timed events)",
+}
+FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# reference arm / CPU baseline: scipy CSR SpMV on a bounded sample of views
+# ---------------------------------------------------------------------------
+def cpu_spmv_sample(n_views=24, reps=3):
+    """Times A@x and A.T@y of the reference's sparse-matrix CPU path on the rows
+    of `n_views` evenly spaced views; returns (updates/s, description, seconds)."""
+    import scipy.sparse  # noqa: F401
+    from oracle import oracle
+    from sgd_b200.phantom import ellipse_phantom
+    views = np.arange(0, NP, NP // n_views)[:n_views]
+    A = oracle.b1_matrix(NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES, views)
+    x = ellipse_phantom(NX, NY, DX, DY, seed=0).ravel()
+    y = A @ x
+    AT = A.T
+    best = float("inf")
+    t_all = time.perf_counter()
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        A @ x
+        AT @ y
+        best = min(best, time.perf_counter() - t0)
+    spent = time.perf_counter() - t_all
+    units = 2.0 * NX * NY * len(views)
+    desc = (f"scipy CSR SpMV (python/operators/operators.py:45-49 path), FP64, single thread; "
+            f"rows of {len(views)} of {NP} views (nnz {A.nnz}), matrix entries from the FP64 replica of "
+            f"layers/A_B1.cu; best of {reps}")
+    return units / best, desc, spent
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = []
+    desc = ""
+    for _ in range(max(1, args.warmup // 3)):
+        cpu_spmv_sample(reps=1)
+    for _ in range(max(1, min(args.steps, 5))):
+        v, desc, _ = cpu_spmv_sample(reps=1)
+        steps.append(v)
+    value = statistics.median(steps)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": len(steps), "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", uuid, f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.file.flush()
+        self.file.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in self.file.read().strip().splitlines():
+            parts = [p.strip() for p in row.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_op_counts():
+    with open(os.path.join(ROOT, "sgd_b200", "op_counts.json")) as f:
+        return json.load(f)
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return {}
+    with open(p) as f:
+        return json.load(f)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from sgd_b200.operators import A_B1_operator
+    from sgd_b200.phantom import ellipse_phantom
+    from sgd_b200.torch_ops import FanProjector
+    from sgd_b200 import _lib
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    P = FanProjector("b1", NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES)
+    x_host = ellipse_phantom(NX, NY, DX, DY, seed=rank)
+    img = torch.tensor(x_host, dtype=torch.float32, device=dev)
+    sino = torch.empty((NP, NU), dtype=torch.float32, device=dev)
+    back = torch.empty((NX, NY), dtype=torch.float32, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        P.forward(img, out=sino)
+        P.backward(sino, out=back)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    sampler = ClockSampler(uuid)
+    time.sleep(0.3)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t_wall = time.perf_counter()
+    for k in range(K):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        P.forward(img, out=sino)
+        ev[k][1].record(stream)
+        P.backward(sino, out=back)
+        ev[k][2].record(stream)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    wall = time.perf_counter() - t_wall
+    clocks = sampler.stop()
+    fwd_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(K)]
+    bwd_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(K)]
+    step_ms = sum(f + b for f, b in zip(fwd_ms, bwd_ms)) / K
+    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms = float(t.item())
+    units = 2.0 * NX * NY * NP
+    value = world * units / (step_ms * 1e-3)
+
+    # end-to-end through the reference-facing C ABI with host FP64 buffers
+    A = A_B1_operator(NX, NY, NP, NU, DX, DY, DU, LSD, LSO, ANGLES)
+    xh = x_host.ravel().astype(np.float64)
+    yh = A.matvec(xh)
+    A.rmatvec(yh)
+    ke = min(K, 20)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for _ in range(ke):
+        yh = A.matvec(xh)
+        A.rmatvec(yh)
+    e2e_s = (time.perf_counter() - t0) / ke
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * units / float(te.item())
+
+    if rank != 0:
+        return
+
+    # roofline of the dominant kernel: algorithmic FLOPs of the reference
+    # formula per launch over its measured duration, against the FP32 FMA
+    # rate measured on this GPU now
+    ops = load_op_counts()["b1_c2"]
+    V = NX * NY * NP
+    E = P.conv_count
+    flops = ops["range_flops_per_pixel_view"] * V + ops["flops_per_evaluation"] * E
+    fwd_avg, bwd_avg = statistics.mean(fwd_ms), statistics.mean(bwd_ms)
+    dom, dom_ms = ("b1_back_kernel", bwd_avg) if bwd_avg >= fwd_avg else ("b1_forward_kernel", fwd_avg)
+    L = _lib.lib()
+    L.sgd_fp32_fma_rate.restype = __import__("ctypes").c_double
+    L.sgd_fp32_fma_rate.argtypes = [__import__("ctypes").c_void_p, __import__("ctypes").c_int,
+                                    __import__("ctypes").c_int, __import__("ctypes").c_void_p]
+    scratch = torch.empty(148 * 64, dtype=torch.float32, device=dev)
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak = max(L.sgd_fp32_fma_rate(scratch.data_ptr(), nsm * 8 * 4, 4096, stream.cuda_stream) for _ in range(3))
+    achieved = flops / (dom_ms * 1e-3)
+    traffic = load_traffic().get(dom)
+    roofline = {
+        "bound": "fp32", "kernel": dom, "achieved": achieved / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+        "frac": achieved / peak, "traffic": traffic,
+        "peak_source": "measured now: FP32 FMA probe kernel (sgd_fp32_fma_rate), same clocks",
+        "flops_per_launch": flops,
+        "flops_model": f"{ops['range_flops_per_pixel_view']:.1f} x pixel-views + "
+                       f"{ops['flops_per_evaluation']:.1f} x footprint evaluations ({E})",
+        "fwd_ms": fwd_avg, "bwd_ms": bwd_avg,
+    }
+
+    cpu = None
+    if world == 1:
+        v, desc, spent = cpu_spmv_sample(reps=3)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": desc, "seconds": round(spent, 2)}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas x{world}"),
+        "roofline": roofline, "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * (NX * NY + NP * NU),
+                "d2h_bytes_per_step": 4 * (NP * NU + NX * NY),
+                "path": "A_B1_operator.matvec/rmatvec -> b1_forward_projection / b1_backward_projection, FP64 numpy"},
+        "gpu_launches": 3 * K,
+        "clocks": clocks,
+        "wall_s": wall,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,75 @@
+/* C ABI of sgd_b200/libnetwork.so, the B200-native CT projector library.
+ *
+ * The first group of each projector keeps the reference's extern "C" names and
+ * signatures (hqpwca/SGD, layers/A_*.hh / layers/A_*.cu) so that callers that
+ * bind the reference's libnetwork.so (python/operators/operators.py through
+ * ctypes) bind this library unchanged.  The second group is new: explicit
+ * destruction, error text, and FP32 device-pointer entry points for callers
+ * that keep images and sinograms on the GPU.
+ *
+ * Conventions (all entry points):
+ *   image    x[ix*ny + iy]        (reference host layout, layers/A_B1.cu:621-623)
+ *   sinogram b[p*nu + u]          (layers/A_B1.cu:639-641)
+ *   angles   radians, one per view
+ *   errors   never thrown across the ABI: a failing call returns NULL / -1
+ *            (void reference functions return nothing) and sgd_last_error()
+ *            gives the message of the last failure on the calling thread.
+ *   threads  calls on one handle must not overlap; distinct handles are
+ *            independent.
+ */
+#ifndef SGD_B200_H
+#define SGD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Message of the last failure on this thread (new; the reference has no
+ * error reporting, utils/exception.hh throws across the ABI). */
+const char* sgd_last_error(void);
+
+/* ---- B1 bilinear box-spline, 2D fan beam ---------------------------------- */
+
+/* Replaces b1_init, layers/A_B1.hh:24 / layers/A_B1.cu:595-603.  dz and drho
+ * may be NULL (the reference declares them with C++ default arguments; a C
+ * caller must pass all twelve).  Returns NULL on failure. */
+void* b1_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+              double* angles, double* dz, double* drho);
+
+/* Replaces b1_forward_projection, layers/A_B1.hh:25 / layers/A_B1.cu:605-644:
+ * b = A x (b overwritten).  Returns the reference's footprint-evaluation count
+ * for this geometry (its conv_count), or -1 on failure. */
+int b1_forward_projection(double* b, double* x, void* layer);
+
+/* Replaces b1_backward_projection, layers/A_B1.hh:26 / layers/A_B1.cu:646-678:
+ * x = A^T b (x overwritten). */
+void b1_backward_projection(double* b, double* x, void* layer);
+
+/* New: b1_backward_projection with a status (0 ok, -1 failure). */
+int sgd_b1_backward_projection(double* b, double* x, void* layer);
+
+/* New: frees a layer returned by b1_init (the reference never frees). */
+void b1_destroy(void* layer);
+
+/* New: FP32 device entry points on a caller's stream (cudaStream_t, NULL =
+ * legacy default stream).  d_img: nx*ny floats, d_sino: np*nu floats, both
+ * device memory.  The forward overwrites d_sino, the backward d_img.
+ * Return 0 on success, -1 on failure. */
+int sgd_b1_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream);
+int sgd_b1_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
+
+/* New: the reference's footprint-evaluation count for the layer's geometry. */
+unsigned long long sgd_b1_count(void* layer);
+
+/* ---- measurement ---------------------------------------------------------- */
+
+/* New (no reference counterpart): FP32 FMA throughput of the current GPU in
+ * FLOP/s (FMA = 2 FLOPs), the roofline denominator of the projectors.
+ * scratch: >= blocks floats of device memory.  Returns -1 on failure. */
+double sgd_fp32_fma_rate(float* scratch, int blocks, int iters, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGD_B200_H */

@@ -1,0 +1,112 @@
+"""ORACLE — test infrastructure only (tests/, smoke() and bench.py's CPU-baseline
+leg).  ctypes bindings of oracle/liboracle.so, the CPU restatement of the
+reference projector layer (oracle/sgd_oracle.cpp).  The product package never
+imports this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle library missing: {path} (run `make -C oracle`)")
+        _LIB = ctypes.CDLL(path)
+        L = _LIB
+        L.oracle_geometry.restype = None
+        L.oracle_b1_forward.restype = ctypes.c_longlong
+        L.oracle_b1_backward.restype = None
+        L.oracle_b1_matrix.restype = ctypes.c_longlong
+        L.oracle_b1_flops.restype = None
+    return _LIB
+
+
+def _p(a):
+    if a is None:
+        return None
+    return a.ctypes.data_as(_dp)
+
+
+def _c(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def geometry(nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, dzs=None, drho=None):
+    """utils/geo.cu geometry: dict of src/dtv/puv/pvv (np,3), pm (np,12), pmi (np,12) float32."""
+    angles = _c(angles)
+    n = len(angles)
+    out = {k: np.zeros((n, 3)) for k in ("src", "dtv", "puv", "pvv")}
+    out["pm"] = np.zeros((n, 12))
+    out["pmi"] = np.zeros((n, 12), dtype=np.float32)
+    lib().oracle_geometry(nx, ny, nz, n, nu, nv, ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(dz),
+                          ctypes.c_double(du), ctypes.c_double(dv), ctypes.c_double(lsd), ctypes.c_double(lso),
+                          _p(angles), _p(_c(dzs)), _p(_c(drho)), _p(out["src"]), _p(out["dtv"]),
+                          _p(out["puv"]), _p(out["pvv"]), _p(out["pm"]), out["pmi"].ctypes.data_as(_fp))
+    return out
+
+
+def b1_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
+    """FP64 replica (precision=0) or FP32 emulation (1) of b1_forward_projection.
+
+    x: host layout x[ix*ny+iy]; returns (b[np*nu], footprint-evaluation count).
+    """
+    angles = _c(angles)
+    x = _c(np.ravel(x))
+    b = np.zeros(len(angles) * nu)
+    cnt = lib().oracle_b1_forward(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy),
+                                  ctypes.c_double(du), ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles),
+                                  _p(_c(dzs)), _p(_c(drho)), _p(x), _p(b), precision)
+    return b, int(cnt)
+
+
+def b1_backward(b, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
+    """FP64 replica (precision=0) or FP32 emulation (1) of b1_backward_projection."""
+    angles = _c(angles)
+    b = _c(np.ravel(b))
+    x = np.zeros(nx * ny)
+    lib().oracle_b1_backward(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(du),
+                             ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), _p(_c(dzs)), _p(_c(drho)),
+                             _p(b), _p(x), precision)
+    return x
+
+
+def b1_flops(nx, ny, nu, dx, dy, du, lsd, lso, angles, nviews=8):
+    """(range FLOPs per pixel-view, FLOPs per footprint evaluation, evaluations per pixel-view)."""
+    angles = _c(angles)
+    out = np.zeros(3)
+    lib().oracle_b1_flops(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(du),
+                          ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), nviews, _p(out))
+    return tuple(out)
+
+
+def b1_matrix(nx, ny, nu, dx, dy, du, lsd, lso, angles, views):
+    """scipy CSR rows of the B1 system matrix for the listed views (FP64 replica)."""
+    import scipy.sparse as sp
+    angles = _c(angles)
+    views = np.ascontiguousarray(views, dtype=np.int32)
+    cap = int(len(views) * nx * ny * 4.5)
+    while True:
+        rows = np.empty(cap, dtype=np.int32)
+        cols = np.empty(cap, dtype=np.int32)
+        vals = np.empty(cap, dtype=np.float64)
+        n = lib().oracle_b1_matrix(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy),
+                                   ctypes.c_double(du), ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles),
+                                   views.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(views),
+                                   ctypes.c_longlong(cap), rows.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                   cols.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _p(vals))
+        if n <= cap:
+            break
+        cap = int(n)
+    return sp.csr_matrix((vals[:n], (rows[:n], cols[:n])), shape=(len(views) * nu, nx * ny))

@@ -1,0 +1,507 @@
+// ORACLE — test infrastructure only, never part of the product path.
+//
+// A CPU restatement of the hqpwca/SGD CT projector layer, used by the tests, by
+// `__graft_entry__.smoke()` and by the CPU-baseline leg of `bench.py` as the
+// checker for the CUDA kernels in `sgd_b200/`.  Nothing in `sgd_b200/` links,
+// loads or calls this file.
+//
+// Two kinds of function live here:
+//   * formula replicas: the reference kernel's arithmetic restated on the CPU,
+//     with the same visited-bin ranges, thresholds and normalisations.  They
+//     are templated on the arithmetic type: `double` gives the FP64 replica,
+//     `float` an FP32 emulation of the reference kernel (without its FMA
+//     contraction) that shows how far the reference's own FP32 rounding sits
+//     from the FP64 replica;
+//   * geometry: `utils/geo.cu` restated (rotation, 45-degree snapping,
+//     3x4 projection matrix and its index-space FP32 form `pmi`).
+//
+// Each function cites the reference file:line it follows.  The parity of this
+// restatement with the reference itself is pinned by fixtures produced by the
+// reference library built from source and run on a B200 (tests/golden/).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <cstdlib>
+#include <vector>
+#include <algorithm>
+#include <atomic>
+#include <type_traits>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+const double kPI = 3.14159265358979323846;  // utils/geo.hh:7
+
+// ---------------------------------------------------------------------------
+// geometry: utils/geo.cu
+// ---------------------------------------------------------------------------
+
+// utils/geo.cu:3-28 (row-major a[x*y] times b[y*z], result written to b)
+void multm(const double* a, double* b, int x, int y, int z) {
+    std::vector<double> c(x * z);
+    for (int i = 0; i < x; i++)
+        for (int j = 0; j < z; j++) {
+            double s = 0.0;
+            for (int k = 0; k < y; k++) s += a[i * y + k] * b[k * z + j];
+            c[i * z + j] = s;
+        }
+    for (int i = 0; i < x * z; i++) b[i] = c[i];
+}
+
+// utils/geo.cu:30-56: inverse of a 3x3, identity when |det| < 1e-10
+void invert3(double* m) {
+    double n[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double det = m[0] * ((m[4] * m[8]) - (m[5] * m[7])) - m[1] * ((m[3] * m[8]) - (m[5] * m[6])) +
+                 m[2] * ((m[3] * m[7]) - (m[4] * m[6]));
+    if (std::fabs(det) < 1e-10) {
+        n[0] = 1, n[4] = 1, n[8] = 1;
+    } else {
+        n[0] = ((m[4] * m[8]) - (m[5] * m[7])) / det;
+        n[1] = -1 * ((m[1] * m[8]) - (m[2] * m[7])) / det;
+        n[2] = ((m[1] * m[5]) - (m[2] * m[4])) / det;
+        n[3] = -1 * ((m[3] * m[8]) - (m[5] * m[6])) / det;
+        n[4] = ((m[0] * m[8]) - (m[2] * m[6])) / det;
+        n[5] = -1 * ((m[0] * m[5]) - (m[2] * m[3])) / det;
+        n[6] = ((m[3] * m[7]) - (m[4] * m[6])) / det;
+        n[7] = -1 * ((m[0] * m[7]) - (m[1] * m[6])) / det;
+        n[8] = ((m[0] * m[4]) - (m[1] * m[3])) / det;
+    }
+    for (int i = 0; i < 9; i++) m[i] = n[i];
+}
+
+// utils/geo.cu:58-161
+void projection_matrix(double* pm, float* pmi, const double* src, const double* dtv, const double* puv,
+                       const double* pvv, double uc, double vc, int nx, int ny, int nz, double ddx,
+                       double ddy, double ddz) {
+    double norm[3], vec[3];
+    norm[0] = puv[1] * pvv[2] - puv[2] * pvv[1];
+    norm[1] = puv[2] * pvv[0] - puv[0] * pvv[2];
+    norm[2] = puv[0] * pvv[1] - puv[1] * pvv[0];
+    double k = 0.0;
+    for (int i = 0; i < 3; i++) k += norm[i] * (dtv[i] - src[i]);
+    for (int i = 0; i < 3; i++) vec[i] = src[i] - dtv[i] + (uc * puv[i]) + (vc * pvv[i]) + 1;
+    double pm4[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    double trans[16] = {1, 0, 0, -src[0], 0, 1, 0, -src[1], 0, 0, 1, -src[2], 0, 0, 0, 1};
+    multm(trans, pm4, 4, 4, 4);
+    double divdot[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, norm[0], norm[1], norm[2], 0};
+    multm(divdot, pm4, 4, 4, 4);
+    double scale[16] = {k, 0, 0, 0, 0, k, 0, 0, 0, 0, k, 0, 0, 0, 0, 1};
+    multm(scale, pm4, 4, 4, 4);
+    double trans2[12] = {1, 0, 0, vec[0], 0, 1, 0, vec[1], 0, 0, 1, vec[2]};
+    multm(trans2, pm4, 3, 4, 4);
+    double align[9] = {puv[0], pvv[0], 1, puv[1], pvv[1], 1, puv[2], pvv[2], 1};
+    invert3(align);
+    multm(align, pm4, 3, 3, 4);
+    for (int i = 0; i < 12; i++) pm[i] = pm4[i] / pm4[11];
+    // geo.cu:141-160: the index-space form is computed in FP32
+    float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+    float ox = (nx - 1) * dx / 2.0f, oy = (ny - 1) * dy / 2.0f, oz = (nz - 1) * dz / 2.0f;
+    pmi[0] = dx * pm[0]; pmi[1] = dy * pm[1]; pmi[2] = dz * pm[2];
+    pmi[3] = pm[3] - ox * pm[0] - oy * pm[1] - oz * pm[2];
+    pmi[4] = dx * pm[4]; pmi[5] = dy * pm[5]; pmi[6] = dz * pm[6];
+    pmi[7] = pm[7] - ox * pm[4] - oy * pm[5] - oz * pm[6];
+    pmi[8] = dx * pm[8]; pmi[9] = dy * pm[9]; pmi[10] = dz * pm[10];
+    pmi[11] = pm[11] - ox * pm[8] - oy * pm[9] - oz * pm[10];
+}
+
+void rotate(const double* vec, double* res, double angle) {  // utils/geo.cu:203-207
+    res[0] = vec[0] * std::cos(angle) - vec[1] * std::sin(angle);
+    res[1] = vec[0] * std::sin(angle) + vec[1] * std::cos(angle);
+    res[2] = vec[2];
+}
+
+struct Geo {
+    int nx, ny, nz, nu, nv, np;
+    double dx, dy, dz, du, dv;
+    std::vector<double> src, dtv, puv, pvv, pm;
+    std::vector<float> pmi;
+};
+
+// utils/geo.cu:232-269 (mode 0, per-view angles with 45-degree snapping) and
+// utils/geo.cu:209-230 (mode 1, uniform angles without snapping), followed by
+// utils/geo.cu:188-201 (projection matrices).
+void build_geo(Geo& g, double lsd, double lso, const double* angles, const double* dzs,
+               const double* drho) {
+    int np = g.np;
+    g.src.assign(3 * np, 0.0); g.dtv.assign(3 * np, 0.0);
+    g.puv.assign(3 * np, 0.0); g.pvv.assign(3 * np, 0.0);
+    g.pm.assign(12 * np, 0.0); g.pmi.assign(12 * np, 0.0f);
+    double src0[3] = {-lso, 0.0, 0.0};
+    double dtv0[3] = {lsd - lso, 0.0, 0.0};
+    double puv0[3] = {0.0, g.du, 0.0};
+    double pvv0[3] = {0.0, 0.0, g.dv};
+    for (int i = 0; i < np; ++i) {
+        long double beta = angles[i];
+        double s[3] = {src0[0], src0[1], 0.0};
+        if (dzs) s[2] = dzs[i];
+        if (drho) s[0] = src0[0] + drho[i];
+        if (std::fabs(std::sin(beta) - std::cos(beta)) < 1e-7L)
+            beta = (std::sin(beta) > 0) ? kPI / 4 : -kPI * 3 / 4;
+        else if (std::fabs(std::sin(beta) + std::cos(beta)) < 1e-7L)
+            beta = (std::sin(beta) > 0) ? kPI * 3 / 4 : -kPI / 4;
+        double b = (double)beta;
+        rotate(s, &g.src[3 * i], b);
+        rotate(dtv0, &g.dtv[3 * i], b);
+        rotate(puv0, &g.puv[3 * i], b);
+        rotate(pvv0, &g.pvv[3 * i], b);
+    }
+    for (int p = 0; p < np; ++p)
+        projection_matrix(&g.pm[12 * p], &g.pmi[12 * p], &g.src[3 * p], &g.dtv[3 * p], &g.puv[3 * p],
+                          &g.pvv[3 * p], g.nu / 2.0, g.nv / 2.0, g.nx, g.ny, g.nz, g.dx, g.dy, g.dz);
+}
+
+// ---------------------------------------------------------------------------
+// box-spline closed forms: layers/spline_conv.hh
+// ---------------------------------------------------------------------------
+
+// FLOP-counting scalar: every +, -, *, /, sqrt on it adds one to the counter
+// (comparisons, abs, min/max are not counted).  Used once to freeze the
+// algorithmic work of the reference formulas for the roofline.
+struct CountedF {
+    double v;
+    static thread_local long long flops;
+    CountedF(double x = 0.0) : v(x) {}
+    explicit operator double() const { return v; }
+};
+thread_local long long CountedF::flops = 0;
+inline CountedF operator+(CountedF a, CountedF b) { ++CountedF::flops; return a.v + b.v; }
+inline CountedF operator-(CountedF a, CountedF b) { ++CountedF::flops; return a.v - b.v; }
+inline CountedF operator*(CountedF a, CountedF b) { ++CountedF::flops; return a.v * b.v; }
+inline CountedF operator/(CountedF a, CountedF b) { ++CountedF::flops; return a.v / b.v; }
+inline CountedF operator-(CountedF a) { return -a.v; }
+inline CountedF& operator+=(CountedF& a, CountedF b) { ++CountedF::flops; a.v += b.v; return a; }
+inline bool operator<(CountedF a, CountedF b) { return a.v < b.v; }
+inline bool operator>(CountedF a, CountedF b) { return a.v > b.v; }
+inline bool operator<=(CountedF a, CountedF b) { return a.v <= b.v; }
+inline bool operator>=(CountedF a, CountedF b) { return a.v >= b.v; }
+inline bool operator==(CountedF a, CountedF b) { return a.v == b.v; }
+inline CountedF sqrt(CountedF a) { ++CountedF::flops; return std::sqrt(a.v); }
+inline CountedF fabs(CountedF a) { return std::fabs(a.v); }
+inline CountedF floor(CountedF a) { return std::floor(a.v); }
+inline CountedF max(CountedF a, CountedF b) { return a.v > b.v ? a : b; }
+inline CountedF min(CountedF a, CountedF b) { return a.v < b.v ? a : b; }
+using std::sqrt;
+using std::fabs;
+using std::floor;
+using std::max;
+using std::min;
+
+template <class T> inline void sort2(T& a, T& b) { if (a > b) std::swap(a, b); }  // :6-14
+template <class T> inline void sort4(T* u) {  // :25-39
+    sort2(u[0], u[1]); sort2(u[2], u[3]); sort2(u[0], u[2]); sort2(u[1], u[3]); sort2(u[1], u[2]);
+}
+
+// layers/spline_conv.hh:295-332 (b <= a - b)
+template <class T> T conv_2tri_1box_ag2b(T a, T b, T x) {
+    T a3 = a * a * a, ab2 = a * b * b, b3 = b * b * b;
+    T k1 = (6 * a * a * b * b);
+    T sum = 0;
+    if (x <= b) return (x * (12 * ab2 - 4 * b3 - 4 * b * x * x + x * x * x)) / (2 * k1);
+    sum += ((12 * a - 7 * b) * b) / (12 * a * a);
+    if (x <= a - b) return sum + (-2 * a * b + b * b + 2 * a * x - x * x) / (2 * a * a);
+    sum += T(0.5) - b / a;
+    if (x <= a)
+        return sum + ((a - b - x) * (a3 - 13 * b3 + 9 * b * b * x - 3 * b * x * x - x * x * x -
+                                     3 * a * a * (b + x) - 3 * a * (b - x) * (3 * b + x))) / (4 * k1);
+    sum += (13 * b * b) / (24 * a * a);
+    if (x < a + b)
+        return sum + ((x - a) * (a + 2 * b - x) * (a * a + 2 * a * b + 2 * b * b - 2 * (a + b) * x + x * x)) /
+                         (4 * k1);
+    return sum + b * b / (24 * a * a);
+}
+
+// layers/spline_conv.hh:334-370 (b > a - b)
+template <class T> T conv_2tri_1box_al2b(T a, T b, T x) {
+    T a3 = a * a * a, a2b = a * a * b, ab2 = a * b * b, b3 = b * b * b;
+    T k1 = (6 * a * a * b * b), k2 = a - b;
+    T sum = 0;
+    if (x <= a - b) return (x * (12 * ab2 - 4 * b3 - 4 * b * x * x + x * x * x)) / (2 * k1);
+    sum += ((a - b) * (a3 - 7 * a2b + 23 * ab2 - 9 * b3)) / (2 * k1);
+    if (x <= b)
+        return sum + (((x - a + b) * (a3 - 11 * a2b + 43 * ab2 - 17 * b3 + (5 * a - 13 * b) * k2 * x -
+                                      (a + 7 * b) * x * x + 3 * x * x * x)) / (4 * k1));
+    sum += (((2 * b - a) * (a3 - 6 * a2b + 24 * ab2 - 8 * b3)) / (4 * k1));
+    if (x <= a)
+        return sum + (((b - x) * (4 * a3 - 3 * b3 + b * b * x - 5 * b * x * x - x * x * x - 6 * a * a * (3 * b + x) +
+                                  4 * a * (b * b + 4 * b * x + x * x))) / (4 * k1));
+    sum += (((b - a) * (a3 - 7 * a2b + 5 * ab2 - 3 * b3)) / (4 * k1));
+    if (x < a + b)
+        return sum + ((x - a) * (a + 2 * b - x) * (a * a + 2 * a * b + 2 * b * b - 2 * (a + b) * x + x * x)) /
+                         (4 * k1);
+    return sum + b * b / (24 * a * a);
+}
+
+// layers/spline_conv.hh:372-390
+template <class T> T fast_2tri_1box_spline(T a, T b, T x1, T x2) {
+    bool side = (x1 * x2) > T(0);
+    x1 = fabs(x1), x2 = fabs(x2);
+    T s1, s2;
+    if (b <= a - b) { s1 = conv_2tri_1box_ag2b(a, b, x1); s2 = conv_2tri_1box_ag2b(a, b, x2); }
+    else { s1 = conv_2tri_1box_al2b(a, b, x1); s2 = conv_2tri_1box_al2b(a, b, x2); }
+    return side ? fabs(s1 - s2) : (s1 + s2);
+}
+
+// layers/spline_conv.hh:393-405
+template <class T> T fast_1tri_1box_spline(T a, T x1, T x2) {
+    bool side = (x1 * x2) > T(0);
+    x1 = fabs(x1), x2 = fabs(x2);
+    T s1 = (x1 >= a) ? T(0.5) : (x1 / a - (x1 * x1) / (2 * a * a));
+    T s2 = (x2 >= a) ? T(0.5) : (x2 / a - (x2 * x2) / (2 * a * a));
+    return side ? fabs(s1 - s2) : (s1 + s2);
+}
+
+// layers/A_B1.cu:48-59
+template <class T> T b1_linear_convolution_1d(T x1, T x2, T a, T b) {
+    if (b > T(1e-7f)) return fast_2tri_1box_spline<T>(a, b, x1, x2) / fabs(x2 - x1);
+    return fast_1tri_1box_spline<T>(a, x1, x2) / fabs(x2 - x1);
+}
+
+// ---------------------------------------------------------------------------
+// visited bin range (every 2D kernel, e.g. layers/A_B1.cu:120-151): the corners
+// (ix+-h, iy+-h) projected through pmi in FP32, sorted, floored and clamped.
+// ---------------------------------------------------------------------------
+template <class T = float>
+inline void bin_range(const float* pm, float puvx, bool singular, float sx1, float sx2, float sy1, float sy2,
+                      int nu, int& minu, int& maxu, float* us_out = nullptr) {
+    T us[4];
+    T xs[4] = {sx1, sx1, sx2, sx2};
+    T ys[4] = {sy1, sy2, sy1, sy2};
+    for (int k = 0; k < 4; ++k) {
+        T num = T(pm[0]) * xs[k] + T(pm[3]) + T(pm[1]) * ys[k];
+        T den = T(pm[8]) * xs[k] + T(pm[11]) + T(pm[9]) * ys[k];
+        us[k] = num / den;
+        if (singular) us[k] = (us[k] * T(1.5f) - T(1.0f)) / T(puvx);
+    }
+    sort4(us);
+    minu = std::min(std::max(0, (int)(double)floor(us[0])), nu - 1);
+    maxu = std::min(std::max(0, (int)(double)floor(us[3])), nu - 1);
+    if (us_out) for (int k = 0; k < 4; ++k) us_out[k] = (float)(double)us[k];
+}
+
+// ---------------------------------------------------------------------------
+// B1 (bilinear) fan-beam projector: layers/A_B1.cu
+// ---------------------------------------------------------------------------
+
+// per-(view,bin) vx, vy in FP32: layers/A_B1.cu:429-478
+void b1_vectors(const Geo& g, std::vector<float>& vecs) {
+    int np = g.np, nu = g.nu;
+    vecs.assign((size_t)2 * np * nu, 0.0f);
+    for (int p = 0; p < np; ++p) {
+        double cx = g.dtv[3 * p], cy = g.dtv[3 * p + 1];
+        double ux = g.puv[3 * p], uy = g.puv[3 * p + 1];
+        double px = g.src[3 * p], py = g.src[3 * p + 1];
+        for (int u = 0; u < nu; ++u) {
+            double sx = cx + ux * (u - 0.5 * nu + 0.5), sy = cy + uy * (u - 0.5 * nu + 0.5);
+            double theta = std::atan2(std::fabs(px - sx), std::fabs(py - sy));
+            vecs[(size_t)p * nu * 2 + u] = (float)std::fabs(g.dx * std::cos(theta));
+            vecs[(size_t)p * nu * 2 + nu + u] = (float)std::fabs(g.dy * std::sin(theta));
+        }
+    }
+}
+
+// The per-(pixel,view) body shared by b1_forward_projection (layers/A_B1.cu:62-208)
+// and b1_backward_projection (:211-353).  `visit(u, conv)` is called for every
+// bin the reference keeps (conv > 1e-7, :203 and :347).  Returns the number of
+// footprint evaluations (the reference's conv_count increments, :50).
+template <class T, class Visit>
+long long b1_pixel_view(const Geo& g, const float* vecs_p, int p, int ix, int iy, Visit visit) {
+    int nx = g.nx, ny = g.ny, nu = g.nu;
+    float dx = (float)g.dx, dy = (float)g.dy;
+    const float* pm = &g.pmi[12 * p];
+    float srcx = (float)g.src[3 * p], srcy = (float)g.src[3 * p + 1];
+    float puvx = (float)g.puv[3 * p], puvy = (float)g.puv[3 * p + 1];
+    float dtvx = (float)g.dtv[3 * p], dtvy = (float)g.dtv[3 * p + 1];
+    bool singular = std::fabs(puvx - puvy) < 1e-7f;  // :103
+    float fox = (ix - 0.5f * (nx - 1)) * dx;       // :96
+    float foy = (iy - 0.5f * (ny - 1)) * dy;       // :98
+    int minu, maxu;
+    // :100-151 (the range always runs in FP32, except under op counting)
+    if (std::is_same<T, CountedF>::value)
+        bin_range<CountedF>(pm, puvx, singular, ix - 1.0f, ix + 1.0f, iy - 1.0f, iy + 1.0f, nu, minu, maxu);
+    else
+        bin_range<float>(pm, puvx, singular, ix - 1.0f, ix + 1.0f, iy - 1.0f, iy + 1.0f, nu, minu, maxu);
+    T ox = fox, oy = foy, px = srcx, py = srcy;
+    long long cnt = 0;
+    for (int u = minu; u <= maxu; ++u) {
+        T off = T(u) - T(0.5f) * nu + T(0.5f);
+        T sx = T(dtvx) + T(puvx) * off, sy = T(dtvy) + T(puvy) * off;  // :153-154, :160
+        T vx = vecs_p[u], vy = vecs_p[nu + u];                         // :163-164
+        T ax = sx - T(puvx) * T(0.5f), ay = sy - T(puvy) * T(0.5f);   // :182-185
+        T bx = sx + T(puvx) * T(0.5f), by = sy + T(puvy) * T(0.5f);
+        T num = (ox - px) * (sx - px) + (oy - py) * (sy - py);
+        T ra = num / ((ax - px) * (sx - px) + (ay - py) * (sy - py));  // :187-188
+        T rb = num / ((bx - px) * (sx - px) + (by - py) * (sy - py));
+        T ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;      // :189-190
+        T bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
+        T x1 = sqrt((ax1 - ox) * (ax1 - ox) + (ay1 - oy) * (ay1 - oy));  // :192-193
+        T x2 = sqrt((bx1 - ox) * (bx1 - ox) + (by1 - oy) * (by1 - oy));
+        T sgn = ((ax1 - ox) * (bx1 - ox) + (ay1 - oy) * (by1 - oy) > T(0)) ? T(1) : T(-1);  // :195
+        T conv = b1_linear_convolution_1d<T>(x1 * sgn, x2, max(vx, vy), min(vx, vy));  // :197
+        ++cnt;
+        if (conv == conv && conv > T(1e-7f)) visit(u, (double)conv);
+    }
+    return cnt;
+}
+
+template <class T>
+long long b1_forward(const Geo& g, const std::vector<float>& vecs, const double* x, double* b) {
+    int nx = g.nx, ny = g.ny, nu = g.nu, np = g.np;
+    double dxy = (double)(float)g.dx * (double)(float)g.dy;
+    std::memset(b, 0, sizeof(double) * (size_t)np * nu);
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : total)
+    for (int p = 0; p < np; ++p) {
+        double* bp = b + (size_t)p * nu;
+        const float* vp = &vecs[(size_t)p * nu * 2];
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                double C = x[(size_t)ix * ny + iy];  // host layout x[ix*ny+iy], A_B1.cu:621-623
+                total += b1_pixel_view<T>(g, vp, p, ix, iy, [&](int u, double conv) { bp[u] += conv * C * dxy; });
+            }
+    }
+    return total;
+}
+
+template <class T>
+void b1_backward(const Geo& g, const std::vector<float>& vecs, const double* b, double* x) {
+    int nx = g.nx, ny = g.ny, nu = g.nu, np = g.np;
+    double dxy = (double)(float)g.dx * (double)(float)g.dy;
+#pragma omp parallel for schedule(dynamic)
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            double acc = 0.0;
+            for (int p = 0; p < np; ++p) {
+                const double* bp = b + (size_t)p * nu;
+                const float* vp = &vecs[(size_t)p * nu * 2];
+                double val = 0.0;  // :304, one partial per view, :351
+                b1_pixel_view<T>(g, vp, p, ix, iy, [&](int u, double conv) { val += conv * bp[u] * dxy; });
+                acc += val;
+            }
+            x[(size_t)ix * ny + iy] = acc;
+        }
+}
+
+Geo make_geo(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
+             double dv) {
+    Geo g;
+    g.nx = nx; g.ny = ny; g.nz = nz; g.np = np; g.nu = nu; g.nv = nv;
+    g.dx = dx; g.dy = dy; g.dz = dz; g.du = du; g.dv = dv;
+    return g;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Geometry tables exactly as utils/geo.cu builds them (2D inits use nz = nv = 1,
+// dz = dv = 1, layers/A_B1.cu:596).
+void oracle_geometry(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
+                     double dv, double lsd, double lso, const double* angles, const double* dzs,
+                     const double* drho, double* src, double* dtv, double* puv, double* pvv, double* pm,
+                     float* pmi) {
+    Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
+    build_geo(g, lsd, lso, angles, dzs, drho);
+    std::memcpy(src, g.src.data(), sizeof(double) * 3 * np);
+    std::memcpy(dtv, g.dtv.data(), sizeof(double) * 3 * np);
+    std::memcpy(puv, g.puv.data(), sizeof(double) * 3 * np);
+    std::memcpy(pvv, g.pvv.data(), sizeof(double) * 3 * np);
+    std::memcpy(pm, g.pm.data(), sizeof(double) * 12 * np);
+    std::memcpy(pmi, g.pmi.data(), sizeof(float) * 12 * np);
+}
+
+// b1_forward_projection / b1_backward_projection (layers/A_B1.cu:605-678) with the
+// same host layouts: x[ix*ny+iy], b[p*nu+u].  precision: 0 = FP64 replica,
+// 1 = FP32 emulation.  dz/drho may be null.  Returns the footprint-evaluation count.
+long long oracle_b1_forward(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd,
+                            double lso, const double* angles, const double* dzs, const double* drho,
+                            const double* x, double* b, int precision) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, dzs, drho);
+    std::vector<float> vecs;
+    b1_vectors(g, vecs);
+    return precision ? b1_forward<float>(g, vecs, x, b) : b1_forward<double>(g, vecs, x, b);
+}
+
+void oracle_b1_backward(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                        const double* angles, const double* dzs, const double* drho, const double* b, double* x,
+                        int precision) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, dzs, drho);
+    std::vector<float> vecs;
+    b1_vectors(g, vecs);
+    if (precision) b1_backward<float>(g, vecs, b, x); else b1_backward<double>(g, vecs, b, x);
+}
+
+// Rows of the B1 system matrix for the views listed in `views` (the entries the
+// reference's kernels produce, FP64 replica), as COO triplets in row-major
+// order: row = k*nu + u for the k-th listed view, col = ix*ny + iy (the column
+// convention of layers/A_B1.cu:580-582).  Writes at most `cap` entries and
+// returns the count needed (call again with a larger buffer if it exceeds cap).
+long long oracle_b1_matrix(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd,
+                           double lso, const double* angles, const int* views, int nviews, long long cap,
+                           int* rows, int* cols, double* vals) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::vector<float> vecs;
+    b1_vectors(g, vecs);
+    double dxy = (double)(float)g.dx * (double)(float)g.dy;
+    long long n = 0;
+    for (int k = 0; k < nviews; ++k) {
+        int p = views[k];
+        const float* vp = &vecs[(size_t)p * nu * 2];
+        std::vector<std::vector<std::pair<int, double>>> byrow(nu);
+        for (int ix = 0; ix < nx; ++ix)
+            for (int iy = 0; iy < ny; ++iy)
+                b1_pixel_view<double>(g, vp, p, ix, iy, [&](int u, double conv) {
+                    byrow[u].push_back({ix * ny + iy, conv * dxy});
+                });
+        for (int u = 0; u < nu; ++u)
+            for (auto& e : byrow[u]) {
+                if (n < cap) { rows[n] = k * nu + u; cols[n] = e.first; vals[n] = e.second; }
+                ++n;
+            }
+    }
+    return n;
+}
+
+// Algorithmic FLOPs of the reference B1 formula on this geometry, counted over
+// `nviews` views spread evenly over the scan: out[0] = FLOPs of the bin-range
+// step per pixel-view, out[1] = FLOPs per footprint evaluation (forward body,
+// layers/A_B1.cu:120-206, without the accumulation), out[2] = evaluations per
+// pixel-view.
+void oracle_b1_flops(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                     const double* angles, int nviews, double* out) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::vector<float> vecs;
+    b1_vectors(g, vecs);
+    long long range_flops = 0, eval_flops = 0, evals = 0, pv = 0;
+    for (int k = 0; k < nviews; ++k) {
+        int p = (int)((long long)k * np / nviews);
+        const float* vp = &vecs[(size_t)p * nu * 2];
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                // range alone
+                CountedF::flops = 0;
+                int minu, maxu;
+                bin_range<CountedF>(&g.pmi[12 * p], (float)g.puv[3 * p], std::fabs((float)g.puv[3 * p] - (float)g.puv[3 * p + 1]) < 1e-7f,
+                                    ix - 1.0f, ix + 1.0f, iy - 1.0f, iy + 1.0f, nu, minu, maxu);
+                long long r = CountedF::flops;
+                CountedF::flops = 0;
+                long long n = b1_pixel_view<CountedF>(g, vp, p, ix, iy, [](int, double) {});
+                range_flops += r;
+                eval_flops += CountedF::flops - r;
+                evals += n;
+                ++pv;
+            }
+    }
+    out[0] = (double)range_flops / pv;
+    out[1] = evals ? (double)eval_flops / evals : 0.0;
+    out[2] = (double)evals / pv;
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+"""ctypes binding of sgd_b200/libnetwork.so, the CUDA projector library.
+
+The library is built in-tree (``make -C sgd_b200/csrc`` or
+``__graft_entry__.build()``).  There is no CPU fallback: if it is missing or
+fails to load, every projector raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libnetwork.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+_i = ctypes.c_int
+_d = ctypes.c_double
+
+_LIB = None
+
+
+class ProjectorError(RuntimeError):
+    """A failure reported by the CUDA library (sgd_last_error())."""
+
+
+def lib() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ProjectorError(f"CUDA projector library not built: {LIB_PATH} (run `make -C sgd_b200/csrc`)")
+    L = ctypes.CDLL(LIB_PATH)
+    L.sgd_last_error.restype = ctypes.c_char_p
+    L.sgd_last_error.argtypes = []
+    _declare_fan2d(L, "b1")
+    _LIB = L
+    return L
+
+
+def _declare_fan2d(L, pre: str) -> None:
+    init = getattr(L, f"{pre}_init")
+    init.restype = _vp
+    init.argtypes = [_i, _i, _i, _i, _d, _d, _d, _d, _d, _dp, _dp, _dp]
+    f = getattr(L, f"{pre}_forward_projection")
+    f.restype = _i
+    f.argtypes = [_dp, _dp, _vp]
+    b = getattr(L, f"{pre}_backward_projection")
+    b.restype = None
+    b.argtypes = [_dp, _dp, _vp]
+    sb = getattr(L, f"sgd_{pre}_backward_projection")
+    sb.restype = _i
+    sb.argtypes = [_dp, _dp, _vp]
+    d = getattr(L, f"{pre}_destroy")
+    d.restype = None
+    d.argtypes = [_vp]
+    fd = getattr(L, f"sgd_{pre}_forward_dev")
+    fd.restype = _i
+    fd.argtypes = [_vp, _vp, _vp, _vp]
+    bd = getattr(L, f"sgd_{pre}_backward_dev")
+    bd.restype = _i
+    bd.argtypes = [_vp, _vp, _vp, _vp]
+    c = getattr(L, f"sgd_{pre}_count")
+    c.restype = ctypes.c_ulonglong
+    c.argtypes = [_vp]
+
+
+def last_error() -> str:
+    msg = lib().sgd_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int, what: str) -> None:
+    if status != 0:
+        raise ProjectorError(f"{what}: {last_error()}")

@@ -1,0 +1,34 @@
+// B1 fan-beam projector: device tables and kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "fan_geometry.h"
+
+namespace sgd {
+
+// Device-resident tables of one B1 geometry.
+struct B1Device {
+    int nx = 0, ny = 0, np = 0, nu = 0;
+    float dxdy = 1.f;
+    const float* rec = nullptr;          // [np][nu][kB1Rec]
+    const float* strip = nullptr;        // [np][nu][kStripRec]
+    const BinHomography* hom = nullptr;  // [np]
+    int wpad = 1;                        // shared-memory window of the back kernel (bins)
+    int vchunk = 4;                      // views staged per step by the back kernel
+};
+
+int b1_back_wpad(const FanGeometry& g, const std::vector<BinHomography>& hom);
+size_t b1_back_smem_bytes(int wpad, int vchunk);
+void b1_prepare_device();
+
+// sino[p * nu + u] = sum_{i,j} A[(p,u),(i,j)] img[i * ny + j]; imgT is scratch of nx*ny floats.
+void b1_forward_launch(const B1Device& d, const float* img, float* imgT, float* sino, cudaStream_t s);
+// img[i * ny + j] = sum_{p,u} A[(p,u),(i,j)] sino[p * nu + u]
+void b1_back_launch(const B1Device& d, const float* sino, float* img, cudaStream_t s);
+// Footprint evaluations the reference kernel performs for this geometry.
+unsigned long long b1_count(const B1Device& d, cudaStream_t s);
+
+}  // namespace sgd

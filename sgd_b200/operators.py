@@ -1,0 +1,99 @@
+"""LinearOperator wrappers with the names, arguments and behaviour of the
+reference's python/operators/operators.py.
+
+Each ``A_*_operator`` builds its geometry once through the library's
+``*_init`` entry point (the same C signature as the reference's) and applies
+the CUDA forward/back projectors on FP64 numpy vectors through
+``*_forward_projection`` / ``*_backward_projection``:
+
+* ``matvec(x)``: x flat of length nx*ny in the layout x[ix*ny + iy];
+  returns y of length np*nu in the layout y[p*nu + u]
+  (python/operators/operators.py:201-209);
+* ``rmatvec(y)``: the adjoint (operators.py:211-219).
+
+The base class is pylops.LinearOperator when pylops is importable (as in the
+reference) and scipy.sparse.linalg.LinearOperator otherwise; both take
+``dtype``/``shape`` and dispatch to ``_matvec``/``_rmatvec``.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+try:  # the reference's base class
+    from pylops import LinearOperator  # type: ignore
+except ImportError:  # pragma: no cover - pylops is not installed in this image
+    from scipy.sparse.linalg import LinearOperator
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+class _Fan2DOperator(LinearOperator):
+    """Common body of the 2D fan-beam operators over one C entry-point prefix."""
+
+    _prefix = ""
+
+    def __init__(self, nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dz=None, drho=None, dtype=np.float64):
+        super().__init__(dtype=dtype, shape=(nnp * nu, nx * ny))
+        self.vol_shape = (nx, ny)
+        self.proj_shape = (nnp, nu)
+        self.lsd = lsd
+        self.lso = lso
+        self.dimension = (dx, dy)
+        self.blur = du
+        self.angles = angles
+        if dz is not None and drho is None:
+            # python/operators/operators.py:171-172
+            raise AssertionError("Error: drho should be provided if dz is provided.")
+        angles = np.ascontiguousarray(angles, dtype=np.float64)
+        if angles.shape != (nnp,):
+            raise ValueError(f"angles must have shape ({nnp},), got {angles.shape}")
+        self._angles = angles
+        self._dz = None if dz is None else np.ascontiguousarray(dz, dtype=np.float64)
+        self._drho = None if drho is None else np.ascontiguousarray(drho, dtype=np.float64)
+        L = _lib.lib()
+        self._L = L
+        init = getattr(L, f"{self._prefix}_init")
+        self.cpointer = init(nx, ny, nnp, nu, dx, dy, du, lsd, lso, _ptr(angles), _ptr(self._dz), _ptr(self._drho))
+        if not self.cpointer:
+            raise _lib.ProjectorError(f"{self._prefix}_init: {_lib.last_error()}")
+        self._fwd = getattr(L, f"{self._prefix}_forward_projection")
+        self._bwd = getattr(L, f"sgd_{self._prefix}_backward_projection")
+        self._destroy = getattr(L, f"{self._prefix}_destroy")
+        self.conv_count = int(getattr(L, f"sgd_{self._prefix}_count")(self.cpointer))
+
+    def __del__(self):
+        p = getattr(self, "cpointer", None)
+        if p:
+            self._destroy(p)
+            self.cpointer = None
+
+    def _matvec(self, x):
+        x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
+        if x.size != self.shape[1]:
+            raise ValueError(f"expected {self.shape[1]} image values, got {x.size}")
+        y = np.zeros((self.shape[0],), dtype=np.float64)
+        if self._fwd(_ptr(y), _ptr(x), self.cpointer) < 0:
+            raise _lib.ProjectorError(f"{self._prefix}_forward_projection: {_lib.last_error()}")
+        return y.astype(self.dtype, copy=False)
+
+    def _rmatvec(self, y):
+        y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
+        if y.size != self.shape[0]:
+            raise ValueError(f"expected {self.shape[0]} sinogram values, got {y.size}")
+        x = np.zeros((self.shape[1],), dtype=np.float64)
+        _lib.check(self._bwd(_ptr(y), _ptr(x), self.cpointer), f"{self._prefix}_backward_projection")
+        return x.astype(self.dtype, copy=False)
+
+
+class A_B1_operator(_Fan2DOperator):
+    """Bilinear box-spline fan-beam projector (python/operators/operators.py:156-219)."""
+
+    _prefix = "b1"

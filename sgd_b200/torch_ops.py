@@ -1,0 +1,129 @@
+"""The projectors on CUDA tensors, and their torch.autograd.Function.
+
+PyTorch is used here for device memory and streams only: every projection runs
+the hand-written kernels of ``libnetwork.so`` through the library's device
+entry points, on ``torch.cuda.current_stream()``.
+
+Layouts (FP32, contiguous):
+* image    (nx, ny)  -> element (ix, iy), the reference host layout x[ix*ny+iy]
+* sinogram (np, nu)  -> element (p, u), y[p*nu+u]
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+class FanProjector:
+    """One fan-beam geometry bound to the current CUDA device.
+
+    ``kind`` selects the basis ("b1").  Arguments follow the reference's
+    ``*_init`` entry points (layers/A_B1.cu:595-603): image nx x ny with pixel
+    dx x dy, np views at ``angles`` (radians), nu bins of pitch du,
+    source-detector distance lsd, source-isocentre distance lso, optional
+    per-view source offsets dz/drho.
+    """
+
+    def __init__(self, kind, nx, ny, nu, dx, dy, du, lsd, lso, angles, dz=None, drho=None):
+        if not torch.cuda.is_available():
+            raise _lib.ProjectorError("FanProjector needs a CUDA device")
+        self.kind = kind
+        angles = np.ascontiguousarray(angles, dtype=np.float64)
+        self.nx, self.ny, self.np, self.nu = int(nx), int(ny), int(angles.shape[0]), int(nu)
+        self.image_shape = (self.nx, self.ny)
+        self.sino_shape = (self.np, self.nu)
+        self.device = torch.device("cuda", torch.cuda.current_device())
+        L = _lib.lib()
+        self._L = L
+        dz = None if dz is None else np.ascontiguousarray(dz, dtype=np.float64)
+        drho = None if drho is None else np.ascontiguousarray(drho, dtype=np.float64)
+        self.handle = getattr(L, f"{kind}_init")(self.nx, self.ny, self.np, self.nu, dx, dy, du, lsd, lso,
+                                                  _ptr(angles), _ptr(dz), _ptr(drho))
+        if not self.handle:
+            raise _lib.ProjectorError(f"{kind}_init: {_lib.last_error()}")
+        self._fwd = getattr(L, f"sgd_{kind}_forward_dev")
+        self._bwd = getattr(L, f"sgd_{kind}_backward_dev")
+        self._destroy = getattr(L, f"{kind}_destroy")
+        self.conv_count = int(getattr(L, f"sgd_{kind}_count")(self.handle))
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            self._destroy(h)
+            self.handle = None
+
+    def _check(self, t, shape, name):
+        if t.device != self.device or t.dtype != torch.float32 or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous float32 tensor on {self.device}")
+        if tuple(t.shape) != shape:
+            raise ValueError(f"{name} must have shape {shape}, got {tuple(t.shape)}")
+
+    def forward(self, img: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Sinogram (np, nu) of an image (nx, ny)."""
+        self._check(img, self.image_shape, "image")
+        if out is None:
+            out = torch.empty(self.sino_shape, dtype=torch.float32, device=self.device)
+        self._check(out, self.sino_shape, "out")
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(self._fwd(self.handle, img.data_ptr(), out.data_ptr(), s), f"sgd_{self.kind}_forward_dev")
+        return out
+
+    def backward(self, sino: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        """Adjoint (back projection) image (nx, ny) of a sinogram (np, nu)."""
+        self._check(sino, self.sino_shape, "sinogram")
+        if out is None:
+            out = torch.empty(self.image_shape, dtype=torch.float32, device=self.device)
+        self._check(out, self.image_shape, "out")
+        s = torch.cuda.current_stream(self.device).cuda_stream
+        _lib.check(self._bwd(self.handle, sino.data_ptr(), out.data_ptr(), s), f"sgd_{self.kind}_backward_dev")
+        return out
+
+
+class ProjectFunction(torch.autograd.Function):
+    """y = A x with dL/dx = A^T dL/dy computed by the hand-written back projector."""
+
+    @staticmethod
+    def forward(ctx, img, projector: FanProjector):
+        ctx.projector = projector
+        return projector.forward(img.contiguous())
+
+    @staticmethod
+    def backward(ctx, grad):
+        return ctx.projector.backward(grad.contiguous()), None
+
+
+class BackProjectFunction(torch.autograd.Function):
+    """x = A^T y with dL/dy = A dL/dx."""
+
+    @staticmethod
+    def forward(ctx, sino, projector: FanProjector):
+        ctx.projector = projector
+        return projector.backward(sino.contiguous())
+
+    @staticmethod
+    def backward(ctx, grad):
+        return ctx.projector.forward(grad.contiguous()), None
+
+
+def project(img: torch.Tensor, projector: FanProjector) -> torch.Tensor:
+    """Differentiable forward projection; batched over leading dimensions."""
+    if img.dim() == 2:
+        return ProjectFunction.apply(img, projector)
+    return torch.stack([project(x, projector) for x in img])
+
+
+def back_project(sino: torch.Tensor, projector: FanProjector) -> torch.Tensor:
+    """Differentiable back projection; batched over leading dimensions."""
+    if sino.dim() == 2:
+        return BackProjectFunction.apply(sino, projector)
+    return torch.stack([back_project(y, projector) for y in sino])

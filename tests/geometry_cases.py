@@ -1,0 +1,28 @@
+"""Geometries used by the parity tests (sizes of the benchmark configurations
+and small cases the CPU oracle finishes in seconds)."""
+import numpy as np
+
+LSD, LSO = 1085.6, 595.0
+
+
+def fan_case(name):
+    """(nx, ny, nu, dx, dy, du, lsd, lso, angles) of a named fan-beam case."""
+    if name == "c2":      # 512^2 at 0.5 mm, 720 views over 2pi, 736 bins at 1 mm
+        return 512, 512, 736, 0.5, 0.5, 1.0, LSD, LSO, 2 * np.pi * np.arange(720) / 720
+    if name == "small":   # 128^2 at 2 mm, 180 views, 185 bins at 1 mm
+        return 128, 128, 185, 2.0, 2.0, 1.0, LSD, LSO, 2 * np.pi * np.arange(180) / 180
+    if name == "rect":    # nx != ny, anisotropic pixels, odd sizes
+        return 97, 64, 151, 1.5, 2.0, 1.3, LSD, LSO, 2 * np.pi * np.arange(37) / 37 + 0.1
+    if name == "tiny":    # one view, few bins
+        return 16, 16, 24, 1.0, 1.0, 1.0, 40.0, 20.0, np.array([0.3])
+    if name == "snap":    # views exactly at odd multiples of 45 degrees (the reference's singular path)
+        return 64, 64, 96, 1.0, 1.0, 1.0, 200.0, 100.0, np.array([np.pi / 4, 3 * np.pi / 4, 5 * np.pi / 4, 7 * np.pi / 4, 0.0, np.pi / 2])
+    if name == "wide":    # detector narrower than the object: truncated projections
+        return 96, 96, 40, 1.0, 1.0, 1.0, 300.0, 150.0, 2 * np.pi * np.arange(24) / 24
+    raise KeyError(name)
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64).ravel()
+    b = np.asarray(b, dtype=np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))

@@ -1,0 +1,47 @@
+"""Writes the golden vectors of tests/golden/ by running the reference projector
+library built from its own sources (oracle/_ref/libnetwork.so) on a GPU.
+
+    python tests/golden/make_golden.py OUTDIR
+
+Each fixture holds the geometry, a seeded phantom x, the reference's forward
+b = A x and footprint count, a second sinogram y (forward of another phantom)
+and the reference's back projection xt = A^T y.  The CPU oracle is checked
+against them by tests/test_oracle.py.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+import reflib  # noqa: E402
+from geometry_cases import fan_case  # noqa: E402
+from sgd_b200.phantom import ellipse_phantom  # noqa: E402
+
+CASES = {
+    "b1_tiny": ("b1", "tiny"),
+    "b1_snap": ("b1", "snap"),
+    "b1_wide": ("b1", "wide"),
+}
+
+
+def main(out):
+    os.makedirs(out, exist_ok=True)
+    for name, (kind, case) in CASES.items():
+        nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case(case)
+        R = reflib.RefFan2D(kind, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+        x = ellipse_phantom(nx, ny, dx, dy, seed=11).ravel()
+        b, cnt = R.forward(x)
+        y, _ = R.forward(ellipse_phantom(nx, ny, dx, dy, seed=12).ravel())
+        xt = R.backward(y)
+        np.savez_compressed(os.path.join(out, f"{name}.npz"), kind=kind, sizes=np.array([nx, ny, nu]),
+                            params=np.array([dx, dy, du, lsd, lso]), angles=ang, x=x, b=b, count=cnt, y=y,
+                            xt=xt, tol=1e-5)
+        print(name, "count", cnt, "norm b", np.linalg.norm(b))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE)

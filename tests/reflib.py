@@ -1,0 +1,72 @@
+"""ctypes access to the reference projector library built from its own sources
+(oracle/_ref/libnetwork.so, made by `make -C oracle ref`).  Test
+infrastructure: it runs the reference's CUDA kernels, so only GPU tests and
+the golden-vector script use it."""
+import ctypes
+import os
+
+import numpy as np
+
+from conftest import ROOT
+
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libnetwork.so")
+_dp = ctypes.POINTER(ctypes.c_double)
+_L = None
+
+
+def available():
+    return os.path.exists(REF_LIB)
+
+
+def lib():
+    global _L
+    if _L is None:
+        L = ctypes.CDLL(REF_LIB)
+        for pre in ("b0", "b1", "h0", "hl"):
+            init = getattr(L, f"{pre}_init")
+            init.restype = ctypes.c_void_p
+            f = getattr(L, f"{pre}_forward_projection")
+            f.restype = ctypes.c_int
+            f.argtypes = [_dp, _dp, ctypes.c_void_p]
+            b = getattr(L, f"{pre}_backward_projection")
+            b.restype = None
+            b.argtypes = [_dp, _dp, ctypes.c_void_p]
+        L.b0_init.argtypes = L.b1_init.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [_dp] * 3
+        L.SF_init.restype = ctypes.c_void_p
+        L.SF_init.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [_dp]
+        for n in ("SF_forward_projection",):
+            getattr(L, n).restype = ctypes.c_int
+            getattr(L, n).argtypes = [_dp, _dp, ctypes.c_void_p]
+        L.SF_backward_projection.restype = None
+        L.SF_backward_projection.argtypes = [_dp, _dp, ctypes.c_void_p]
+        L.ref_b1_kernel_ms.restype = ctypes.c_float
+        L.ref_b1_kernel_ms.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+        _L = L
+    return _L
+
+
+class RefFan2D:
+    """The reference's 2D fan projector `kind` (b0, b1, SF) on one geometry."""
+
+    def __init__(self, kind, nx, ny, nu, dx, dy, du, lsd, lso, angles):
+        L = lib()
+        self.kind, self.nx, self.ny, self.nu, self.np = kind, nx, ny, nu, len(angles)
+        self._ang = np.ascontiguousarray(angles, dtype=np.float64)
+        p = self._ang.ctypes.data_as(_dp)
+        if kind == "SF":
+            self.h = L.SF_init(nx, ny, self.np, nu, dx, dy, du, lsd, lso, p)
+        else:
+            self.h = getattr(L, f"{kind}_init")(nx, ny, self.np, nu, dx, dy, du, lsd, lso, p, None, None)
+        assert self.h
+
+    def forward(self, x):
+        x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
+        b = np.zeros(self.np * self.nu)
+        cnt = getattr(lib(), f"{self.kind}_forward_projection")(b.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
+        return b, cnt
+
+    def backward(self, y):
+        y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
+        x = np.zeros(self.nx * self.ny)
+        getattr(lib(), f"{self.kind}_backward_projection")(y.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
+        return x
