@@ -61,6 +61,11 @@ int sgd_b1_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
 /* New: the reference's footprint-evaluation count for the layer's geometry. */
 unsigned long long sgd_b1_count(void* layer);
 
+/* New: synchronises and reports (0 / -1, then clears) a device-side failure of
+ * an earlier *_dev call: a kernel's bounded wait for its shared-memory staging
+ * gave up, and the output of that call was not written. */
+int sgd_b1_status(void* layer);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* New (no reference counterpart): FP32 FMA throughput of the current GPU in

@@ -1,16 +1,18 @@
 // B1 fan-beam projector kernels (sm_100a).
 //
 //   b1_forward_kernel   detector-driven: one warp per (view, bin).  Lanes split
-//                       the rows (major axis) the bin's ray strip crosses, each
+//                       the rows (major axis) the bin's ray strip crosses; each
 //                       lane evaluates the footprint of the few pixels of its
 //                       row inside the strip, and the warp reduces with
 //                       shuffles.  The sinogram is written once, no atomics.
 //   b1_back_kernel      voxel-driven: one thread per pixel, a CTA per 32x8
-//                       tile.  Per chunk of views the CTA stages the bin
-//                       window its tile projects onto (footprint tables and
-//                       sinogram values) in shared memory; each thread
-//                       accumulates over all views in registers and writes
-//                       its pixel once, no atomics.
+//                       tile.  Per chunk of views the CTA stages the bin window
+//                       its tile projects onto in shared memory: the 64-byte
+//                       footprint records by TMA bulk copies completed on an
+//                       mbarrier (double-buffered, the next chunk in flight
+//                       while this one is evaluated), the sinogram values by
+//                       plain loads.  Each thread accumulates over all views in
+//                       registers and writes its pixel once, no atomics.
 //
 // Reference: layers/A_B1.cu:62-208 (forward, one launch per view, FP64
 // atomics) and :211-353 (backward).
@@ -21,6 +23,7 @@
 
 #include "b1_kernels.cuh"
 #include "common.h"
+#include "tma.cuh"
 
 namespace sgd {
 
@@ -30,17 +33,9 @@ constexpr int kFwdWarps = 8;
 constexpr int kBackTI = 8;    // tile extent along i (x), threadIdx.y
 constexpr int kBackTJ = 32;   // tile extent along j (y), threadIdx.x: contiguous in memory
 constexpr int kBackThreads = kBackTI * kBackTJ;
-
-struct RegTab {
-    const float* p;
-    __device__ __forceinline__ float operator()(int k) const { return p[k]; }
-};
-
-struct SoATab {
-    const float* p;  // field k of this bin at p[k * stride]
-    int stride;
-    __device__ __forceinline__ float operator()(int k) const { return p[k * stride]; }
-};
+constexpr int kVC = 4;        // views per staged chunk
+constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr int kHeaderBytes = 512;  // 2 mbarriers | 3 x kVC windows | 3 x kVC homographies (8 floats)
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -48,138 +43,207 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// Records are float4 chunks laid out [view][chunk][bin] (fan_geometry.h).
+__device__ __forceinline__ B1Bin load_bin(const float4* rec, int p, int u, int nu) {
+    const float4* q = rec + (size_t)p * 4 * nu + u;
+    return B1Bin{__ldg(q), __ldg(q + nu), __ldg(q + 2 * nu), __ldg(q + 3 * nu)};
+}
+
+// Candidate minor indices of major line m: the strip between the edge rays over
+// the lines m-1..m+1 a pixel's support covers, widened by the +-1 pixel support
+// along the minor axis.
+__device__ __forceinline__ void strip_span(const float4& st, float aa, float ab, float fm, int nmin, int& nlo,
+                                           int& nhi) {
+    const float fa = fmaf(st.y, fm, st.x);
+    const float fb = fmaf(st.w, fm, st.z);
+    const float lo = fminf(fa - aa, fb - ab) - 1.0f;
+    const float hi = fmaxf(fa + aa, fb + ab) + 1.0f;
+    nlo = max(0, (int)ceilf(lo));
+    nhi = min(nmin - 1, (int)floorf(hi));
+}
+
 // img (i, j) at img[i * ny + j]; imgT (i, j) at imgT[j * nx + i].
 __global__ void __launch_bounds__(kFwdWarps * 32)
-b1_forward_kernel(const float* __restrict__ rec, const float* __restrict__ strip, const float* __restrict__ img,
+b1_forward_kernel(const float4* __restrict__ rec, const float* __restrict__ strip, const float* __restrict__ img,
                   const float* __restrict__ imgT, float* __restrict__ sino, int nx, int ny, int np, int nu,
                   float dxdy) {
-    __shared__ float s_tab[kFwdWarps][kB1Rec];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long long gw = (long long)blockIdx.x * kFwdWarps + warp;
     if (gw >= (long long)np * nu) return;
-    const float* r = rec + gw * kB1Rec;
-    s_tab[warp][lane] = __ldg(r + lane);
-    if (lane < kB1Rec - 32) s_tab[warp][32 + lane] = __ldg(r + 32 + lane);
-    __syncwarp();
-    float c[10];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) c[k] = s_tab[warp][k];
-    const RegTab T{s_tab[warp]};
-
+    const int p = (int)(gw / nu), u = (int)(gw - (long long)p * nu);
+    const B1Bin r = load_bin(rec, p, u, nu);
     const float4 st = __ldg(reinterpret_cast<const float4*>(strip + gw * kStripRec));
     const bool ydom = __ldg(strip + gw * kStripRec + 4) > 0.5f;
-    const int nmaj = ydom ? ny : nx, nmin = ydom ? nx : ny;
-    const float* src = ydom ? img : imgT;   // minor index n, major m: src[n * nmaj + m]
     const float aa = fabsf(st.y), ab = fabsf(st.w);
 
-    // FP32 sums within a row (a few terms), FP64 across rows and lanes: the
+    // FP32 sums within a line (a few terms), FP64 across lines and lanes: the
     // forward and back kernels then round the same products to within FP64
     // accumulation error, which the dot-product adjoint test needs.
     double acc = 0.0;
-    for (int m = lane; m < nmaj; m += 32) {
-        const float fa = fmaf(st.y, (float)m, st.x);
-        const float fb = fmaf(st.w, (float)m, st.z);
-        // strip extent over the rows m-1..m+1 covered by a pixel's support,
-        // widened by the +-1 pixel support along the minor axis
-        const float lo = fminf(fa - aa, fb - ab) - 1.0f;
-        const float hi = fmaxf(fa + aa, fb + ab) + 1.0f;
-        const int nlo = max(0, (int)ceilf(lo));
-        const int nhi = min(nmin - 1, (int)floorf(hi));
-        float row = 0.f;
-        for (int n = nlo; n <= nhi; ++n) {
-            const float fi = ydom ? (float)n : (float)m;
-            const float fj = ydom ? (float)m : (float)n;
-            const float conv = b1_conv(fi, fj, c, T);
-            if (conv > kConvEps) row = fmaf(conv, __ldg(src + (size_t)n * nmaj + m), row);
+    if (ydom) {
+        // rows j = m, candidate columns i = n; the j terms are hoisted
+        for (int m = lane; m < ny; m += 32) {
+            const float fm = (float)m;
+            int nlo, nhi;
+            strip_span(st, aa, ab, fm, nx, nlo, nhi);
+            const float ia = b1_xa_inner(fm, r), ib = b1_xb_inner(fm, r);
+            float row = 0.f, fn = (float)nlo;
+            const float* sp = img + (size_t)nlo * ny + m;
+            for (int n = nlo; n <= nhi; ++n, fn += 1.0f, sp += ny) {
+                const float conv = b1_conv_x(b1_xa(fn, ia, r), b1_xb(fn, ib, r), r);
+                if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
+            }
+            acc += (double)row;
         }
-        acc += (double)row;
+    } else {
+        // columns i = m, candidate rows j = n
+        for (int m = lane; m < nx; m += 32) {
+            const float fm = (float)m;
+            int nlo, nhi;
+            strip_span(st, aa, ab, fm, ny, nlo, nhi);
+            float row = 0.f, fn = (float)nlo;
+            const float* sp = imgT + (size_t)nlo * nx + m;
+            for (int n = nlo; n <= nhi; ++n, fn += 1.0f, sp += nx) {
+                const float conv = b1_conv(fm, fn, r);
+                if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
+            }
+            acc += (double)row;
+        }
     }
     acc = warp_sum(acc);
     if (lane == 0) sino[gw] = (float)acc * dxdy;
 }
 
-// Bin window [lo, hi] covered by pixels i in [i0, i1], j in [j0, j1] (with the
-// +-1 pixel B1 support already applied by the caller), clamped to the detector.
-__device__ __forceinline__ void bin_window(const BinHomography& H, float i0, float i1, float j0, float j1, int nu,
-                                           int& lo, int& hi) {
-    const float u00 = __fdividef(fmaf(H.n0, i0, fmaf(H.n1, j0, H.n2)), fmaf(H.d0, i0, fmaf(H.d1, j0, H.d2)));
-    const float u01 = __fdividef(fmaf(H.n0, i0, fmaf(H.n1, j1, H.n2)), fmaf(H.d0, i0, fmaf(H.d1, j1, H.d2)));
-    const float u10 = __fdividef(fmaf(H.n0, i1, fmaf(H.n1, j0, H.n2)), fmaf(H.d0, i1, fmaf(H.d1, j0, H.d2)));
-    const float u11 = __fdividef(fmaf(H.n0, i1, fmaf(H.n1, j1, H.n2)), fmaf(H.d0, i1, fmaf(H.d1, j1, H.d2)));
-    const float umin = fminf(fminf(u00, u01), fminf(u10, u11));
-    const float umax = fmaxf(fmaxf(u00, u01), fmaxf(u10, u11));
-    lo = max(0, (int)floorf(umin));
-    hi = min(nu - 1, (int)floorf(umax));
+__device__ __forceinline__ float hom_u(const float* h, float fi, float fj) {
+    return __fdividef(fmaf(h[0], fi, fmaf(h[1], fj, h[2])), fmaf(h[3], fi, fmaf(h[4], fj, h[5])));
 }
 
-// Shared memory per view: header (8 floats: homography) | window start |
-// footprint fields [kB1Rec][wpad] | sinogram [wpad].
-__host__ __device__ __forceinline__ int back_view_floats(int wpad) { return 16 + (kB1Rec + 1) * wpad; }
+// Clamped bin range of the box [i0, i1] x [j0, j1] (pixel-index coordinates)
+// under the view's homography: extremes of a linear-fractional map over a box
+// are at its corners.
+__device__ __forceinline__ void box_bins(const float* h, float i0, float i1, float j0, float j1, int nu, int& lo,
+                                         int& hi) {
+    const float u00 = hom_u(h, i0, j0), u01 = hom_u(h, i0, j1), u10 = hom_u(h, i1, j0), u11 = hom_u(h, i1, j1);
+    lo = max(0, (int)floorf(fminf(fminf(u00, u01), fminf(u10, u11))));
+    hi = min(nu - 1, (int)floorf(fmaxf(fmaxf(u00, u01), fmaxf(u10, u11))));
+}
 
 __global__ void __launch_bounds__(kBackThreads)
-b1_back_kernel(const float* __restrict__ rec, const BinHomography* __restrict__ hom, const float* __restrict__ sino,
-               float* __restrict__ img, int nx, int ny, int np, int nu, int wpad, int vchunk, float dxdy) {
-    extern __shared__ float smem[];
-    const int tj = threadIdx.x, ti = threadIdx.y, tid = ti * kBackTJ + tj;
+b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__ hom, const float* __restrict__ sino,
+               float* __restrict__ img, int nx, int ny, int np, int nu, int wcap, float dxdy, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem);           // [2]
+    int* win = reinterpret_cast<int*>(smem + 16);                   // [3][kVC][2]
+    float* hs = reinterpret_cast<float*>(smem + 16 + 3 * kVC * 8);  // [3][kVC][8]
+    float4* srec = reinterpret_cast<float4*>(smem + kHeaderBytes);  // [2][kVC][4 chunks][wcap]
+    float* ssino = reinterpret_cast<float*>(srec + 2 * kVC * 4 * wcap);  // [2][kVC][wcap]
+    __shared__ int s_abort;
+
+    // each warp covers an 8 (j) x 4 (i) block of the 32 x 8 tile, so that its
+    // lanes read few distinct bins of a view
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
     const int i0 = blockIdx.y * kBackTI, j0 = blockIdx.x * kBackTJ;
-    const int i = i0 + ti, j = j0 + tj;
+    const int i = i0 + 4 * (w >> 2) + (l >> 3), j = j0 + 8 * (w & 3) + (l & 7);
     const float fi = (float)i, fj = (float)j;
-    const int vfl = back_view_floats(wpad);
-    int* s_lo = reinterpret_cast<int*>(smem);            // [vchunk]
-    int* s_hi = s_lo + vchunk;                            // [vchunk]
-    float* s_view = smem + 2 * ((vchunk + 3) & ~3);       // [vchunk][vfl]
+    const int nchunks = (np + kVC - 1) / kVC;
+
+    // tile window of chunk c's views (one thread per view), with one bin of
+    // margin on each side for rounding
+    auto windows = [&](int c) {
+        if (tid < kVC) {
+            const int p = c * kVC + tid, slot = c % 3;
+            int lo = 0, hi = -1;
+            float* h = hs + (slot * kVC + tid) * 8;
+            if (p < np) {
+                const BinHomography H = hom[p];
+                h[0] = H.n0; h[1] = H.n1; h[2] = H.n2; h[3] = H.d0; h[4] = H.d1; h[5] = H.d2;
+                box_bins(h, (float)i0 - 1.f, (float)(i0 + kBackTI), (float)j0 - 1.f, (float)(j0 + kBackTJ), nu, lo,
+                         hi);
+                lo = max(0, lo - 1);
+                hi = min(nu - 1, hi + 1);
+                if (hi - lo + 1 > wcap) hi = lo + wcap - 1;  // wcap is sized on the host; never taken
+            }
+            win[(slot * kVC + tid) * 2] = lo;
+            win[(slot * kVC + tid) * 2 + 1] = hi;
+        }
+    };
+    // stage chunk c: records by TMA (thread 0), sinogram values by all threads
+    auto stage = [&](int c) {
+        const int st = c & 1, slot = c % 3;
+        if (tid == 0) {
+            uint32_t bytes = 0;
+            for (int v = 0; v < kVC; ++v) {
+                const int W = win[(slot * kVC + v) * 2 + 1] - win[(slot * kVC + v) * 2] + 1;
+                if (W > 0) bytes += (uint32_t)W * sizeof(B1Bin);
+            }
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&bars[st], bytes);
+            for (int v = 0; v < kVC; ++v) {
+                const int lo = win[(slot * kVC + v) * 2], W = win[(slot * kVC + v) * 2 + 1] - lo + 1;
+                if (W > 0)
+                    for (int q = 0; q < 4; ++q)
+                        bulk_copy_g2s(srec + ((st * kVC + v) * 4 + q) * wcap,
+                                      rec + ((size_t)(c * kVC + v) * 4 + q) * nu + lo, (uint32_t)W * 16u, &bars[st]);
+            }
+        }
+        for (int v = 0; v < kVC; ++v) {
+            const int lo = win[(slot * kVC + v) * 2], W = win[(slot * kVC + v) * 2 + 1] - lo + 1;
+            const float* sp = sino + (size_t)(c * kVC + v) * nu + lo;
+            float* dp = ssino + (st * kVC + v) * wcap;
+            for (int w = tid; w < W; w += kBackThreads) dp[w] = __ldg(sp + w);
+        }
+    };
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    windows(0);
+    __syncthreads();
+    stage(0);
 
     double acc = 0.0;  // FP32 within a view (a few bins), FP64 across views
-    for (int p0 = 0; p0 < np; p0 += vchunk) {
-        const int nv = min(vchunk, np - p0);
-        __syncthreads();
-        if (tid < nv) {
-            const BinHomography H = hom[p0 + tid];
-            int lo, hi;
-            bin_window(H, (float)i0 - 1.f, (float)(i0 + kBackTI), (float)j0 - 1.f, (float)(j0 + kBackTJ), nu, lo, hi);
-            if (hi - lo + 1 > wpad) hi = lo + wpad - 1;  // cannot happen: wpad is sized on the host
-            s_lo[tid] = lo;
-            s_hi[tid] = hi;
-            float* v = s_view + tid * vfl;
-            v[0] = H.n0; v[1] = H.n1; v[2] = H.n2; v[3] = H.d0; v[4] = H.d1; v[5] = H.d2;
+    int c = 0;
+    for (; c < nchunks; ++c) {
+        if (c + 1 < nchunks) windows(c + 1);
+        __syncthreads();  // windows(c+1) and sinogram(c) visible; chunk c-1 fully consumed
+        if (s_abort) break;
+        if (c + 1 < nchunks) stage(c + 1);
+        const int st = c & 1, slot = c % 3;
+        if (!mbar_wait_bounded(&bars[st], (uint32_t)((c >> 1) & 1), kWaitLimit)) {
+            s_abort = 1;
+            atomicExch(err, 1);
+            continue;
         }
-        __syncthreads();
-        // stage footprint records and sinogram values of each view's window
-        for (int v = 0; v < nv; ++v) {
-            const int lo = s_lo[v], W = s_hi[v] - lo + 1;
-            if (W <= 0) continue;
-            const float* g = rec + ((size_t)(p0 + v) * nu + lo) * kB1Rec;
-            float* f = s_view + v * vfl + 16;
-            for (int e = tid; e < W * kB1Rec; e += kBackThreads) {
-                const int w = e / kB1Rec, k = e - w * kB1Rec;
-                f[k * wpad + w] = __ldg(g + e);
+        if (i >= nx || j >= ny) continue;
+        for (int v = 0; v < kVC; ++v) {
+            const int lo = win[(slot * kVC + v) * 2], hi = win[(slot * kVC + v) * 2 + 1];
+            if (hi < lo) continue;
+            int ulo, uhi;
+            box_bins(hs + (slot * kVC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, ulo, uhi);
+            ulo = max(ulo, lo);
+            uhi = min(uhi, hi);
+            const float4* rb = srec + (st * kVC + v) * 4 * wcap - lo;
+            const float* sb = ssino + (st * kVC + v) * wcap - lo;
+            float vsum = 0.f;
+            for (int u = ulo; u <= uhi; ++u) {
+                const B1Bin r{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]};
+                const float conv = b1_conv(fi, fj, r);
+                if (conv > kConvEps) vsum = fmaf(conv, sb[u], vsum);
             }
-            const float* sp = sino + (size_t)(p0 + v) * nu + lo;
-            for (int w = tid; w < W; w += kBackThreads) f[kB1Rec * wpad + w] = __ldg(sp + w);
+            acc += (double)vsum;
         }
-        __syncthreads();
-        if (i < nx && j < ny) {
-            for (int v = 0; v < nv; ++v) {
-                const float* vw = s_view + v * vfl;
-                const BinHomography H = {vw[0], vw[1], vw[2], vw[3], vw[4], vw[5], 0.f, 0.f};
-                int ulo, uhi;
-                bin_window(H, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, ulo, uhi);
-                const int lo = s_lo[v];
-                ulo = max(ulo, lo);
-                uhi = min(uhi, s_hi[v]);
-                float vsum = 0.f;
-                for (int u = ulo; u <= uhi; ++u) {
-                    const float* fb = vw + 16 + (u - lo);
-                    const SoATab T{fb, wpad};
-                    float c[10];
-#pragma unroll
-                    for (int k = 0; k < 10; ++k) c[k] = fb[k * wpad];
-                    const float conv = b1_conv(fi, fj, c, T);
-                    if (conv > kConvEps) vsum = fmaf(conv, fb[kB1Rec * wpad], vsum);
-                }
-                acc += (double)vsum;
-            }
+    }
+    if (c < nchunks) {
+        // a staged chunk never arrived: wait (bounded) for the copies still in
+        // flight into this CTA's shared memory, then leave the tile unwritten
+        if (tid == 0) {
+            mbar_wait_bounded(&bars[c & 1], (uint32_t)((c >> 1) & 1), kWaitLimit);
+            if (c + 1 < nchunks) mbar_wait_bounded(&bars[(c + 1) & 1], (uint32_t)(((c + 1) >> 1) & 1), kWaitLimit);
         }
+        return;
     }
     if (i < nx && j < ny) img[(size_t)i * ny + j] = (float)acc * dxdy;
 }
@@ -202,20 +266,19 @@ __global__ void transpose_kernel(const float* __restrict__ in, float* __restrict
 
 // Footprint evaluations the reference performs (its conv_count): per pixel and
 // view, the width of the clamped bin range of the +-1 pixel support
-// (layers/A_B1.cu:148-160).  Accumulated per block, one atomic per block.
+// (layers/A_B1.cu:148-160).  One atomic per warp.
 __global__ void b1_count_kernel(const BinHomography* __restrict__ hom, int nx, int ny, int np, int nu,
                                 unsigned long long* out) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     const int i = blockIdx.y;
     unsigned long long n = 0;
     if (j < ny) {
+        const float fi = (float)i, fj = (float)j;
         for (int p = 0; p < np; ++p) {
             const BinHomography H = hom[p];
-            const float fi = (float)i, fj = (float)j;
-            const float a = (fmaf(H.n0, fi - 1.f, fmaf(H.n1, fj - 1.f, H.n2))) / fmaf(H.d0, fi - 1.f, fmaf(H.d1, fj - 1.f, H.d2));
-            const float b = (fmaf(H.n0, fi - 1.f, fmaf(H.n1, fj + 1.f, H.n2))) / fmaf(H.d0, fi - 1.f, fmaf(H.d1, fj + 1.f, H.d2));
-            const float c = (fmaf(H.n0, fi + 1.f, fmaf(H.n1, fj - 1.f, H.n2))) / fmaf(H.d0, fi + 1.f, fmaf(H.d1, fj - 1.f, H.d2));
-            const float d = (fmaf(H.n0, fi + 1.f, fmaf(H.n1, fj + 1.f, H.n2))) / fmaf(H.d0, fi + 1.f, fmaf(H.d1, fj + 1.f, H.d2));
+            const float h[6] = {H.n0, H.n1, H.n2, H.d0, H.d1, H.d2};
+            const float a = hom_u(h, fi - 1.f, fj - 1.f), b = hom_u(h, fi - 1.f, fj + 1.f);
+            const float c = hom_u(h, fi + 1.f, fj - 1.f), d = hom_u(h, fi + 1.f, fj + 1.f);
             const int lo = min(max(0, (int)floorf(fminf(fminf(a, b), fminf(c, d)))), nu - 1);
             const int hi = min(max(0, (int)floorf(fmaxf(fmaxf(a, b), fmaxf(c, d)))), nu - 1);
             n += (unsigned long long)(hi - lo + 1);
@@ -227,10 +290,10 @@ __global__ void b1_count_kernel(const BinHomography* __restrict__ hom, int nx, i
 
 }  // namespace
 
-int b1_back_wpad(const FanGeometry& g, const std::vector<BinHomography>& hom) {
-    // Largest bin window of any 32x8 tile over all views (host replay of the
-    // kernel's window rule, in double with a one-bin margin), rounded up to odd
-    // so that per-bin fields fall into distinct shared-memory banks.
+int b1_back_wcap(const FanGeometry& g, const std::vector<BinHomography>& hom) {
+    // Largest staged window of any 32x8 tile over all views: a host replay of
+    // the kernel's window rule in double, with one more bin of margin each
+    // side, rounded up to a multiple of 4.
     int wmax = 1;
     for (int p = 0; p < g.np; ++p) {
         const BinHomography& H = hom[p];
@@ -244,15 +307,15 @@ int b1_back_wpad(const FanGeometry& g, const std::vector<BinHomography>& hom) {
                         umin = std::min(umin, u);
                         umax = std::max(umax, u);
                     }
-                int lo = std::max(0, (int)std::floor(umin) - 1), hi = std::min(g.nu - 1, (int)std::floor(umax) + 1);
+                int lo = std::max(0, (int)std::floor(umin) - 2), hi = std::min(g.nu - 1, (int)std::floor(umax) + 2);
                 wmax = std::max(wmax, hi - lo + 1);
             }
     }
-    return wmax | 1;
+    return (wmax + 3) & ~3;
 }
 
-size_t b1_back_smem_bytes(int wpad, int vchunk) {
-    return sizeof(float) * (2 * ((vchunk + 3) & ~3) + (size_t)vchunk * back_view_floats(wpad));
+size_t b1_back_smem_bytes(int wcap) {
+    return kHeaderBytes + (size_t)2 * kVC * wcap * (sizeof(B1Bin) + sizeof(float));
 }
 
 void b1_prepare_device() {
@@ -265,15 +328,16 @@ void b1_forward_launch(const B1Device& d, const float* img, float* imgT, float* 
     SGD_LAUNCH_CHECK();
     const long long warps = (long long)d.np * d.nu;
     const unsigned blocks = (unsigned)((warps + kFwdWarps - 1) / kFwdWarps);
-    b1_forward_kernel<<<blocks, kFwdWarps * 32, 0, s>>>(d.rec, d.strip, img, imgT, sino, d.nx, d.ny, d.np, d.nu,
-                                                        d.dxdy);
+    b1_forward_kernel<<<blocks, kFwdWarps * 32, 0, s>>>(reinterpret_cast<const float4*>(d.rec), d.strip, img,
+                                                        imgT, sino, d.nx, d.ny, d.np, d.nu, d.dxdy);
     SGD_LAUNCH_CHECK();
 }
 
 void b1_back_launch(const B1Device& d, const float* sino, float* img, cudaStream_t s) {
-    const size_t smem = b1_back_smem_bytes(d.wpad, d.vchunk);
-    dim3 tb(kBackTJ, kBackTI), tg((d.ny + kBackTJ - 1) / kBackTJ, (d.nx + kBackTI - 1) / kBackTI);
-    b1_back_kernel<<<tg, tb, smem, s>>>(d.rec, d.hom, sino, img, d.nx, d.ny, d.np, d.nu, d.wpad, d.vchunk, d.dxdy);
+    dim3 tg((d.ny + kBackTJ - 1) / kBackTJ, (d.nx + kBackTI - 1) / kBackTI);
+    b1_back_kernel<<<tg, kBackThreads, b1_back_smem_bytes(d.wcap), s>>>(reinterpret_cast<const float4*>(d.rec), d.hom,
+                                                                         sino, img, d.nx, d.ny, d.np, d.nu, d.wcap,
+                                                                         d.dxdy, d.err);
     SGD_LAUNCH_CHECK();
 }
 

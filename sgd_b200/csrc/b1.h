@@ -16,12 +16,12 @@ struct B1Device {
     const float* rec = nullptr;          // [np][nu][kB1Rec]
     const float* strip = nullptr;        // [np][nu][kStripRec]
     const BinHomography* hom = nullptr;  // [np]
-    int wpad = 1;                        // shared-memory window of the back kernel (bins)
-    int vchunk = 4;                      // views staged per step by the back kernel
+    int wcap = 4;                        // bins of a staged view window in the back kernel
+    int* err = nullptr;                  // device flag: a bounded wait in a kernel gave up
 };
 
-int b1_back_wpad(const FanGeometry& g, const std::vector<BinHomography>& hom);
-size_t b1_back_smem_bytes(int wpad, int vchunk);
+int b1_back_wcap(const FanGeometry& g, const std::vector<BinHomography>& hom);
+size_t b1_back_smem_bytes(int wcap);
 void b1_prepare_device();
 
 // sino[p * nu + u] = sum_{i,j} A[(p,u),(i,j)] img[i * ny + j]; imgT is scratch of nx*ny floats.

@@ -60,10 +60,12 @@ A_B1::A_B1(int nx, int ny, int np, int nu, double dx, double dy, double du, doub
     dev.nx = nx; dev.ny = ny; dev.np = np; dev.nu = nu;
     dev.dxdy = (float)(dx * dy);
     dev.rec = d_rec_; dev.strip = d_strip_; dev.hom = d_hom_;
-    dev.wpad = b1_back_wpad(geo, hom);
-    dev.vchunk = 4;
-    if (b1_back_smem_bytes(dev.wpad, dev.vchunk) > 200 * 1024)
-        fail("B1 back projector: bin window of %d bins does not fit in shared memory", dev.wpad);
+    dev.wcap = b1_back_wcap(geo, hom);
+    if (b1_back_smem_bytes(dev.wcap) > 200 * 1024)
+        fail("B1 back projector: bin window of %d bins does not fit in shared memory", dev.wcap);
+    SGD_CUDA(cudaMalloc(&d_err_, sizeof(int)));
+    SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
+    dev.err = d_err_;
     b1_prepare_device();
 
     const size_t nimg = (size_t)nx * ny, nsino = (size_t)np * nu;
@@ -80,6 +82,7 @@ A_B1::~A_B1() {
     cudaFree(d_rec_);
     cudaFree(d_strip_);
     cudaFree(d_hom_);
+    cudaFree(d_err_);
     cudaFree(st.d_img);
     cudaFree(st.d_imgT);
     cudaFree(st.d_sino);
@@ -102,6 +105,7 @@ void A_B1::forward_host(double* b, const double* x) {
     forward_dev(st.d_img, st.d_sino, stream);
     SGD_CUDA(cudaMemcpyAsync(st.h_sino, st.d_sino, nsino * sizeof(float), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
+    check_device_status();
 #pragma omp parallel for schedule(static) if (nsino > (1 << 16))
     for (long long e = 0; e < nsino; ++e) b[e] = (double)st.h_sino[e];
 }
@@ -114,8 +118,18 @@ void A_B1::backward_host(const double* b, double* x) {
     backward_dev(st.d_sino, st.d_img, stream);
     SGD_CUDA(cudaMemcpyAsync(st.h_img, st.d_img, nimg * sizeof(float), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
+    check_device_status();
 #pragma omp parallel for schedule(static) if (nimg > (1 << 16))
     for (long long e = 0; e < nimg; ++e) x[e] = (double)st.h_img[e];
+}
+
+void A_B1::check_device_status() {
+    int e = 0;
+    SGD_CUDA(cudaMemcpy(&e, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
+        fail("B1 back projector: a shared-memory staging wait timed out; output not written");
+    }
 }
 
 void A_B1::project(MatrixD& vol, MatrixD& proj, double /*weight*/) {
@@ -128,6 +142,7 @@ void A_B1::project(MatrixD& vol, MatrixD& proj, double /*weight*/) {
     add_sino_to_umajor_kernel<<<blocks_for(nsino, 256), 256, 0, stream>>>(st.d_sino, proj(0), dev.np, dev.nu);
     SGD_LAUNCH_CHECK();
     SGD_CUDA(cudaStreamSynchronize(stream));
+    check_device_status();
 }
 
 void A_B1::back_project(MatrixD& vol, MatrixD& proj, double /*weight*/) {
@@ -139,6 +154,7 @@ void A_B1::back_project(MatrixD& vol, MatrixD& proj, double /*weight*/) {
     add_img_to_vol_kernel<<<blocks_for(nimg, 256), 256, 0, stream>>>(st.d_img, vol(0), dev.nx, dev.ny);
     SGD_LAUNCH_CHECK();
     SGD_CUDA(cudaStreamSynchronize(stream));
+    check_device_status();
 }
 
 }  // namespace sgd

@@ -49,7 +49,12 @@ public:
     void forward_host(double* b, const double* x);
     void backward_host(const double* b, double* x);
 
+    // Raises (and clears) the device error flag set by a kernel whose bounded
+    // wait gave up.  Synchronous.
+    void check_device_status();
+
 private:
+    int* d_err_ = nullptr;
     float* d_rec_ = nullptr;
     float* d_strip_ = nullptr;
     BinHomography* d_hom_ = nullptr;

@@ -57,6 +57,13 @@ int sgd_b1_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
     });
 }
 
+int sgd_b1_status(void* layer) {
+    return sgd::guarded_status([&] {
+        if (!layer) sgd::fail("sgd_b1_status: null layer");
+        static_cast<A_B1*>(layer)->check_device_status();
+    });
+}
+
 unsigned long long sgd_b1_count(void* layer) {
     return layer ? static_cast<A_B1*>(layer)->count : 0ull;
 }

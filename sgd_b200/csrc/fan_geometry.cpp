@@ -66,70 +66,18 @@ void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out) {
     }
 }
 
-namespace {
-// g(kr + h) accumulated as a cubic in h: w * (kappa - h)^3
-inline void add_cube(double* gc, double w, double kappa) {
-    gc[0] += w * kappa * kappa * kappa;
-    gc[1] += -3.0 * w * kappa * kappa;
-    gc[2] += 3.0 * w * kappa;
-    gc[3] += -w;
-}
-// w * (kappa - h)
-inline void add_lin(double* gc, double w, double kappa) {
-    gc[0] += w * kappa;
-    gc[1] += -w;
-}
-}  // namespace
-
-void b1_profile_table(double a, double b, double* out) {
-    // Profile g = tri_a * tri_b (unit-area triangles), written from the right as
-    // g(x) = sum_{knots k > x} c_k (k - x)^3 / (6 a^2 b^2) with the stencil
-    // (+1 at a+b, -2 at a, +1 at a-b, -2 at b, ...), and on [0, min(b, a-b)] as
-    // (a - x)/a^2 - (b - x)^3 / (3 a^2 b^2).  Every term is a power of a distance
-    // to a nearby knot, so the coefficients stay accurate as b -> 0.
-    double kr[5];
-    double gc[4][4] = {{0}};
-    if (b <= 1e-7) {
-        // single-triangle limit: S(x) = x/a - x^2/(2a^2) on [0, a]
-        kr[0] = 0; kr[1] = kr[2] = kr[3] = kr[4] = a;
-        add_lin(gc[0], 1.0 / (a * a), a);
-    } else {
-        const double w6 = 1.0 / (6.0 * a * a * b * b);
-        kr[0] = 0;
-        kr[3] = a;
-        kr[4] = a + b;
-        add_lin(gc[0], 1.0 / (a * a), a);
-        add_cube(gc[0], -2.0 * w6, b);
-        if (b <= a - b) {
-            kr[1] = b; kr[2] = a - b;
-            add_lin(gc[1], 1.0 / (a * a), a - b);
-            add_cube(gc[2], w6, 2.0 * b);
-            add_cube(gc[2], -2.0 * w6, b);
-        } else {
-            kr[1] = a - b; kr[2] = b;
-            add_cube(gc[1], w6, 2.0 * b);
-            add_cube(gc[1], -2.0 * w6, b);
-            add_cube(gc[1], -2.0 * w6, 2.0 * b - a);
-            add_cube(gc[2], w6, a);
-            add_cube(gc[2], -2.0 * w6, a - b);
-        }
-        add_cube(gc[3], w6, b);
-    }
-    out[0] = kr[1]; out[1] = kr[2]; out[2] = kr[3]; out[3] = kr[4];
-    double s0 = 0.0;
-    for (int r = 0; r < 4; ++r) {
-        double* o = out + 4 + 6 * r;
-        o[0] = kr[r];
-        o[1] = s0;
-        o[2] = gc[r][0];
-        o[3] = gc[r][1] / 2.0;
-        o[4] = gc[r][2] / 3.0;
-        o[5] = gc[r][3] / 4.0;
-        double w = kr[r + 1] - kr[r];
-        s0 += w * (o[2] + w * (o[3] + w * (o[4] + w * o[5])));
-    }
-    double* o = out + 4 + 24;  // beyond the support: S = 1/2
-    o[0] = kr[4]; o[1] = 0.5; o[2] = o[3] = o[4] = o[5] = 0.0;
+void b1_profile_constants(double a, double b, float* r) {
+    if (b <= 1e-7) b = 0.0;  // single-triangle limit
+    r[6] = (float)a;
+    r[7] = (float)b;
+    r[8] = (float)(a + b);
+    r[9] = (float)(a - b);
+    r[10] = (float)(1.0 / a);
+    r[11] = (float)(1.0 / (2.0 * a * a));
+    r[12] = (float)(b * b / (12.0 * a * a));
+    r[13] = b > 0 ? (float)(1.0 / (12.0 * a * a * b * b)) : 0.f;
+    r[14] = b > 0 ? (float)(1.0 / (24.0 * a * a * b * b)) : 0.f;
+    r[15] = 0.f;
 }
 
 void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>& strip) {
@@ -156,7 +104,7 @@ void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>
             // x_E(O) = t k_E - q = (O - P).(k_E t - n)
             const double mAx = ka * tx - nxv, mAy = ka * ty - nyv;
             const double mBx = kb * tx - nxv, mBy = kb * ty - nyv;
-            float* r = &rec[((size_t)p * nu + u) * kB1Rec];
+            float r[kB1Rec];
             r[0] = (float)(mAx * g.dx);
             r[1] = (float)(mAy * g.dy);
             r[2] = (float)((x0 - px) * mAx + (y0 - py) * mAy);
@@ -166,10 +114,9 @@ void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>
             // profile half-widths (layers/A_B1.cu:429-478): vx = |dx cos(theta)|,
             // vy = |dy sin(theta)| with theta = atan2(|px - sx|, |py - sy|)
             const double vx = std::fabs(g.dx * ty), vy = std::fabs(g.dy * tx);
-            const double a = std::max(vx, vy), b = std::min(vx, vy);
-            double tab[34];
-            b1_profile_table(a, b, tab);
-            for (int k = 0; k < 34; ++k) r[6 + k] = (float)tab[k];
+            b1_profile_constants(std::max(vx, vy), std::min(vx, vy), r);
+            for (int q = 0; q < 4; ++q)
+                for (int k = 0; k < 4; ++k) rec[(((size_t)p * 4 + q) * nu + u) * 4 + k] = r[4 * q + k];
 
             // strip of the bin in index space for the forward kernel
             float* s = &strip[((size_t)p * nu + u) * kStripRec];

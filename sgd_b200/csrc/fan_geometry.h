@@ -36,7 +36,7 @@ struct BinHomography {
 void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out);
 
 // ---------------------------------------------------------------------------
-// B1 (bilinear box-spline) footprint tables.
+// B1 (bilinear box-spline) footprint records.
 //
 // For bin u of view p and pixel (i, j) the reference footprint
 // (layers/A_B1.cu:182-197) is
@@ -45,16 +45,22 @@ void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out);
 // centre perpendicular to the bin's central ray, of the bin's two edge rays, and
 // G is the odd extension of the cumulative profile S of the convolution of two
 // unit-area triangles of half-widths a = max(vx, vy), b = min(vx, vy)
-// (conv_2tri_1box_* of layers/spline_conv.hh:295-390).  xa, xb are affine in
-// (i, j); S is a quartic on each of five intervals of |x|.  The table stores,
-// per (view, bin):
-//   [0..2]  xa = i*c[0] + j*c[1] + c[2]
-//   [3..5]  xb = i*c[3] + j*c[4] + c[5]
-//   [6..9]  the four interval ends k1 <= k2 <= k3 <= k4 of |x|
-//   [10 + 6r .. 15 + 6r], r = 0..4: interval start kr and the Taylor
-//           coefficients s0..s4 of S(kr + h) in h.
+// (conv_2tri_1box_* of layers/spline_conv.hh:295-390).  With
+// w = (b - x)+, p = (a + b - x)+, q = (a - x)+ (x >= 0):
+//     S(x) = x/a - x^2/(2a^2) - b^2/(12a^2) + w^4/(12a^2b^2)   for x <= a - b
+//     S(x) = 1/2 - (p^4 - 2q^4 - 2w^4)/(24a^2b^2)               for x >  a - b
+// Every power is of a distance to a nearby knot, so FP32 keeps its accuracy as
+// b -> 0; b <= 1e-7 uses the single-triangle limit as the reference does
+// (layers/A_B1.cu:52-55).  One 64-byte record per (view, bin), stored as four
+// float4 chunks in the layout [view][chunk][bin] so that consecutive bins of
+// one chunk are consecutive 16-byte words (shared-memory bank groups):
+//   [0..2]  xa = i*r[0] + j*r[1] + r[2]
+//   [3..5]  xb = i*r[3] + j*r[4] + r[5]
+//   [6] a   [7] b   [8] a+b   [9] a-b
+//   [10] 1/a   [11] 1/(2a^2)   [12] b^2/(12a^2)   [13] 1/(12a^2b^2)   [14] 1/(24a^2b^2)
+//   [15] unused (0)
 // ---------------------------------------------------------------------------
-constexpr int kB1Rec = 40;
+constexpr int kB1Rec = 16;
 
 // Strip parameters for the detector-driven forward kernel: along the major
 // axis index m, the two edge rays cross the minor axis at
@@ -62,10 +68,8 @@ constexpr int kB1Rec = 40;
 // [4] = 1 when the major axis is y (rows), 0 when it is x (columns).
 constexpr int kStripRec = 8;
 
-// S(kr + h) tables for profile half-widths a >= b (b <= 1e-7 selects the
-// single-triangle limit, layers/A_B1.cu:52-55).  out[0..3] = k1..k4,
-// out[4 + 6r + c] = (kr, s0, s1, s2, s3, s4).
-void b1_profile_table(double a, double b, double* out);
+// Fills r[6..15] for profile half-widths a >= b.
+void b1_profile_constants(double a, double b, float* r);
 
 void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>& strip);
 

@@ -67,7 +67,15 @@ def test_b1_adjoint_dot_product(case):
 
 
 @pytest.mark.parametrize("case", ["small", "snap", "c2"])
-def test_b1_matches_reference_library(case):
+def test_b1_matches_reference_library(oracle_mod, case):
+    """Against the reference's own CUDA layer (built from its sources).
+
+    The reference steps the bin position in FP32 (`sx += puv.x`,
+    layers/A_B1.cu:160), which moves its forward output by ~1e-5 rel-L2 from
+    its own FP64 formula at 512^2 x 720 views.  Where that happens the test
+    requires the whole gap to be the reference's: ours within 1e-6 of the
+    FP64 replica and ours-vs-reference within the reference's own distance
+    to the replica plus ours."""
     import reflib
     if not reflib.available():
         pytest.fail("reference library oracle/_ref/libnetwork.so not built (make -C oracle ref)")
@@ -75,7 +83,12 @@ def test_b1_matches_reference_library(case):
     R = reflib.RefFan2D("b1", nx, ny, nu, dx, dy, du, lsd, lso, ang)
     x = ellipse_phantom(nx, ny, dx, dy, seed=5).ravel()
     b_ref, cnt = R.forward(x)
-    assert rel_l2(A.matvec(x), b_ref) < TOL_PHANTOM
+    b = A.matvec(x)
+    e = rel_l2(b, b_ref)
+    if e >= TOL_PHANTOM:
+        b64, _ = oracle_mod.b1_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+        ours, theirs = rel_l2(b, b64), rel_l2(b_ref, b64)
+        assert ours < 1e-6 and theirs >= TOL_PHANTOM and e <= theirs + ours, (e, ours, theirs)
     assert rel_l2(A.rmatvec(b_ref), R.backward(b_ref)) < TOL_PHANTOM
     assert abs(A.conv_count - cnt) <= 1e-4 * cnt + 2
 
