@@ -66,6 +66,19 @@ unsigned long long sgd_b1_count(void* layer);
  * gave up, and the output of that call was not written. */
 int sgd_b1_status(void* layer);
 
+/* New, with no counterpart in the reference: the B1 forward projection of
+ * sgd_b1_forward_dev without any device allocation during the call, for
+ * callers that cannot call cudaMalloc while they run (code under another
+ * framework's memory pool that owns the device heap; real-time loops where
+ * cudaMalloc's implicit synchronisation is not allowed).  Its scratch is a
+ * fixed 4 MiB __device__ array that every GPU loading this library holds until
+ * exit, so images are limited to 1,048,576 pixels (1024 x 1024); larger ones
+ * are rejected with -1 and a message.  The first call on each device looks up
+ * the array's address (make it before any stream capture).  All calls share
+ * the array: calls that overlap on the GPU race.  The layer's device must be
+ * current.  Returns 0 on success, -1 on failure. */
+int sgd_b1_forward_noalloc(void* layer, const float* d_img, float* d_sino, void* stream);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* New (no reference counterpart): FP32 FMA throughput of the current GPU in

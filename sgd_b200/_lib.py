@@ -34,6 +34,8 @@ def lib() -> ctypes.CDLL:
     L.sgd_last_error.restype = ctypes.c_char_p
     L.sgd_last_error.argtypes = []
     _declare_fan2d(L, "b1")
+    L.sgd_b1_forward_noalloc.restype = _i
+    L.sgd_b1_forward_noalloc.argtypes = [_vp, _vp, _vp, _vp]
     _LIB = L
     return L
 
