@@ -35,7 +35,8 @@ constexpr int kBackTJ = 32;   // tile extent along j (y), threadIdx.x: contiguou
 constexpr int kBackThreads = kBackTI * kBackTJ;
 constexpr int kVC = 4;        // views per staged chunk
 constexpr uint32_t kWaitLimit = 1u << 22;
-constexpr int kHeaderBytes = 512;  // 2 mbarriers | 3 x kVC windows | 3 x kVC homographies (8 floats)
+constexpr int kHeaderBytes = 16 + 3 * kVC * 8 + 3 * kVC * 32;  // 2 mbarriers | 3 x kVC windows | 3 x kVC homographies
+static_assert(kHeaderBytes % 16 == 0, "staged records must start 16-byte aligned");
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -128,9 +129,20 @@ __device__ __forceinline__ void box_bins(const float* h, float i0, float i1, flo
     hi = min(nu - 1, (int)floorf(fmaxf(fmaxf(u00, u01), fmaxf(u10, u11))));
 }
 
-__global__ void __launch_bounds__(kBackThreads)
-b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__ hom, const float* __restrict__ sino,
-               float* __restrict__ img, int nx, int ny, int np, int nu, int wcap, float dxdy, int* __restrict__ err) {
+template <int N>
+__device__ __forceinline__ int pick(const int (&a)[N], int v) {
+    int r = a[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k) r = (v == k) ? a[k] : r;
+    return r;
+}
+
+// wins[tile * np + p] = (lo, hi): bins of view p that tile's pixels can touch
+// (host-computed, conservative; fits in wcap).
+__global__ void __launch_bounds__(kBackThreads, 5)
+b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__ hom, const int2* __restrict__ wins,
+               const float* __restrict__ sino, float* __restrict__ img, int nx, int ny, int np, int nu, int wcap,
+               float dxdy, int* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);           // [2]
     int* win = reinterpret_cast<int*>(smem + 16);                   // [3][kVC][2]
@@ -146,35 +158,26 @@ b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__
     const int i = i0 + 4 * (w >> 2) + (l >> 3), j = j0 + 8 * (w & 3) + (l & 7);
     const float fi = (float)i, fj = (float)j;
     const int nchunks = (np + kVC - 1) / kVC;
+    const int2* twin = wins + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * np;
 
-    // tile window of chunk c's views (one thread per view), with one bin of
-    // margin on each side for rounding
-    auto windows = [&](int c) {
-        if (tid < kVC) {
-            const int p = c * kVC + tid, slot = c % 3;
-            int lo = 0, hi = -1;
-            float* h = hs + (slot * kVC + tid) * 8;
-            if (p < np) {
-                const BinHomography H = hom[p];
-                h[0] = H.n0; h[1] = H.n1; h[2] = H.n2; h[3] = H.d0; h[4] = H.d1; h[5] = H.d2;
-                box_bins(h, (float)i0 - 1.f, (float)(i0 + kBackTI), (float)j0 - 1.f, (float)(j0 + kBackTJ), nu, lo,
-                         hi);
-                lo = max(0, lo - 1);
-                hi = min(nu - 1, hi + 1);
-                if (hi - lo + 1 > wcap) hi = lo + wcap - 1;  // wcap is sized on the host; never taken
-            }
-            win[(slot * kVC + tid) * 2] = lo;
-            win[(slot * kVC + tid) * 2 + 1] = hi;
-        }
-    };
-    // stage chunk c: records by TMA (thread 0), sinogram values by all threads
+    // stage chunk c: windows and homographies (thread 0, read after the next
+    // barrier), footprint records by TMA (thread 0), sinogram values (all)
     auto stage = [&](int c) {
         const int st = c & 1, slot = c % 3;
         if (tid == 0) {
             uint32_t bytes = 0;
             for (int v = 0; v < kVC; ++v) {
-                const int W = win[(slot * kVC + v) * 2 + 1] - win[(slot * kVC + v) * 2] + 1;
-                if (W > 0) bytes += (uint32_t)W * sizeof(B1Bin);
+                const int p = c * kVC + v;
+                int2 lh = make_int2(0, -1);
+                if (p < np) {
+                    lh = __ldg(twin + p);
+                    const BinHomography H = hom[p];
+                    float* h = hs + (slot * kVC + v) * 8;
+                    h[0] = H.n0; h[1] = H.n1; h[2] = H.n2; h[3] = H.d0; h[4] = H.d1; h[5] = H.d2;
+                }
+                win[(slot * kVC + v) * 2] = lh.x;
+                win[(slot * kVC + v) * 2 + 1] = lh.y;
+                if (lh.y >= lh.x) bytes += (uint32_t)(lh.y - lh.x + 1) * sizeof(B1Bin);
             }
             fence_proxy_async_smem();
             mbar_arrive_expect_tx(&bars[st], bytes);
@@ -187,10 +190,12 @@ b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__
             }
         }
         for (int v = 0; v < kVC; ++v) {
-            const int lo = win[(slot * kVC + v) * 2], W = win[(slot * kVC + v) * 2 + 1] - lo + 1;
-            const float* sp = sino + (size_t)(c * kVC + v) * nu + lo;
+            const int p = c * kVC + v;
+            if (p >= np) break;
+            const int2 lh = __ldg(twin + p);
+            const float* sp = sino + (size_t)p * nu + lh.x;
             float* dp = ssino + (st * kVC + v) * wcap;
-            for (int w = tid; w < W; w += kBackThreads) dp[w] = __ldg(sp + w);
+            for (int k = tid; k <= lh.y - lh.x; k += kBackThreads) dp[k] = __ldg(sp + k);
         }
     };
 
@@ -200,15 +205,13 @@ b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__
         fence_mbar_init();
         s_abort = 0;
     }
-    windows(0);
     __syncthreads();
     stage(0);
 
-    double acc = 0.0;  // FP32 within a view (a few bins), FP64 across views
+    double acc = 0.0;  // FP32 within a chunk (a few tens of terms), FP64 across chunks
     int c = 0;
     for (; c < nchunks; ++c) {
-        if (c + 1 < nchunks) windows(c + 1);
-        __syncthreads();  // windows(c+1) and sinogram(c) visible; chunk c-1 fully consumed
+        __syncthreads();  // chunk c's windows and sinogram visible; chunk c-1 fully consumed
         if (s_abort) break;
         if (c + 1 < nchunks) stage(c + 1);
         const int st = c & 1, slot = c % 3;
@@ -218,23 +221,42 @@ b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__
             continue;
         }
         if (i >= nx || j >= ny) continue;
+        // this pixel's bins in each view of the chunk, then one flat loop over
+        // all of them: lanes run nearly equal trip counts
+        int ulo[kVC], uhi[kVC], roff[kVC], soff[kVC];
+        int total = 0;
+#pragma unroll
         for (int v = 0; v < kVC; ++v) {
             const int lo = win[(slot * kVC + v) * 2], hi = win[(slot * kVC + v) * 2 + 1];
-            if (hi < lo) continue;
-            int ulo, uhi;
-            box_bins(hs + (slot * kVC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, ulo, uhi);
-            ulo = max(ulo, lo);
-            uhi = min(uhi, hi);
-            const float4* rb = srec + (st * kVC + v) * 4 * wcap - lo;
-            const float* sb = ssino + (st * kVC + v) * wcap - lo;
-            float vsum = 0.f;
-            for (int u = ulo; u <= uhi; ++u) {
-                const B1Bin r{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]};
-                const float conv = b1_conv(fi, fj, r);
-                if (conv > kConvEps) vsum = fmaf(conv, sb[u], vsum);
+            int a = 0, b = -1;
+            if (hi >= lo) {
+                box_bins(hs + (slot * kVC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, a, b);
+                a = max(a, lo);
+                b = min(b, hi);
             }
-            acc += (double)vsum;
+            ulo[v] = a;
+            uhi[v] = b;
+            roff[v] = (st * kVC + v) * 4 * wcap - lo;
+            soff[v] = (st * kVC + v) * wcap - lo;
+            total += max(0, b - a + 1);
         }
+        float csum = 0.f;
+        int v = 0, u = ulo[0], ue = uhi[0], ro = roff[0], so = soff[0];
+        for (int k = 0; k < total; ++k) {
+            while (u > ue) {
+                ++v;
+                u = pick(ulo, v);
+                ue = pick(uhi, v);
+                ro = pick(roff, v);
+                so = pick(soff, v);
+            }
+            const float4* rb = srec + ro + u;
+            const B1Bin r{rb[0], rb[wcap], rb[2 * wcap], rb[3 * wcap]};
+            const float conv = b1_conv(fi, fj, r);
+            if (conv > kConvEps) csum = fmaf(conv, ssino[so + u], csum);
+            ++u;
+        }
+        acc += (double)csum;
     }
     if (c < nchunks) {
         // a staged chunk never arrived: wait (bounded) for the copies still in
@@ -290,27 +312,36 @@ __global__ void b1_count_kernel(const BinHomography* __restrict__ hom, int nx, i
 
 }  // namespace
 
-int b1_back_wcap(const FanGeometry& g, const std::vector<BinHomography>& hom) {
-    // Largest staged window of any 32x8 tile over all views: a host replay of
-    // the kernel's window rule in double, with one more bin of margin each
-    // side, rounded up to a multiple of 4.
+int b1_back_windows(const FanGeometry& g, const std::vector<BinHomography>& hom, std::vector<int>& wins) {
+    // Per 32x8 tile and view, the bins its pixels' +-1 supports can reach: the
+    // kernel's corner rule in double, one extra bin each side so the kernel's
+    // FP32 per-pixel ranges always fall inside.  Returns the largest window,
+    // rounded up to a multiple of 4 (the shared-memory capacity per view).
+    const int gx = (g.ny + kBackTJ - 1) / kBackTJ, gy = (g.nx + kBackTI - 1) / kBackTI;
+    wins.assign((size_t)gx * gy * g.np * 2, 0);
     int wmax = 1;
-    for (int p = 0; p < g.np; ++p) {
-        const BinHomography& H = hom[p];
-        for (int i0 = 0; i0 < g.nx; i0 += kBackTI)
-            for (int j0 = 0; j0 < g.ny; j0 += kBackTJ) {
-                double is[2] = {i0 - 1.0, (double)(i0 + kBackTI)}, js[2] = {j0 - 1.0, (double)(j0 + kBackTJ)};
+    for (int by = 0; by < gy; ++by)
+        for (int bx = 0; bx < gx; ++bx) {
+            const int i0 = by * kBackTI, j0 = bx * kBackTJ;
+            const double is[2] = {i0 - 1.0, (double)(i0 + kBackTI)}, js[2] = {j0 - 1.0, (double)(j0 + kBackTJ)};
+            int* out = &wins[((size_t)by * gx + bx) * g.np * 2];
+            for (int p = 0; p < g.np; ++p) {
+                const BinHomography& H = hom[p];
                 double umin = 1e300, umax = -1e300;
                 for (double a : is)
                     for (double b : js) {
-                        double u = (H.n0 * a + H.n1 * b + H.n2) / (H.d0 * a + H.d1 * b + H.d2);
+                        const double u = ((double)H.n0 * a + (double)H.n1 * b + H.n2) /
+                                         ((double)H.d0 * a + (double)H.d1 * b + H.d2);
                         umin = std::min(umin, u);
                         umax = std::max(umax, u);
                     }
-                int lo = std::max(0, (int)std::floor(umin) - 2), hi = std::min(g.nu - 1, (int)std::floor(umax) + 2);
+                const int lo = std::max(0, (int)std::floor(umin) - 1);
+                const int hi = std::min(g.nu - 1, (int)std::floor(umax) + 1);
+                out[2 * p] = lo;
+                out[2 * p + 1] = hi;
                 wmax = std::max(wmax, hi - lo + 1);
             }
-    }
+        }
     return (wmax + 3) & ~3;
 }
 
@@ -335,9 +366,9 @@ void b1_forward_launch(const B1Device& d, const float* img, float* imgT, float* 
 
 void b1_back_launch(const B1Device& d, const float* sino, float* img, cudaStream_t s) {
     dim3 tg((d.ny + kBackTJ - 1) / kBackTJ, (d.nx + kBackTI - 1) / kBackTI);
-    b1_back_kernel<<<tg, kBackThreads, b1_back_smem_bytes(d.wcap), s>>>(reinterpret_cast<const float4*>(d.rec), d.hom,
-                                                                         sino, img, d.nx, d.ny, d.np, d.nu, d.wcap,
-                                                                         d.dxdy, d.err);
+    b1_back_kernel<<<tg, kBackThreads, b1_back_smem_bytes(d.wcap), s>>>(
+        reinterpret_cast<const float4*>(d.rec), d.hom, reinterpret_cast<const int2*>(d.wins), sino, img, d.nx, d.ny,
+        d.np, d.nu, d.wcap, d.dxdy, d.err);
     SGD_LAUNCH_CHECK();
 }
 

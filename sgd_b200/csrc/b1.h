@@ -16,11 +16,12 @@ struct B1Device {
     const float* rec = nullptr;          // [np][nu][kB1Rec]
     const float* strip = nullptr;        // [np][nu][kStripRec]
     const BinHomography* hom = nullptr;  // [np]
+    const int* wins = nullptr;           // [tiles][np][2] bin windows of the back kernel's tiles
     int wcap = 4;                        // bins of a staged view window in the back kernel
     int* err = nullptr;                  // device flag: a bounded wait in a kernel gave up
 };
 
-int b1_back_wcap(const FanGeometry& g, const std::vector<BinHomography>& hom);
+int b1_back_windows(const FanGeometry& g, const std::vector<BinHomography>& hom, std::vector<int>& wins);
 size_t b1_back_smem_bytes(int wcap);
 void b1_prepare_device();
 

@@ -46,11 +46,19 @@ __device__ __forceinline__ float b1_xb_inner(float fj, const B1Bin& r) { return 
 __device__ __forceinline__ float b1_xa(float fi, float inner, const B1Bin& r) { return __fmaf_rn(fi, r.q0.x, inner); }
 __device__ __forceinline__ float b1_xb(float fi, float inner, const B1Bin& r) { return __fmaf_rn(fi, r.q0.w, inner); }
 
+// One MUFU reciprocal (|x| >= 2^-126 here: xb - xa is a bin width at the
+// pixel, ~0.1..10 mm).
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // conv from the two edge offsets.
 __device__ __forceinline__ float b1_conv_x(float xa, float xb, const B1Bin& r) {
     const float ga = b1_G(xa, r);
     const float gb = b1_G(xb, r);
-    return __fdividef(__fsub_rn(gb, ga), __fsub_rn(xb, xa));
+    return __fmul_rn(__fsub_rn(gb, ga), rcp_approx(__fsub_rn(xb, xa)));
 }
 
 // conv of layers/A_B1.cu:182-197 for pixel (fi, fj) given as float indices.

@@ -60,7 +60,11 @@ A_B1::A_B1(int nx, int ny, int np, int nu, double dx, double dy, double du, doub
     dev.nx = nx; dev.ny = ny; dev.np = np; dev.nu = nu;
     dev.dxdy = (float)(dx * dy);
     dev.rec = d_rec_; dev.strip = d_strip_; dev.hom = d_hom_;
-    dev.wcap = b1_back_wcap(geo, hom);
+    std::vector<int> wins;
+    dev.wcap = b1_back_windows(geo, hom, wins);
+    SGD_CUDA(cudaMalloc(&d_wins_, wins.size() * sizeof(int)));
+    SGD_CUDA(cudaMemcpy(d_wins_, wins.data(), wins.size() * sizeof(int), cudaMemcpyHostToDevice));
+    dev.wins = d_wins_;
     if (b1_back_smem_bytes(dev.wcap) > 200 * 1024)
         fail("B1 back projector: bin window of %d bins does not fit in shared memory", dev.wcap);
     SGD_CUDA(cudaMalloc(&d_err_, sizeof(int)));
@@ -83,6 +87,7 @@ A_B1::~A_B1() {
     cudaFree(d_strip_);
     cudaFree(d_hom_);
     cudaFree(d_err_);
+    cudaFree(d_wins_);
     cudaFree(st.d_img);
     cudaFree(st.d_imgT);
     cudaFree(st.d_sino);

@@ -55,6 +55,7 @@ public:
 
 private:
     int* d_err_ = nullptr;
+    int* d_wins_ = nullptr;
     float* d_rec_ = nullptr;
     float* d_strip_ = nullptr;
     BinHomography* d_hom_ = nullptr;
