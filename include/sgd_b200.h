@@ -28,6 +28,16 @@ extern "C" {
  * error reporting, utils/exception.hh throws across the ABI). */
 const char* sgd_last_error(void);
 
+/* ---- geometry --------------------------------------------------------------- */
+
+/* New, host only: per-view 3x4 projection matrices pm (FP64, may be NULL) and
+ * their index-space FP32 form pmi, 12 values per view, as the reference's
+ * GeoData::initialize_projection_matrix builds them (utils/geo.cu:58-201,
+ * after geo_init_angles :232-269).  dz_off/drho may be NULL.  0 / -1. */
+int sgd_geometry_pmi(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
+                     double dv, double lsd, double lso, const double* angles, const double* dz_off,
+                     const double* drho, double* pm_out, float* pmi_out);
+
 /* ---- B1 bilinear box-spline, 2D fan beam ---------------------------------- */
 
 /* Replaces b1_init, layers/A_B1.hh:24 / layers/A_B1.cu:595-603.  dz and drho
@@ -78,6 +88,23 @@ int sgd_b1_status(void* layer);
  * the array: calls that overlap on the GPU race.  The layer's device must be
  * current.  Returns 0 on success, -1 on failure. */
 int sgd_b1_forward_noalloc(void* layer, const float* d_img, float* d_sino, void* stream);
+
+/* ---- A_SF separable footprint (SF-TR), 2D fan beam -------------------------- */
+
+/* Replace SF_init / SF_forward_projection / SF_backward_projection,
+ * layers/A_SF.hh:23-25 / layers/A_SF.cu:395-479 (same layouts as B1).  The
+ * forward returns 0 as the reference does (its SF kernels never count), -1
+ * on failure. */
+void* SF_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+              double* angles);
+int SF_forward_projection(double* b, double* x, void* layer);
+void SF_backward_projection(double* b, double* x, void* layer);
+/* New: status-returning backward, destruction, device entry points, count. */
+int sgd_SF_backward_projection(double* b, double* x, void* layer);
+void SF_destroy(void* layer);
+int sgd_SF_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream);
+int sgd_SF_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
+unsigned long long sgd_SF_count(void* layer);
 
 /* ---- measurement ---------------------------------------------------------- */
 

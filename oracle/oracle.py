@@ -29,6 +29,8 @@ def lib():
         L.oracle_b1_forward.restype = ctypes.c_longlong
         L.oracle_b1_backward.restype = None
         L.oracle_b1_matrix.restype = ctypes.c_longlong
+        L.oracle_sf_forward.restype = None
+        L.oracle_sf_backward.restype = None
         L.oracle_b1_flops.restype = None
     return _LIB
 
@@ -110,3 +112,21 @@ def b1_matrix(nx, ny, nu, dx, dy, du, lsd, lso, angles, views):
             break
         cap = int(n)
     return sp.csr_matrix((vals[:n], (rows[:n], cols[:n])), shape=(len(views) * nu, nx * ny))
+
+
+def _fan2d(name, nx, ny, nu, dx, dy, du, lsd, lso, angles, vec, out_len, precision):
+    angles = _c(angles)
+    vec = _c(np.ravel(vec))
+    out = np.zeros(out_len)
+    getattr(lib(), name)(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(du),
+                         ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), _p(vec), _p(out), precision)
+    return out
+
+
+def sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
+    """FP64 replica of SF_forward_projection; returns (b, 0): the reference's SF never counts."""
+    return _fan2d("oracle_sf_forward", nx, ny, nu, dx, dy, du, lsd, lso, angles, x, len(angles) * nu, precision), 0
+
+
+def sf_backward(b, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
+    return _fan2d("oracle_sf_backward", nx, ny, nu, dx, dy, du, lsd, lso, angles, b, nx * ny, precision)

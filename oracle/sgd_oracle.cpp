@@ -385,6 +385,50 @@ void b1_backward(const Geo& g, const std::vector<float>& vecs, const double* b, 
         }
 }
 
+// ---------------------------------------------------------------------------
+// A_SF separable footprint (SF-TR) fan-beam projector: layers/A_SF.cu
+// ---------------------------------------------------------------------------
+
+// layers/A_SF.cu:48-84
+template <class T> T sf_gamma(T s1, T s2, const T* us) {
+    T g = 0, tmp, b1, b2;
+    b1 = max(s1, us[0]); b2 = min(s2, us[1]);
+    tmp = (b2 > b1) ? (T(1) / (T(2) * (us[1] - us[0]))) * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0])) : T(0);
+    if (tmp == tmp) g += tmp;
+    b1 = max(s1, us[1]); b2 = min(s2, us[2]);
+    tmp = (b2 > b1) ? b2 - b1 : T(0);
+    if (tmp == tmp) g += tmp;
+    b1 = max(s1, us[2]); b2 = min(s2, us[3]);
+    tmp = (b2 > b1) ? (T(1) / (T(2) * (us[3] - us[2]))) * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3])) : T(0);
+    if (tmp == tmp) g += tmp;
+    return g;
+}
+
+// Per-(pixel, view) body of SF_forward_projection (layers/A_SF.cu:87-225) and
+// SF_backward_projection (:228-334): visit(u, weight*gamma) for kept bins.
+template <class T, class Visit>
+void sf_pixel_view(const Geo& g, int p, int ix, int iy, Visit visit) {
+    int nx = g.nx, ny = g.ny, nu = g.nu;
+    float dx = (float)g.dx, dy = (float)g.dy;
+    const float* pm = &g.pmi[12 * p];
+    float srcx = (float)g.src[3 * p], srcy = (float)g.src[3 * p + 1];
+    float puvx = (float)g.puv[3 * p], puvy = (float)g.puv[3 * p + 1];
+    bool singular = std::fabs(puvx - puvy) < 1e-7f;            // :119
+    float nx2 = (nx - 1) / 2.0f, ny2 = (ny - 1) / 2.0f;        // :101
+    int minu, maxu;
+    float usf[4];
+    bin_range<float>(pm, puvx, singular, ix - 0.5f, ix + 0.5f, iy - 0.5f, iy + 0.5f, nu, minu, maxu, usf);  // :116-167
+    T us[4] = {usf[0], usf[1], usf[2], usf[3]};
+    T theta = std::atan2((double)(dx * (ix - nx2) - srcx), (double)(dy * (iy - ny2) - srcy));  // :174
+    T st = std::fabs(std::sin((double)theta)), ct = std::fabs(std::cos((double)theta));
+    T weight = T(dx) / max(st, ct);                             // :177
+    for (int u = minu; u <= maxu; ++u) {
+        T gm = sf_gamma<T>(T(u), T(u) + T(1), us);              // :209
+        T val = weight * gm;
+        if (val == val && gm > T(1e-7f)) visit(u, (double)val);  // :214
+    }
+}
+
 Geo make_geo(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
              double dv) {
     Geo g;
@@ -434,6 +478,44 @@ void oracle_b1_backward(int nx, int ny, int np, int nu, double dx, double dy, do
     std::vector<float> vecs;
     b1_vectors(g, vecs);
     if (precision) b1_backward<float>(g, vecs, b, x); else b1_backward<double>(g, vecs, b, x);
+}
+
+// SF_forward_projection / SF_backward_projection (layers/A_SF.cu:406-479),
+// same host layouts as B1.  FP64 replica (precision 0) or FP32 (1).
+void oracle_sf_forward(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                       const double* angles, const double* x, double* b, int precision) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::memset(b, 0, sizeof(double) * (size_t)np * nu);
+#pragma omp parallel for schedule(dynamic)
+    for (int p = 0; p < np; ++p) {
+        double* bp = b + (size_t)p * nu;
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                double C = x[(size_t)ix * ny + iy];
+                auto visit = [&](int u, double v) { bp[u] += v * C; };
+                if (precision) sf_pixel_view<float>(g, p, ix, iy, visit); else sf_pixel_view<double>(g, p, ix, iy, visit);
+            }
+    }
+}
+
+void oracle_sf_backward(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                        const double* angles, const double* b, double* x, int precision) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+#pragma omp parallel for schedule(dynamic)
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            double acc = 0.0;
+            for (int p = 0; p < np; ++p) {
+                const double* bp = b + (size_t)p * nu;
+                double val = 0.0;
+                auto visit = [&](int u, double v) { val += v * bp[u]; };
+                if (precision) sf_pixel_view<float>(g, p, ix, iy, visit); else sf_pixel_view<double>(g, p, ix, iy, visit);
+                acc += val;
+            }
+            x[(size_t)ix * ny + iy] = acc;
+        }
 }
 
 // Rows of the B1 system matrix for the views listed in `views` (the entries the

@@ -33,17 +33,29 @@ def lib() -> ctypes.CDLL:
     L = ctypes.CDLL(LIB_PATH)
     L.sgd_last_error.restype = ctypes.c_char_p
     L.sgd_last_error.argtypes = []
-    _declare_fan2d(L, "b1")
+    for pre in ("b1", "SF"):
+        _declare_fan2d(L, pre)
+    L.sgd_geometry_pmi.restype = _i
     L.sgd_b1_forward_noalloc.restype = _i
     L.sgd_b1_forward_noalloc.argtypes = [_vp, _vp, _vp, _vp]
     _LIB = L
     return L
 
 
+# per-prefix init argument lists (the reference's signatures)
+_INIT_ARGS = {
+    "b1": [_i, _i, _i, _i, _d, _d, _d, _d, _d, _dp, _dp, _dp],
+    "b0": [_i, _i, _i, _i, _d, _d, _d, _d, _d, _dp, _dp, _dp],
+    "SF": [_i, _i, _i, _i, _d, _d, _d, _d, _d, _dp],
+    "h0": [_i, _i, _i, _i, _d, _d, _d, _d, _dp, _dp, _dp],
+    "hl": [_i, _i, _i, _i, _d, _d, _d, _d, _dp, _dp, _dp],
+}
+
+
 def _declare_fan2d(L, pre: str) -> None:
     init = getattr(L, f"{pre}_init")
     init.restype = _vp
-    init.argtypes = [_i, _i, _i, _i, _d, _d, _d, _d, _d, _dp, _dp, _dp]
+    init.argtypes = _INIT_ARGS[pre]
     f = getattr(L, f"{pre}_forward_projection")
     f.restype = _i
     f.argtypes = [_dp, _dp, _vp]

@@ -1,0 +1,66 @@
+// extern "C" entry points of the generic 2D projectors (A_SF, B0, H0, Hl).
+// Names and signatures of the reference ones are kept; see include/sgd_b200.h.
+#include <cuda_runtime.h>
+
+#include "common.h"
+#include "proj2d.h"
+
+namespace sgd {
+Proj2D* make_sf_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                      const double* angles);
+}
+
+using sgd::Proj2D;
+
+namespace {
+int fwd_host(double* b, double* x, void* layer, const char* what) {
+    return sgd::guarded<int>(-1, [&]() -> int {
+        if (!layer || !b || !x) sgd::fail("%s: null argument", what);
+        Proj2D* L = static_cast<Proj2D*>(layer);
+        L->forward_host(b, x);
+        return (int)L->count;
+    });
+}
+int bwd_host(double* b, double* x, void* layer, const char* what) {
+    return sgd::guarded_status([&] {
+        if (!layer || !b || !x) sgd::fail("%s: null argument", what);
+        static_cast<Proj2D*>(layer)->backward_host(b, x);
+    });
+}
+int fwd_dev(void* layer, const float* img, float* sino, void* stream, const char* what) {
+    return sgd::guarded_status([&] {
+        if (!layer || !img || !sino) sgd::fail("%s: null argument", what);
+        static_cast<Proj2D*>(layer)->forward_dev(img, sino, static_cast<cudaStream_t>(stream));
+    });
+}
+int bwd_dev(void* layer, const float* sino, float* img, void* stream, const char* what) {
+    return sgd::guarded_status([&] {
+        if (!layer || !img || !sino) sgd::fail("%s: null argument", what);
+        static_cast<Proj2D*>(layer)->backward_dev(sino, img, static_cast<cudaStream_t>(stream));
+    });
+}
+}  // namespace
+
+extern "C" {
+
+void* SF_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+              double* angles) {
+    return sgd::guarded<void*>(nullptr, [&]() -> void* {
+        return sgd::make_sf_layer(nx, ny, np, nu, dx, dy, du, lsd, lso, angles);
+    });
+}
+int SF_forward_projection(double* b, double* x, void* layer) { return fwd_host(b, x, layer, "SF_forward_projection"); }
+void SF_backward_projection(double* b, double* x, void* layer) { bwd_host(b, x, layer, "SF_backward_projection"); }
+int sgd_SF_backward_projection(double* b, double* x, void* layer) {
+    return bwd_host(b, x, layer, "SF_backward_projection");
+}
+void SF_destroy(void* layer) { delete static_cast<Proj2D*>(layer); }
+int sgd_SF_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream) {
+    return fwd_dev(layer, d_img, d_sino, stream, "sgd_SF_forward_dev");
+}
+int sgd_SF_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream) {
+    return bwd_dev(layer, d_sino, d_img, stream, "sgd_SF_backward_dev");
+}
+unsigned long long sgd_SF_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
+
+}  // extern "C"

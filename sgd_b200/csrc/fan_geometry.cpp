@@ -13,8 +13,98 @@ const double kPI = 3.14159265358979323846;
 inline double cross(double ax, double ay, double bx, double by) { return ax * by - ay * bx; }
 }  // namespace
 
+std::vector<ViewFrame> view_frames(int np, double lsd, double lso, double du, double dv, const double* angles,
+                                   const double* dz, const double* drho) {
+    std::vector<ViewFrame> out(np);
+    for (int p = 0; p < np; ++p) {
+        long double b = angles[p];
+        if (std::fabs(std::sin(b) - std::cos(b)) < 1e-7L)
+            b = (std::sin(b) > 0) ? kPI / 4 : -kPI * 3 / 4;
+        else if (std::fabs(std::sin(b) + std::cos(b)) < 1e-7L)
+            b = (std::sin(b) > 0) ? kPI * 3 / 4 : -kPI / 4;
+        const double bb = (double)b, c = std::cos(bb), s = std::sin(bb);
+        const double v[4][3] = {{-lso + (drho ? drho[p] : 0.0), 0.0, dz ? dz[p] : 0.0},
+                                {lsd - lso, 0.0, 0.0},
+                                {0.0, du, 0.0},
+                                {0.0, 0.0, dv}};
+        double* dst[4] = {out[p].src, out[p].dtv, out[p].puv, out[p].pvv};
+        for (int k = 0; k < 4; ++k) {  // rotation about z, utils/geo.cu:203-207
+            dst[k][0] = v[k][0] * c - v[k][1] * s;
+            dst[k][1] = v[k][0] * s + v[k][1] * c;
+            dst[k][2] = v[k][2];
+        }
+    }
+    return out;
+}
+
+namespace {
+// out = a (r x n) times b (n x 4), row-major, sums in index order from 0.0
+void mat_mul(const double* a, int r, int n, const double* b, double* out) {
+    double t[16];
+    for (int i = 0; i < r; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < n; ++k) acc += a[i * n + k] * b[k * 4 + j];
+            t[i * 4 + j] = acc;
+        }
+    for (int i = 0; i < r * 4; ++i) out[i] = t[i];
+}
+}  // namespace
+
+void reference_pmi(const ViewFrame& f, double uc, double vc, int nx, int ny, int nz, double ddx, double ddy,
+                   double ddz, double pm[12], float pmi[12]) {
+    const double *src = f.src, *dtv = f.dtv, *puv = f.puv, *pvv = f.pvv;
+    // detector normal, and k = n . (D - S): source-to-detector distance along n
+    const double n[3] = {puv[1] * pvv[2] - puv[2] * pvv[1], puv[2] * pvv[0] - puv[0] * pvv[2],
+                         puv[0] * pvv[1] - puv[1] * pvv[0]};
+    double k = 0.0;
+    for (int i = 0; i < 3; ++i) k += n[i] * (dtv[i] - src[i]);
+    double off[3];
+    for (int i = 0; i < 3; ++i) off[i] = src[i] - dtv[i] + (uc * puv[i]) + (vc * pvv[i]) + 1;
+    // X -> X - S, -> (X - S, n.(X - S)), scaled by k, shifted to detector
+    // corner coordinates, then expressed in the (puv, pvv, 1) basis
+    double m[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1};
+    const double t1[16] = {1, 0, 0, -src[0], 0, 1, 0, -src[1], 0, 0, 1, -src[2], 0, 0, 0, 1};
+    mat_mul(t1, 4, 4, m, m);
+    const double t2[16] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0, n[0], n[1], n[2], 0};
+    mat_mul(t2, 4, 4, m, m);
+    const double t3[16] = {k, 0, 0, 0, 0, k, 0, 0, 0, 0, k, 0, 0, 0, 0, 1};
+    mat_mul(t3, 4, 4, m, m);
+    const double t4[12] = {1, 0, 0, off[0], 0, 1, 0, off[1], 0, 0, 1, off[2]};
+    mat_mul(t4, 3, 4, m, m);
+    // inverse of B = [puv pvv 1] by cofactors; identity when |det| < 1e-10
+    // (views at odd multiples of 45 degrees, utils/geo.cu:36-41)
+    const double B[9] = {puv[0], pvv[0], 1, puv[1], pvv[1], 1, puv[2], pvv[2], 1};
+    double Bi[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    const double det = B[0] * ((B[4] * B[8]) - (B[5] * B[7])) - B[1] * ((B[3] * B[8]) - (B[5] * B[6])) +
+                       B[2] * ((B[3] * B[7]) - (B[4] * B[6]));
+    if (!(std::fabs(det) < 1e-10)) {
+        Bi[0] = ((B[4] * B[8]) - (B[5] * B[7])) / det;
+        Bi[1] = -1 * ((B[1] * B[8]) - (B[2] * B[7])) / det;
+        Bi[2] = ((B[1] * B[5]) - (B[2] * B[4])) / det;
+        Bi[3] = -1 * ((B[3] * B[8]) - (B[5] * B[6])) / det;
+        Bi[4] = ((B[0] * B[8]) - (B[2] * B[6])) / det;
+        Bi[5] = -1 * ((B[0] * B[5]) - (B[2] * B[3])) / det;
+        Bi[6] = ((B[3] * B[7]) - (B[4] * B[6])) / det;
+        Bi[7] = -1 * ((B[0] * B[7]) - (B[1] * B[6])) / det;
+        Bi[8] = ((B[0] * B[4]) - (B[1] * B[3])) / det;
+    }
+    mat_mul(Bi, 3, 3, m, m);
+    for (int i = 0; i < 12; ++i) pm[i] = m[i] / m[11];
+    // index space: X = (i dx - ox, j dy - oy, k dz - oz), origin offsets in FP32
+    const float dx = (float)ddx, dy = (float)ddy, dz = (float)ddz;
+    const float ox = (nx - 1) * dx / 2.0f, oy = (ny - 1) * dy / 2.0f, oz = (nz - 1) * dz / 2.0f;
+    for (int r = 0; r < 3; ++r) {
+        const double* q = pm + 4 * r;
+        pmi[4 * r + 0] = dx * q[0];
+        pmi[4 * r + 1] = dy * q[1];
+        pmi[4 * r + 2] = dz * q[2];
+        pmi[4 * r + 3] = q[3] - ox * q[0] - oy * q[1] - oz * q[2];
+    }
+}
+
 void FanGeometry::init(int nx_, int ny_, int np_, int nu_, double dx_, double dy_, double du_, double lsd_,
-                       double lso_, const double* angles, const double* /*dz*/, const double* drho) {
+                       double lso_, const double* angles, const double* dz, const double* drho) {
     if (nx_ <= 0 || ny_ <= 0 || np_ <= 0 || nu_ <= 0) fail("invalid sizes nx=%d ny=%d np=%d nu=%d", nx_, ny_, np_, nu_);
     if (!(dx_ > 0) || !(dy_ > 0) || !(du_ > 0)) fail("pixel and bin pitches must be positive");
     if (!(lso_ > 0) || !(lsd_ > lso_)) fail("need 0 < lso < lsd (lso=%g lsd=%g)", lso_, lsd_);
@@ -39,6 +129,13 @@ void FanGeometry::init(int nx_, int ny_, int np_, int nu_, double dx_, double dy
         dtv[2 * p + 1] = (lsd - lso) * s;
         puv[2 * p] = -du * s;                // rotate((0, du), beta)
         puv[2 * p + 1] = du * c;
+    }
+    // 2D layers use nz = nv = 1 and dz = dv = 1 (layers/A_B1.cu:596)
+    frames = view_frames(np, lsd, lso, du, 1.0, angles, dz, drho);
+    pmi.resize(12 * (size_t)np);
+    for (int p = 0; p < np; ++p) {
+        double pm[12];
+        reference_pmi(frames[p], nu / 2.0, 0.5, nx, ny, 1, dx, dy, 1.0, pm, &pmi[12 * (size_t)p]);
     }
 }
 

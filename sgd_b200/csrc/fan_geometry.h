@@ -12,11 +12,34 @@
 
 namespace sgd {
 
+// One view of a circular (fan or cone) geometry in 3D: source, detector
+// centre, detector u step and v step (utils/geo.cu:232-269).
+struct ViewFrame {
+    double src[3], dtv[3], puv[3], pvv[3];
+};
+
+// geo_init_angles of utils/geo.cu:232-269: per-view rotation by beta (snapped
+// to an exact odd multiple of 45 degrees within 1e-7, the test in long
+// double), source offsets dz (along z) and drho (along the source axis).
+std::vector<ViewFrame> view_frames(int np, double lsd, double lso, double du, double dv, const double* angles,
+                                   const double* dz, const double* drho);
+
+// The reference's 3x4 projection matrix of a view and its index-space FP32
+// form (utils/geo.cu:58-161): pmi maps voxel indices (i, j, k, 1) to
+// homogeneous detector coordinates (u w, v w, w), with uc = nu/2, vc = nv/2.
+// The arithmetic is done in the same order as the reference so that pmi is
+// bit-identical (the visited-bin ranges of the separable-footprint and 3D
+// kernels are floors of pmi projections).
+void reference_pmi(const ViewFrame& f, double uc, double vc, int nx, int ny, int nz, double dx, double dy,
+                   double dz, double pm[12], float pmi[12]);
+
 struct FanGeometry {
     int nx = 0, ny = 0, np = 0, nu = 0;
     double dx = 1, dy = 1, du = 1, lsd = 0, lso = 0;
     std::vector<double> beta;            // per-view angle after the 45-degree snap
     std::vector<double> src, dtv, puv;   // per view, (x, y)
+    std::vector<ViewFrame> frames;       // per view, 3D (2D layers: nz = nv = 1, dz = dv = 1)
+    std::vector<float> pmi;              // per view, 12 floats (reference_pmi)
 
     // geo_init_angles of utils/geo.cu:232-269, including its snapping of
     // angles within 1e-7 of an odd multiple of 45 degrees.

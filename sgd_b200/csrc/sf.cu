@@ -1,0 +1,141 @@
+// A_SF: separable-footprint (SF-TR) 2D fan-beam projector on the generic 2D
+// kernels.  Reference: layers/A_SF.cu:48-84 (gamma_calculate), :87-225
+// (forward), :228-334 (backward), :395-479 (C entry points).
+//
+// Per pixel and view the four pixel corners (i +- 1/2, j +- 1/2) are projected
+// through the view's index-space matrix pmi (bit-identical to the reference's,
+// fan_geometry.h) into bin coordinates, sorted into a trapezoid us[0..3]; the
+// footprint in bin u is the trapezoid's integral over [u, u+1] (unit plateau)
+// times dx / max(|sin t|, |cos t|), t the direction of the pixel centre from
+// the source.  The expressions are written as the reference writes them so
+// that the compiler forms the same operations; bins with gamma <= 1e-7 are
+// dropped as the reference drops them.
+#include <cmath>
+
+#include "common.h"
+#include "proj2d_impl.cuh"
+
+namespace sgd {
+
+struct SFBasis {
+    static constexpr int kViewFloats = 16;
+    // [0..5] pmi 0,1,3,8,9,11  [6] puv.x  [7] singular  [8] src.x  [9] src.y
+    // [10] dx  [11] dy  [12] (nx-1)/2  [13] (ny-1)/2
+    struct View {
+        float pm0, pm1, pm3, pm8, pm9, pm11, puvx, singular, srcx, srcy, dx, dy, nx2, ny2;
+    };
+    struct Cell {
+        float us[4];
+        float weight;
+        int lo, hi;
+    };
+    __device__ static void load_view(const float* v, View& V) {
+        const float4* q = reinterpret_cast<const float4*>(v);
+        const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+        V = View{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y};
+    }
+    __device__ static bool valid(int, int, const Fan2DParams&) { return true; }
+
+    __device__ static void sort2(float& a, float& b) {
+        if (a > b) {
+            const float t = b;
+            b = a;
+            a = t;
+        }
+    }
+    // layers/A_SF.cu:116-177
+    __device__ static void setup(const View& V, int ix, int iy, const Fan2DParams& P, Cell& c) {
+        const float signx1 = ix - 0.5f, signx2 = ix + 0.5f, signy1 = iy - 0.5f, signy2 = iy + 0.5f;
+        float* us = c.us;
+        us[0] = (V.pm0 * signx1 + V.pm3 + V.pm1 * signy1) / (V.pm8 * signx1 + V.pm11 + V.pm9 * signy1);
+        us[1] = (V.pm0 * signx1 + V.pm3 + V.pm1 * signy2) / (V.pm8 * signx1 + V.pm11 + V.pm9 * signy2);
+        us[2] = (V.pm0 * signx2 + V.pm3 + V.pm1 * signy1) / (V.pm8 * signx2 + V.pm11 + V.pm9 * signy1);
+        us[3] = (V.pm0 * signx2 + V.pm3 + V.pm1 * signy2) / (V.pm8 * signx2 + V.pm11 + V.pm9 * signy2);
+        if (V.singular != 0.f) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) us[k] = (us[k] * 1.5f - 1.0f) / V.puvx;
+        }
+        sort2(us[0], us[1]);
+        sort2(us[2], us[3]);
+        sort2(us[0], us[2]);
+        sort2(us[1], us[3]);
+        sort2(us[1], us[2]);
+        c.lo = min(max(0, (int)floorf(us[0])), P.nu - 1);
+        c.hi = min(max(0, (int)floorf(us[3])), P.nu - 1);
+        const float theta = atan2f((V.dx * (ix - V.nx2) - V.srcx), (V.dy * (iy - V.ny2) - V.srcy));
+        const float st = fabsf(sinf(theta)), ct = fabsf(cosf(theta));
+        c.weight = V.dx / fmaxf(st, ct);
+    }
+    // layers/A_SF.cu:48-84
+    __device__ static float gamma(float s1, float s2, const float* us) {
+        float g = 0.0f, tmp, b1, b2;
+        b1 = fmaxf(s1, us[0]);
+        b2 = fminf(s2, us[1]);
+        tmp = (b2 > b1) ? (1 / (2 * (us[1] - us[0]))) * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0]))
+                        : 0.0f;
+        if (tmp == tmp) g += tmp;
+        b1 = fmaxf(s1, us[1]);
+        b2 = fminf(s2, us[2]);
+        tmp = (b2 > b1) ? b2 - b1 : 0.0f;
+        if (tmp == tmp) g += tmp;
+        b1 = fmaxf(s1, us[2]);
+        b2 = fminf(s2, us[3]);
+        tmp = (b2 > b1) ? (1 / (2 * (us[3] - us[2]))) * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3]))
+                        : 0.0f;
+        if (tmp == tmp) g += tmp;
+        return g;
+    }
+    __device__ static float value(const View&, const Cell& c, int u, int, const Fan2DParams&) {
+        const float g = gamma((float)u, u + 1.0f, c.us);
+        const float val = c.weight * g;
+        return (g > 1e-7f && val == val) ? val : 0.f;
+    }
+};
+
+namespace {
+
+class SFLayer final : public Proj2D {
+public:
+    SFLayer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+            const double* angles) {
+        geo.init(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, nullptr, nullptr);
+        P.ni = nx;
+        P.nj = ny;
+        std::vector<float> view((size_t)np * SFBasis::kViewFloats, 0.f);
+        for (int p = 0; p < np; ++p) {
+            float* v = &view[(size_t)p * SFBasis::kViewFloats];
+            const float* m = &geo.pmi[12 * (size_t)p];
+            v[0] = m[0]; v[1] = m[1]; v[2] = m[3]; v[3] = m[8]; v[4] = m[9]; v[5] = m[11];
+            const float puvx = (float)geo.frames[p].puv[0], puvy = (float)geo.frames[p].puv[1];
+            v[6] = puvx;
+            v[7] = (std::fabs(puvx - puvy) < 1e-7f) ? 1.f : 0.f;  // layers/A_SF.cu:119
+            v[8] = (float)geo.frames[p].src[0];
+            v[9] = (float)geo.frames[p].src[1];
+            v[10] = (float)dx;
+            v[11] = (float)dy;
+            v[12] = (nx - 1) / 2.0f;
+            v[13] = (ny - 1) / 2.0f;
+        }
+        const double hx = 0.5 * dx, hy = 0.5 * dy;
+        const double x0 = geo.x0(), y0 = geo.y0();
+        finish_init(view, SFBasis::kViewFloats, {}, [&](int i0, int i1, int j0, int j1) {
+            return Box2{x0 + i0 * dx - hx, x0 + i1 * dx + hx, y0 + j0 * dy - hy, y0 + j1 * dy + hy};
+        });
+        count = 0;  // the reference's SF kernels never count (layers/A_SF.cu:19)
+    }
+    void forward_dev(const float* img, float* sino, cudaStream_t s) override {
+        fan2d_forward<SFBasis>(P, img, d_sino64_, sino, 1.f, smem_fwd_, s);
+    }
+    void backward_dev(const float* sino, float* img, cudaStream_t s) override {
+        fan2d_back<SFBasis>(P, sino, img, 1.f, s);
+    }
+};
+
+}  // namespace
+
+Proj2D* make_sf_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                      const double* angles) {
+    return new SFLayer(nx, ny, np, nu, dx, dy, du, lsd, lso, angles);
+}
+
+}  // namespace sgd

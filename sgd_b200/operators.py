@@ -39,6 +39,7 @@ class _Fan2DOperator(LinearOperator):
     """Common body of the 2D fan-beam operators over one C entry-point prefix."""
 
     _prefix = ""
+    _offsets = True  # the init takes per-view dz/drho
 
     def __init__(self, nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dz=None, drho=None, dtype=np.float64):
         super().__init__(dtype=dtype, shape=(nnp * nu, nx * ny))
@@ -61,7 +62,11 @@ class _Fan2DOperator(LinearOperator):
         L = _lib.lib()
         self._L = L
         init = getattr(L, f"{self._prefix}_init")
-        self.cpointer = init(nx, ny, nnp, nu, dx, dy, du, lsd, lso, _ptr(angles), _ptr(self._dz), _ptr(self._drho))
+        if self._offsets:
+            self.cpointer = init(nx, ny, nnp, nu, dx, dy, du, lsd, lso, _ptr(angles), _ptr(self._dz),
+                                 _ptr(self._drho))
+        else:
+            self.cpointer = init(nx, ny, nnp, nu, dx, dy, du, lsd, lso, _ptr(angles))
         if not self.cpointer:
             raise _lib.ProjectorError(f"{self._prefix}_init: {_lib.last_error()}")
         self._fwd = getattr(L, f"{self._prefix}_forward_projection")
@@ -97,3 +102,13 @@ class A_B1_operator(_Fan2DOperator):
     """Bilinear box-spline fan-beam projector (python/operators/operators.py:156-219)."""
 
     _prefix = "b1"
+
+
+class A_SF_operator(_Fan2DOperator):
+    """Separable-footprint fan-beam projector (python/operators/operators.py:351-399)."""
+
+    _prefix = "SF"
+    _offsets = False
+
+    def __init__(self, nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dtype=np.float64):
+        super().__init__(nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dtype=dtype)

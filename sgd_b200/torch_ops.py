@@ -27,7 +27,7 @@ def _ptr(a):
 class FanProjector:
     """One fan-beam geometry bound to the current CUDA device.
 
-    ``kind`` selects the basis ("b1").  Arguments follow the reference's
+    ``kind`` selects the basis ("b1" bilinear, "SF" separable footprint).  Arguments follow the reference's
     ``*_init`` entry points (layers/A_B1.cu:595-603): image nx x ny with pixel
     dx x dy, np views at ``angles`` (radians), nu bins of pitch du,
     source-detector distance lsd, source-isocentre distance lso, optional
@@ -47,8 +47,12 @@ class FanProjector:
         self._L = L
         dz = None if dz is None else np.ascontiguousarray(dz, dtype=np.float64)
         drho = None if drho is None else np.ascontiguousarray(drho, dtype=np.float64)
-        self.handle = getattr(L, f"{kind}_init")(self.nx, self.ny, self.np, self.nu, dx, dy, du, lsd, lso,
-                                                  _ptr(angles), _ptr(dz), _ptr(drho))
+        init = getattr(L, f"{kind}_init")
+        if kind == "SF":
+            self.handle = init(self.nx, self.ny, self.np, self.nu, dx, dy, du, lsd, lso, _ptr(angles))
+        else:
+            self.handle = init(self.nx, self.ny, self.np, self.nu, dx, dy, du, lsd, lso, _ptr(angles), _ptr(dz),
+                               _ptr(drho))
         if not self.handle:
             raise _lib.ProjectorError(f"{kind}_init: {_lib.last_error()}")
         self._fwd = getattr(L, f"sgd_{kind}_forward_dev")

@@ -25,6 +25,9 @@ CASES = {
     "b1_tiny": ("b1", "tiny"),
     "b1_snap": ("b1", "snap"),
     "b1_wide": ("b1", "wide"),
+    "sf_tiny": ("SF", "tiny"),
+    "sf_snap": ("SF", "snap"),
+    "sf_wide": ("SF", "wide"),
 }
 
 
@@ -37,7 +40,7 @@ def main(out):
         b, cnt = R.forward(x)
         y, _ = R.forward(ellipse_phantom(nx, ny, dx, dy, seed=12).ravel())
         xt = R.backward(y)
-        np.savez_compressed(os.path.join(out, f"{name}.npz"), kind=kind, sizes=np.array([nx, ny, nu]),
+        np.savez_compressed(os.path.join(out, f"{name}.npz"), kind=kind.lower(), sizes=np.array([nx, ny, nu]),
                             params=np.array([dx, dy, du, lsd, lso]), angles=ang, x=x, b=b, count=cnt, y=y,
                             xt=xt, tol=1e-5)
         print(name, "count", cnt, "norm b", np.linalg.norm(b))

@@ -102,3 +102,25 @@ def test_oracle_matches_reference_golden(oracle_mod, fname):
     assert cnt == int(z["count"])
     xt = bwd(z["y"], nx, ny, nu, dx, dy, du, lsd, lso, ang)
     assert rel_l2(xt, z["xt"]) < float(z["tol"])
+
+
+@pytest.mark.parametrize("case", ["c2", "snap", "rect"])
+def test_product_pmi_bit_identical_to_oracle(oracle_mod, case):
+    """The library's projection matrices (host code) equal the restatement of
+    utils/geo.cu bit for bit: the separable-footprint and 3D kernels take
+    their visited bins from floors of pmi projections."""
+    import ctypes
+    from sgd_b200 import _lib
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case(case)
+    ang = np.ascontiguousarray(ang, dtype=np.float64)
+    L = _lib.lib()
+    pm = np.zeros((len(ang), 12))
+    pmi = np.zeros((len(ang), 12), dtype=np.float32)
+    dp = ctypes.POINTER(ctypes.c_double)
+    assert L.sgd_geometry_pmi(nx, ny, 1, len(ang), nu, 1, ctypes.c_double(dx), ctypes.c_double(dy),
+                              ctypes.c_double(1.0), ctypes.c_double(du), ctypes.c_double(1.0), ctypes.c_double(lsd),
+                              ctypes.c_double(lso), ang.ctypes.data_as(dp), None, None, pm.ctypes.data_as(dp),
+                              pmi.ctypes.data_as(ctypes.POINTER(ctypes.c_float))) == 0
+    g = oracle_mod.geometry(nx, ny, 1, nu, 1, dx, dy, 1, du, 1, lsd, lso, ang)
+    assert np.array_equal(pm, g["pm"])
+    assert np.array_equal(pmi, g["pmi"])
