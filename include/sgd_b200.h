@@ -106,6 +106,22 @@ int sgd_SF_forward_dev(void* layer, const float* d_img, float* d_sino, void* str
 int sgd_SF_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
 unsigned long long sgd_SF_count(void* layer);
 
+/* ---- B0 pixel indicator, 2D fan beam ----------------------------------------- */
+
+/* Replace b0_init / b0_forward_projection / b0_backward_projection,
+ * layers/A_B0.hh:24-26 / layers/A_B0.cu:494-575 (same layouts as B1; the
+ * forward returns the reference's footprint-evaluation count). */
+void* b0_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+              double* angles, double* dz, double* drho);
+int b0_forward_projection(double* b, double* x, void* layer);
+void b0_backward_projection(double* b, double* x, void* layer);
+/* New: status-returning backward, destruction, device entry points, count. */
+int sgd_b0_backward_projection(double* b, double* x, void* layer);
+void b0_destroy(void* layer);
+int sgd_b0_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream);
+int sgd_b0_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
+unsigned long long sgd_b0_count(void* layer);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* New (no reference counterpart): FP32 FMA throughput of the current GPU in

@@ -30,6 +30,8 @@ def lib():
         L.oracle_b1_backward.restype = None
         L.oracle_b1_matrix.restype = ctypes.c_longlong
         L.oracle_sf_forward.restype = None
+        L.oracle_b0_forward.restype = ctypes.c_longlong
+        L.oracle_b0_backward.restype = None
         L.oracle_sf_backward.restype = None
         L.oracle_b1_flops.restype = None
     return _LIB
@@ -130,3 +132,24 @@ def sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None,
 
 def sf_backward(b, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
     return _fan2d("oracle_sf_backward", nx, ny, nu, dx, dy, du, lsd, lso, angles, b, nx * ny, precision)
+
+
+def b0_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
+    """FP64 replica of b0_forward_projection: (b, footprint-evaluation count)."""
+    angles = _c(angles)
+    x = _c(np.ravel(x))
+    b = np.zeros(len(angles) * nu)
+    cnt = lib().oracle_b0_forward(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy),
+                                  ctypes.c_double(du), ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles),
+                                  _p(_c(dzs)), _p(_c(drho)), _p(x), _p(b), precision)
+    return b, int(cnt)
+
+
+def b0_backward(b, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
+    angles = _c(angles)
+    b = _c(np.ravel(b))
+    x = np.zeros(nx * ny)
+    lib().oracle_b0_backward(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(du),
+                             ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), _p(_c(dzs)), _p(_c(drho)),
+                             _p(b), _p(x), precision)
+    return x

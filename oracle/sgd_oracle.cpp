@@ -271,8 +271,16 @@ inline void bin_range(const float* pm, float puvx, bool singular, float sx1, flo
     T xs[4] = {sx1, sx1, sx2, sx2};
     T ys[4] = {sy1, sy2, sy1, sy2};
     for (int k = 0; k < 4; ++k) {
-        T num = T(pm[0]) * xs[k] + T(pm[3]) + T(pm[1]) * ys[k];
-        T den = T(pm[8]) * xs[k] + T(pm[11]) + T(pm[9]) * ys[k];
+        T num, den;
+        if constexpr (std::is_same<T, float>::value) {
+            // the reference's FP32 expression as its compiler contracts it
+            // into fused multiply-adds: (pm0 x + pm3) + pm1 y
+            num = (T)std::fmaf(pm[1], (float)ys[k], std::fmaf(pm[0], (float)xs[k], pm[3]));
+            den = (T)std::fmaf(pm[9], (float)ys[k], std::fmaf(pm[8], (float)xs[k], pm[11]));
+        } else {
+            num = T(pm[0]) * xs[k] + T(pm[3]) + T(pm[1]) * ys[k];
+            den = T(pm[8]) * xs[k] + T(pm[11]) + T(pm[9]) * ys[k];
+        }
         us[k] = num / den;
         if (singular) us[k] = (us[k] * T(1.5f) - T(1.0f)) / T(puvx);
     }
@@ -429,6 +437,100 @@ void sf_pixel_view(const Geo& g, int p, int ix, int iy, Visit visit) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// B0 pixel-indicator fan-beam projector: layers/A_B0.cu
+// ---------------------------------------------------------------------------
+
+// layers/spline_conv.hh:52-58 (descending sort)
+template <class T> inline void sort2d(T& a, T& b) { if (a < b) std::swap(a, b); }
+
+// layers/spline_conv.hh:239-293: value of the 3-direction box spline at x for
+// |directions| sorted in descending order
+template <class T> T univariate3dir_fast3(T x, const T* xi) {
+    T h = T(1) / xi[0];
+    T p = xi[0] * xi[1] * xi[2];
+    T K0 = (xi[0] - xi[1] - xi[2]) / T(2), K1 = (xi[0] - xi[1] + xi[2]) / T(2);
+    T K2 = (xi[0] + xi[1] - xi[2]) / T(2), K3 = (xi[0] + xi[1] + xi[2]) / T(2);
+    if (x >= K3) return T(0);
+    if (x >= K2) return T(0.5f) * (K3 - x) * (K3 - x) / p;
+    if (x >= K1) return ((xi[0] + xi[1]) / T(2) - x) * xi[2] / p;
+    if (x < -K0) return h - (K0 * K0 + x * x) / p;
+    if (x < K0) return h;
+    return h - T(0.5f) * (K0 - x) * (K0 - x) / p;
+}
+template <class T> T univariate3dir_fast2(T x, const T* xi) {
+    return max(T(0), min(T(1) / xi[0], ((xi[0] + xi[1]) / T(2) - x) / (xi[0] * xi[1])));
+}
+
+// layers/A_B0.cu:20-35
+template <class T> T b0_linear_convolution_1d(T y, T v1, T v2, T v3) {
+    T vs[3];
+    y = fabs(y - (v1 + v2 + v3) / T(2));
+    vs[0] = fabs(v1), vs[1] = fabs(v2), vs[2] = fabs(v3);
+    sort2d(vs[1], vs[2]); sort2d(vs[0], vs[1]); sort2d(vs[1], vs[2]);
+    if (vs[2] > T(1e-7f)) return univariate3dir_fast3<T>(y, vs);
+    return univariate3dir_fast2<T>(y, vs);
+}
+
+// per-(view, bin) vx, vy, a0s, sb0, lsp in FP64: layers/A_B0.cu:338-388
+void b0_vectors(const Geo& g, std::vector<double>& vecs) {
+    int np = g.np, nu = g.nu;
+    vecs.assign((size_t)5 * np * nu, 0.0);
+    for (int p = 0; p < np; ++p) {
+        double cx = g.dtv[3 * p], cy = g.dtv[3 * p + 1], ux = g.puv[3 * p], uy = g.puv[3 * p + 1];
+        double px = g.src[3 * p], py = g.src[3 * p + 1];
+        for (int u = 0; u < nu; ++u) {
+            double sx = cx + ux * (u - 0.5 * nu + 0.5), sy = cy + uy * (u - 0.5 * nu + 0.5);
+            double ax = sx - ux * 0.5, ay = sy - uy * 0.5, bx = sx + ux * 0.5, by = sy + uy * 0.5;
+            double lsp = std::sqrt((px - sx) * (px - sx) + (py - sy) * (py - sy));
+            double theta = std::atan2(std::fabs(px - sx), std::fabs(py - sy));
+            double vx = std::fabs(g.dx * std::cos(theta)), vy = std::fabs(g.dy * std::sin(theta));
+            if (py < sy) vx = -vx;
+            if (px < sx) vy = -vy;
+            double a0s = std::fabs((sx - px) * (ay - py) - (ax - px) * (sy - py)) / lsp;
+            double sb0 = std::fabs((sx - px) * (by - py) - (bx - px) * (sy - py)) / lsp;
+            a0s /= ((ax - px) * (sx - px) + (ay - py) * (sy - py)) / (lsp * lsp);
+            sb0 /= ((bx - px) * (sx - px) + (by - py) * (sy - py)) / (lsp * lsp);
+            double* v = &vecs[(size_t)p * nu * 5];
+            v[u] = vx; v[nu + u] = vy; v[2 * nu + u] = a0s; v[3 * nu + u] = sb0; v[4 * nu + u] = lsp;
+        }
+    }
+}
+
+// Per-(pixel, view) body of b0_forward_projection (layers/A_B0.cu:123-229)
+// and b0_backward_projection (:231-336).  visit(u, conv*dx*dy) for kept bins;
+// returns the evaluation count (the reference's conv_count).
+template <class T, class Visit>
+long long b0_pixel_view(const Geo& g, const double* vp, int p, int ix, int iy, Visit visit) {
+    int nx = g.nx, ny = g.ny, nu = g.nu;
+    float dx = (float)g.dx, dy = (float)g.dy;
+    float nx2 = 0.5f * (nx - 1), ny2 = 0.5f * (ny - 1);
+    const float* pm = &g.pmi[12 * p];
+    float srcx = (float)g.src[3 * p], srcy = (float)g.src[3 * p + 1];
+    float puvx = (float)g.puv[3 * p], puvy = (float)g.puv[3 * p + 1];
+    float dtvx = (float)g.dtv[3 * p], dtvy = (float)g.dtv[3 * p + 1];
+    bool singular = std::fabs(puvx - puvy) < 1e-7f;
+    float fox = (ix - nx2) * dx, foy = (iy - ny2) * dy;          // :152-153
+    int minu, maxu;
+    bin_range<float>(pm, puvx, singular, ix - 0.5f, ix + 0.5f, iy - 0.5f, iy + 0.5f, nu, minu, maxu);  // :158-195
+    T ox = fox, oy = foy, px = srcx, py = srcy;
+    T cx = ox - T(0.5f * dx), cy = oy + T(0.5f * dy);         // pixel corner, :213
+    long long cnt = 0;
+    for (int u = minu; u <= maxu; ++u) {
+        T off = T(u) - T(0.5f) * nu + T(0.5f);
+        T sx = T(dtvx) + T(puvx) * off, sy = T(dtvy) + T(puvy) * off;  // :197-198, :202
+        T vx = vp[u], vy = vp[nu + u], a0s = vp[2 * nu + u], sb0 = vp[3 * nu + u], lsp = vp[4 * nu + u];
+        T r1 = ((ox - px) * (sx - px) + (oy - py) * (sy - py)) / (lsp * lsp);  // :211
+        T vblur = (a0s + sb0) * (-r1);
+        T y = ((sx - px) * (cy - py) - (cx - px) * (sy - py)) / lsp;       // :213
+        y = y + a0s * r1;
+        T conv = b0_linear_convolution_1d<T>(-y, vx, vy, vblur);             // :219
+        ++cnt;
+        if (conv == conv && conv > T(1e-7f)) visit(u, (double)conv * (double)dx * (double)dy);  // :223-225
+    }
+    return cnt;
+}
+
 Geo make_geo(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
              double dv) {
     Geo g;
@@ -478,6 +580,56 @@ void oracle_b1_backward(int nx, int ny, int np, int nu, double dx, double dy, do
     std::vector<float> vecs;
     b1_vectors(g, vecs);
     if (precision) b1_backward<float>(g, vecs, b, x); else b1_backward<double>(g, vecs, b, x);
+}
+
+// b0_forward_projection / b0_backward_projection (layers/A_B0.cu:504-575),
+// same host layouts as B1.  FP64 replica (precision 0) or FP32 (1).
+long long oracle_b0_forward(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                            const double* angles, const double* dzs, const double* drho, const double* x, double* b,
+                            int precision) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, dzs, drho);
+    std::vector<double> vecs;
+    b0_vectors(g, vecs);
+    std::memset(b, 0, sizeof(double) * (size_t)np * nu);
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : total)
+    for (int p = 0; p < np; ++p) {
+        double* bp = b + (size_t)p * nu;
+        const double* vp = &vecs[(size_t)p * nu * 5];
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix) {
+                double C = x[(size_t)ix * ny + iy];
+                auto visit = [&](int u, double v) { bp[u] += v * C; };
+                total += precision ? b0_pixel_view<float>(g, vp, p, ix, iy, visit)
+                                   : b0_pixel_view<double>(g, vp, p, ix, iy, visit);
+            }
+    }
+    return total;
+}
+
+void oracle_b0_backward(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                        const double* angles, const double* dzs, const double* drho, const double* b, double* x,
+                        int precision) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, dzs, drho);
+    std::vector<double> vecs;
+    b0_vectors(g, vecs);
+#pragma omp parallel for schedule(dynamic)
+    for (int ix = 0; ix < nx; ++ix)
+        for (int iy = 0; iy < ny; ++iy) {
+            double acc = 0.0;
+            for (int p = 0; p < np; ++p) {
+                const double* bp = b + (size_t)p * nu;
+                const double* vp = &vecs[(size_t)p * nu * 5];
+                double val = 0.0;
+                auto visit = [&](int u, double v) { val += v * bp[u]; };
+                if (precision) b0_pixel_view<float>(g, vp, p, ix, iy, visit);
+                else b0_pixel_view<double>(g, vp, p, ix, iy, visit);
+                acc += val;
+            }
+            x[(size_t)ix * ny + iy] = acc;
+        }
 }
 
 // SF_forward_projection / SF_backward_projection (layers/A_SF.cu:406-479),

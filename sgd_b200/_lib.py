@@ -33,7 +33,7 @@ def lib() -> ctypes.CDLL:
     L = ctypes.CDLL(LIB_PATH)
     L.sgd_last_error.restype = ctypes.c_char_p
     L.sgd_last_error.argtypes = []
-    for pre in ("b1", "SF"):
+    for pre in ("b1", "SF", "b0"):
         _declare_fan2d(L, pre)
     L.sgd_geometry_pmi.restype = _i
     L.sgd_b1_forward_noalloc.restype = _i

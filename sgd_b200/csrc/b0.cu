@@ -1,0 +1,189 @@
+// B0: pixel-indicator fan-beam projector on the generic 2D kernels.
+// Reference: layers/A_B0.cu:20-35 (footprint), :123-229 (forward), :231-336
+// (backward), :338-388 (per-bin vectors), :494-575 (C entry points).
+//
+// Per pixel and view the bin range comes from the pixel's four corners through
+// pmi (bit-identical to the reference's); per bin, the footprint is the
+// 3-direction box spline of layers/spline_conv.hh:239-293 with directions
+// (vx, vy, vblur) at an offset y measured from the pixel corner, vblur being
+// the bin's width at the pixel's depth.  The reference's mix of FP32 geometry
+// (including its FP32 stepping of the bin centre, sx += puv.x, :202) and FP64
+// per-bin vectors is kept; the two FP64 divisions by the source-bin distance
+// are multiplications by its FP64 reciprocals.
+#include <cmath>
+
+#include "common.h"
+#include "proj2d_impl.cuh"
+
+namespace sgd {
+
+struct B0Basis {
+    static constexpr int kViewFloats = 20;
+    // [0..5] pmi 0,1,3,8,9,11 [6] puv.x [7] singular [8] src.x [9] src.y [10] dtv.x
+    // [11] dtv.y [12] puv.y [13] dx [14] dy [15] (nx-1)/2 [16] (ny-1)/2
+    struct View {
+        float pm0, pm1, pm3, pm8, pm9, pm11, puvx, singular, srcx, srcy, dtvx, dtvy, puvy, dx, dy, nx2, ny2;
+    };
+    struct Cell {
+        float ox, oy, sx0, sy0;
+        int lo, hi;
+    };
+    __device__ static void load_view(const float* v, View& V) {
+        const float4* q = reinterpret_cast<const float4*>(v);
+        const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
+        V = View{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w, e.x};
+    }
+    __device__ static bool valid(int, int, const Fan2DParams&) { return true; }
+    __device__ static void sort2(float& a, float& b) {
+        if (a > b) {
+            const float t = b;
+            b = a;
+            a = t;
+        }
+    }
+    __device__ static void sort2d(float& a, float& b) {
+        if (a < b) {
+            const float t = b;
+            b = a;
+            a = t;
+        }
+    }
+    // layers/A_B0.cu:152-198
+    __device__ static void setup(const View& V, int ix, int iy, const Fan2DParams& P, Cell& c) {
+        c.ox = (ix - V.nx2) * V.dx;
+        c.oy = (iy - V.ny2) * V.dy;
+        const float signx1 = ix - 0.5f, signx2 = ix + 0.5f, signy1 = iy - 0.5f, signy2 = iy + 0.5f;
+        const float u1 = V.pm0 * signx1 + V.pm3, u2 = V.pm8 * signx1 + V.pm11;
+        const float u3 = V.pm0 * signx2 + V.pm3, u4 = V.pm8 * signx2 + V.pm11;
+        float us[4];
+        us[0] = (u1 + V.pm1 * signy1) / (u2 + V.pm9 * signy1);
+        us[1] = (u1 + V.pm1 * signy2) / (u2 + V.pm9 * signy2);
+        us[2] = (u3 + V.pm1 * signy1) / (u4 + V.pm9 * signy1);
+        us[3] = (u3 + V.pm1 * signy2) / (u4 + V.pm9 * signy2);
+        if (V.singular != 0.f) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) us[k] = (us[k] * 1.5f - 1.0f) / V.puvx;
+        }
+        sort2(us[0], us[1]);
+        sort2(us[2], us[3]);
+        sort2(us[0], us[2]);
+        sort2(us[1], us[3]);
+        sort2(us[1], us[2]);
+        c.lo = min(max(0, (int)floorf(us[0])), P.nu - 1);
+        c.hi = min(max(0, (int)floorf(us[3])), P.nu - 1);
+        const float fl = (float)c.lo;
+        c.sx0 = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
+        c.sy0 = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
+    }
+    // layers/spline_conv.hh:244-293 (T = float)
+    __device__ static float fast3(float x, const float* xi) {
+        const float h = 1.0f / xi[0];
+        const float p = xi[0] * xi[1] * xi[2];
+        const float K0 = (xi[0] - xi[1] - xi[2]) / 2.0f, K1 = (xi[0] - xi[1] + xi[2]) / 2.0f;
+        const float K2 = (xi[0] + xi[1] - xi[2]) / 2.0f, K3 = (xi[0] + xi[1] + xi[2]) / 2.0f;
+        float v;
+        if (x >= K3) v = 0.0f;
+        else if (x >= K2) v = 0.5f * (K3 - x) * (K3 - x) / p;
+        else if (x >= K1) v = ((xi[0] + xi[1]) / 2.0f - x) * xi[2] / p;
+        else if (x < -K0) v = h - (K0 * K0 + x * x) / p;
+        else if (x < K0) v = h;
+        else v = h - 0.5f * (K0 - x) * (K0 - x) / p;
+        return v;
+    }
+    // layers/A_B0.cu:20-35
+    __device__ static float conv1d(float y, float v1, float v2, float v3) {
+        float vs[3];
+        y = fabsf(y - (v1 + v2 + v3) / 2.0f);
+        vs[0] = fabsf(v1), vs[1] = fabsf(v2), vs[2] = fabsf(v3);
+        sort2d(vs[1], vs[2]);
+        sort2d(vs[0], vs[1]);
+        sort2d(vs[1], vs[2]);
+        if (vs[2] > 1e-7f) return fast3(y, vs);
+        return fmaxf(0.0f, fminf(1.0f / vs[0], ((vs[0] + vs[1]) / 2.0f - y) / (vs[0] * vs[1])));
+    }
+    // bins: [view][bin][vx, vy, a0s, sb0, 1/lsp, 1/lsp^2] doubles
+    __device__ static float value(const View& V, const Cell& c, int u, int p, const Fan2DParams& P) {
+        float sx = c.sx0, sy = c.sy0;
+        for (int t = c.lo; t < u; ++t) {  // the reference's FP32 stepping
+            sx += V.puvx;
+            sy += V.puvy;
+        }
+        const double* b = reinterpret_cast<const double*>(P.bins) + ((size_t)p * P.nu + u) * 6;
+        const double vx = __ldg(b), vy = __ldg(b + 1), a0s = __ldg(b + 2), sb0 = __ldg(b + 3);
+        const double ilsp = __ldg(b + 4), ilsp2 = __ldg(b + 5);
+        const float px = V.srcx, py = V.srcy;
+        const double r1 = (double)((c.ox - px) * (sx - px) + (c.oy - py) * (sy - py)) * ilsp2;
+        const double vblur = (a0s + sb0) * (-r1);
+        const float x1 = sx - px, y1 = sy - py, x2 = c.ox - 0.5f * V.dx - px, y2 = c.oy + 0.5f * V.dy - py;
+        double y = (double)(x1 * y2 - x2 * y1) * ilsp;
+        y += a0s * r1;
+        const float conv = conv1d((float)(-y), (float)vx, (float)vy, (float)vblur);
+        return (conv > 1e-7f && conv == conv) ? conv : 0.f;
+    }
+};
+
+namespace {
+
+class B0Layer final : public Proj2D {
+public:
+    B0Layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+            const double* angles, const double* dz, const double* drho) {
+        geo.init(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, dz, drho);
+        P.ni = nx;
+        P.nj = ny;
+        std::vector<float> view((size_t)np * B0Basis::kViewFloats, 0.f);
+        std::vector<float4> bins((size_t)np * nu * 3);
+        double* bd = reinterpret_cast<double*>(bins.data());
+        for (int p = 0; p < np; ++p) {
+            const ViewFrame& f = geo.frames[p];
+            float* v = &view[(size_t)p * B0Basis::kViewFloats];
+            const float* m = &geo.pmi[12 * (size_t)p];
+            v[0] = m[0]; v[1] = m[1]; v[2] = m[3]; v[3] = m[8]; v[4] = m[9]; v[5] = m[11];
+            v[6] = (float)f.puv[0];
+            v[7] = (std::fabs((float)f.puv[0] - (float)f.puv[1]) < 1e-7f) ? 1.f : 0.f;  // layers/A_B0.cu:161
+            v[8] = (float)f.src[0]; v[9] = (float)f.src[1];
+            v[10] = (float)f.dtv[0]; v[11] = (float)f.dtv[1];
+            v[12] = (float)f.puv[1];
+            v[13] = (float)dx; v[14] = (float)dy;
+            v[15] = 0.5f * (nx - 1); v[16] = 0.5f * (ny - 1);
+            // layers/A_B0.cu:338-388, FP64
+            const double cx = f.dtv[0], cy = f.dtv[1], ux = f.puv[0], uy = f.puv[1], px = f.src[0], py = f.src[1];
+            for (int u = 0; u < nu; ++u) {
+                const double sx = cx + ux * (u - 0.5 * nu + 0.5), sy = cy + uy * (u - 0.5 * nu + 0.5);
+                const double ax = sx - ux * 0.5, ay = sy - uy * 0.5, bx = sx + ux * 0.5, by = sy + uy * 0.5;
+                const double lsp = std::sqrt((px - sx) * (px - sx) + (py - sy) * (py - sy));
+                const double th = std::atan2(std::fabs(px - sx), std::fabs(py - sy));
+                double vx = std::fabs(dx * std::cos(th)), vy = std::fabs(dy * std::sin(th));
+                if (py < sy) vx = -vx;
+                if (px < sx) vy = -vy;
+                double a0s = std::fabs((sx - px) * (ay - py) - (ax - px) * (sy - py)) / lsp;
+                double sb0 = std::fabs((sx - px) * (by - py) - (bx - px) * (sy - py)) / lsp;
+                a0s /= ((ax - px) * (sx - px) + (ay - py) * (sy - py)) / (lsp * lsp);
+                sb0 /= ((bx - px) * (sx - px) + (by - py) * (sy - py)) / (lsp * lsp);
+                double* o = bd + ((size_t)p * nu + u) * 6;
+                o[0] = vx; o[1] = vy; o[2] = a0s; o[3] = sb0; o[4] = 1.0 / lsp; o[5] = 1.0 / (lsp * lsp);
+            }
+        }
+        const double hx = 0.5 * dx, hy = 0.5 * dy, x0 = geo.x0(), y0 = geo.y0();
+        finish_init(view, B0Basis::kViewFloats, bins, [&](int i0, int i1, int j0, int j1) {
+            return Box2{x0 + i0 * dx - hx, x0 + i1 * dx + hx, y0 + j0 * dy - hy, y0 + j1 * dy + hy};
+        });
+        out_scale = (float)dx * (float)dy;
+        count = fan2d_count<B0Basis>(P, stream);
+    }
+    void forward_dev(const float* img, float* sino, cudaStream_t s) override {
+        fan2d_forward<B0Basis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
+    }
+    void backward_dev(const float* sino, float* img, cudaStream_t s) override {
+        fan2d_back<B0Basis>(P, sino, img, out_scale, s);
+    }
+};
+
+}  // namespace
+
+Proj2D* make_b0_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                      const double* angles, const double* dz, const double* drho) {
+    return new B0Layer(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, dz, drho);
+}
+
+}  // namespace sgd

@@ -8,6 +8,8 @@
 namespace sgd {
 Proj2D* make_sf_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
                       const double* angles);
+Proj2D* make_b0_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                      const double* angles, const double* dz, const double* drho);
 }
 
 using sgd::Proj2D;
@@ -62,5 +64,25 @@ int sgd_SF_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
     return bwd_dev(layer, d_sino, d_img, stream, "sgd_SF_backward_dev");
 }
 unsigned long long sgd_SF_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
+
+void* b0_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+              double* angles, double* dz, double* drho) {
+    return sgd::guarded<void*>(nullptr, [&]() -> void* {
+        return sgd::make_b0_layer(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, dz, drho);
+    });
+}
+int b0_forward_projection(double* b, double* x, void* layer) { return fwd_host(b, x, layer, "b0_forward_projection"); }
+void b0_backward_projection(double* b, double* x, void* layer) { bwd_host(b, x, layer, "b0_backward_projection"); }
+int sgd_b0_backward_projection(double* b, double* x, void* layer) {
+    return bwd_host(b, x, layer, "b0_backward_projection");
+}
+void b0_destroy(void* layer) { delete static_cast<Proj2D*>(layer); }
+int sgd_b0_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream) {
+    return fwd_dev(layer, d_img, d_sino, stream, "sgd_b0_forward_dev");
+}
+int sgd_b0_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream) {
+    return bwd_dev(layer, d_sino, d_img, stream, "sgd_b0_backward_dev");
+}
+unsigned long long sgd_b0_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
 
 }  // extern "C"

@@ -93,6 +93,27 @@ __global__ void __launch_bounds__(kF2Threads) fan2d_forward_kernel(Fan2DParams P
     }
 }
 
+// The reference's footprint-evaluation count: sum over cells and views of the
+// width of the (clamped) bin range.  One atomic per warp.
+template <class B>
+__global__ void fan2d_count_kernel(Fan2DParams P, unsigned long long* out) {
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long n = 0;
+    if (idx < (long long)P.ni * P.nj) {
+        const int i = (int)(idx / P.nj), j = (int)(idx - (long long)i * P.nj);
+        if (B::valid(i, j, P))
+            for (int p = 0; p < P.np; ++p) {
+                typename B::View V;
+                B::load_view(P.view + (size_t)p * B::kViewFloats, V);
+                typename B::Cell c;
+                B::setup(V, i, j, P, c);
+                if (c.hi >= c.lo) n += (unsigned long long)(c.hi - c.lo + 1);
+            }
+    }
+    for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
+    if ((threadIdx.x & 31) == 0 && n) atomicAdd(out, n);
+}
+
 __global__ void fan2d_finish_kernel(const double* __restrict__ s64, float* __restrict__ s32, long long n, float scale);
 
 }  // namespace sgd

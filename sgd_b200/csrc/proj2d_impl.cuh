@@ -71,6 +71,21 @@ void fan2d_forward(const Fan2DParams& P, const float* img, double* s64, float* s
 __global__ void scale_kernel(float* a, long long n, float scale);
 
 template <class B>
+unsigned long long fan2d_count(const Fan2DParams& P, cudaStream_t s) {
+    unsigned long long* d = nullptr;
+    SGD_CUDA(cudaMallocAsync(&d, sizeof(unsigned long long), s));
+    SGD_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), s));
+    const long long n = (long long)P.ni * P.nj;
+    fan2d_count_kernel<B><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, d);
+    SGD_LAUNCH_CHECK();
+    unsigned long long h = 0;
+    SGD_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, s));
+    SGD_CUDA(cudaFreeAsync(d, s));
+    SGD_CUDA(cudaStreamSynchronize(s));
+    return h;
+}
+
+template <class B>
 void fan2d_back(const Fan2DParams& P, const float* sino, float* img, float scale, cudaStream_t s) {
     const long long n = (long long)P.ni * P.nj;
     fan2d_back_kernel<B><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, sino, img);

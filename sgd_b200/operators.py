@@ -112,3 +112,9 @@ class A_SF_operator(_Fan2DOperator):
 
     def __init__(self, nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dtype=np.float64):
         super().__init__(nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dtype=dtype)
+
+
+class A_B0_operator(_Fan2DOperator):
+    """Pixel-indicator fan-beam projector (python/operators/operators.py:91-154)."""
+
+    _prefix = "b0"

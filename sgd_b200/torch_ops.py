@@ -27,7 +27,8 @@ def _ptr(a):
 class FanProjector:
     """One fan-beam geometry bound to the current CUDA device.
 
-    ``kind`` selects the basis ("b1" bilinear, "SF" separable footprint).  Arguments follow the reference's
+    ``kind`` selects the basis ("b1" bilinear, "SF" separable footprint,
+    "b0" pixel indicator).  Arguments follow the reference's
     ``*_init`` entry points (layers/A_B1.cu:595-603): image nx x ny with pixel
     dx x dy, np views at ``angles`` (radians), nu bins of pitch du,
     source-detector distance lsd, source-isocentre distance lso, optional

@@ -28,6 +28,9 @@ CASES = {
     "sf_tiny": ("SF", "tiny"),
     "sf_snap": ("SF", "snap"),
     "sf_wide": ("SF", "wide"),
+    "b0_tiny": ("b0", "tiny"),
+    "b0_snap": ("b0", "snap"),
+    "b0_wide": ("b0", "wide"),
 }
 
 

@@ -11,10 +11,16 @@ pytestmark = pytest.mark.gpu
 
 TOL_PHANTOM = 1e-5
 TOL_ADJOINT = 1e-6
+# Against the FP64 replica.  B0 reproduces the reference's FP32 arithmetic,
+# including its FP32 stepping of the bin centre (layers/A_B0.cu:202), so it
+# sits from the FP64 replica where the reference itself sits (up to ~2e-5 on
+# these cases); its parity bar is the reference library, at TOL_PHANTOM.
+TOL_ORACLE = {"SF": 1e-5, "b0": 5e-5}
 
 KINDS = {
     # kind: (operator class name, oracle prefix, reference-library prefix)
     "SF": ("A_SF_operator", "sf", "SF"),
+    "b0": ("A_B0_operator", "b0", "b0"),
 }
 
 
@@ -40,8 +46,8 @@ def test_matches_fp64_oracle(oracle_mod, kind, case):
     bwd = getattr(oracle_mod, KINDS[kind][1] + "_backward")
     x = ellipse_phantom(nx, ny, dx, dy, seed=0).ravel()
     b_ref, _ = fwd(x, *g)
-    assert rel_l2(A.matvec(x), b_ref) < TOL_PHANTOM
-    assert rel_l2(A.rmatvec(b_ref), bwd(b_ref, *g)) < TOL_PHANTOM
+    assert rel_l2(A.matvec(x), b_ref) < TOL_ORACLE[kind]
+    assert rel_l2(A.rmatvec(b_ref), bwd(b_ref, *g)) < TOL_ORACLE[kind]
 
 
 @pytest.mark.parametrize("kind", list(KINDS))
