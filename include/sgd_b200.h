@@ -122,6 +122,40 @@ int sgd_b0_forward_dev(void* layer, const float* d_img, float* d_sino, void* str
 int sgd_b0_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
 unsigned long long sgd_b0_count(void* layer);
 
+/* ---- H0 / Hl hexagonal lattices, 2D fan beam --------------------------------- */
+
+/* Replace h0_init / hl_init (layers/A_H0.cu:555-563, layers/A_Hl.cu:569-577):
+ * nl rows of nc sites (odd rows nc-1 sites, shifted half a site), site
+ * spacing dt; host layout x[ic*nl + il], sinogram b[p*nu + u].  h0_init
+ * reproduces the reference including its bin bounds at the 0.5 dt row pitch
+ * and its extra skip test in the back projection; hl_init the Hl basis. */
+void* h0_init(int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso, double* angles,
+              double* dz, double* drho);
+void* hl_init(int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso, double* angles,
+              double* dz, double* drho);
+/* Replace h0_/hl_forward_projection and _backward_projection
+ * (layers/A_H0.cu:565-642, layers/A_Hl.cu:579-656).  The H0 forward returns
+ * the reference's count (three per visited bin), Hl 0 as the reference. */
+int h0_forward_projection(double* b, double* x, void* layer);
+void h0_backward_projection(double* b, double* x, void* layer);
+int hl_forward_projection(double* b, double* x, void* layer);
+void hl_backward_projection(double* b, double* x, void* layer);
+/* New: any hexagonal mode.  mode 0 = H0 with the true hexagon bounds and no
+ * skip test (an exact adjoint pair), 1 = H0 as the reference (h0_init),
+ * 2 = Hl (hl_init).  Use the h0_* entry points below on a mode-0 layer. */
+void* sgd_hex_init(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                   double* angles, double* dz, double* drho);
+int sgd_h0_backward_projection(double* b, double* x, void* layer);
+int sgd_hl_backward_projection(double* b, double* x, void* layer);
+void h0_destroy(void* layer);
+void hl_destroy(void* layer);
+int sgd_h0_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream);
+int sgd_h0_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
+int sgd_hl_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream);
+int sgd_hl_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
+unsigned long long sgd_h0_count(void* layer);
+unsigned long long sgd_hl_count(void* layer);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* New (no reference counterpart): FP32 FMA throughput of the current GPU in

@@ -32,6 +32,8 @@ def lib():
         L.oracle_sf_forward.restype = None
         L.oracle_b0_forward.restype = ctypes.c_longlong
         L.oracle_b0_backward.restype = None
+        L.oracle_hex_forward.restype = ctypes.c_longlong
+        L.oracle_hex_backward.restype = None
         L.oracle_sf_backward.restype = None
         L.oracle_b1_flops.restype = None
     return _LIB
@@ -152,4 +154,27 @@ def b0_backward(b, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None
     lib().oracle_b0_backward(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(du),
                              ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), _p(_c(dzs)), _p(_c(drho)),
                              _p(b), _p(x), precision)
+    return x
+
+
+HEX_MODES = {"h0c": 0, "h0": 1, "hl": 2}
+
+
+def hex_forward(mode, x, nl, nc, nu, dt, du, lsd, lso, angles, precision=0):
+    """FP64 replica of h0_/hl_forward_projection: (b, count).  mode: 'h0' (as
+    the reference), 'h0c' (true hexagon bounds), 'hl'."""
+    angles = _c(angles)
+    x = _c(np.ravel(x))
+    b = np.zeros(len(angles) * nu)
+    cnt = lib().oracle_hex_forward(HEX_MODES[mode], nl, nc, len(angles), nu, ctypes.c_double(dt), ctypes.c_double(du),
+                                   ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), _p(x), _p(b), precision)
+    return b, int(cnt)
+
+
+def hex_backward(mode, b, nl, nc, nu, dt, du, lsd, lso, angles, precision=0):
+    angles = _c(angles)
+    b = _c(np.ravel(b))
+    x = np.zeros(nl * nc)
+    lib().oracle_hex_backward(HEX_MODES[mode], nl, nc, len(angles), nu, ctypes.c_double(dt), ctypes.c_double(du),
+                              ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), _p(b), _p(x), precision)
     return x

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <atomic>
 #include <type_traits>
+#include <functional>
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -531,6 +532,115 @@ long long b0_pixel_view(const Geo& g, const double* vp, int p, int ix, int iy, V
     return cnt;
 }
 
+// ---------------------------------------------------------------------------
+// Hexagonal lattices: H0 (layers/A_H0.cu) and Hl (layers/A_Hl.cu)
+// ---------------------------------------------------------------------------
+const double kSQRT3 = 1.7320508075688772935274463415;
+
+// layers/A_Hl.cu:21-46 with layers/spline_conv.hh:151-229
+double hl_linear_convolution_1d(double y, double h1, double h2, double h3, double h4) {
+    double hs[4];
+    int m = 0;
+    if (std::fabs(h1) > 1e-8) hs[m++] = h1;
+    if (std::fabs(h2) > 1e-8) hs[m++] = h2;
+    if (std::fabs(h3) > 1e-8) hs[m++] = h3;
+    if (std::fabs(h4) > 1e-8) hs[m++] = h4;
+    if (m < 2) return 0.0;
+    // recursive divided difference: D(y, k) over hs[0..k]
+    std::function<double(double, int)> D = [&](double yy, int k) -> double {
+        if (k < 0) return yy > 0 ? (m == 2 ? yy : (m == 3 ? yy * yy : yy * yy * yy)) : 0.0;
+        return (D(yy, k - 1) - D(yy - hs[k], k - 1)) / hs[k];
+    };
+    double v = D(y, m - 1);
+    return m == 2 ? v : (m == 3 ? v / 2.0 : v / 6.0);
+}
+
+// mode 0: H0 with the true hexagon bounds, 1: H0 as the reference (pmi bounds
+// at the 0.5 dt row pitch, skip test in the back projection), 2: Hl.
+// visit(u, conv*dx*dy) for kept bins; returns the evaluation count.
+template <class T, class Visit>
+long long hex_site_view(const Geo& g, int mode, bool back, int p, int ic, int il, Visit visit) {
+    int nc = g.nx, nl = g.ny, nu = g.nu;
+    float dt = (float)g.dy * 2.0f;                         // A_H0.cu:171
+    float dx = dt * (float)kSQRT3;
+    float dy = dt * (mode == 2 ? 0.5f : 1.5f);
+    float nl2 = 0.5f * (nl - 1), nc2 = 0.5f * (nc - 1), nc3 = 0.5f * (nc - 2);
+    float foy = (il - nl2) * dy;
+    float fox = ((il & 1) ? (ic - nc3) : (ic - nc2)) * dx;
+    const float* pm = &g.pmi[12 * p];
+    float srcx = (float)g.src[3 * p], srcy = (float)g.src[3 * p + 1];
+    float puvx = (float)g.puv[3 * p], puvy = (float)g.puv[3 * p + 1];
+    float dtvx = (float)g.dtv[3 * p], dtvy = (float)g.dtv[3 * p + 1];
+    int minu, maxu;
+    if (mode == 0) {
+        // true hexagon, FP64 through the exact detector mapping
+        double px = g.src[3 * p], py = g.src[3 * p + 1], Dx = g.dtv[3 * p], Dy = g.dtv[3 * p + 1];
+        double ex = g.puv[3 * p], ey = g.puv[3 * p + 1];
+        double hx = 0.8660254037844386 * dt, hy = 0.5 * dt;
+        double xs[6] = {fox, fox + hx, fox + hx, (double)fox, fox - hx, fox - hx};
+        double ys[6] = {foy - (double)dt, foy - hy, foy + hy, foy + (double)dt, foy + hy, foy - hy};
+        double umin = 1e300, umax = -1e300;
+        for (int k = 0; k < 6; ++k) {
+            double wx = xs[k] - px, wy = ys[k] - py;
+            double u = ((px - Dx) * wy - (py - Dy) * wx) / (ex * wy - ey * wx) + 0.5 * nu;
+            umin = std::min(umin, u); umax = std::max(umax, u);
+        }
+        minu = std::min(std::max(0, (int)std::floor(umin)), nu - 1);
+        maxu = std::min(std::max(0, (int)std::floor(umax)), nu - 1);
+    } else {
+        // layers/A_H0.cu:84-156 (first stage)
+        float icc = (float)ic + ((il & 1) ? 0.5f : 0.0f), ilc = (float)il;
+        const float offc[6] = {0.0f, +0.5f, +0.5f, 0.0f, -0.5f, -0.5f};
+        const float offl[6] = {-2.0f, -1.0f, +1.0f, +2.0f, +1.0f, -1.0f};
+        float umin = 1e30f, umax = -1e30f;
+        for (int k = 0; k < 6; ++k) {
+            float ix = icc + offc[k], iy = ilc + offl[k];
+            float num = std::fmaf(pm[0], ix, std::fmaf(pm[1], iy, pm[3]));
+            float den = std::fmaf(pm[8], ix, std::fmaf(pm[9], iy, pm[11]));
+            float u = num / den;
+            umin = std::min(umin, u); umax = std::max(umax, u);
+        }
+        minu = std::min(std::max(0, (int)std::floor(umin)), nu - 1);
+        maxu = std::min(std::max(0, (int)std::floor(umax)), nu - 1);
+        if (maxu < minu) maxu = minu;
+    }
+    T ox = fox, oy = foy, px = srcx, py = srcy;
+    long long cnt = 0;
+    for (int u = minu; u <= maxu; ++u) {
+        T off = T(u) - T(0.5f) * nu + T(0.5f);
+        T sx = T(dtvx) + T(puvx) * off, sy = T(dtvy) + T(puvy) * off;
+        T ax = sx - T(puvx) * T(0.5f), ay = sy - T(puvy) * T(0.5f);
+        T bx = sx + T(puvx) * T(0.5f), by = sy + T(puvy) * T(0.5f);
+        T num = (ox - px) * (sx - px) + (oy - py) * (sy - py);
+        T ra = num / ((ax - px) * (sx - px) + (ay - py) * (sy - py));
+        T rb = num / ((bx - px) * (sx - px) + (by - py) * (sy - py));
+        T ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;
+        T bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
+        if (mode == 1 && back) {  // A_H0.cu:331-334
+            T da = std::hypot((double)(ax1 - ox), (double)(ay1 - oy)), db = std::hypot((double)(bx1 - ox), (double)(by1 - oy));
+            if (da > T(dt) && db > T(dt) && (ax1 - ox) * (bx1 - ox) >= T(0) && (ay1 - oy) * (by1 - oy) >= T(0)) continue;
+        }
+        double theta = std::atan2((double)(sx - px), (double)(sy - py));
+        double va = (double)dt * std::sin(theta);
+        double vb = (double)dt * std::sin(theta + 2.0 * kPI / 3.0);
+        double vc = (double)dt * std::sin(theta + 4.0 * kPI / 3.0);
+        double vblur = -std::sqrt((double)((bx1 - ax1) * (bx1 - ax1) + (by1 - ay1) * (by1 - ay1)));
+        double y = std::sqrt((double)((ax1 - ox) * (ax1 - ox) + (ay1 - oy) * (ay1 - oy)));
+        if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) y = -y;
+        double conv;
+        if (mode == 2) {
+            conv = hl_linear_convolution_1d(y, vblur, va, vb, vc);
+        } else {
+            conv = (double)b0_linear_convolution_1d<T>(T(y), T(vblur), T(va), T(vb)) +
+                   (double)b0_linear_convolution_1d<T>(T(y), T(vblur), T(vb), T(vc)) +
+                   (double)b0_linear_convolution_1d<T>(T(y), T(vblur), T(vc), T(va));
+            cnt += 3;
+        }
+        if (conv == conv && conv > 0.0) visit(u, conv * (double)dx * (double)dy);
+    }
+    return cnt;
+}
+
 Geo make_geo(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
              double dv) {
     Geo g;
@@ -629,6 +739,51 @@ void oracle_b0_backward(int nx, int ny, int np, int nu, double dx, double dy, do
                 acc += val;
             }
             x[(size_t)ix * ny + iy] = acc;
+        }
+}
+
+// h0_/hl_ forward and backward (layers/A_H0.cu:565-642, layers/A_Hl.cu:579-656):
+// nl rows of nc sites, host layout x[ic*nl + il], b[p*nu + u]; mode as
+// hex_site_view.  GeoData(nc, nl, 1, nu, 1, np, dt*sqrt3, dt*0.5, 1, du, 1).
+long long oracle_hex_forward(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                             const double* angles, const double* x, double* b, int precision) {
+    Geo g = make_geo(nc, nl, 1, np, nu, 1, dt * kSQRT3, dt * 0.5f, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::memset(b, 0, sizeof(double) * (size_t)np * nu);
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : total)
+    for (int p = 0; p < np; ++p) {
+        double* bp = b + (size_t)p * nu;
+        for (int ic = 0; ic < nc; ++ic)
+            for (int il = 0; il < nl; ++il) {
+                if ((il & 1) && ic == nc - 1) continue;
+                double C = x[(size_t)ic * nl + il];
+                auto visit = [&](int u, double v) { bp[u] += v * C; };
+                total += precision ? hex_site_view<float>(g, mode, false, p, ic, il, visit)
+                                   : hex_site_view<double>(g, mode, false, p, ic, il, visit);
+            }
+    }
+    return total;
+}
+
+void oracle_hex_backward(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                         const double* angles, const double* b, double* x, int precision) {
+    Geo g = make_geo(nc, nl, 1, np, nu, 1, dt * kSQRT3, dt * 0.5f, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+#pragma omp parallel for schedule(dynamic)
+    for (int ic = 0; ic < nc; ++ic)
+        for (int il = 0; il < nl; ++il) {
+            double acc = 0.0;
+            if (!((il & 1) && ic == nc - 1))
+                for (int p = 0; p < np; ++p) {
+                    const double* bp = b + (size_t)p * nu;
+                    double val = 0.0;
+                    auto visit = [&](int u, double v) { val += v * bp[u]; };
+                    if (precision) hex_site_view<float>(g, mode, true, p, ic, il, visit);
+                    else hex_site_view<double>(g, mode, true, p, ic, il, visit);
+                    acc += val;
+                }
+            x[(size_t)ic * nl + il] = acc;
         }
 }
 

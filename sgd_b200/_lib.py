@@ -33,8 +33,10 @@ def lib() -> ctypes.CDLL:
     L = ctypes.CDLL(LIB_PATH)
     L.sgd_last_error.restype = ctypes.c_char_p
     L.sgd_last_error.argtypes = []
-    for pre in ("b1", "SF", "b0"):
+    for pre in ("b1", "SF", "b0", "h0", "hl"):
         _declare_fan2d(L, pre)
+    L.sgd_hex_init.restype = _vp
+    L.sgd_hex_init.argtypes = [_i] + _INIT_ARGS["h0"]
     L.sgd_geometry_pmi.restype = _i
     L.sgd_b1_forward_noalloc.restype = _i
     L.sgd_b1_forward_noalloc.argtypes = [_vp, _vp, _vp, _vp]

@@ -10,6 +10,8 @@ Proj2D* make_sf_layer(int nx, int ny, int np, int nu, double dx, double dy, doub
                       const double* angles);
 Proj2D* make_b0_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
                       const double* angles, const double* dz, const double* drho);
+Proj2D* make_hex_layer(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                       const double* angles, const double* dz, const double* drho);
 }
 
 using sgd::Proj2D;
@@ -84,5 +86,47 @@ int sgd_b0_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
     return bwd_dev(layer, d_sino, d_img, stream, "sgd_b0_backward_dev");
 }
 unsigned long long sgd_b0_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
+
+void* sgd_hex_init(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                   double* angles, double* dz, double* drho) {
+    return sgd::guarded<void*>(nullptr, [&]() -> void* {
+        if (mode < 0 || mode > 2) sgd::fail("sgd_hex_init: mode must be 0, 1 or 2");
+        return sgd::make_hex_layer(mode, nl, nc, np, nu, dt, du, lsd, lso, angles, dz, drho);
+    });
+}
+void* h0_init(int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso, double* angles,
+              double* dz, double* drho) {
+    return sgd_hex_init(1, nl, nc, np, nu, dt, du, lsd, lso, angles, dz, drho);
+}
+void* hl_init(int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso, double* angles,
+              double* dz, double* drho) {
+    return sgd_hex_init(2, nl, nc, np, nu, dt, du, lsd, lso, angles, dz, drho);
+}
+int h0_forward_projection(double* b, double* x, void* layer) { return fwd_host(b, x, layer, "h0_forward_projection"); }
+void h0_backward_projection(double* b, double* x, void* layer) { bwd_host(b, x, layer, "h0_backward_projection"); }
+int hl_forward_projection(double* b, double* x, void* layer) { return fwd_host(b, x, layer, "hl_forward_projection"); }
+void hl_backward_projection(double* b, double* x, void* layer) { bwd_host(b, x, layer, "hl_backward_projection"); }
+int sgd_h0_backward_projection(double* b, double* x, void* layer) {
+    return bwd_host(b, x, layer, "h0_backward_projection");
+}
+int sgd_hl_backward_projection(double* b, double* x, void* layer) {
+    return bwd_host(b, x, layer, "hl_backward_projection");
+}
+void h0_destroy(void* layer) { delete static_cast<Proj2D*>(layer); }
+void hl_destroy(void* layer) { delete static_cast<Proj2D*>(layer); }
+int sgd_h0_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream) {
+    return fwd_dev(layer, d_img, d_sino, stream, "sgd_h0_forward_dev");
+}
+int sgd_h0_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream) {
+    return bwd_dev(layer, d_sino, d_img, stream, "sgd_h0_backward_dev");
+}
+int sgd_hl_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream) {
+    return fwd_dev(layer, d_img, d_sino, stream, "sgd_hl_forward_dev");
+}
+int sgd_hl_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream) {
+    return bwd_dev(layer, d_sino, d_img, stream, "sgd_hl_backward_dev");
+}
+unsigned long long sgd_h0_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
+unsigned long long sgd_hl_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
 
 }  // extern "C"

@@ -1,0 +1,320 @@
+// Hexagonal-lattice projectors H0 (hexagon indicator) and Hl (hexagonal
+// linear box spline) on the generic 2D kernels.
+// Reference: layers/A_H0.cu:84-358, :555-643 and layers/A_Hl.cu:21-46,
+// :168-368, :569-656.
+//
+// Lattice: nl rows (il) of nc sites (ic), odd rows one site shorter and
+// shifted by half a site; site (ic, il) at
+//     x = (ic - (nc-1)/2 [odd rows: (nc-2)/2]) * sqrt(3) dt,  y = (il - (nl-1)/2) * dy
+// with dy = 1.5 dt for H0 and 0.5 dt for Hl (A_H0.cu:174-183, A_Hl.cu:184-193).
+// Host layout x[ic*nl + il] (A_H0.cu:581-583): cell (i, j) = (ic, il).
+//
+// Per (site, view, bin) the footprint follows the reference's FP32 geometry
+// (bin centre stepped in FP32 from the first bin, edge rays intersected with
+// the line through the site perpendicular to the bin's central ray: offset y
+// and blur width vblur in FP64) and evaluates
+//   H0: the sum of three 3-direction box splines (vblur, va, vb), (vblur, vb,
+//       vc), (vblur, vc, va), FP32 closed form (layers/spline_conv.hh:244-293);
+//   Hl: the 4-direction box spline (vblur, va, vb, vc) by FP64 divided
+//       differences of truncated cubes, directions below 1e-8 dropped
+//       (A_Hl.cu:21-46);
+// va, vb, vc = dt sin(theta + {0, 2pi/3, 4pi/3}) with theta the bin's ray
+// direction (FP64, per view and bin on the host; the reference recomputes them
+// per pair from the stepped FP32 bin centre, a difference far below 1e-6).
+//
+// Bin ranges.  Hl and "H0 reference-compatible" take the reference's six-vertex
+// bounds through pmi (A_H0.cu:84-156), including H0's use of the 0.5 dt row
+// pitch pmi was built with (h0_init, A_H0.cu:556) although its sites sit at
+// 1.5 dt, so that off-centre rows lose footprint exactly as in the reference,
+// and H0's extra skip test in the back projection (A_H0.cu:333-334).
+// "H0 corrected" bounds the true hexagon of each site and has no skip test:
+// the pair is then an exact transpose.
+#include <cmath>
+
+#include "common.h"
+#include "proj2d_impl.cuh"
+
+namespace sgd {
+
+enum HexMode : int { kH0Corrected = 0, kH0Reference = 1, kHl = 2 };
+
+struct HexBasis {
+    static constexpr int kViewFloats = 28;
+    // [0..5] pmi 0,1,3,8,9,11 [6] puv.x [7] puv.y [8] src.x [9] src.y [10] dtv.x [11] dtv.y
+    // [12] dt [13] dx [14] dy [15] (nl-1)/2 [16] (nc-1)/2 [17] (nc-2)/2
+    // [18..23] world homography n0 n1 n2 d0 d1 d2 (u = (n0 x + n1 y + n2)/(d0 x + d1 y + d2))
+    // [24] mode [25] back (1 in the back projection's view table, for H0's skip test)
+    struct View {
+        float pm0, pm1, pm3, pm8, pm9, pm11, puvx, puvy, srcx, srcy, dtvx, dtvy, dt, dx, dy, nl2, nc2, nc3;
+        float h0, h1, h2, h3, h4, h5;
+        int mode, back;
+    };
+    struct Cell {
+        float ox, oy, sx0, sy0;
+        int lo, hi;
+    };
+    __device__ static void load_view(const float* v, View& V) {
+        const float4* q = reinterpret_cast<const float4*>(v);
+        const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4),
+                     f = __ldg(q + 5), g = __ldg(q + 6);
+        V = View{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w, e.x, e.y,
+                 e.z, e.w, f.x, f.y, f.z, f.w, (int)g.x, (int)g.y};
+    }
+    // nc = P.nj? no: cells are (ic, il) with ic in [0, nc) along i, il in [0, nl) along j
+    __device__ static bool valid(int ic, int il, const Fan2DParams& P) { return !((il & 1) && ic == P.ni - 1); }
+
+    // layers/A_H0.cu:47-156 (first stage; the jittered and linearised stages
+    // only apply to singular projections, which a source outside the field of
+    // view never produces; a full scan stays as the last resort)
+    __device__ static void pmi_bounds(const View& V, int ic, int il, int nu, int& lo, int& hi) {
+        const float icc = (float)ic + ((il & 1) ? 0.5f : 0.0f), ilc = (float)il;
+        const float offc[6] = {0.0f, +0.5f, +0.5f, 0.0f, -0.5f, -0.5f};
+        const float offl[6] = {-2.0f, -1.0f, +1.0f, +2.0f, +1.0f, -1.0f};
+        float umin = 1e30f, umax = -1e30f;
+        int nvalid = 0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float ix = icc + offc[k], iy = ilc + offl[k];
+            const float num = fmaf(V.pm0, ix, fmaf(V.pm1, iy, V.pm3));
+            const float den = fmaf(V.pm8, ix, fmaf(V.pm9, iy, V.pm11));
+            if (!isfinite(num) || !isfinite(den) || fabsf(den) < 1e-8f) continue;
+            const float u = num / den;
+            if (!isfinite(u)) continue;
+            umin = fminf(umin, u);
+            umax = fmaxf(umax, u);
+            ++nvalid;
+        }
+        if (nvalid < 2) {
+            lo = 0;
+            hi = nu - 1;
+            return;
+        }
+        lo = min(max(0, (int)floorf(umin)), nu - 1);
+        hi = min(max(0, (int)floorf(umax)), nu - 1);
+        if (hi < lo) hi = lo;
+    }
+    // bins of the true hexagon (vertices at distance dt from the site)
+    __device__ static void true_bounds(const View& V, float ox, float oy, int nu, int& lo, int& hi) {
+        const float hx = 0.8660254037844386f * V.dt, hy = 0.5f * V.dt;
+        const float xs[6] = {ox, ox + hx, ox + hx, ox, ox - hx, ox - hx};
+        const float ys[6] = {oy - V.dt, oy - hy, oy + hy, oy + V.dt, oy + hy, oy - hy};
+        float umin = 1e30f, umax = -1e30f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float u = fmaf(V.h0, xs[k], fmaf(V.h1, ys[k], V.h2)) / fmaf(V.h3, xs[k], fmaf(V.h4, ys[k], V.h5));
+            umin = fminf(umin, u);
+            umax = fmaxf(umax, u);
+        }
+        lo = min(max(0, (int)floorf(umin)), nu - 1);
+        hi = min(max(0, (int)floorf(umax)), nu - 1);
+    }
+    __device__ static void setup(const View& V, int ic, int il, const Fan2DParams& P, Cell& c) {
+        c.oy = (il - V.nl2) * V.dy;
+        c.ox = ((il & 1) ? (ic - V.nc3) : (ic - V.nc2)) * V.dx;
+        if (V.mode == kH0Corrected)
+            true_bounds(V, c.ox, c.oy, P.nu, c.lo, c.hi);
+        else
+            pmi_bounds(V, ic, il, P.nu, c.lo, c.hi);
+        const float fl = (float)c.lo;
+        c.sx0 = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
+        c.sy0 = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
+    }
+    __device__ static void sort2d(float& a, float& b) {
+        if (a < b) {
+            const float t = b;
+            b = a;
+            a = t;
+        }
+    }
+    // layers/A_H0.cu:21-36 / spline_conv.hh:244-293 (T = float)
+    __device__ static float conv3(float y, float v1, float v2, float v3) {
+        float vs[3];
+        y = fabsf(y - (v1 + v2 + v3) / 2.0f);
+        vs[0] = fabsf(v1), vs[1] = fabsf(v2), vs[2] = fabsf(v3);
+        sort2d(vs[1], vs[2]);
+        sort2d(vs[0], vs[1]);
+        sort2d(vs[1], vs[2]);
+        if (!(vs[2] > 1e-7f)) return fmaxf(0.0f, fminf(1.0f / vs[0], ((vs[0] + vs[1]) / 2.0f - y) / (vs[0] * vs[1])));
+        const float* xi = vs;
+        const float h = 1.0f / xi[0], p = xi[0] * xi[1] * xi[2];
+        const float K0 = (xi[0] - xi[1] - xi[2]) / 2.0f, K1 = (xi[0] - xi[1] + xi[2]) / 2.0f;
+        const float K2 = (xi[0] + xi[1] - xi[2]) / 2.0f, K3 = (xi[0] + xi[1] + xi[2]) / 2.0f;
+        if (y >= K3) return 0.0f;
+        if (y >= K2) return 0.5f * (K3 - y) * (K3 - y) / p;
+        if (y >= K1) return ((xi[0] + xi[1]) / 2.0f - y) * xi[2] / p;
+        if (y < -K0) return h - (K0 * K0 + y * y) / p;
+        if (y < K0) return h;
+        return h - 0.5f * (K0 - y) * (K0 - y) / p;
+    }
+    // layers/A_Hl.cu:21-46 with spline_conv.hh:151-229: divided differences of
+    // truncated powers y+^(m-1), m = number of kept directions
+    __device__ static double tp(double y, int m) {
+        if (!(y > 0)) return 0.0;
+        return m == 2 ? y : (m == 3 ? y * y : y * y * y);
+    }
+    __device__ static double conv4(double y, double h1, double h2, double h3, double h4) {
+        double hs[4];
+        int m = 0;
+        if (fabs(h1) > 1e-8) hs[m++] = h1;
+        if (fabs(h2) > 1e-8) hs[m++] = h2;
+        if (fabs(h3) > 1e-8) hs[m++] = h3;
+        if (fabs(h4) > 1e-8) hs[m++] = h4;
+        if (m < 2) return 0.0;
+        // Delta_{h_{m-1}} ... Delta_{h_0} of tp, nested as the reference nests
+        // forward_difference_mx_1 (outermost difference over the last kept h)
+        double v[16];
+        const int n = 1 << m;
+        for (int s = 0; s < n; ++s) {
+            double yy = y;
+            for (int k = m - 1; k >= 0; --k)
+                if (s & (1 << (m - 1 - k))) yy = yy - hs[k];
+            v[s] = tp(yy, m);
+        }
+        for (int k = 0; k < m; ++k) {  // innermost difference first: h_0
+            const int bit = 1 << (m - 1 - k);
+            for (int s = 0; s < n; ++s)
+                if (!(s & bit)) v[s] = (v[s] - v[s | bit]) / hs[k];
+        }
+        return m == 2 ? v[0] : (m == 3 ? v[0] / 2.0 : v[0] / 6.0);
+    }
+    // bins: [view][bin][va, vb, vc, 0] doubles
+    __device__ static float value(const View& V, const Cell& c, int u, int p, const Fan2DParams& P) {
+        float sx = c.sx0, sy = c.sy0;
+        for (int t = c.lo; t < u; ++t) {  // the reference's FP32 stepping
+            sx += V.puvx;
+            sy += V.puvy;
+        }
+        const float px = V.srcx, py = V.srcy, ox = c.ox, oy = c.oy;
+        const float ax = sx - V.puvx * 0.5f, ay = sy - V.puvy * 0.5f;
+        const float bx = sx + V.puvx * 0.5f, by = sy + V.puvy * 0.5f;
+        const float num = ((ox - px) * (sx - px) + (oy - py) * (sy - py));
+        const float dena = ((ax - px) * (sx - px) + (ay - py) * (sy - py));
+        const float denb = ((bx - px) * (sx - px) + (by - py) * (sy - py));
+        const float ra = num / dena, rb = num / denb;
+        const float ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;
+        const float bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
+        if (V.mode == kH0Reference && V.back) {  // layers/A_H0.cu:331-334
+            const float da = hypotf(ax1 - ox, ay1 - oy), db = hypotf(bx1 - ox, by1 - oy);
+            if (da > V.dt && db > V.dt && (ax1 - ox) * (bx1 - ox) >= 0.0f && (ay1 - oy) * (by1 - oy) >= 0.0f)
+                return 0.f;
+        }
+        const double* b = reinterpret_cast<const double*>(P.bins) + ((size_t)p * P.nu + u) * 4;
+        const double va = __ldg(b), vb = __ldg(b + 1), vc = __ldg(b + 2);
+        const double vblur = -sqrt((double)(bx1 - ax1) * (bx1 - ax1) + (double)(by1 - ay1) * (by1 - ay1));
+        double y = sqrt((double)(ax1 - ox) * (ax1 - ox) + (double)(ay1 - oy) * (ay1 - oy));
+        if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) y = -y;
+        double conv;
+        if (V.mode == kHl) {
+            conv = conv4(y, vblur, va, vb, vc);
+        } else {
+            const float fy = (float)y, fb = (float)vblur, fa = (float)va, fv = (float)vb, fc = (float)vc;
+            conv = (double)conv3(fy, fb, fa, fv) + (double)conv3(fy, fb, fv, fc) + (double)conv3(fy, fb, fc, fa);
+        }
+        return (conv == conv && conv > 0.0) ? (float)conv : 0.f;
+    }
+};
+
+namespace {
+
+const double kSqrt3 = 1.7320508075688772935274463415;
+const double kPi = 3.14159265358979323846;
+
+class HexLayer final : public Proj2D {
+public:
+    // nl rows, nc sites per row (the reference's h0_init/hl_init argument order)
+    HexLayer(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+             const double* angles, const double* dz, const double* drho)
+        : mode_(mode) {
+        if (nl <= 0 || nc <= 1 || !(dt > 0)) fail("invalid hexagonal lattice nl=%d nc=%d dt=%g", nl, nc, dt);
+        // GeoData(nc, nl, 1, nu, 1, np, dt*sqrt3, dt*0.5, 1, du, 1), A_H0.cu:556 / A_Hl.cu:570
+        geo.init(nc, nl, np, nu, dt * kSqrt3, dt * 0.5f, du, lsd, lso, angles, dz, drho);
+        P.ni = nc;
+        P.nj = nl;
+        const float fdt = (float)(dt * 0.5f) * 2.0f;  // d3xyz.y * 2.0f (A_H0.cu:171)
+        const float fdx = fdt * (float)kSqrt3;
+        const float fdy = fdt * (mode == kHl ? 0.5f : 1.5f);
+        std::vector<float> view((size_t)np * HexBasis::kViewFloats, 0.f);
+        std::vector<float4> bins((size_t)np * nu * 2);
+        double* bd = reinterpret_cast<double*>(bins.data());
+        std::vector<BinHomography> hom;
+        bin_homographies(geo, hom);
+        for (int p = 0; p < np; ++p) {
+            const ViewFrame& f = geo.frames[p];
+            float* v = &view[(size_t)p * HexBasis::kViewFloats];
+            const float* m = &geo.pmi[12 * (size_t)p];
+            v[0] = m[0]; v[1] = m[1]; v[2] = m[3]; v[3] = m[8]; v[4] = m[9]; v[5] = m[11];
+            v[6] = (float)f.puv[0]; v[7] = (float)f.puv[1];
+            v[8] = (float)f.src[0]; v[9] = (float)f.src[1];
+            v[10] = (float)f.dtv[0]; v[11] = (float)f.dtv[1];
+            v[12] = fdt; v[13] = fdx; v[14] = fdy;
+            v[15] = 0.5f * (nl - 1); v[16] = 0.5f * (nc - 1); v[17] = 0.5f * (nc - 2);
+            // world homography from the index one: x = x0 + i dx  =>  i = (x - x0)/dx
+            const BinHomography& H = hom[p];
+            const double ix = 1.0 / geo.dx, iy = 1.0 / geo.dy, x0 = geo.x0(), y0 = geo.y0();
+            v[18] = (float)(H.n0 * ix); v[19] = (float)(H.n1 * iy); v[20] = (float)(H.n2 - H.n0 * x0 * ix - H.n1 * y0 * iy);
+            v[21] = (float)(H.d0 * ix); v[22] = (float)(H.d1 * iy); v[23] = (float)(H.d2 - H.d0 * x0 * ix - H.d1 * y0 * iy);
+            v[24] = (float)mode;
+            v[25] = 0.f;
+            // va, vb, vc per bin from the bin's ray direction as the reference
+            // computes it (FP32 atan2 of the FP32 bin centre, FP64 sines)
+            const float px = (float)f.src[0], py = (float)f.src[1];
+            for (int u = 0; u < nu; ++u) {
+                const float sx = (float)f.dtv[0] + (float)f.puv[0] * (u - 0.5f * nu + 0.5f);
+                const float sy = (float)f.dtv[1] + (float)f.puv[1] * (u - 0.5f * nu + 0.5f);
+                const float th = std::atan2(sx - px, sy - py);
+                double* o = bd + ((size_t)p * nu + u) * 4;
+                o[0] = (double)fdt * std::sin((double)th);
+                o[1] = (double)fdt * std::sin((double)th + 2.0 * kPi / 3.0);
+                o[2] = (double)fdt * std::sin((double)th + 4.0 * kPi / 3.0);
+                o[3] = 0.0;
+            }
+        }
+        back_view_ = view;
+        for (int p = 0; p < np; ++p) back_view_[(size_t)p * HexBasis::kViewFloats + 25] = 1.f;
+        // tile boxes: site centres of the tile's rows and columns, plus the
+        // hexagon radius dt (H0) or the linear element's radius dt (Hl); the
+        // reference-compatible H0 bounds are at 0.5 dt row pitch, inside this
+        // box scaled to 1.5 dt only for rows near the centre, so the box also
+        // covers the rows at the pmi positions
+        const double rdt = dt, sdx = dt * kSqrt3;
+        const double ny_pitch = (mode == kHl ? 0.5 : 1.5) * dt;
+        finish_init(view, HexBasis::kViewFloats, bins, [&](int i0, int i1, int j0, int j1) {
+            const double xa = (i0 - 0.5 * (nc - 1)) * sdx - rdt - 0.5 * sdx, xb = (i1 - 0.5 * (nc - 2)) * sdx + rdt;
+            double ya = (j0 - 0.5 * (nl - 1)) * ny_pitch - rdt, yb = (j1 - 0.5 * (nl - 1)) * ny_pitch + rdt;
+            if (mode == kH0Reference) {
+                ya = std::min(ya, (j0 - 0.5 * (nl - 1)) * 0.5 * dt - rdt);
+                yb = std::max(yb, (j1 - 0.5 * (nl - 1)) * 0.5 * dt + rdt);
+            }
+            return Box2{xa, xb, ya, yb};
+        });
+        SGD_CUDA(cudaMalloc(&d_back_view_, back_view_.size() * sizeof(float)));
+        SGD_CUDA(cudaMemcpy(d_back_view_, back_view_.data(), back_view_.size() * sizeof(float),
+                            cudaMemcpyHostToDevice));
+        out_scale = fdx * fdy;  // area factor (double)dx * (double)dy of the reference
+        // the reference's H0 counts footprint evaluations three per bin; Hl never counts
+        count = (mode == kHl) ? 0 : 3 * fan2d_count<HexBasis>(P, stream);
+    }
+    ~HexLayer() override { cudaFree(d_back_view_); }
+    void forward_dev(const float* img, float* sino, cudaStream_t s) override {
+        fan2d_forward<HexBasis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
+    }
+    void backward_dev(const float* sino, float* img, cudaStream_t s) override {
+        Fan2DParams Q = P;
+        Q.view = d_back_view_;
+        fan2d_back<HexBasis>(Q, sino, img, out_scale, s);
+    }
+
+private:
+    int mode_;
+    std::vector<float> back_view_;
+    float* d_back_view_ = nullptr;
+};
+
+}  // namespace
+
+Proj2D* make_hex_layer(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                       const double* angles, const double* dz, const double* drho) {
+    return new HexLayer(mode, nl, nc, np, nu, dt, du, lsd, lso, angles, dz, drho);
+}
+
+}  // namespace sgd

@@ -118,3 +118,62 @@ class A_B0_operator(_Fan2DOperator):
     """Pixel-indicator fan-beam projector (python/operators/operators.py:91-154)."""
 
     _prefix = "b0"
+
+
+class _HexOperator(_Fan2DOperator):
+    """Common body of the hexagonal-lattice operators.  The reference names
+    the lattice sizes (nx, ny) in Python and (nl, nc) in C: nx rows of ny
+    sites, host layout x[ic*nl + il] (python/operators/operators.py:221-349)."""
+
+    _mode = 1
+
+    def __init__(self, nx, ny, nnp, nu, dt, du, lsd, lso, angles, dz=None, drho=None, dtype=np.float64):
+        LinearOperator.__init__(self, dtype=dtype, shape=(nnp * nu, nx * ny))
+        self.vol_shape = (nx, ny)
+        self.proj_shape = (nnp, nu)
+        self.lsd = lsd
+        self.lso = lso
+        self.dimension = dt
+        self.blur = du
+        self.angles = angles
+        if dz is not None and drho is None:
+            raise AssertionError("Error: drho should be provided if dz is provided.")
+        angles = np.ascontiguousarray(angles, dtype=np.float64)
+        if angles.shape != (nnp,):
+            raise ValueError(f"angles must have shape ({nnp},), got {angles.shape}")
+        self._angles = angles
+        self._dz = None if dz is None else np.ascontiguousarray(dz, dtype=np.float64)
+        self._drho = None if drho is None else np.ascontiguousarray(drho, dtype=np.float64)
+        L = _lib.lib()
+        self._L = L
+        self.cpointer = L.sgd_hex_init(self._mode, nx, ny, nnp, nu, dt, du, lsd, lso, _ptr(angles), _ptr(self._dz),
+                                       _ptr(self._drho))
+        if not self.cpointer:
+            raise _lib.ProjectorError(f"{self._prefix}_init: {_lib.last_error()}")
+        self._fwd = getattr(L, f"{self._prefix}_forward_projection")
+        self._bwd = getattr(L, f"sgd_{self._prefix}_backward_projection")
+        self._destroy = getattr(L, f"{self._prefix}_destroy")
+        self.conv_count = int(getattr(L, f"sgd_{self._prefix}_count")(self.cpointer))
+
+
+class A_H0_operator(_HexOperator):
+    """Hexagon-indicator projector (python/operators/operators.py:221-284).
+
+    ``exact_bounds=True`` bounds each site's true hexagon (an exact adjoint
+    pair); the default reproduces the reference, whose bounds are computed at
+    the 0.5 dt row pitch of its projection matrices (layers/A_H0.cu:556) and
+    so drop footprint away from the centre row."""
+
+    _prefix = "h0"
+
+    def __init__(self, nx, ny, nnp, nu, dt, du, lsd, lso, angles, dz=None, drho=None, dtype=np.float64,
+                 exact_bounds=False):
+        self._mode = 0 if exact_bounds else 1
+        super().__init__(nx, ny, nnp, nu, dt, du, lsd, lso, angles, dz, drho, dtype=dtype)
+
+
+class A_Hl_operator(_HexOperator):
+    """Hexagonal linear box-spline projector (python/operators/operators.py:286-349)."""
+
+    _prefix = "hl"
+    _mode = 2

@@ -110,3 +110,26 @@ def ellipsoid_phantom(nx: int, ny: int, nz: int, dx: float, dy: float, dz: float
         zr = z - c[k, 2]
         out += rho[k] * ((xr / ax[k, 0]) ** 2 + (yr / ax[k, 1]) ** 2 + (zr / ax[k, 2]) ** 2 <= 1.0)
     return out
+
+
+def hex_sites(nl: int, nc: int, dt: float, row_pitch: float):
+    """Site centres of the hexagonal lattice of layers/A_H0.cu:174-183 (H0:
+    row_pitch = 1.5 dt; Hl: 0.5 dt, layers/A_Hl.cu:184-193), as arrays indexed
+    [ic, il] (host layout x[ic*nl + il]); odd rows have nc-1 sites, the last
+    column of odd rows is not a site (mask False)."""
+    ic, il = np.meshgrid(np.arange(nc), np.arange(nl), indexing="ij")
+    dx = dt * np.sqrt(3.0)
+    shift = np.where(il % 2 == 1, 0.5 * (nc - 2), 0.5 * (nc - 1))
+    x = (ic - shift) * dx
+    y = (il - 0.5 * (nl - 1)) * row_pitch
+    mask = ~((il % 2 == 1) & (ic == nc - 1))
+    return x, y, mask
+
+
+def hex_phantom(nl: int, nc: int, dt: float, row_pitch: float, seed: int = 0, n: int = 10) -> np.ndarray:
+    """Seeded ellipse phantom sampled at the hexagonal sites, float64 (nc, nl)."""
+    x, y, mask = hex_sites(nl, nc, dt, row_pitch)
+    radius = 0.5 * min(np.ptp(x[mask]), np.ptp(y[mask]))
+    out = sample_ellipses(random_ellipses(seed, n, radius), x, y)
+    out[~mask] = 0.0
+    return out

@@ -26,3 +26,16 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64).ravel()
     b = np.asarray(b, dtype=np.float64).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def hex_case(name):
+    """(nl, nc, nu, dt, du, lsd, lso, angles) of a hexagonal-lattice case."""
+    if name == "small":      # 64 rows of 40 sites at dt = 2 mm
+        return 64, 40, 300, 2.0, 1.5, LSD, LSO, 2 * np.pi * np.arange(90) / 90
+    if name == "tall":       # Hl-like row pitch: more rows
+        return 128, 40, 300, 2.0, 1.5, LSD, LSO, 2 * np.pi * np.arange(90) / 90
+    if name == "c3_h0":      # ~2^18 sites over 512 mm, 360 views x 736 bins
+        return 550, 477, 736, 0.62, 1.0, LSD, LSO, 2 * np.pi * np.arange(360) / 360
+    if name == "c3_hl":
+        return 953, 275, 736, 1.075, 1.0, LSD, LSO, 2 * np.pi * np.arange(360) / 360
+    raise KeyError(name)

@@ -18,8 +18,8 @@ sys.path.insert(0, os.path.dirname(HERE))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 import reflib  # noqa: E402
-from geometry_cases import fan_case  # noqa: E402
-from sgd_b200.phantom import ellipse_phantom  # noqa: E402
+from geometry_cases import fan_case, hex_case  # noqa: E402
+from sgd_b200.phantom import ellipse_phantom, hex_phantom  # noqa: E402
 
 CASES = {
     "b1_tiny": ("b1", "tiny"),
@@ -34,8 +34,25 @@ CASES = {
 }
 
 
+HEX_CASES = {
+    "hex_h0_small": ("h0", "small", 1.5),
+    "hex_hl_small": ("hl", "small", 0.5),
+}
+
+
 def main(out):
     os.makedirs(out, exist_ok=True)
+    for name, (kind, case, pitch) in HEX_CASES.items():
+        nl, nc, nu, dt, du, lsd, lso, ang = hex_case(case)
+        R = reflib.RefHex(kind, nl, nc, nu, dt, du, lsd, lso, ang)
+        x = hex_phantom(nl, nc, dt, pitch * dt, seed=11).ravel()
+        b, cnt = R.forward(x)
+        y, _ = R.forward(hex_phantom(nl, nc, dt, pitch * dt, seed=12).ravel())
+        xt = R.backward(y)
+        np.savez_compressed(os.path.join(out, f"{name}.npz"), kind="hex_" + kind, sizes=np.array([nl, nc, nu]),
+                            params=np.array([dt, du, lsd, lso]), angles=ang, x=x, b=b, count=cnt, y=y, xt=xt,
+                            tol=1e-5)
+        print(name, "count", cnt, "norm b", np.linalg.norm(b))
     for name, (kind, case) in CASES.items():
         nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case(case)
         R = reflib.RefFan2D(kind, nx, ny, nu, dx, dy, du, lsd, lso, ang)

@@ -32,6 +32,8 @@ def lib():
             b.restype = None
             b.argtypes = [_dp, _dp, ctypes.c_void_p]
         L.b0_init.argtypes = L.b1_init.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [_dp] * 3
+        for pre in ("h0", "hl"):
+            getattr(L, f"{pre}_init").argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 4 + [_dp] * 3
         L.SF_init.restype = ctypes.c_void_p
         L.SF_init.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [_dp]
         for n in ("SF_forward_projection",):
@@ -68,5 +70,29 @@ class RefFan2D:
     def backward(self, y):
         y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
         x = np.zeros(self.nx * self.ny)
+        getattr(lib(), f"{self.kind}_backward_projection")(y.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
+        return x
+
+
+class RefHex:
+    """The reference's hexagonal projector `kind` (h0, hl): nl rows of nc sites."""
+
+    def __init__(self, kind, nl, nc, nu, dt, du, lsd, lso, angles):
+        L = lib()
+        self.kind, self.nl, self.nc, self.nu, self.np = kind, nl, nc, nu, len(angles)
+        self._ang = np.ascontiguousarray(angles, dtype=np.float64)
+        self.h = getattr(L, f"{kind}_init")(nl, nc, self.np, nu, dt, du, lsd, lso, self._ang.ctypes.data_as(_dp),
+                                           None, None)
+        assert self.h
+
+    def forward(self, x):
+        x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
+        b = np.zeros(self.np * self.nu)
+        cnt = getattr(lib(), f"{self.kind}_forward_projection")(b.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
+        return b, cnt
+
+    def backward(self, y):
+        y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
+        x = np.zeros(self.nl * self.nc)
         getattr(lib(), f"{self.kind}_backward_projection")(y.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
         return x
