@@ -156,6 +156,29 @@ int sgd_hl_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
 unsigned long long sgd_h0_count(void* layer);
 unsigned long long sgd_hl_count(void* layer);
 
+/* ---- A_B1_3D cone beam ---------------------------------------------------- */
+
+/* Replace b1_3d_init / b1_3d_forward_projection / b1_3d_backward_projection,
+ * layers/A_B1_3D.hh:24 / layers/A_B1_3D.cu:686-772: volume x[(iz*ny + iy)*nx
+ * + ix], projections b[(p*nv + v)*nu + u].  Both kernels reproduce the
+ * reference, whose backward is not the transpose of its forward (no
+ * 2/width factor, single-bin ranges skipped, layers/A_B1_3D.cu:404,433,436).
+ * The forward returns the reference's footprint-evaluation count (~0 on
+ * failure). */
+void* b1_3d_init(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
+                 double dv, double lsd, double lso, double* angles);
+unsigned long long b1_3d_forward_projection(double* b, double* x, void* layer);
+void b1_3d_backward_projection(double* b, double* x, void* layer);
+/* New: mode 0 = as b1_3d_init, mode 1 = the backward is the exact transpose of
+ * the forward (the dot-product-consistent pair autograd uses). */
+void* sgd_b1_3d_init(int mode, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz,
+                     double du, double dv, double lsd, double lso, double* angles);
+int sgd_b1_3d_backward_projection(double* b, double* x, void* layer);
+void b1_3d_destroy(void* layer);
+int sgd_b1_3d_forward_dev(void* layer, const float* d_vol, float* d_proj, void* stream);
+int sgd_b1_3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void* stream);
+unsigned long long sgd_b1_3d_count(void* layer);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* New (no reference counterpart): FP32 FMA throughput of the current GPU in

@@ -34,6 +34,8 @@ def lib():
         L.oracle_b0_backward.restype = None
         L.oracle_hex_forward.restype = ctypes.c_longlong
         L.oracle_hex_backward.restype = None
+        L.oracle_b1_3d_forward.restype = ctypes.c_ulonglong
+        L.oracle_b1_3d_backward.restype = None
         L.oracle_sf_backward.restype = None
         L.oracle_b1_flops.restype = None
     return _LIB
@@ -177,4 +179,27 @@ def hex_backward(mode, b, nl, nc, nu, dt, du, lsd, lso, angles, precision=0):
     x = np.zeros(nl * nc)
     lib().oracle_hex_backward(HEX_MODES[mode], nl, nc, len(angles), nu, ctypes.c_double(dt), ctypes.c_double(du),
                               ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), _p(b), _p(x), precision)
+    return x
+
+
+def b1_3d_forward(x, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles):
+    """FP64 replica of b1_3d_forward_projection: (b[(p*nv+v)*nu+u], count)."""
+    angles = _c(angles)
+    x = _c(np.ravel(x))
+    b = np.zeros(len(angles) * nu * nv)
+    d = ctypes.c_double
+    cnt = lib().oracle_b1_3d_forward(nx, ny, nz, len(angles), nu, nv, d(dx), d(dy), d(dz), d(du), d(dv), d(lsd), d(lso),
+                                     _p(angles), _p(x), _p(b))
+    return b, int(cnt)
+
+
+def b1_3d_backward(b, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, exact=False):
+    """FP64 replica of b1_3d_backward_projection (exact=False) or of the exact
+    transpose of the forward (exact=True)."""
+    angles = _c(angles)
+    b = _c(np.ravel(b))
+    x = np.zeros(nx * ny * nz)
+    d = ctypes.c_double
+    lib().oracle_b1_3d_backward(2 if exact else 1, nx, ny, nz, len(angles), nu, nv, d(dx), d(dy), d(dz), d(du), d(dv),
+                                d(lsd), d(lso), _p(angles), _p(b), _p(x))
     return x

@@ -641,6 +641,80 @@ long long hex_site_view(const Geo& g, int mode, bool back, int p, int ic, int il
     return cnt;
 }
 
+// ---------------------------------------------------------------------------
+// A_B1_3D cone beam: layers/A_B1_3D.cu
+// ---------------------------------------------------------------------------
+
+// mode 0: forward as the reference (:82-312); mode 1: backward as the
+// reference (:314-531); mode 2: backward as the exact transpose of the
+// forward.  visit(u, v, weight) for every kept (u, v) of voxel (ix, iy, iz)
+// in view p; returns the footprint-evaluation count (forward).
+template <class T, class Visit>
+long long b1_3d_voxel_view(const Geo& g, const float* vecs_p, int mode, int p, int ix, int iy, int iz, Visit visit) {
+    int nx = g.nx, ny = g.ny, nz = g.nz, nu = g.nu, nv = g.nv;
+    float dx = (float)g.dx, dy = (float)g.dy, dz = (float)g.dz;
+    const float* pm = &g.pmi[12 * p];
+    float srcx = (float)g.src[3 * p], srcy = (float)g.src[3 * p + 1], srcz = (float)g.src[3 * p + 2];
+    float puvx = (float)g.puv[3 * p], puvy = (float)g.puv[3 * p + 1];
+    float dtvx = (float)g.dtv[3 * p], dtvy = (float)g.dtv[3 * p + 1];
+    bool singular = std::fabs(puvx - puvy) < 1e-7f;
+    float fox = (ix - 0.5f * (nx - 1)) * dx, foy = (iy - 0.5f * (ny - 1)) * dy, foz = (iz - 0.5f * (nz - 1)) * dz;
+    float sx1 = ix - 1.0f, sx2 = ix + 1.0f, sy1 = iy - 1.0f, sy2 = iy + 1.0f;
+    // FP32 ranges as the reference computes them (with its contractions)
+    auto U = [&](float x, float y) {
+        float n = std::fmaf(pm[1], y, pm[0] * x) + pm[3], d = std::fmaf(pm[9], y, pm[8] * x) + pm[11];
+        float u = n / d;
+        return singular ? (u * 1.5f - 1.0f) / puvx : u;
+    };
+    float us[4] = {U(sx1, sy1), U(sx2, sy1), U(sx1, sy2), U(sx2, sy2)};
+    sort4(us);
+    int minu = std::min(std::max(0, (int)std::floor(us[0])), nu - 1);
+    int maxu = std::min(std::max(0, (int)std::floor(us[3])), nu - 1);
+    if (mode == 1 && minu >= maxu) return 0;
+    float v1 = std::fmaf(pm[5], (float)iy, pm[4] * sx1) + pm[7], v2 = std::fmaf(pm[5], (float)iy, pm[4] * sx2) + pm[7];
+    float v3 = std::fmaf(pm[9], (float)iy, pm[8] * sx1) + pm[11], v4 = std::fmaf(pm[9], (float)iy, pm[8] * sx2) + pm[11];
+    auto V = [&](float a, float b, float z) {
+        float v = std::fmaf(pm[6], z, a) / std::fmaf(pm[10], z, b);
+        return singular ? (v * 1.5f - 1.0f) / puvy : v;
+    };
+    float sz1 = iz - 0.5f, sz2 = iz + 0.5f;
+    float vsf[4] = {V(v1, v3, sz1), V(v1, v3, sz2), V(v2, v4, sz1), V(v2, v4, sz2)};
+    sort4(vsf);
+    if (vsf[0] >= nv) return -1;  // the reference returns for the rest of its z chunk
+    int minv = std::min(std::max(0, (int)std::floor(vsf[0])), nv - 1);
+    int maxv = std::min(std::max(0, (int)std::floor(vsf[3])), nv - 1);
+    if (mode == 1 && minv >= maxv) return 0;
+    T ox = fox, oy = foy, oz = foz, px = srcx, py = srcy, pz = srcz;
+    T vs[4] = {vsf[0], vsf[1], vsf[2], vsf[3]};
+    T weight = sqrt(((ox - px) * (ox - px) + (oy - py) * (oy - py) + (oz - pz) * (oz - pz)) /
+                    ((ox - px) * (ox - px) + (oy - py) * (oy - py)));
+    T C = T(dx) * T(dy) * T(dz) * weight;
+    if (mode != 1) C = C * (T(2) / ((vs[3] - vs[0]) + (vs[2] - vs[1])));
+    long long cnt = 0;
+    for (int u = minu; u <= maxu; ++u) {
+        T off = T(u) - T(0.5f) * nu + T(0.5f);
+        T sx = T(dtvx) + T(puvx) * off, sy = T(dtvy) + T(puvy) * off;
+        T vx = vecs_p[u], vy = vecs_p[nu + u];
+        T ax = sx - T(puvx) * T(0.5f), ay = sy - T(puvy) * T(0.5f), bx = sx + T(puvx) * T(0.5f), by = sy + T(puvy) * T(0.5f);
+        T num = (ox - px) * (sx - px) + (oy - py) * (sy - py);
+        T ra = num / ((ax - px) * (sx - px) + (ay - py) * (sy - py));
+        T rb = num / ((bx - px) * (sx - px) + (by - py) * (sy - py));
+        T ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra, bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
+        T x1 = sqrt((ax1 - ox) * (ax1 - ox) + (ay1 - oy) * (ay1 - oy));
+        T x2 = sqrt((bx1 - ox) * (bx1 - ox) + (by1 - oy) * (by1 - oy));
+        T sgn = ((ax1 - ox) * (bx1 - ox) + (ay1 - oy) * (by1 - oy) > T(0)) ? T(1) : T(-1);
+        T conv = b1_linear_convolution_1d<T>(x1 * sgn, x2, max(vx, vy), min(vx, vy));
+        ++cnt;
+        if (mode == 1) { if (!(conv == conv && conv > T(1e-7f))) continue; }
+        else if (!(conv * C == conv * C)) continue;
+        for (int j = minv; j <= maxv; ++j) {
+            T gm = sf_gamma<T>(T(j), T(j) + T(1), vs);
+            if (gm > T(1e-7f)) visit(u, j, (double)(conv * C * gm));
+        }
+    }
+    return cnt;
+}
+
 Geo make_geo(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
              double dv) {
     Geo g;
@@ -690,6 +764,63 @@ void oracle_b1_backward(int nx, int ny, int np, int nu, double dx, double dy, do
     std::vector<float> vecs;
     b1_vectors(g, vecs);
     if (precision) b1_backward<float>(g, vecs, b, x); else b1_backward<double>(g, vecs, b, x);
+}
+
+// b1_3d_forward_projection / b1_3d_backward_projection (layers/A_B1_3D.cu:
+// 696-772): volume x[(iz*ny + iy)*nx + ix], projections b[(p*nv + v)*nu + u].
+// back_mode 1: the reference's backward, 2: exact transpose of the forward.
+unsigned long long oracle_b1_3d_forward(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
+                                        double dz, double du, double dv, double lsd, double lso, const double* angles,
+                                        const double* x, double* b) {
+    Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::vector<float> vecs;
+    b1_vectors(g, vecs);
+    std::memset(b, 0, sizeof(double) * (size_t)np * nu * nv);
+    long long total = 0;
+#pragma omp parallel for schedule(dynamic) reduction(+ : total)
+    for (int p = 0; p < np; ++p) {
+        double* bp = b + (size_t)p * nu * nv;
+        const float* vp = &vecs[(size_t)p * nu * 2];
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix)
+                for (int z0 = 0; z0 < nz; z0 += 32)
+                    for (int iz = z0; iz < std::min(nz, z0 + 32); ++iz) {
+                        double C = x[((size_t)iz * ny + iy) * nx + ix];
+                        long long n = b1_3d_voxel_view<double>(g, vp, 0, p, ix, iy, iz, [&](int u, int v, double w) {
+                            bp[(size_t)v * nu + u] += w * C;
+                        });
+                        if (n < 0) break;
+                        total += n;
+                    }
+    }
+    return (unsigned long long)total;
+}
+
+void oracle_b1_3d_backward(int back_mode, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
+                           double dz, double du, double dv, double lsd, double lso, const double* angles,
+                           const double* b, double* x) {
+    Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::vector<float> vecs;
+    b1_vectors(g, vecs);
+    std::memset(x, 0, sizeof(double) * (size_t)nx * ny * nz);
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix)
+            for (int p = 0; p < np; ++p) {
+                const double* bp = b + (size_t)p * nu * nv;
+                const float* vp = &vecs[(size_t)p * nu * 2];
+                for (int z0 = 0; z0 < nz; z0 += 32)
+                    for (int iz = z0; iz < std::min(nz, z0 + 32); ++iz) {
+                        double acc = 0.0;
+                        long long n = b1_3d_voxel_view<double>(g, vp, back_mode, p, ix, iy, iz, [&](int u, int v, double w) {
+                            acc += w * bp[(size_t)v * nu + u];
+                        });
+                        if (n < 0) break;
+                        x[((size_t)iz * ny + iy) * nx + ix] += acc;
+                    }
+            }
 }
 
 // b0_forward_projection / b0_backward_projection (layers/A_B0.cu:504-575),

@@ -35,6 +35,22 @@ def lib() -> ctypes.CDLL:
     L.sgd_last_error.argtypes = []
     for pre in ("b1", "SF", "b0", "h0", "hl"):
         _declare_fan2d(L, pre)
+    cone = [_i] * 6 + [_d] * 7 + [_dp]
+    L.b1_3d_init.restype = _vp
+    L.b1_3d_init.argtypes = cone
+    L.sgd_b1_3d_init.restype = _vp
+    L.sgd_b1_3d_init.argtypes = [_i] + cone
+    L.b1_3d_forward_projection.restype = ctypes.c_ulonglong
+    L.b1_3d_forward_projection.argtypes = [_dp, _dp, _vp]
+    L.sgd_b1_3d_backward_projection.restype = _i
+    L.sgd_b1_3d_backward_projection.argtypes = [_dp, _dp, _vp]
+    L.b1_3d_destroy.restype = None
+    L.b1_3d_destroy.argtypes = [_vp]
+    for n in ("sgd_b1_3d_forward_dev", "sgd_b1_3d_backward_dev"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = [_vp, _vp, _vp, _vp]
+    L.sgd_b1_3d_count.restype = ctypes.c_ulonglong
+    L.sgd_b1_3d_count.argtypes = [_vp]
     L.sgd_hex_init.restype = _vp
     L.sgd_hex_init.argtypes = [_i] + _INIT_ARGS["h0"]
     L.sgd_geometry_pmi.restype = _i

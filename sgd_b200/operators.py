@@ -177,3 +177,56 @@ class A_Hl_operator(_HexOperator):
 
     _prefix = "hl"
     _mode = 2
+
+
+class A_B1_3D_operator(LinearOperator):
+    """Cone-beam bilinear x separable-footprint projector
+    (python/operators/operators.py:401-449): x flat [z][y][x], y flat
+    [p][v][u].  ``exact_adjoint=True`` makes rmatvec the exact transpose of
+    matvec; the default reproduces the reference's backward."""
+
+    def __init__(self, nx, ny, nz, nnp, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, dtype=np.float64,
+                 exact_adjoint=False):
+        super().__init__(dtype=dtype, shape=(nnp * nu * nv, nx * ny * nz))
+        self.vol_shape = (nz, ny, nx)
+        self.proj_shape = (nnp, nu, nv)
+        self.lsd = lsd
+        self.lso = lso
+        self.dimension = (dx, dy, dz)
+        self.blur = (du, dv)
+        self.angles = angles
+        angles = np.ascontiguousarray(angles, dtype=np.float64)
+        if angles.shape != (nnp,):
+            raise ValueError(f"angles must have shape ({nnp},), got {angles.shape}")
+        self._angles = angles
+        L = _lib.lib()
+        self._L = L
+        self.cpointer = L.sgd_b1_3d_init(1 if exact_adjoint else 0, nx, ny, nz, nnp, nu, nv, dx, dy, dz, du, dv, lsd,
+                                         lso, _ptr(angles))
+        if not self.cpointer:
+            raise _lib.ProjectorError(f"b1_3d_init: {_lib.last_error()}")
+        self.conv_count = int(L.sgd_b1_3d_count(self.cpointer))
+
+    def __del__(self):
+        p = getattr(self, "cpointer", None)
+        if p:
+            self._L.b1_3d_destroy(p)
+            self.cpointer = None
+
+    def _matvec(self, x):
+        x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
+        if x.size != self.shape[1]:
+            raise ValueError(f"expected {self.shape[1]} volume values, got {x.size}")
+        y = np.zeros((self.shape[0],), dtype=np.float64)
+        if self._L.b1_3d_forward_projection(_ptr(y), _ptr(x), self.cpointer) == 2 ** 64 - 1:
+            raise _lib.ProjectorError(f"b1_3d_forward_projection: {_lib.last_error()}")
+        return y.astype(self.dtype, copy=False)
+
+    def _rmatvec(self, y):
+        y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
+        if y.size != self.shape[0]:
+            raise ValueError(f"expected {self.shape[0]} projection values, got {y.size}")
+        x = np.zeros((self.shape[1],), dtype=np.float64)
+        _lib.check(self._L.sgd_b1_3d_backward_projection(_ptr(y), _ptr(x), self.cpointer),
+                   "b1_3d_backward_projection")
+        return x.astype(self.dtype, copy=False)

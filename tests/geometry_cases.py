@@ -39,3 +39,14 @@ def hex_case(name):
     if name == "c3_hl":
         return 953, 275, 736, 1.075, 1.0, LSD, LSO, 2 * np.pi * np.arange(360) / 360
     raise KeyError(name)
+
+
+def cone_case(name):
+    """(nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles) of a cone-beam case."""
+    if name == "small":   # 32^3 at 2 mm, 24 views, 48 x 40 detector at 3 mm
+        return 32, 32, 32, 48, 40, 2.0, 2.0, 2.0, 3.0, 3.0, LSD, LSO, 2 * np.pi * np.arange(24) / 24
+    if name == "rect":    # anisotropic, non-cubic, odd sizes, a snapped 45-degree view
+        return 27, 20, 45, 40, 52, 2.0, 2.5, 1.5, 3.0, 2.0, LSD, LSO, np.array([0.3, np.pi / 4, 2.0, 3 * np.pi / 4 + 0.01])
+    if name == "c5":      # 256^3 at 1 mm, 360 views over 2 pi, 384 x 384 at 1.5 mm
+        return 256, 256, 256, 384, 384, 1.0, 1.0, 1.0, 1.5, 1.5, LSD, LSO, 2 * np.pi * np.arange(360) / 360
+    raise KeyError(name)

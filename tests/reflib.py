@@ -34,6 +34,12 @@ def lib():
         L.b0_init.argtypes = L.b1_init.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [_dp] * 3
         for pre in ("h0", "hl"):
             getattr(L, f"{pre}_init").argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 4 + [_dp] * 3
+        L.b1_3d_init.restype = ctypes.c_void_p
+        L.b1_3d_init.argtypes = [ctypes.c_int] * 6 + [ctypes.c_double] * 7 + [_dp]
+        L.b1_3d_forward_projection.restype = ctypes.c_ulonglong
+        L.b1_3d_forward_projection.argtypes = [_dp, _dp, ctypes.c_void_p]
+        L.b1_3d_backward_projection.restype = None
+        L.b1_3d_backward_projection.argtypes = [_dp, _dp, ctypes.c_void_p]
         L.SF_init.restype = ctypes.c_void_p
         L.SF_init.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [_dp]
         for n in ("SF_forward_projection",):
@@ -95,4 +101,29 @@ class RefHex:
         y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
         x = np.zeros(self.nl * self.nc)
         getattr(lib(), f"{self.kind}_backward_projection")(y.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
+        return x
+
+
+class RefCone:
+    """The reference's A_B1_3D projector on one geometry."""
+
+    def __init__(self, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles):
+        L = lib()
+        self.n = nx * ny * nz
+        self.m = len(angles) * nu * nv
+        self._ang = np.ascontiguousarray(angles, dtype=np.float64)
+        self.h = L.b1_3d_init(nx, ny, nz, len(angles), nu, nv, dx, dy, dz, du, dv, lsd, lso,
+                              self._ang.ctypes.data_as(_dp))
+        assert self.h
+
+    def forward(self, x):
+        x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
+        b = np.zeros(self.m)
+        cnt = lib().b1_3d_forward_projection(b.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
+        return b, cnt
+
+    def backward(self, y):
+        y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
+        x = np.zeros(self.n)
+        lib().b1_3d_backward_projection(y.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
         return x
