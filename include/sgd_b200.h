@@ -179,6 +179,53 @@ int sgd_b1_3d_forward_dev(void* layer, const float* d_vol, float* d_proj, void* 
 int sgd_b1_3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void* stream);
 unsigned long long sgd_b1_3d_count(void* layer);
 
+/* ---- SF_projector: 3D separable footprint --------------------------------- */
+
+/* New entry points for the class SF of layers/SF_projector.hh:9-23, which the
+ * reference exposes only as a C++ Layer (SF::SF(GeoData*), SF::project,
+ * SF::back_project, layers/SF_projector.cu:359-400); the geometry is that of
+ * b1_3d_init (GeoData::geo_init_angles).  Layouts as A_B1_3D.
+ * mode 0 reproduces the reference kernels: the forward accumulates the
+ * footprint of every non-zero voxel without its value or amplitude, and bins
+ * past the u edges wrap into neighbouring detector rows.  mode 1 applies the
+ * voxel value and amplitude, drops out-of-detector bins, and its backward is
+ * the exact transpose of its forward.  trap_v: SF-TT (trapezoid in v) in the
+ * forward (the reference's `tt` argument); mode 1's backward follows it. */
+void* sgd_sf3d_init(int mode, int trap_v, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
+                    double dz, double du, double dv, double lsd, double lso, double* angles);
+int sgd_sf3d_forward_projection(double* b, double* x, void* layer);
+int sgd_sf3d_backward_projection(double* b, double* x, void* layer);
+void sgd_sf3d_destroy(void* layer);
+int sgd_sf3d_forward_dev(void* layer, const float* d_vol, float* d_proj, void* stream);
+int sgd_sf3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void* stream);
+
+/* ---- system matrices ------------------------------------------------------ */
+
+/* Replace pixel_matrix_generation / bilinear_matrix_generation
+ * (layers/A_B0.cu:449-492, layers/A_B1.cu:545-593; python/matrix_gen/
+ * A_B0_project.py:16, A_B1_project.py:16): uniform angles 2 pi p / np
+ * (geo_init_example, no 45-degree snap), triplets (row p*nu + u, column
+ * i*ny + j, value) as three doubles each in spmat, row-major, values > 0
+ * without the dx*dy factor, each generator's own footprint formula.  Built on
+ * the GPU in O(entries) instead of one dense nu x nx*ny slab per view.
+ * Returns the entry count; -1 (with sgd_last_error) when buffer_size entries
+ * do not hold the matrix, where the reference asserts. */
+int pixel_matrix_generation(int np, int nu, int nx, int ny, double dx, double dy, double du, double lsd, double lso,
+                            double* spmat, int buffer_size);
+int bilinear_matrix_generation(int np, int nu, int nx, int ny, double dx, double dy, double du, double lsd,
+                               double lso, double* spmat, int buffer_size);
+/* New: the system matrix of a layer as CSR (rowptr[np*nu + 1] int64, cols
+ * int32, vals FP64; rows p*nu + u, columns in the layer's host layout), the
+ * same pairs and FP32 footprints its kernels use, area factor included, so
+ * that A x equals the layer's forward projection.  With all three outputs
+ * null it only counts.  Returns the entry count, -1 on error (cap too small
+ * included). */
+long long sgd_b1_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
+long long sgd_b0_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
+long long sgd_SF_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
+long long sgd_h0_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
+long long sgd_hl_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
+
 /* ---- measurement ---------------------------------------------------------- */
 
 /* New (no reference counterpart): FP32 FMA throughput of the current GPU in

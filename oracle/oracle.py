@@ -36,6 +36,11 @@ def lib():
         L.oracle_hex_backward.restype = None
         L.oracle_b1_3d_forward.restype = ctypes.c_ulonglong
         L.oracle_b1_3d_backward.restype = None
+        L.oracle_sf3d_forward.restype = None
+        L.oracle_exact_fan2d_matrix.restype = None
+        L.oracle_matrix_generation.restype = ctypes.c_longlong
+        L.oracle_ref_simpson_3d.restype = None
+        L.oracle_sf3d_backward.restype = None
         L.oracle_sf_backward.restype = None
         L.oracle_b1_flops.restype = None
     return _LIB
@@ -203,3 +208,71 @@ def b1_3d_backward(b, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, 
     lib().oracle_b1_3d_backward(2 if exact else 1, nx, ny, nz, len(angles), nu, nv, d(dx), d(dy), d(dz), d(du), d(dv),
                                 d(lsd), d(lso), _p(angles), _p(b), _p(x))
     return x
+
+
+def sf3d_forward(x, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, mode=0, trap=False):
+    """FP64 replica of SF::project (mode 0) or of the corrected forward (mode 1):
+    b[(p*nv+v)*nu+u] from x[(iz*ny+iy)*nx+ix]."""
+    angles = _c(angles)
+    x = _c(np.ravel(x))
+    b = np.zeros(len(angles) * nu * nv)
+    d = ctypes.c_double
+    lib().oracle_sf3d_forward(mode, int(trap), nx, ny, nz, len(angles), nu, nv, d(dx), d(dy), d(dz), d(du), d(dv),
+                              d(lsd), d(lso), _p(angles), _p(x), _p(b))
+    return b
+
+
+def sf3d_backward(b, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, mode=0, trap=False):
+    """FP64 replica of SF::back_project (mode 0) or the exact transpose of the
+    corrected forward (mode 1)."""
+    angles = _c(angles)
+    b = _c(np.ravel(b))
+    x = np.zeros(nx * ny * nz)
+    d = ctypes.c_double
+    lib().oracle_sf3d_backward(mode, int(trap), nx, ny, nz, len(angles), nu, nv, d(dx), d(dy), d(dz), d(du), d(dv),
+                               d(lsd), d(lso), _p(angles), _p(b), _p(x))
+    return x
+
+
+def exact_fan2d_matrix(kind, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, tol=1e-10):
+    """Dense exact FP64 system matrix (np*nu, nx*ny) of the pixel-indicator
+    ("b0") or bilinear ("b1") basis: bin-averaged line integrals by adaptive
+    Simpson (the exact projectors of python/matrix_gen/*_ref_project.py).
+    Columns in the host layout ix*ny + iy."""
+    angles = _c(angles)
+    M = np.zeros(len(angles) * nu * nx * ny)
+    d = ctypes.c_double
+    lib().oracle_exact_fan2d_matrix({"b0": 0, "b1": 1}[kind], nx, ny, len(angles), nu, d(dx), d(dy), d(du), d(lsd),
+                                    d(lso), _p(angles), _p(_c(dzs)), _p(_c(drho)), d(tol), _p(M))
+    return M.reshape(len(angles) * nu, nx * ny)
+
+
+def ref_simpson_3d(x, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, adaptive=False, max_depth=6,
+                   eps=1e-9):
+    """Ref_project_Simpson (layers/Ref_projector.cu:217-367) over a whole
+    volume in FP64: voxel-indicator projections b[(p*nv+v)*nu+u], chord lengths
+    averaged over each detector cell by 3x3 Simpson or adaptively."""
+    angles = _c(angles)
+    x = _c(np.ravel(x))
+    b = np.zeros(len(angles) * nu * nv)
+    d = ctypes.c_double
+    lib().oracle_ref_simpson_3d(int(adaptive), max_depth, d(eps), nx, ny, nz, len(angles), nu, nv, d(dx), d(dy),
+                                d(dz), d(du), d(dv), d(lsd), d(lso), _p(angles), _p(x), _p(b))
+    return b
+
+
+def matrix_generation(kind, np_, nu, nx, ny, dx, dy, du, lsd, lso, precision=1):
+    """Replica of pixel_matrix_generation ("b0") / bilinear_matrix_generation
+    ("b1"): (rows int64, cols int32, vals f64) COO in row-major order."""
+    d = ctypes.c_double
+    k = {"b0": 0, "b1": 1}[kind]
+    L = lib()
+    n = L.oracle_matrix_generation(k, np_, nu, nx, ny, d(dx), d(dy), d(du), d(lsd), d(lso), precision, 0, None,
+                                   None, None)
+    rows = np.zeros(n, dtype=np.int64)
+    cols = np.zeros(n, dtype=np.int32)
+    vals = np.zeros(n)
+    L.oracle_matrix_generation(k, np_, nu, nx, ny, d(dx), d(dy), d(du), d(lsd), d(lso), precision, n,
+                               rows.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                               cols.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _p(vals))
+    return rows, cols, vals

@@ -715,6 +715,255 @@ long long b1_3d_voxel_view(const Geo& g, const float* vecs_p, int mode, int p, i
     return cnt;
 }
 
+// ---------------------------------------------------------------------------
+// SF_projector 3D separable footprint: layers/SF_projector.cu
+// ---------------------------------------------------------------------------
+
+// One voxel (ix, iy, iz) in view p.  fwd: the forward's amplitude (1/r^2,
+// lsd^2 dy dz / (du dv)) and, with trap, the SF-TT v trapezoid
+// (:81-234); otherwise the backward's (1/r, lsd dx / np, :237-356).
+// mode 0 visits exactly the bins the reference visits (unclamped u, wrap into
+// neighbouring rows through j * nu + i, :216, :336) with the footprint alone
+// in the forward (the reference never applies C or the voxel value there,
+// :190-221); mode 1 keeps in-detector bins only and multiplies by the
+// amplitude.  visit(index into the view's nu*nv plane, weight).
+// Returns -1 when the reference leaves the rest of its z chunk (:150, :286),
+// 0 when the voxel is skipped, 1 when it was visited.
+template <class T, class Visit>
+int sf3d_voxel_view(const Geo& g, double lsd, int mode, bool fwd, bool trap, int p, int ix, int iy, int iz,
+                    Visit visit) {
+    const int nu = g.nu, nv = g.nv, nuv = nu * nv;
+    const float* pm = &g.pmi[12 * p];
+    // FP32 corner projections as the kernel computes them (ranges and skips)
+    auto lin = [&](int r, float x, float y) { return std::fmaf(pm[4 * r + 1], y, pm[4 * r] * x) + pm[4 * r + 3]; };
+    const float sx1 = ix - 0.5f, sx2 = ix + 0.5f, sy1 = iy - 0.5f, sy2 = iy + 0.5f;
+    const float sz1 = iz - 0.5f, sz2 = iz + 0.5f;
+    T vs[4];
+    float min_v, max_v;
+    if (!(fwd && trap)) {
+        const float a = lin(1, (float)ix, (float)iy), b = lin(2, (float)ix, (float)iy);
+        const float v0 = std::fmaf(pm[6], sz1, a) / std::fmaf(pm[10], sz1, b);
+        min_v = std::ceil(v0 - 0.5f);
+        if (min_v >= nv) return -1;
+        const float v1 = std::fmaf(pm[6], sz2, a) / std::fmaf(pm[10], sz2, b);
+        max_v = std::ceil(v1 - 0.5f);
+        if (max_v < 0) return 0;
+        vs[0] = v0; vs[1] = v1;
+    } else {
+        const float a1 = lin(1, sx1, (float)iy), a2 = lin(1, sx2, (float)iy);
+        const float b1 = lin(2, sx1, (float)iy), b2 = lin(2, sx2, (float)iy);
+        float v[4] = {std::fmaf(pm[6], sz1, a1) / std::fmaf(pm[10], sz1, b1),
+                      std::fmaf(pm[6], sz2, a1) / std::fmaf(pm[10], sz2, b1),
+                      std::fmaf(pm[6], sz1, a2) / std::fmaf(pm[10], sz1, b2),
+                      std::fmaf(pm[6], sz2, a2) / std::fmaf(pm[10], sz2, b2)};
+        sort4(v);
+        min_v = std::ceil(v[0] - 0.5f);
+        max_v = std::ceil(v[3] - 0.5f);
+        if (max_v < 0 || min_v >= nv) return 0;
+        for (int k = 0; k < 4; ++k) vs[k] = v[k];
+    }
+    float uf[4] = {std::fmaf(pm[2], (float)iz, lin(0, sx1, sy1)) / std::fmaf(pm[10], (float)iz, lin(2, sx1, sy1)),
+                   std::fmaf(pm[2], (float)iz, lin(0, sx2, sy1)) / std::fmaf(pm[10], (float)iz, lin(2, sx2, sy1)),
+                   std::fmaf(pm[2], (float)iz, lin(0, sx1, sy2)) / std::fmaf(pm[10], (float)iz, lin(2, sx1, sy2)),
+                   std::fmaf(pm[2], (float)iz, lin(0, sx2, sy2)) / std::fmaf(pm[10], (float)iz, lin(2, sx2, sy2))};
+    sort4(uf);
+    const float min_u = std::ceil(uf[0] - 0.5f), max_u = std::ceil(uf[3] - 0.5f);
+    if (max_u < 0 || min_u >= nu) return 0;
+    T us[4] = {uf[0], uf[1], uf[2], uf[3]};
+    // :173 / :300 with the integer halves of :104-105
+    const double ddx = g.dx * (ix - g.nx / 2) - g.src[3 * p], ddy = g.dy * (iy - g.ny / 2) - g.src[3 * p + 1];
+    const double ddz = g.dz * (iz - g.nz / 2) - g.src[3 * p + 2];
+    T w = T(1) / sqrt(T(ddx * ddx + ddy * ddy + ddz * ddz));
+    const double flsd = (double)(float)lsd;  // float lsd = *lsds[p] (:362, :384)
+    T C;
+    const T tw = T(2) / ((us[3] - us[0]) + (us[2] - us[1]));
+    if (fwd) {
+        const double factor = (double)((float)flsd * (float)flsd) * g.dy * g.dz / (g.du * g.dv);
+        C = w * w * T(factor) * tw * (trap ? T(2) / ((vs[3] - vs[0]) + (vs[2] - vs[1])) : T(1) / (vs[1] - vs[0]));
+    } else {
+        C = w * T(flsd * g.dx / g.np) * tw * (T(1) / (vs[1] - vs[0]));
+    }
+    const T amp = (mode == 0 && fwd) ? T(1) : C;
+    for (int i = (int)min_u; i <= (int)max_u; ++i) {
+        if (mode == 1 && (i < 0 || i >= nu)) continue;
+        const T gu = sf_gamma<T>(T(i) - T(0.5), T(i) + T(0.5), us);
+        for (int j = (int)min_v; j <= (int)max_v; ++j) {
+            if (mode == 1 && (j < 0 || j >= nv)) continue;
+            const T fv = (fwd && trap) ? sf_gamma<T>(T(j) - T(0.5), T(j) + T(0.5), vs)
+                                       : max(min(T(j) + T(0.5), vs[1]) - max(T(j) - T(0.5), vs[0]), T(0));
+            const long long idx = (long long)j * nu + i;
+            if (idx >= 0 && idx < nuv) visit((int)idx, (double)(gu * fv * amp));
+        }
+    }
+    return 1;
+}
+
+// ---------------------------------------------------------------------------
+// exact FP64 projectors: layers/Ref_projector.cu, python/matrix_gen/*_ref_project.py
+// ---------------------------------------------------------------------------
+
+// Parameter interval [t0, t1] of the line a + t d inside the box [lo, hi]
+// (slab method); false when the line misses it.  Replaces the six face tests
+// of lineInBox (layers/Ref_projector.cu:99-154), which gather the crossing
+// points with a 1e-13 tolerance and return |max - min| of them.
+bool line_box(const double* a, const double* d, const double* lo, const double* hi, int dim, double& t0,
+              double& t1) {
+    t0 = -INFINITY; t1 = INFINITY;
+    for (int k = 0; k < dim; ++k) {
+        if (d[k] == 0.0) {
+            if (a[k] < lo[k] || a[k] > hi[k]) return false;
+            continue;
+        }
+        double ta = (lo[k] - a[k]) / d[k], tb = (hi[k] - a[k]) / d[k];
+        if (ta > tb) std::swap(ta, tb);
+        t0 = std::max(t0, ta); t1 = std::min(t1, tb);
+    }
+    return t1 > t0;
+}
+
+// Chord length of the line through p1 and p2 inside the box [c1, c1 + d]
+// (layers/Ref_projector.cu:99-154, in FP64 throughout; the reference returns
+// sqrtf of it, FP32 precision).
+double chord3(const double* p1, const double* p2, const double* c1, const double* d) {
+    double dir[3] = {p2[0] - p1[0], p2[1] - p1[1], p2[2] - p1[2]};
+    double hi[3] = {c1[0] + d[0], c1[1] + d[1], c1[2] + d[2]};
+    double t0, t1;
+    if (!line_box(p1, dir, c1, hi, 3, t0, t1)) return 0.0;
+    return (t1 - t0) * std::sqrt(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+}
+
+// Line integral, in mm, of a 2D pixel basis centred at o along the line from
+// s through q: kind 0 the pixel indicator of size dx x dy (the A_B0 model),
+// kind 1 the bilinear hat (1 - |x|/dx)+ (1 - |y|/dy)+ (the A_B1 model).  For
+// the hat the line is cut at the hat's cell edges; on each piece the
+// integrand is a product of two affine functions of the arc length, so
+// Simpson's rule is exact there.
+double pixel_line_integral(int kind, const double* s, const double* q, const double* o, double dx, double dy) {
+    double d[2] = {q[0] - s[0], q[1] - s[1]};
+    const double len = std::sqrt(d[0] * d[0] + d[1] * d[1]);
+    d[0] /= len; d[1] /= len;
+    const double hx = kind == 0 ? 0.5 * dx : dx, hy = kind == 0 ? 0.5 * dy : dy;
+    double lo[2] = {o[0] - hx, o[1] - hy}, hi[2] = {o[0] + hx, o[1] + hy};
+    double t0, t1;
+    if (!line_box(s, d, lo, hi, 2, t0, t1)) return 0.0;
+    if (kind == 0) return t1 - t0;
+    double cut[4];
+    int nc = 0;
+    cut[nc++] = t0;
+    for (int k = 0; k < 2; ++k)
+        if (d[k] != 0.0) {
+            double t = (o[k] - s[k]) / d[k];
+            if (t > t0 && t < t1) cut[nc++] = t;
+        }
+    cut[nc++] = t1;
+    std::sort(cut, cut + nc);
+    auto h = [&](double t) {
+        double x = s[0] + t * d[0] - o[0], y = s[1] + t * d[1] - o[1];
+        return std::max(0.0, 1.0 - std::fabs(x) / dx) * std::max(0.0, 1.0 - std::fabs(y) / dy);
+    };
+    double sum = 0.0;
+    for (int k = 0; k + 1 < nc; ++k) {
+        double a = cut[k], b = cut[k + 1];
+        sum += (b - a) / 6.0 * (h(a) + 4.0 * h(0.5 * (a + b)) + h(b));
+    }
+    return sum;
+}
+
+// Adaptive Simpson with Richardson's correction (q + (q - v)/15), the scheme
+// of simpson_layer (layers/Ref_projector.cu:156-214) in one dimension.
+template <class F>
+double adaptive_simpson(F f, double a, double b, double fa, double fm, double fb, double whole, double eps,
+                        int depth) {
+    const double m = 0.5 * (a + b), lm = 0.5 * (a + m), rm = 0.5 * (m + b);
+    const double flm = f(lm), frm = f(rm);
+    const double left = (m - a) / 6.0 * (fa + 4.0 * flm + fm), right = (b - m) / 6.0 * (fm + 4.0 * frm + fb);
+    const double q = left + right;
+    if (depth <= 0 || std::fabs(q - whole) <= 15.0 * eps) return q + (q - whole) / 15.0;
+    return adaptive_simpson(f, a, m, fa, flm, fm, left, 0.5 * eps, depth - 1) +
+           adaptive_simpson(f, m, b, fm, frm, fb, right, 0.5 * eps, depth - 1);
+}
+
+template <class F>
+double integrate(F f, double a, double b, double eps) {
+    const double fa = f(a), fm = f(0.5 * (a + b)), fb = f(b);
+    return adaptive_simpson(f, a, b, fa, fm, fb, (b - a) / 6.0 * (fa + 4.0 * fm + fb), eps, 40);
+}
+
+// geo_init_example (utils/geo.cu:209-230) with the arguments the matrix
+// generators pass (start 0, end 2 pi (np - 1)/np, layers/A_B1.cu:547): uniform
+// angles without the 45-degree snap.  (np = 1 divides 0 by 0 there; it is
+// taken as the single angle 0 here.)
+void build_geo_example(Geo& g, double lsd, double lso) {
+    const int np = g.np;
+    g.src.assign(3 * np, 0.0); g.dtv.assign(3 * np, 0.0);
+    g.puv.assign(3 * np, 0.0); g.pvv.assign(3 * np, 0.0);
+    const double end = kPI * 2 * (np - 1) / np;
+    const double dangle = np > 1 ? (end - (double)0.0f) / (np - 1) : 0.0;
+    double src0[3] = {-lso, 0.0, 0.0}, dtv0[3] = {lsd - lso, 0.0, 0.0};
+    double puv0[3] = {0.0, g.du, 0.0}, pvv0[3] = {0.0, 0.0, g.dv};
+    for (int i = 0; i < np; ++i) {
+        const double beta = (double)0.0f + i * dangle;
+        rotate(src0, &g.src[3 * i], beta);
+        rotate(dtv0, &g.dtv[3 * i], beta);
+        rotate(puv0, &g.puv[3 * i], beta);
+        rotate(pvv0, &g.pvv[3 * i], beta);
+    }
+}
+
+// One (view, bin) row of the generators' dense slab: bilinear_matrix_generate
+// (layers/A_B1.cu:355-427, kind 1) or b0_matrix_generate (layers/A_B0.cu:
+// 37-121, kind 0).  FP64 geometry; the footprint in T (float: the reference,
+// whose FP64 arguments meet its float-only linear_convolution_1d).
+// visit(col, value) for every entry with value > 0, in column order.
+template <class T, class Visit>
+void generator_row(const Geo& g, int kind, int p, int iu, Visit visit) {
+    const int nx = g.nx, ny = g.ny, nu = g.nu;
+    const double nx2 = 0.5 * (nx - 1), ny2 = 0.5 * (ny - 1), dx = g.dx, dy = g.dy;
+    const double px = g.src[3 * p], py = g.src[3 * p + 1];
+    const double sx = g.dtv[3 * p] + g.puv[3 * p] * (iu - 0.5 * nu + 0.5);
+    const double sy = g.dtv[3 * p + 1] + g.puv[3 * p + 1] * (iu - 0.5 * nu + 0.5);
+    const double ax = sx - g.puv[3 * p] * 0.5, ay = sy - g.puv[3 * p + 1] * 0.5;
+    const double bx = sx + g.puv[3 * p] * 0.5, by = sy + g.puv[3 * p + 1] * 0.5;
+    const double theta = std::atan2(std::fabs(px - sx), std::fabs(py - sy));
+    const double sint = std::sin(theta), cost = std::cos(theta);
+    double vx = dx * cost, vy = dy * sint;
+    if (kind == 0) {
+        vx = std::fabs(vx); vy = std::fabs(vy);
+        if (py < sy) vx = -vx;
+        if (px < sx) vy = -vy;
+    }
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j) {
+            const double ox = (i - nx2) * dx, oy = (j - ny2) * dy;
+            const double num = (ox - px) * (sx - px) + (oy - py) * (sy - py);
+            const double ra = num / ((ax - px) * (sx - px) + (ay - py) * (sy - py));
+            const double rb = num / ((bx - px) * (sx - px) + (by - py) * (sy - py));
+            const double ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;
+            const double bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
+            if (std::fabs(ax1 - ox) > dx && std::fabs(bx1 - ox) > dx && std::fabs(ay1 - oy) > dy &&
+                std::fabs(by1 - oy) > dy)
+                continue;
+            T conv;
+            if (kind == 1) {
+                const double vblur = std::sqrt((bx1 - ax1) * (bx1 - ax1) + (by1 - ay1) * (by1 - ay1));
+                double y = std::sqrt((ax1 - ox) * (ax1 - ox) + (ay1 - oy) * (ay1 - oy));
+                if (y > 2 * std::fabs(vx) + 2 * std::fabs(vy) + std::fabs(vblur)) continue;
+                if ((ay - py) * (ox - px) > (oy - py) * (ax - px)) y = -y;
+                conv = b1_linear_convolution_1d<T>(T(y), T(y + vblur), T(std::max(vx, vy)), T(std::min(vx, vy)));
+            } else {
+                const double om = -0.5 * dx * (px - sx) + 0.5 * dy * (py - sy);
+                const double l2 = (sx - px) * (sx - px) + (sy - py) * (sy - py);
+                const double zx = ox - 0.5 * dx - om * (px - sx) / l2, zy = oy + 0.5 * dy - om * (py - sy) / l2;
+                const double vblur = -std::sqrt((bx1 - ax1) * (bx1 - ax1) + (by1 - ay1) * (by1 - ay1));
+                double y = std::sqrt((ax1 - zx) * (ax1 - zx) + (ay1 - zy) * (ay1 - zy));
+                if (y > std::fabs(vx) + std::fabs(vy) + std::fabs(vblur)) continue;
+                if ((ay - py) * (zx - px) < (zy - py) * (ax - px)) y = -y;
+                conv = b0_linear_convolution_1d<T>(T(y), T(vx), T(vy), T(vblur));
+            }
+            if (conv > T(0)) visit(i * ny + j, (double)conv);
+        }
+}
+
 Geo make_geo(int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
              double dv) {
     Geo g;
@@ -821,6 +1070,228 @@ void oracle_b1_3d_backward(int back_mode, int nx, int ny, int nz, int np, int nu
                         x[((size_t)iz * ny + iy) * nx + ix] += acc;
                     }
             }
+}
+
+// SF::project / SF::back_project (layers/SF_projector.cu:359-400) over all
+// views: volume x[(iz*ny + iy)*nx + ix], projections b[(p*nv + v)*nu + u].
+// mode 0 reproduces the reference kernels, mode 1 the corrected forward and
+// its exact transpose (trap selects SF-TT in v for mode-1 backward too).
+void oracle_sf3d_forward(int mode, int trap, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
+                         double dz, double du, double dv, double lsd, double lso, const double* angles,
+                         const double* x, double* b) {
+    Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::memset(b, 0, sizeof(double) * (size_t)np * nu * nv);
+#pragma omp parallel for schedule(dynamic)
+    for (int p = 0; p < np; ++p) {
+        double* bp = b + (size_t)p * nu * nv;
+        for (int iy = 0; iy < ny; ++iy)
+            for (int ix = 0; ix < nx; ++ix)
+                for (int z0 = 0; z0 < nz; z0 += 64)
+                    for (int iz = z0; iz < std::min(nz, z0 + 64); ++iz) {
+                        const double C = x[((size_t)iz * ny + iy) * nx + ix];
+                        // the reference reads the voxel after the v tests (:170-171)
+                        int r = sf3d_voxel_view<double>(g, lsd, mode, true, trap != 0, p, ix, iy, iz,
+                                                        [&](int idx, double w) {
+                                                            if (C != 0) bp[idx] += mode == 0 ? w : w * C;
+                                                        });
+                        if (r < 0 && mode == 0) break;
+                    }
+    }
+}
+
+void oracle_sf3d_backward(int mode, int trap, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
+                          double dz, double du, double dv, double lsd, double lso, const double* angles,
+                          const double* b, double* x) {
+    Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::memset(x, 0, sizeof(double) * (size_t)nx * ny * nz);
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int iy = 0; iy < ny; ++iy)
+        for (int ix = 0; ix < nx; ++ix)
+            for (int p = 0; p < np; ++p) {
+                const double* bp = b + (size_t)p * nu * nv;
+                for (int z0 = 0; z0 < nz; z0 += 64)
+                    for (int iz = z0; iz < std::min(nz, z0 + 64); ++iz) {
+                        double acc = 0.0;
+                        int r = sf3d_voxel_view<double>(g, lsd, mode, mode == 1, trap != 0, p, ix, iy, iz,
+                                                        [&](int idx, double w) { acc += w * bp[idx]; });
+                        if (r < 0 && mode == 0) break;
+                        x[((size_t)iz * ny + iy) * nx + ix] += acc;
+                    }
+            }
+}
+
+// Exact fan-beam system matrix of the pixel-indicator (kind 0) or bilinear
+// (kind 1) basis, dense, M[(p*nu + u)*(nx*ny) + ix*ny + iy]: the line
+// integral of the basis function along the ray from the source to each point
+// of bin u, averaged over the bin (python/matrix_gen/A_B0_ref_project.py:
+// 137-193, A_B1_ref_project.py:83-139, with scipy's quad replaced by the
+// adaptive Simpson above to a relative tolerance `tol`).  Bin u spans
+// dtv + puv (u - nu/2 + t), t in [0, 1] (layers/A_B1.cu:153); pixel centres
+// ((i - (nx-1)/2) dx, (j - (ny-1)/2) dy).  The integrand has kinks where the
+// ray meets pixel corners; the adaptive rule resolves them.
+void oracle_exact_fan2d_matrix(int kind, int nx, int ny, int np, int nu, double dx, double dy, double du,
+                               double lsd, double lso, const double* angles, const double* dzs, const double* drho,
+                               double tol, double* M) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, dzs, drho);
+    const size_t ncol = (size_t)nx * ny;
+    std::memset(M, 0, sizeof(double) * ncol * np * nu);
+    const double reach = kind == 0 ? 0.5 * std::hypot(dx, dy) : std::hypot(dx, dy);
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int p = 0; p < np; ++p)
+        for (int u = 0; u < nu; ++u) {
+            const double* s = &g.src[3 * p];
+            const double* dt = &g.dtv[3 * p];
+            const double* pu = &g.puv[3 * p];
+            double* row = M + ((size_t)p * nu + u) * ncol;
+            double e0[2], e1[2];
+            for (int k = 0; k < 2; ++k) {
+                e0[k] = dt[k] + pu[k] * (u - 0.5 * nu) - s[k];
+                e1[k] = dt[k] + pu[k] * (u - 0.5 * nu + 1.0) - s[k];
+            }
+            const double n0 = std::hypot(e0[0], e0[1]), n1 = std::hypot(e1[0], e1[1]);
+            for (int ix = 0; ix < nx; ++ix)
+                for (int iy = 0; iy < ny; ++iy) {
+                    const double o[2] = {(ix - 0.5 * (nx - 1)) * dx, (iy - 0.5 * (ny - 1)) * dy};
+                    const double r[2] = {o[0] - s[0], o[1] - s[1]};
+                    // signed distances of the centre from the two edge rays:
+                    // outside the wedge by more than the support radius -> 0
+                    const double c0 = (e0[0] * r[1] - e0[1] * r[0]) / n0, c1 = (e1[0] * r[1] - e1[1] * r[0]) / n1;
+                    if ((c0 > reach && c1 > reach) || (c0 < -reach && c1 < -reach)) continue;
+                    auto f = [&](double t) {
+                        double q[2] = {dt[0] + pu[0] * (u - 0.5 * nu + t), dt[1] + pu[1] * (u - 0.5 * nu + t)};
+                        return pixel_line_integral(kind, s, q, o, dx, dy);
+                    };
+                    const double scale = kind == 0 ? std::hypot(dx, dy) : std::max(dx, dy);
+                    row[(size_t)ix * ny + iy] = integrate(f, 0.0, 1.0, tol * scale);
+                }
+        }
+}
+
+// Ref_project_Simpson (layers/Ref_projector.cu:217-367) over a whole volume:
+// for every non-zero voxel (x[(iz*ny + iy)*nx + ix]) and view, the detector
+// cells its eight corners project onto (ranges ceil(u - 1/2), as SF) receive
+// the voxel value times the chord length of the voxel box along the ray from
+// the source to points of the cell, averaged over the cell with the 3 x 3
+// Simpson rule (adaptive = 0, :330-361) or with the adaptive rule of
+// simpson_layer (adaptive = 1: 5 x 5 composite against 3 x 3, Richardson
+// correction, recursion into quarter cells to `max_depth`, :156-214).  The
+// reference runs voxel (0, 0, z < 64) of views 0, 15, 35, 45 only and takes
+// sqrtf of the FP64 chord; this restatement covers every voxel and view in
+// FP64.  Cell (i, j) is centred at dtv + (i - nu/2) puv + (j - nv/2) pvv.
+void oracle_ref_simpson_3d(int adaptive, int max_depth, double eps, int nx, int ny, int nz, int np, int nu, int nv,
+                           double dx, double dy, double dz, double du, double dv, double lsd, double lso,
+                           const double* angles, const double* x, double* b) {
+    Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::memset(b, 0, sizeof(double) * (size_t)np * nu * nv);
+    const double d3[3] = {dx, dy, dz};
+#pragma omp parallel for schedule(dynamic)
+    for (int p = 0; p < np; ++p) {
+        const double* s = &g.src[3 * p];
+        const double* dt = &g.dtv[3 * p];
+        const double* pu = &g.puv[3 * p];
+        const double* pv = &g.pvv[3 * p];
+        const double* pm = &g.pm[12 * p];
+        double* bp = b + (size_t)p * nu * nv;
+        for (int iz = 0; iz < nz; ++iz)
+            for (int iy = 0; iy < ny; ++iy)
+                for (int ix = 0; ix < nx; ++ix) {
+                    const double C = x[((size_t)iz * ny + iy) * nx + ix];
+                    if (C == 0) continue;
+                    const double c1[3] = {-(nx * dx) / 2 + ix * dx, -(ny * dy) / 2 + iy * dy, -(nz * dz) / 2 + iz * dz};
+                    // detector coordinates of the eight corners (world-space pm)
+                    double umin = INFINITY, umax = -INFINITY, vmin = INFINITY, vmax = -INFINITY;
+                    for (int k = 0; k < 8; ++k) {
+                        const double w[3] = {c1[0] + (k & 1) * dx, c1[1] + ((k >> 1) & 1) * dy,
+                                             c1[2] + ((k >> 2) & 1) * dz};
+                        const double h = pm[8] * w[0] + pm[9] * w[1] + pm[10] * w[2] + pm[11];
+                        const double uu = (pm[0] * w[0] + pm[1] * w[1] + pm[2] * w[2] + pm[3]) / h;
+                        const double vv = (pm[4] * w[0] + pm[5] * w[1] + pm[6] * w[2] + pm[7]) / h;
+                        umin = std::min(umin, uu); umax = std::max(umax, uu);
+                        vmin = std::min(vmin, vv); vmax = std::max(vmax, vv);
+                    }
+                    const int i0 = std::max(0, (int)std::ceil(umin - 0.5)), i1 = std::min(nu - 1, (int)std::ceil(umax - 0.5));
+                    const int j0 = std::max(0, (int)std::ceil(vmin - 0.5)), j1 = std::min(nv - 1, (int)std::ceil(vmax - 0.5));
+                    for (int i = i0; i <= i1; ++i)
+                        for (int j = j0; j <= j1; ++j) {
+                            double M[3], U[3], V[3];
+                            for (int k = 0; k < 3; ++k) {
+                                M[k] = dt[k] + (i - 0.5 * nu) * pu[k] + (j - 0.5 * nv) * pv[k];
+                                U[k] = 0.5 * pu[k]; V[k] = 0.5 * pv[k];
+                            }
+                            auto chord = [&](double a, double c) {
+                                double q[3] = {M[0] + a * U[0] + c * V[0], M[1] + a * U[1] + c * V[1],
+                                               M[2] + a * U[2] + c * V[2]};
+                                return chord3(s, q, c1, d3);
+                            };
+                            double val;
+                            if (!adaptive) {
+                                val = (chord(-1, -1) + chord(1, -1) + chord(-1, 1) + chord(1, 1) +
+                                       4 * (chord(0, -1) + chord(-1, 0) + chord(1, 0) + chord(0, 1)) + 16 * chord(0, 0)) / 36;
+                            } else {
+                                std::function<double(double, double, double, int)> layer =
+                                    [&](double a, double c, double hsz, int depth) -> double {
+                                    // 5 x 5 samples at steps hsz/2 around (a, c), cell half-size hsz
+                                    double t[5][5];
+                                    for (int r = 0; r < 5; ++r)
+                                        for (int q = 0; q < 5; ++q)
+                                            t[r][q] = chord(a + (r - 2) * 0.5 * hsz, c + (q - 2) * 0.5 * hsz);
+                                    const double v3 = (t[0][0] + t[0][4] + t[4][0] + t[4][4] +
+                                                       4 * (t[0][2] + t[2][0] + t[2][4] + t[4][2]) + 16 * t[2][2]) / 36;
+                                    double q5 = 0;
+                                    const double wv[5] = {1, 4, 2, 4, 1};
+                                    for (int r = 0; r < 5; ++r)
+                                        for (int q = 0; q < 5; ++q) q5 += wv[r] * wv[q] * t[r][q];
+                                    q5 /= 144;
+                                    if (std::fabs(q5 - v3) <= eps || depth <= 0) return q5 + (q5 - v3) / 15;
+                                    const double hh = 0.5 * hsz;
+                                    return 0.25 * (layer(a - hh, c - hh, hh, depth - 1) + layer(a + hh, c - hh, hh, depth - 1) +
+                                                   layer(a - hh, c + hh, hh, depth - 1) + layer(a + hh, c + hh, hh, depth - 1));
+                                };
+                                val = layer(0, 0, 1.0, max_depth);
+                            }
+                            bp[(size_t)j * nu + i] += C * val;
+                        }
+                }
+    }
+}
+
+// pixel_matrix_generation (kind 0, layers/A_B0.cu:449-492) and
+// bilinear_matrix_generation (kind 1, layers/A_B1.cu:545-593): COO triplets
+// (row p*nu + u, col i*ny + j, value) in row-major order over all views, no
+// dx*dy factor, entries > 0.  precision 1 evaluates the footprint in float as
+// the reference does, 0 in FP64.  Writes at most `cap` entries; returns nnz.
+long long oracle_matrix_generation(int kind, int np, int nu, int nx, int ny, double dx, double dy, double du,
+                                   double lsd, double lso, int precision, long long cap, long long* rows,
+                                   int* cols, double* vals) {
+    Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 0, du, 0);
+    build_geo_example(g, lsd, lso);
+    std::vector<long long> cnt((size_t)np * nu, 0);
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int p = 0; p < np; ++p)
+        for (int u = 0; u < nu; ++u) {
+            long long c = 0;
+            auto count = [&](int, double) { ++c; };
+            if (precision) generator_row<float>(g, kind, p, u, count); else generator_row<double>(g, kind, p, u, count);
+            cnt[(size_t)p * nu + u] = c;
+        }
+    std::vector<long long> off(cnt.size() + 1, 0);
+    for (size_t r = 0; r < cnt.size(); ++r) off[r + 1] = off[r] + cnt[r];
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int p = 0; p < np; ++p)
+        for (int u = 0; u < nu; ++u) {
+            long long k = off[(size_t)p * nu + u];
+            const long long row = (long long)p * nu + u;
+            auto put = [&](int col, double v) {
+                if (k < cap) { rows[k] = row; cols[k] = col; vals[k] = v; }
+                ++k;
+            };
+            if (precision) generator_row<float>(g, kind, p, u, put); else generator_row<double>(g, kind, p, u, put);
+        }
+    return off.back();
 }
 
 // b0_forward_projection / b0_backward_projection (layers/A_B0.cu:504-575),

@@ -51,6 +51,24 @@ def lib() -> ctypes.CDLL:
         getattr(L, n).argtypes = [_vp, _vp, _vp, _vp]
     L.sgd_b1_3d_count.restype = ctypes.c_ulonglong
     L.sgd_b1_3d_count.argtypes = [_vp]
+    L.sgd_sf3d_init.restype = _vp
+    L.sgd_sf3d_init.argtypes = [_i, _i] + cone
+    for n in ("sgd_sf3d_forward_projection", "sgd_sf3d_backward_projection"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = [_dp, _dp, _vp]
+    L.sgd_sf3d_destroy.restype = None
+    L.sgd_sf3d_destroy.argtypes = [_vp]
+    for n in ("sgd_sf3d_forward_dev", "sgd_sf3d_backward_dev"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = [_vp, _vp, _vp, _vp]
+    gen = [_i] * 4 + [_d] * 5 + [_dp, _i]
+    for n in ("pixel_matrix_generation", "bilinear_matrix_generation"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = gen
+    for pre in ("b1", "b0", "SF", "h0", "hl"):
+        f = getattr(L, f"sgd_{pre}_matrix_csr")
+        f.restype = ctypes.c_longlong
+        f.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_longlong]
     L.sgd_hex_init.restype = _vp
     L.sgd_hex_init.argtypes = [_i] + _INIT_ARGS["h0"]
     L.sgd_geometry_pmi.restype = _i

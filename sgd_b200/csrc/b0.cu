@@ -10,9 +10,12 @@
 // (including its FP32 stepping of the bin centre, sx += puv.x, :202) and FP64
 // per-bin vectors is kept; the two FP64 divisions by the source-bin distance
 // are multiplications by its FP64 reciprocals.
+#include <climits>
 #include <cmath>
+#include <vector>
 
 #include "common.h"
+#include "hom.cuh"
 #include "proj2d_impl.cuh"
 
 namespace sgd {
@@ -174,11 +177,123 @@ public:
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
         fan2d_forward<B0Basis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
     }
+    long long csr(const CsrOut& out) override { return fan2d_csr<B0Basis>(P, out_scale, out, stream); }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
         fan2d_back<B0Basis>(P, sino, img, out_scale, s);
     }
 };
 
+
+// The reference's pixel_matrix_generation (layers/A_B0.cu:37-121, 449-492):
+// per (view, bin) and pixel, in FP64 there, a1/b1 = the edge rays' crossings
+// of the line through the pixel centre o perpendicular to the central ray,
+// z = o + (-dx/2, dy/2) - NM (a corner shifted onto that line), y = |a1 - z|
+// negated when z lies counter-clockwise of edge ray a, vblur = -|b1 - a1|,
+// and the footprint conv1d(y, vx, vy, vblur) with the signs of vx, vy set
+// by the view (:69-70); entries > 0, no dx*dy.  Here a1 - z = xa n + c with
+// xa affine in the pixel indices (fan_geometry.h), so one bin's constants
+// are 16 floats: [xa_i xa_j xa_0 xb_i][xb_j xb_0 n.x n.y][c.x c.y k_i k_j]
+// [k_0 vx vy 0], k the cross product of ray a with z - source, affine too.
+struct B0GenVisit {
+    const float4* rec;  // [view][bin][4]
+    const BinHomography* hom;
+    int nu;
+    float dx, dy;
+    __device__ bool valid(int, int) const { return true; }
+    template <class F>
+    __device__ void visit(int p, int i, int j, F&& f) const {
+        const BinHomography H = hom[p];
+        const float h[6] = {H.n0, H.n1, H.n2, H.d0, H.d1, H.d2};
+        const float fi = (float)i, fj = (float)j;
+        int lo, hi;
+        box_bins(h, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, lo, hi);
+        lo = max(0, lo - 1);
+        hi = min(nu - 1, hi + 1);
+        for (int u = lo; u <= hi; ++u) {
+            const float4* q = rec + ((size_t)p * nu + u) * 4;
+            const float4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3);
+            const float xa = fmaf(fi, q0.x, fmaf(fj, q0.y, q0.z)), xb = fmaf(fi, q0.w, fmaf(fj, q1.x, q1.y));
+            const float m = fminf(fabsf(xa), fabsf(xb));
+            if (m * fabsf(q1.z) > dx && m * fabsf(q1.w) > dy) continue;  // :98-99
+            const float ex = fmaf(xa, q1.z, q2.x), ey = fmaf(xa, q1.w, q2.y);
+            float y = sqrtf(ex * ex + ey * ey);
+            const float vblur = -fabsf(xb - xa);
+            if (y > fabsf(q3.y) + fabsf(q3.z) + fabsf(vblur)) continue;  // :112-113
+            if (fmaf(fi, q2.z, fmaf(fj, q2.w, q3.x)) > 0.f) y = -y;      // :115-116
+            const float conv = B0Basis::conv1d(y, q3.y, q3.z, vblur);
+            if (conv > 0.f) f(u, conv);
+        }
+    }
+};
+
+long long b0_generator(int np, int nu, int nx, int ny, double dx, double dy, double du, double lsd, double lso,
+                       const CsrOut& out) {
+    if (np < 1 || nu < 1 || nx < 1 || ny < 1) fail("pixel_matrix_generation: invalid sizes");
+    // geo_init_example(lsd, lso, 0.0f, PI*2 * (np-1)/np) (utils/geo.cu:209-230)
+    const double pi = 3.14159265358979323846;
+    const double end = pi * 2 * (np - 1) / np;
+    const double dangle = np > 1 ? (end - (double)0.0f) / (np - 1) : 0.0;
+    std::vector<double> ang(np);
+    for (int p = 0; p < np; ++p) ang[p] = (double)0.0f + p * dangle;
+    FanGeometry g;
+    g.init(nx, ny, np, nu, dx, dy, du, lsd, lso, ang.data(), nullptr, nullptr);
+    std::vector<BinHomography> hom;
+    bin_homographies(g, hom);
+    std::vector<float4> rec((size_t)np * nu * 4);
+    const double x0 = g.x0(), y0 = g.y0();
+    for (int p = 0; p < np; ++p) {
+        const double px = g.src[2 * p], py = g.src[2 * p + 1];
+        const double ex = g.puv[2 * p], ey = g.puv[2 * p + 1];
+        for (int u = 0; u < nu; ++u) {
+            const double off = u - 0.5 * nu + 0.5;
+            const double sx = g.dtv[2 * p] + ex * off, sy = g.dtv[2 * p + 1] + ey * off;
+            const double ax = sx - 0.5 * ex, ay = sy - 0.5 * ey, bx = sx + 0.5 * ex, by = sy + 0.5 * ey;
+            const double L = std::sqrt((sx - px) * (sx - px) + (sy - py) * (sy - py));
+            const double tx = (sx - px) / L, ty = (sy - py) / L, nxv = -ty, nyv = tx;
+            // lateral offsets of the edge crossings (as the B1 tables)
+            const double ka = ((ax - px) * nxv + (ay - py) * nyv) / ((ax - px) * tx + (ay - py) * ty);
+            const double kb = ((bx - px) * nxv + (by - py) * nyv) / ((bx - px) * tx + (by - py) * ty);
+            const double mAx = ka * tx - nxv, mAy = ka * ty - nyv, mBx = kb * tx - nxv, mBy = kb * ty - nyv;
+            // z = o + (-dx/2, dy/2) - NM (:93-98)
+            const double om = -0.5 * dx * (px - sx) + 0.5 * dy * (py - sy);
+            const double NMx = om * (px - sx) / (L * L), NMy = om * (py - sy) / (L * L);
+            const double cx = 0.5 * dx + NMx, cy = -0.5 * dy + NMy;
+            // cross(a - src, z - src) / |a - src|, affine in (i, j)
+            const double Ax = ax - px, Ay = ay - py, An = std::sqrt(Ax * Ax + Ay * Ay);
+            const double k0 = -Ay * dx / An, k1 = Ax * dy / An;
+            const double kc = (Ax * (y0 + 0.5 * dy - NMy - py) - Ay * (x0 - 0.5 * dx - NMx - px)) / An;
+            // signed profile directions (:66-70)
+            double vx = std::fabs(dx * std::fabs(py - sy) / L), vy = std::fabs(dy * std::fabs(px - sx) / L);
+            if (py < sy) vx = -vx;
+            if (px < sx) vy = -vy;
+            float4* r = &rec[((size_t)p * nu + u) * 4];
+            r[0] = make_float4((float)(mAx * dx), (float)(mAy * dy), (float)((x0 - px) * mAx + (y0 - py) * mAy),
+                               (float)(mBx * dx));
+            r[1] = make_float4((float)(mBy * dy), (float)((x0 - px) * mBx + (y0 - py) * mBy), (float)nxv, (float)nyv);
+            r[2] = make_float4((float)cx, (float)cy, (float)k0, (float)k1);
+            r[3] = make_float4((float)kc, (float)vx, (float)vy, 0.f);
+        }
+    }
+    cudaStream_t s = nullptr;
+    float4* d_rec = nullptr;
+    BinHomography* d_hom = nullptr;
+    long long n = -1;
+    try {
+        SGD_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        SGD_CUDA(cudaMalloc(&d_rec, rec.size() * sizeof(float4)));
+        SGD_CUDA(cudaMalloc(&d_hom, hom.size() * sizeof(BinHomography)));
+        SGD_CUDA(cudaMemcpy(d_rec, rec.data(), rec.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        SGD_CUDA(cudaMemcpy(d_hom, hom.data(), hom.size() * sizeof(BinHomography), cudaMemcpyHostToDevice));
+        n = build_csr(B0GenVisit{d_rec, d_hom, nu, (float)dx, (float)dy}, np, nu, nx, ny, out, s);
+    } catch (...) {
+        cudaFree(d_rec); cudaFree(d_hom);
+        if (s) cudaStreamDestroy(s);
+        throw;
+    }
+    cudaFree(d_rec); cudaFree(d_hom);
+    cudaStreamDestroy(s);
+    return n;
+}
 }  // namespace
 
 Proj2D* make_b0_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
@@ -187,3 +302,16 @@ Proj2D* make_b0_layer(int nx, int ny, int np, int nu, double dx, double dy, doub
 }
 
 }  // namespace sgd
+
+extern "C" int pixel_matrix_generation(int np, int nu, int nx, int ny, double dx, double dy, double du, double lsd,
+                                       double lso, double* spmat, int buffer_size) {
+    return sgd::guarded<int>(-1, [&]() -> int {
+        if (!spmat || buffer_size < 0) sgd::fail("pixel_matrix_generation: null or negative buffer");
+        sgd::CsrOut out;
+        out.triplets = spmat;
+        out.cap = buffer_size;
+        const long long n = sgd::b0_generator(np, nu, nx, ny, dx, dy, du, lsd, lso, out);
+        if (n > INT_MAX) sgd::fail("pixel_matrix_generation: %lld entries overflow int", n);
+        return (int)n;
+    });
+}

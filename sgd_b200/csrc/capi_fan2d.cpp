@@ -43,6 +43,15 @@ int bwd_dev(void* layer, const float* sino, float* img, void* stream, const char
         static_cast<Proj2D*>(layer)->backward_dev(sino, img, static_cast<cudaStream_t>(stream));
     });
 }
+long long matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap, const char* what) {
+    return sgd::guarded<long long>(-1, [&]() -> long long {
+        if (!layer) sgd::fail("%s: null layer", what);
+        if ((rowptr || cols || vals) && !(rowptr && cols && vals)) sgd::fail("%s: partial output", what);
+        sgd::CsrOut out;
+        out.rowptr = rowptr; out.cols = cols; out.vals = vals; out.cap = cap;
+        return static_cast<Proj2D*>(layer)->csr(out);
+    });
+}
 }  // namespace
 
 extern "C" {
@@ -128,5 +137,18 @@ int sgd_hl_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
 }
 unsigned long long sgd_h0_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
 unsigned long long sgd_hl_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
+
+long long sgd_SF_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap) {
+    return matrix_csr(layer, rowptr, cols, vals, cap, "sgd_SF_matrix_csr");
+}
+long long sgd_b0_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap) {
+    return matrix_csr(layer, rowptr, cols, vals, cap, "sgd_b0_matrix_csr");
+}
+long long sgd_h0_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap) {
+    return matrix_csr(layer, rowptr, cols, vals, cap, "sgd_h0_matrix_csr");
+}
+long long sgd_hl_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap) {
+    return matrix_csr(layer, rowptr, cols, vals, cap, "sgd_hl_matrix_csr");
+}
 
 }  // extern "C"

@@ -298,6 +298,7 @@ public:
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
         fan2d_forward<HexBasis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
     }
+    long long csr(const CsrOut& out) override { return fan2d_csr<HexBasis>(P, out_scale, out, stream); }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
         Fan2DParams Q = P;
         Q.view = d_back_view_;

@@ -8,6 +8,7 @@
 
 #include <vector>
 
+#include "csr_out.h"
 #include "fan2d_params.h"
 #include "fan_geometry.h"
 
@@ -35,6 +36,11 @@ public:
     // the layer's FP64 sinogram scratch.
     virtual void forward_dev(const float* d_img, float* d_sino, cudaStream_t s) = 0;
     virtual void backward_dev(const float* d_sino, float* d_img, cudaStream_t s) = 0;
+
+    // The layer's system matrix, rows p*nu + u, columns i*nj + j: the pairs
+    // and footprints its kernels use, area factor included (csr_build.cuh).
+    // Returns the entry count; copies out when `out` has a destination.
+    virtual long long csr(const CsrOut& out) = 0;
 
     // FP64 host entry points: image x[i*nj + j], sinogram b[p*nu + u].
     void forward_host(double* b, const double* x);

@@ -4,6 +4,7 @@
 #include <algorithm>
 
 #include "common.h"
+#include "csr_build.cuh"
 #include "fan2d.cuh"
 #include "proj2d.h"
 
@@ -94,6 +95,30 @@ void fan2d_back(const Fan2DParams& P, const float* sino, float* img, float scale
         scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(img, n, scale);
         SGD_LAUNCH_CHECK();
     }
+}
+
+// System-matrix visitor of basis B: the bins and values the kernels use.
+template <class B>
+struct Fan2DVisit {
+    Fan2DParams P;
+    float scale;
+    __device__ bool valid(int i, int j) const { return B::valid(i, j, P); }
+    template <class F>
+    __device__ void visit(int p, int i, int j, F&& f) const {
+        typename B::View V;
+        B::load_view(P.view + (size_t)p * B::kViewFloats, V);
+        typename B::Cell c;
+        B::setup(V, i, j, P, c);
+        for (int u = c.lo; u <= c.hi; ++u) {
+            const float v = B::value(V, c, u, p, P);
+            if (v != 0.f) f(u, v * scale);
+        }
+    }
+};
+
+template <class B>
+long long fan2d_csr(const Fan2DParams& P, float scale, const CsrOut& out, cudaStream_t s) {
+    return build_csr(Fan2DVisit<B>{P, scale}, P.np, P.nu, P.ni, P.nj, out, s);
 }
 
 }  // namespace sgd

@@ -126,6 +126,7 @@ public:
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
         fan2d_forward<SFBasis>(P, img, d_sino64_, sino, 1.f, smem_fwd_, s);
     }
+    long long csr(const CsrOut& out) override { return fan2d_csr<SFBasis>(P, 1.f, out, stream); }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
         fan2d_back<SFBasis>(P, sino, img, 1.f, s);
     }

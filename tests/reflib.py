@@ -127,3 +127,52 @@ class RefCone:
         x = np.zeros(self.n)
         lib().b1_3d_backward_projection(y.ctypes.data_as(_dp), x.ctypes.data_as(_dp), self.h)
         return x
+
+
+class RefSF3D:
+    """The reference's SF_projector layer (3D separable footprint) on the
+    geometry of b1_3d_init, through the test shim's ref_sf3d_* entry points."""
+
+    def __init__(self, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles):
+        L = lib()
+        for n in ("ref_sf3d_init",):
+            getattr(L, n).restype = ctypes.c_void_p
+            getattr(L, n).argtypes = [ctypes.c_int] * 6 + [ctypes.c_double] * 7 + [_dp]
+        L.ref_sf3d_forward.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
+        L.ref_sf3d_backward.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.ref_sf3d_destroy.argtypes = [ctypes.c_void_p]
+        self.n = nx * ny * nz
+        self.m = len(angles) * nu * nv
+        self._ang = np.ascontiguousarray(angles, dtype=np.float64)
+        self.h = L.ref_sf3d_init(nx, ny, nz, len(angles), nu, nv, dx, dy, dz, du, dv, lsd, lso,
+                                 self._ang.ctypes.data_as(_dp))
+        assert self.h
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ref_sf3d_destroy(self.h)
+            self.h = None
+
+    def forward(self, x, trap=False):
+        x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
+        b = np.zeros(self.m)
+        assert lib().ref_sf3d_forward(self.h, x.ctypes.data_as(_dp), b.ctypes.data_as(_dp), int(trap)) == 0
+        return b
+
+    def backward(self, y):
+        y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
+        x = np.zeros(self.n)
+        assert lib().ref_sf3d_backward(self.h, y.ctypes.data_as(_dp), x.ctypes.data_as(_dp)) == 0
+        return x
+
+
+def matrix_generation(kind, np_, nu, nx, ny, dx, dy, du, lsd, lso, buffer_size):
+    """The reference's pixel_matrix_generation ("b0") or
+    bilinear_matrix_generation ("b1"): (nnz, triplets (buffer_size, 3))."""
+    L = lib()
+    f = getattr(L, {"b0": "pixel_matrix_generation", "b1": "bilinear_matrix_generation"}[kind])
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [_dp, ctypes.c_int]
+    spmat = np.zeros((buffer_size, 3))
+    n = f(np_, nu, nx, ny, dx, dy, du, lsd, lso, spmat.ctypes.data_as(_dp), buffer_size)
+    return n, spmat

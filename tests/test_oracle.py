@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import ROOT
-from geometry_cases import fan_case, rel_l2
+from geometry_cases import cone_case, fan_case, rel_l2
 from sgd_b200.phantom import ellipse_phantom, ellipse_chords, random_ellipses
 
 
@@ -104,6 +104,30 @@ def test_oracle_matches_reference_golden(oracle_mod, fname):
         xt = oracle_mod.hex_backward(mode, z["y"], nl, nc, nu, dt, du, lsd, lso, z["angles"])
         assert rel_l2(xt, z["xt"]) < 5e-5
         return
+    if kind.startswith("matgen_"):
+        import scipy.sparse
+        import scipy.sparse.linalg
+        npv, nu, nx, ny = (int(v) for v in z["sizes"])
+        dx, dy, du, lsd, lso = (float(v) for v in z["params"])
+        shape = (npv * nu, nx * ny)
+        r, c, v = oracle_mod.matrix_generation(kind[7:], npv, nu, nx, ny, dx, dy, du, lsd, lso, precision=1)
+        M = scipy.sparse.csr_matrix((v, (r, c)), shape=shape)
+        R = scipy.sparse.csr_matrix((z["vals"], (z["rows"], z["cols"])), shape=shape)
+        assert scipy.sparse.linalg.norm(M - R) / scipy.sparse.linalg.norm(R) < 1e-5
+        assert abs(M.nnz - R.nnz) <= 2e-3 * R.nnz
+        return
+    if kind in ("b1_3d", "sf3d"):
+        g = tuple(int(v) for v in z["sizes"]) + tuple(float(v) for v in z["params"]) + (z["angles"],)
+        if kind == "b1_3d":
+            b, cnt = oracle_mod.b1_3d_forward(z["x"], *g)
+            assert rel_l2(b, z["b"]) < 5e-5
+            assert abs(cnt - int(z["count"])) <= 1e-4 * cnt + 3
+            return
+        # FP32 reference against the FP64 replica of its formulas
+        assert rel_l2(oracle_mod.sf3d_forward(z["x"], *g), z["b"]) < 2e-5
+        assert rel_l2(oracle_mod.sf3d_forward(z["x"], *g, trap=True), z["b_tt"]) < 2e-5
+        assert rel_l2(oracle_mod.sf3d_backward(z["y"], *g), z["xt"]) < 2e-5
+        return
     nx, ny, nu = (int(v) for v in z["sizes"])
     dx, dy, du, lsd, lso = (float(v) for v in z["params"])
     ang = z["angles"]
@@ -136,3 +160,78 @@ def test_product_pmi_bit_identical_to_oracle(oracle_mod, case):
     g = oracle_mod.geometry(nx, ny, 1, nu, 1, dx, dy, 1, du, 1, lsd, lso, ang)
     assert np.array_equal(pm, g["pm"])
     assert np.array_equal(pmi, g["pmi"])
+
+
+@pytest.mark.parametrize("trap", [False, True])
+def test_sf3d_corrected_oracle_is_adjoint(oracle_mod, trap):
+    g = cone_case("tallz")
+    nx, ny, nz, nu, nv = g[:5]
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal(nx * ny * nz)
+    y = rng.standard_normal(len(g[-1]) * nu * nv)
+    lhs = np.dot(oracle_mod.sf3d_forward(x, *g, mode=1, trap=trap), y)
+    rhs = np.dot(x, oracle_mod.sf3d_backward(y, *g, mode=1, trap=trap))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-12
+
+
+def test_sf3d_reference_forward_sees_support_only(oracle_mod):
+    """layers/SF_projector.cu:190-221 never multiplies the footprint by the
+    voxel value: the replica's reference mode depends on the support only."""
+    g = cone_case("tallz")
+    nx, ny, nz = g[:3]
+    x = np.random.default_rng(4).random(nx * ny * nz) * (np.arange(nx * ny * nz) % 3 != 0)
+    b = oracle_mod.sf3d_forward(x, *g)
+    assert np.array_equal(b, oracle_mod.sf3d_forward((x != 0).astype(float), *g))
+    assert not np.array_equal(b, oracle_mod.sf3d_forward(x, *g, mode=1))
+
+
+# ---- exact FP64 projectors (the model-error references) --------------------
+
+@pytest.mark.parametrize("kind", ["b0", "b1"])
+def test_exact_matrix_line_integrals(oracle_mod, kind):
+    """Exact matrix times the point-sampled ellipse phantom approaches the
+    analytic ellipse line integrals as the pixels shrink."""
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case("snap")
+    M = oracle_mod.exact_fan2d_matrix(kind, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    assert M.shape == (len(ang) * nu, nx * ny) and np.all(M >= 0)
+    # a single pixel's projections sum over bins to about its area / du (B0)
+    # or the hat's integral dx dy / du (B1), magnified onto the detector
+    col = M[:, (nx // 2) * ny + ny // 2].reshape(len(ang), nu).sum(axis=1)
+    mag = lsd / lso
+    assert np.allclose(col * du / mag, dx * dy, rtol=2e-2)
+
+
+@pytest.mark.parametrize("kind", ["b0", "b1"])
+@pytest.mark.parametrize("case", ["tiny", "snap"])
+def test_formula_replica_model_error_vs_exact(oracle_mod, kind, case):
+    """The reference formulas (replicated in FP64) against the exact
+    bin-averaged line integrals of the same basis: the model error of the
+    footprint approximations, stated per basis."""
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case(case)
+    x = ellipse_phantom(nx, ny, dx, dy, seed=3).ravel()
+    M = oracle_mod.exact_fan2d_matrix(kind, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    b, _ = getattr(oracle_mod, f"{kind}_forward")(x, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    err = rel_l2(b, M @ x)
+    assert err < {"b0": 1e-3, "b1": 5e-4}[kind]
+
+
+def test_chord_simpson_3d(oracle_mod):
+    """Ref_project_Simpson restated: a uniform odd-sized cube seen along +x
+    carries its length on the central cell (the nine samples avoid voxel
+    faces); a row of voxels with an edge on the central ray covers a quarter
+    of the central cell, which the adaptive rule resolves and the reference's
+    fixed 3 x 3 rule does not (its centre sample lies on the edge)."""
+    from geometry_cases import LSD, LSO
+    n, d = 15, 2.0
+    g = (n, n, n, 24, 24, d, d, d, 3.0, 3.0, LSD, LSO, np.array([0.0]))
+    for adaptive in (False, True):
+        b = oracle_mod.ref_simpson_3d(np.ones(n ** 3), *g, adaptive=adaptive).reshape(24, 24)
+        assert abs(b[12, 12] - n * d) / (n * d) < 1e-3
+    g = cone_case("tiny")
+    nx, ny, nz, nu, nv = g[:5]
+    x = np.zeros((nz, ny, nx))
+    x[nz // 2, ny // 2, :] = 1
+    b = oracle_mod.ref_simpson_3d(x.ravel(), *g, adaptive=True, max_depth=6).reshape(len(g[-1]), nv, nu)
+    assert abs(b[0, nv // 2, nu // 2] - nx * g[5] / 4) / (nx * g[5] / 4) < 1e-2
+    b3 = oracle_mod.ref_simpson_3d(x.ravel(), *g).reshape(len(g[-1]), nv, nu)
+    assert b3[0, nv // 2, nu // 2] > 2 * b[0, nv // 2, nu // 2]

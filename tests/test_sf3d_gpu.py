@@ -1,0 +1,125 @@
+"""SF_projector (3D separable footprint) on the GPU: parity with the
+reference's SF layer and with the FP64 replica, adjoint of the corrected
+mode, and the documented behaviour of the reference mode."""
+import numpy as np
+import pytest
+
+from geometry_cases import cone_case, rel_l2
+from sgd_b200.phantom import ellipsoid_phantom
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL_REF = 1e-5      # against the reference kernels (both FP32)
+TOL_ORACLE = 2e-5   # against the FP64 replica of the same formulas
+TOL_ADJOINT = 1e-6
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+
+
+def make(case, mode=0, trap=False):
+    from sgd_b200.operators import SF_projector_operator
+    nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, ang = cone_case(case)
+    A = SF_projector_operator(nx, ny, nz, len(ang), nu, nv, dx, dy, dz, du, dv, lsd, lso, ang, mode=mode,
+                              trap_v=trap)
+    x = ellipsoid_phantom(nx, ny, nz, dx, dy, dz, seed=0).ravel()
+    return A, (nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, ang), x
+
+
+def _ref(g):
+    import reflib
+    if not reflib.available():
+        pytest.fail("reference library oracle/_ref/libnetwork.so not built (make -C oracle ref)")
+    return reflib.RefSF3D(*g)
+
+
+@pytest.mark.parametrize("case", ["small", "rect", "tallz"])
+@pytest.mark.parametrize("trap", [False, True])
+def test_forward_matches_reference_library(case, trap):
+    A, g, x = make(case, 0, trap)
+    b_ref = _ref(g).forward(x, trap=trap)
+    assert np.linalg.norm(b_ref) > 0
+    assert rel_l2(A.matvec(x), b_ref) < TOL_REF
+
+
+@pytest.mark.parametrize("case", ["small", "rect", "tallz"])
+def test_backward_matches_reference_library(case):
+    A, g, x = make(case, 0)
+    rng = np.random.default_rng(5)
+    y = rng.random(A.shape[0])
+    x_ref = _ref(g).backward(y)
+    assert np.linalg.norm(x_ref) > 0
+    assert rel_l2(A.rmatvec(y), x_ref) < TOL_REF
+
+
+@pytest.mark.parametrize("case", ["small", "tallz"])
+@pytest.mark.parametrize("mode,trap", [(0, False), (0, True), (1, False), (1, True)])
+def test_matches_fp64_oracle(oracle_mod, case, mode, trap):
+    A, g, x = make(case, mode, trap)
+    assert rel_l2(A.matvec(x), oracle_mod.sf3d_forward(x, *g, mode=mode, trap=trap)) < TOL_ORACLE
+    y = np.random.default_rng(6).random(A.shape[0])
+    assert rel_l2(A.rmatvec(y), oracle_mod.sf3d_backward(y, *g, mode=mode, trap=trap)) < TOL_ORACLE
+
+
+@pytest.mark.parametrize("case", ["small", "rect", "tallz"])
+@pytest.mark.parametrize("trap", [False, True])
+def test_corrected_mode_is_exact_adjoint(case, trap):
+    A, _, _ = make(case, 1, trap)
+    rng = np.random.default_rng(1234)
+    x = rng.standard_normal(A.shape[1])
+    y = rng.standard_normal(A.shape[0])
+    lhs = float(np.dot(A.matvec(x), y))
+    rhs = float(np.dot(x, A.rmatvec(y)))
+    assert abs(lhs - rhs) / abs(lhs) < TOL_ADJOINT
+
+
+def test_reference_forward_sees_support_only():
+    """The reference forward adds each non-zero voxel's footprint without its
+    value (layers/SF_projector.cu:190-221): scaling the volume, or replacing it
+    by the indicator of its support, leaves the projections unchanged."""
+    A, _, x = make("small", 0)
+    x = x + 0.25 * (x != 0)
+    b = A.matvec(x)
+    assert np.array_equal(b, A.matvec(3.0 * x))
+    assert np.array_equal(b, A.matvec((x != 0).astype(np.float64)))
+
+
+def test_corrected_forward_line_integral():
+    """Mode 1 on a uniform slab: a central ray through a 16 mm-thick cube of
+    ones, perpendicular to it, carries about its length."""
+    from sgd_b200.operators import SF_projector_operator
+    n, d = 16, 1.0
+    ang = np.array([0.0])
+    A = SF_projector_operator(n, n, n, 1, 32, 32, d, d, d, 0.5, 0.5, 1085.6, 595.0, ang, mode=1)
+    b = A.matvec(np.ones(n ** 3)).reshape(32, 32)
+    assert abs(b[16, 16] - n * d) / (n * d) < 0.05
+
+
+def test_device_entry_matches_host_entry():
+    from sgd_b200 import _lib
+    A, g, x = make("rect", 1)
+    L = _lib.lib()
+    nx, ny, nz, nu, nv = g[:5]
+    xd = torch.tensor(x, dtype=torch.float32, device="cuda").contiguous()
+    yd = torch.empty(len(g[-1]) * nu * nv, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    assert L.sgd_sf3d_forward_dev(A.cpointer, xd.data_ptr(), yd.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    assert rel_l2(yd.double().cpu().numpy(), A.matvec(x)) < 1e-6
+    xb = torch.empty_like(xd)
+    assert L.sgd_sf3d_backward_dev(A.cpointer, yd.data_ptr(), xb.data_ptr(), s) == 0
+    torch.cuda.synchronize()
+    assert rel_l2(xb.double().cpu().numpy(), A.rmatvec(yd.double().cpu().numpy())) < 1e-6
+
+
+def test_bad_arguments_raise():
+    from sgd_b200 import _lib
+    from sgd_b200.operators import SF_projector_operator
+    with pytest.raises(_lib.ProjectorError):
+        SF_projector_operator(0, 4, 4, 1, 4, 4, 1, 1, 1, 1, 1, 1085.6, 595.0, np.zeros(1))
+    with pytest.raises(_lib.ProjectorError):
+        SF_projector_operator(4, 4, 4, 1, 4, 4, 1, 1, 1, 1, 1, 1085.6, 595.0, np.zeros(1), mode=3)
