@@ -199,6 +199,71 @@ void sgd_sf3d_destroy(void* layer);
 int sgd_sf3d_forward_dev(void* layer, const float* d_vol, float* d_proj, void* stream);
 int sgd_sf3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void* stream);
 
+/* ---- batched B1: many slices per launch ----------------------------------- */
+
+/* New (the reference launches per view and per slice, layers/A_B1.cu:514-524):
+ * ns fan-beam slices, each with the arguments of b1_init (no dz/drho), in one
+ * persistent launch per direction.  Device arenas hold slice k's image at
+ * img_off[k] (layout i*ny + j) and its sinogram at sino_off[k] ([p][u]);
+ * sgd_b1_batch_offsets fills both arrays (ns + 1 entries each, the last is
+ * the arena length).  capture/replay record forward (img -> sino) and/or
+ * backward (sino_in -> img_out) into a CUDA graph on fixed arenas.  tune
+ * picks the launch shape (warps per forward item, views per staged chunk)
+ * from the cache file or by timing every variant (then appends it); returns
+ * 1 when loaded, 0 when measured, -1 on error. */
+void* sgd_b1_batch_create(int ns, const int* nx, const int* ny, const int* np, const int* nu, const double* dx,
+                          const double* dy, const double* du, const double* lsd, const double* lso,
+                          const double* const* angles);
+void sgd_b1_batch_destroy(void* batch);
+int sgd_b1_batch_offsets(void* batch, long long* img_off, long long* sino_off);
+int sgd_b1_batch_forward(void* batch, const float* d_img, float* d_sino, void* stream);
+int sgd_b1_batch_backward(void* batch, const float* d_sino, float* d_img, void* stream);
+int sgd_b1_batch_capture(void* batch, const float* d_img, float* d_sino, const float* d_sino_in, float* d_img_out);
+int sgd_b1_batch_replay(void* batch, void* stream);
+int sgd_b1_batch_tune(void* batch, const char* cache_path, int* fw, int* vc);
+int sgd_b1_batch_set_variant(void* batch, int fw, int vc);
+int sgd_b1_batch_status(void* batch);
+
+/* ---- ASD-POCS and its phantom simulator ----------------------------------- */
+
+/* New (the reference's optimizer/asd_pocs.cu is empty): ASD-POCS (Sidky and
+ * Pan 2008: SART step, positivity, adaptive TV descent) over the slices of a
+ * batch, every scalar per image on the device, one CUDA graph per iteration.
+ * bind() takes the iterate and data arenas (the batch's layout) and the image
+ * shapes and resets the adaptive state; history() returns (|Ax-b|, |dx_SART|,
+ * |dx_TV|) per iteration and image for the first hist_cap iterations. */
+void* sgd_asd_create(void* batch, float beta, float beta_red, float alpha, float alpha_red, float r_max, float eps,
+                     int ng);
+void sgd_asd_destroy(void* h);
+int sgd_asd_bind(void* h, float* d_x, const float* d_b, const int* nx, const int* ny, int hist_cap);
+int sgd_asd_reset(void* h);
+int sgd_asd_run(void* h, int iters, void* stream);
+int sgd_asd_history(void* h, float* out, int iters);
+/* New: fan-beam sinograms of ellipse phantoms (closed-form chords averaged over
+ * `sub` rays per bin); with i0 > 0, Poisson counts and b = 100 ln(i0/counts),
+ * the noise model of python/FORBILD.py:355-390. */
+int sgd_ellipse_sinograms(const double* ell, int nell, int ni, int np, int nu, double du, double lsd, double lso,
+                          const double* angles, int sub, double i0, unsigned long long seed, float* d_out,
+                          void* stream);
+
+/* ---- warm-start CNN kernels ----------------------------------------------- */
+
+/* New (no reference counterpart; layers/layer.hh:9-17 is an MLP scaffold):
+ * 3x3 convolution, zero padding, NCHW FP32 activations, BF16 weights
+ * [Cout][Cin][3][3], FP32 accumulation; input gradient (scratch: Cin*Cout*9
+ * BF16), weight and bias gradients (accumulated into), ReLU backward, MSE
+ * gradient, Adam on FP32 master weights with a BF16 copy. */
+int sgd_conv3x3_forward(const float* in, const void* w_bf16, const float* bias, float* out, int N, int Cin, int Cout,
+                        int H, int W, int relu, void* stream);
+int sgd_conv3x3_backward_data(const float* gout, const void* w_bf16, void* scratch_bf16, float* gin, int N, int Cin,
+                              int Cout, int H, int W, void* stream);
+int sgd_conv3x3_backward_weight(const float* in, const float* gout, float* gw, float* gbias, int N, int Cin, int Cout,
+                                int H, int W, void* stream);
+int sgd_relu_backward(float* g, const float* out, long long n, void* stream);
+int sgd_mse_grad(const float* y, const float* t, float* g, long long n, double* d_loss, void* stream);
+int sgd_adam_step(float* w, void* w_bf16, const float* g, float* m, float* v, long long n, float lr, float b1,
+                  float b2, float eps, int step, void* stream);
+
 /* ---- system matrices ------------------------------------------------------ */
 
 /* Replace pixel_matrix_generation / bilinear_matrix_generation

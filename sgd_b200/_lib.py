@@ -61,6 +61,16 @@ def lib() -> ctypes.CDLL:
     for n in ("sgd_sf3d_forward_dev", "sgd_sf3d_backward_dev"):
         getattr(L, n).restype = _i
         getattr(L, n).argtypes = [_vp, _vp, _vp, _vp]
+    L.sgd_b1_batch_create.restype = _vp
+    L.sgd_b1_batch_create.argtypes = [_i] + [_vp] * 10
+    L.sgd_b1_batch_destroy.restype = None
+    L.sgd_b1_batch_destroy.argtypes = [_vp]
+    for n, a in (("offsets", [_vp, _vp, _vp]), ("forward", [_vp] * 4), ("backward", [_vp] * 4),
+                 ("capture", [_vp] * 5), ("replay", [_vp, _vp]), ("tune", [_vp, ctypes.c_char_p, _vp, _vp]),
+                 ("set_variant", [_vp, _i, _i]), ("status", [_vp])):
+        f = getattr(L, f"sgd_b1_batch_{n}")
+        f.restype = _i
+        f.argtypes = a
     gen = [_i] * 4 + [_d] * 5 + [_dp, _i]
     for n in ("pixel_matrix_generation", "bilinear_matrix_generation"):
         getattr(L, n).restype = _i

@@ -1,0 +1,273 @@
+"""ASD-POCS reconstruction on the GPU, plain and with the CNN warm start.
+
+The reference's optimizer/asd_pocs.cu is empty; this module drives the
+library's ASD-POCS (``sgd_asd_*``: SART step, positivity, adaptive TV descent,
+every scalar on the device, one CUDA graph per iteration) over a batch of
+fan-beam B1 slices, and the seeded phantom simulator (``sgd_ellipse_sinograms``:
+closed-form ellipse line integrals averaged over the bin, Poisson counts,
+b = 100 ln(I0 / counts) as python/FORBILD.py:355-390).
+
+Learned warm start: plain ASD-POCS run for ``k_in`` iterations gives the
+network's input; the network (sgd_b200.cnn.WarmStartCNN) is trained to map it
+to the converged plain reconstruction; reconstruction then continues with
+ASD-POCS from the network's output.  Plain ASD-POCS remains the fallback.
+
+    python -m sgd_b200.asd [--images 64] [--train 2000] [--iters 100]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .batch import B1Batch
+from .phantom import ellipse_phantom, random_ellipses
+
+_vp = ctypes.c_void_p
+LSD, LSO = 1085.6, 595.0
+
+
+def _declare(L):
+    if getattr(L, "_asd_declared", False):
+        return
+    i, f, d = ctypes.c_int, ctypes.c_float, ctypes.c_double
+    L.sgd_asd_create.restype = _vp
+    L.sgd_asd_create.argtypes = [_vp, f, f, f, f, f, f, i]
+    L.sgd_asd_destroy.restype = None
+    L.sgd_asd_destroy.argtypes = [_vp]
+    L.sgd_asd_bind.restype = i
+    L.sgd_asd_bind.argtypes = [_vp, _vp, _vp, _vp, _vp, i]
+    L.sgd_asd_reset.restype = i
+    L.sgd_asd_reset.argtypes = [_vp]
+    L.sgd_asd_run.restype = i
+    L.sgd_asd_run.argtypes = [_vp, i, _vp]
+    L.sgd_asd_history.restype = i
+    L.sgd_asd_history.argtypes = [_vp, _vp, i]
+    L.sgd_ellipse_sinograms.restype = i
+    L.sgd_ellipse_sinograms.argtypes = [_vp, i, i, i, i, d, d, d, _vp, i, d, ctypes.c_ulonglong, _vp, _vp]
+    L._asd_declared = True
+
+
+class Geometry:
+    """A square fan-beam slice: n x n pixels over a 256 mm field, `views`
+    angles over 2 pi, ceil(1.44 n) bins of 1 mm (the batched workload's rule)."""
+
+    def __init__(self, n=256, views=120, lsd=LSD, lso=LSO):
+        self.n, self.views, self.lsd, self.lso = n, views, lsd, lso
+        self.d = 256.0 / n
+        self.nu = math.ceil(1.44 * n)
+        self.du = 1.0
+        self.angles = 2 * np.pi * np.arange(views) / views
+
+    def slice(self):
+        return (self.n, self.n, self.nu, self.d, self.d, self.du, self.lsd, self.lso, self.angles)
+
+
+def simulate(geo, seeds, i0=1e5, sub=8, noise_seed=0):
+    """(truth (N, n, n) float32 on the device, sinograms (N, views, nu) float32
+    on the device, ellipses (N, 10, 6)).  Truth = the phantom sampled at
+    pixel centres, the basis coefficients the reconstruction estimates."""
+    L = _lib.lib()
+    _declare(L)
+    radius = 0.5 * geo.n * geo.d
+    ell = np.ascontiguousarray(np.stack([random_ellipses(s, 10, radius) for s in seeds]), dtype=np.float64)
+    sino = torch.empty((len(seeds), geo.views, geo.nu), dtype=torch.float32, device="cuda")
+    ang = np.ascontiguousarray(geo.angles, dtype=np.float64)
+    _lib.check(L.sgd_ellipse_sinograms(ell.ctypes.data, 10, len(seeds), geo.views, geo.nu, geo.du, geo.lsd, geo.lso,
+                                       ang.ctypes.data, sub, float(i0), int(noise_seed), sino.data_ptr(),
+                                       torch.cuda.current_stream().cuda_stream), "sgd_ellipse_sinograms")
+    truth = np.stack([ellipse_phantom(geo.n, geo.n, geo.d, geo.d, seed=s) for s in seeds]).astype(np.float32)
+    return torch.tensor(truth, device="cuda"), sino, ell
+
+
+class ASDPOCS:
+    """ASD-POCS over `count` slices of one geometry (Sidky and Pan 2008
+    parameters by default)."""
+
+    def __init__(self, geo, count, beta=1.0, beta_red=0.995, alpha=0.2, alpha_red=0.95, r_max=0.95, eps=0.0,
+                 ng=20):
+        self.L = _lib.lib()
+        _declare(self.L)
+        self.geo, self.count = geo, count
+        self.batch = B1Batch([geo.slice()] * count)
+        self.h = self.L.sgd_asd_create(self.batch.handle, beta, beta_red, alpha, alpha_red, r_max, eps, ng)
+        if not self.h:
+            raise _lib.ProjectorError(f"sgd_asd_create: {_lib.last_error()}")
+        self.x = self.batch.image_arena()
+        self.b = self.batch.sinogram_arena()
+        self._bound = False
+        self.hist_cap = 0
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h:
+            self.L.sgd_asd_destroy(h)
+            self.h = None
+
+    def images(self):
+        return self.x.view(self.count, self.geo.n, self.geo.n)
+
+    def set_data(self, sino, x0=None, hist_cap=0):
+        """Data (count, views, nu) and the starting image (zeros by default);
+        resets the adaptive state."""
+        self.b.copy_(sino.reshape(-1))
+        if x0 is None:
+            self.x.zero_()
+        else:
+            self.x.copy_(x0.reshape(-1))
+        torch.cuda.synchronize()
+        if not self._bound or hist_cap != self.hist_cap:
+            n = np.full(self.count, self.geo.n, dtype=np.int32)
+            _lib.check(self.L.sgd_asd_bind(self.h, self.x.data_ptr(), self.b.data_ptr(), n.ctypes.data, n.ctypes.data,
+                                           hist_cap), "sgd_asd_bind")
+            self._bound = True
+            self.hist_cap = hist_cap
+        else:
+            _lib.check(self.L.sgd_asd_reset(self.h), "sgd_asd_reset")
+
+    def run(self, iters):
+        _lib.check(self.L.sgd_asd_run(self.h, iters, torch.cuda.current_stream().cuda_stream), "sgd_asd_run")
+
+    def history(self, iters):
+        """(iters, count, 3): |Ax - b| entering each SART step, |dx_SART|, |dx_TV|."""
+        out = np.zeros((iters, self.count, 3), dtype=np.float32)
+        _lib.check(self.L.sgd_asd_history(self.h, out.ctypes.data, iters), "sgd_asd_history")
+        return out
+
+    def status(self):
+        self.batch.status()
+
+
+def rmse(x, truth):
+    """Per-image RMSE against the phantom, FP64."""
+    d = (x.double() - truth.double()).reshape(x.shape[0], -1)
+    return torch.sqrt((d * d).mean(dim=1))
+
+
+def timed(fn):
+    """GPU milliseconds of fn() by CUDA events on the current stream."""
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def plain_curve(solver, sino, truth, iters, every=5):
+    """(iterations, GPU ms of the iterations alone, mean RMSE) after each block
+    of `every` iterations; the RMSE evaluation is outside the timed region."""
+    solver.set_data(sino)
+    curve, ms, done = [], 0.0, 0
+    while done < iters:
+        k = min(every, iters - done)
+        ms += timed(lambda: solver.run(k))
+        done += k
+        curve.append((done, ms, float(rmse(solver.images(), truth).mean())))
+    return curve
+
+
+def make_pairs(geo, seeds, iters, k_in, count=64, noise_seed=0):
+    """Training pairs from plain ASD-POCS for the phantoms `seeds`, `count` at
+    a time: (iterate after k_in iterations, iterate after `iters`)."""
+    solver = ASDPOCS(geo, count)
+    xs, ts = [], []
+    for s0 in range(0, len(seeds), count):
+        chunk = list(seeds[s0:s0 + count])
+        while len(chunk) < count:
+            chunk.append(chunk[-1])
+        _, sino, _ = simulate(geo, chunk, noise_seed=noise_seed + s0)
+        solver.set_data(sino)
+        solver.run(k_in)
+        xs.append(solver.images().clone())
+        solver.run(iters - k_in)
+        ts.append(solver.images().clone())
+    solver.status()
+    n = len(seeds)
+    return torch.cat(xs)[:n], torch.cat(ts)[:n]
+
+
+def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0):
+    """Mean per-sample loss per epoch."""
+    gen = torch.Generator().manual_seed(seed)
+    n = x.shape[0]
+    losses = []
+    for _ in range(epochs):
+        perm = torch.randperm(n, generator=gen)
+        tot = 0.0
+        for k in range(0, n - batch + 1, batch):
+            idx = perm[k:k + batch].cuda()
+            loss = net.train_step(x[idx].unsqueeze(1), t[idx].unsqueeze(1), lr=lr)
+            tot += float(loss)
+        losses.append(tot / n)
+    return losses
+
+
+def learned_run(solver, net, sino, truth, k_in, target, max_iters, every=1):
+    """k_in plain iterations, the network, then ASD-POCS until the mean RMSE
+    reaches `target`: (iterations after the network, GPU ms, curve)."""
+    solver.set_data(sino)
+    ms = timed(lambda: solver.run(k_in))
+    x = solver.images().unsqueeze(1).clone()
+    out = {}
+    ms += timed(lambda: out.setdefault("y", net.forward(x)))
+    solver.set_data(sino, x0=torch.clamp(out["y"], min=0.0))
+    curve = [(0, ms, float(rmse(solver.images(), truth).mean()))]
+    done = 0
+    while done < max_iters and curve[-1][2] > target:
+        ms += timed(lambda: solver.run(every))
+        done += every
+        curve.append((done, ms, float(rmse(solver.images(), truth).mean())))
+    return done, ms, curve
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--views", type=int, default=120)
+    ap.add_argument("--images", type=int, default=64)
+    ap.add_argument("--train", type=int, default=2000)
+    ap.add_argument("--iters", type=int, default=100)
+    ap.add_argument("--k-in", type=int, default=5)
+    ap.add_argument("--epochs", type=int, default=8)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    args = ap.parse_args()
+    from .cnn import WarmStartCNN
+    geo = Geometry(args.n, args.views)
+    t0 = time.perf_counter()
+    xs, ts = make_pairs(geo, list(range(1000, 1000 + args.train)), args.iters, args.k_in)
+    t_pairs = time.perf_counter() - t0
+    net = WarmStartCNN(seed=0)
+    t0 = time.perf_counter()
+    losses = train(net, xs, ts, epochs=args.epochs, batch=args.batch, lr=args.lr)
+    t_train = time.perf_counter() - t0
+    del xs, ts
+    truth, sino, _ = simulate(geo, list(range(args.images)), noise_seed=999)
+    solver = ASDPOCS(geo, args.images)
+    plain = plain_curve(solver, sino, truth, args.iters)
+    target = plain[-1][2]
+    it_l, ms_l, curve_l = learned_run(solver, net, sino, truth, args.k_in, target, args.iters)
+    solver.status()
+    line = {
+        "workload": f"{args.images} fan-beam phantoms {args.n}^2 at {geo.d} mm, {args.views} views, {geo.nu} bins, "
+                    f"Poisson I0=1e5; plain ASD-POCS {args.iters} iterations vs CNN warm start after {args.k_in}",
+        "plain": {"iters": args.iters, "gpu_ms": plain[-1][1], "rmse": target, "curve": plain},
+        "learned": {"iters_after_net": it_l, "gpu_ms": ms_l, "rmse": curve_l[-1][2], "curve": curve_l,
+                    "reached": curve_l[-1][2] <= target},
+        "time_ratio": ms_l / plain[-1][1],
+        "training": {"pairs": args.train, "epochs": args.epochs, "loss": losses, "pairs_s": t_pairs,
+                     "train_s": t_train},
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

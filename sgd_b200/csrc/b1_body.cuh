@@ -1,0 +1,266 @@
+// Bodies of the B1 projection kernels, shared by the single-geometry kernels
+// (b1.cu) and the persistent batched kernels (b1_batch.cu).
+//
+//   b1_forward_row   detector-driven: one warp per (view, bin).  Lanes split
+//                    the lines (major axis) the bin's ray strip crosses; each
+//                    lane evaluates the footprint of the few pixels of its line
+//                    inside the strip, and the warp reduces with shuffles.  The
+//                    sinogram value is written once, no atomics.
+//   b1_back_tile     voxel-driven: one thread per pixel of a 32x8 tile.  Per
+//                    chunk of VC views the CTA stages the bin window its tile
+//                    projects onto in shared memory: the 64-byte footprint
+//                    records by TMA bulk copies completed on an mbarrier
+//                    (double-buffered, the next chunk in flight while this one
+//                    is evaluated), the sinogram values by plain loads.  Each
+//                    thread accumulates over all views in registers and writes
+//                    its pixel once, no atomics.
+//
+// Reference: layers/A_B1.cu:62-208 (forward, one launch per view, FP64
+// atomics) and :211-353 (backward).
+#pragma once
+
+#include <cstdint>
+
+#include "b1_kernels.cuh"
+#include "fan_geometry.h"
+#include "hom.cuh"
+#include "tma.cuh"
+
+namespace sgd {
+
+constexpr int kBackTI = 8;    // tile extent along i (x)
+constexpr int kBackTJ = 32;   // tile extent along j (y): contiguous in memory
+constexpr int kBackThreads = kBackTI * kBackTJ;
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+// 2 mbarriers | 3 x VC windows | 3 x VC homographies, then the staged records
+template <int VC>
+__host__ __device__ constexpr int b1_header_bytes() {
+    return 16 + 3 * VC * 8 + 3 * VC * 32;
+}
+
+template <int VC>
+__host__ __device__ constexpr size_t b1_back_smem(int wcap) {
+    return b1_header_bytes<VC>() + (size_t)2 * VC * wcap * (sizeof(B1Bin) + sizeof(float));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Records are float4 chunks laid out [view][chunk][bin] (fan_geometry.h).
+__device__ __forceinline__ B1Bin load_bin(const float4* rec, int p, int u, int nu) {
+    const float4* q = rec + (size_t)p * 4 * nu + u;
+    return B1Bin{__ldg(q), __ldg(q + nu), __ldg(q + 2 * nu), __ldg(q + 3 * nu)};
+}
+
+// Candidate minor indices of major line m: the strip between the edge rays over
+// the lines m-1..m+1 a pixel's support covers, widened by the +-1 pixel support
+// along the minor axis.
+__device__ __forceinline__ void strip_span(const float4& st, float aa, float ab, float fm, int nmin, int& nlo,
+                                           int& nhi) {
+    const float fa = fmaf(st.y, fm, st.x);
+    const float fb = fmaf(st.w, fm, st.z);
+    const float lo = fminf(fa - aa, fb - ab) - 1.0f;
+    const float hi = fmaxf(fa + aa, fb + ab) + 1.0f;
+    nlo = max(0, (int)ceilf(lo));
+    nhi = min(nmin - 1, (int)floorf(hi));
+}
+
+template <int N>
+__device__ __forceinline__ int pick(const int (&a)[N], int v) {
+    int r = a[0];
+#pragma unroll
+    for (int k = 1; k < N; ++k) r = (v == k) ? a[k] : r;
+    return r;
+}
+
+// Sinogram value of row gw = p * nu + u.  img (i, j) at img[i * ny + j];
+// imgT (i, j) at imgT[j * nx + i].
+__device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, const float* __restrict__ strip,
+                                               const float* __restrict__ img, const float* __restrict__ imgT,
+                                               float* __restrict__ sino, int nx, int ny, int nu, float dxdy,
+                                               long long gw, int lane) {
+    const int p = (int)(gw / nu), u = (int)(gw - (long long)p * nu);
+    const B1Bin r = load_bin(rec, p, u, nu);
+    const float4 st = __ldg(reinterpret_cast<const float4*>(strip + gw * kStripRec));
+    const bool ydom = __ldg(strip + gw * kStripRec + 4) > 0.5f;
+    const float aa = fabsf(st.y), ab = fabsf(st.w);
+
+    // FP32 sums within a line (a few terms), FP64 across lines and lanes: the
+    // forward and back kernels then round the same products to within FP64
+    // accumulation error, which the dot-product adjoint test needs.
+    double acc = 0.0;
+    if (ydom) {
+        // rows j = m, candidate columns i = n; the j terms are hoisted
+        for (int m = lane; m < ny; m += 32) {
+            const float fm = (float)m;
+            int nlo, nhi;
+            strip_span(st, aa, ab, fm, nx, nlo, nhi);
+            const float ia = b1_xa_inner(fm, r), ib = b1_xb_inner(fm, r);
+            float row = 0.f, fn = (float)nlo;
+            const float* sp = img + (size_t)nlo * ny + m;
+            for (int n = nlo; n <= nhi; ++n, fn += 1.0f, sp += ny) {
+                const float conv = b1_conv_x(b1_xa(fn, ia, r), b1_xb(fn, ib, r), r);
+                if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
+            }
+            acc += (double)row;
+        }
+    } else {
+        // columns i = m, candidate rows j = n
+        for (int m = lane; m < nx; m += 32) {
+            const float fm = (float)m;
+            int nlo, nhi;
+            strip_span(st, aa, ab, fm, ny, nlo, nhi);
+            float row = 0.f, fn = (float)nlo;
+            const float* sp = imgT + (size_t)nlo * nx + m;
+            for (int n = nlo; n <= nhi; ++n, fn += 1.0f, sp += nx) {
+                const float conv = b1_conv(fm, fn, r);
+                if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
+            }
+            acc += (double)row;
+        }
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) sino[gw] = (float)acc * dxdy;
+}
+
+// Back projection of the 32x8 tile at (i0, j0).  twin[p] = (lo, hi): bins of
+// view p the tile's pixels can touch (host-computed, conservative; fits in
+// wcap).  The CTA's two mbarriers (at the start of smem) are initialised by
+// the caller; use0/use1 count the phases barriers 0/1 completed before this
+// tile, so that a persistent CTA can run many tiles on the same barriers.
+// Returns false, with *err set and the tile unwritten, when a staged chunk
+// never arrived (bounded wait).
+template <int VC>
+__device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, const BinHomography* __restrict__ hom,
+                                             const int2* __restrict__ twin, const float* __restrict__ sino,
+                                             float* __restrict__ img, int nx, int ny, int np, int nu, int wcap,
+                                             float dxdy, int* __restrict__ err, int i0, int j0, unsigned char* smem,
+                                             volatile int& s_abort, uint32_t& use0, uint32_t& use1) {
+    constexpr int kHeader = b1_header_bytes<VC>();
+    static_assert(kHeader % 16 == 0, "staged records must start 16-byte aligned");
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem);           // [2]
+    int* win = reinterpret_cast<int*>(smem + 16);                   // [3][VC][2]
+    float* hs = reinterpret_cast<float*>(smem + 16 + 3 * VC * 8);  // [3][VC][8]
+    float4* srec = reinterpret_cast<float4*>(smem + kHeader);      // [2][VC][4 chunks][wcap]
+    float* ssino = reinterpret_cast<float*>(srec + 2 * VC * 4 * wcap);  // [2][VC][wcap]
+
+    // each warp covers an 8 (j) x 4 (i) block of the 32 x 8 tile, so that its
+    // lanes read few distinct bins of a view
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int i = i0 + 4 * (w >> 2) + (l >> 3), j = j0 + 8 * (w & 3) + (l & 7);
+    const float fi = (float)i, fj = (float)j;
+    const int nchunks = (np + VC - 1) / VC;
+    auto parity = [&](int c) { return (((c & 1) ? use1 : use0) + (uint32_t)(c >> 1)) & 1u; };
+
+    // stage chunk c: windows and homographies (thread 0, read after the next
+    // barrier), footprint records by TMA (thread 0), sinogram values (all)
+    auto stage = [&](int c) {
+        const int st = c & 1, slot = c % 3;
+        if (tid == 0) {
+            uint32_t bytes = 0;
+            for (int v = 0; v < VC; ++v) {
+                const int p = c * VC + v;
+                int2 lh = make_int2(0, -1);
+                if (p < np) {
+                    lh = __ldg(twin + p);
+                    const BinHomography H = hom[p];
+                    float* h = hs + (slot * VC + v) * 8;
+                    h[0] = H.n0; h[1] = H.n1; h[2] = H.n2; h[3] = H.d0; h[4] = H.d1; h[5] = H.d2;
+                }
+                win[(slot * VC + v) * 2] = lh.x;
+                win[(slot * VC + v) * 2 + 1] = lh.y;
+                if (lh.y >= lh.x) bytes += (uint32_t)(lh.y - lh.x + 1) * sizeof(B1Bin);
+            }
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(&bars[st], bytes);
+            for (int v = 0; v < VC; ++v) {
+                const int lo = win[(slot * VC + v) * 2], W = win[(slot * VC + v) * 2 + 1] - lo + 1;
+                if (W > 0)
+                    for (int q = 0; q < 4; ++q)
+                        bulk_copy_g2s(srec + ((st * VC + v) * 4 + q) * wcap,
+                                      rec + ((size_t)(c * VC + v) * 4 + q) * nu + lo, (uint32_t)W * 16u, &bars[st]);
+            }
+        }
+        for (int v = 0; v < VC; ++v) {
+            const int p = c * VC + v;
+            if (p >= np) break;
+            const int2 lh = __ldg(twin + p);
+            const float* sp = sino + (size_t)p * nu + lh.x;
+            float* dp = ssino + (st * VC + v) * wcap;
+            for (int k = tid; k <= lh.y - lh.x; k += kBackThreads) dp[k] = __ldg(sp + k);
+        }
+    };
+
+    __syncthreads();  // the previous tile's last chunk is fully consumed
+    stage(0);
+
+    double acc = 0.0;  // FP32 within a chunk (a few tens of terms), FP64 across chunks
+    int c = 0;
+    for (; c < nchunks; ++c) {
+        __syncthreads();  // chunk c's windows and sinogram visible; chunk c-1 fully consumed
+        if (s_abort) break;
+        if (c + 1 < nchunks) stage(c + 1);
+        const int st = c & 1, slot = c % 3;
+        if (!mbar_wait_bounded(&bars[st], parity(c), kWaitLimit)) {
+            s_abort = 1;
+            atomicExch(err, 1);
+            continue;
+        }
+        if (i >= nx || j >= ny) continue;
+        // this pixel's bins in each view of the chunk, then one flat loop over
+        // all of them: lanes run nearly equal trip counts
+        int ulo[VC], uhi[VC], roff[VC], soff[VC];
+        int total = 0;
+#pragma unroll
+        for (int v = 0; v < VC; ++v) {
+            const int lo = win[(slot * VC + v) * 2], hi = win[(slot * VC + v) * 2 + 1];
+            int a = 0, b = -1;
+            if (hi >= lo) {
+                box_bins(hs + (slot * VC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, a, b);
+                a = max(a, lo);
+                b = min(b, hi);
+            }
+            ulo[v] = a;
+            uhi[v] = b;
+            roff[v] = (st * VC + v) * 4 * wcap - lo;
+            soff[v] = (st * VC + v) * wcap - lo;
+            total += max(0, b - a + 1);
+        }
+        float csum = 0.f;
+        int v = 0, u = ulo[0], ue = uhi[0], ro = roff[0], so = soff[0];
+        for (int k = 0; k < total; ++k) {
+            while (u > ue) {
+                ++v;
+                u = pick(ulo, v);
+                ue = pick(uhi, v);
+                ro = pick(roff, v);
+                so = pick(soff, v);
+            }
+            const float4* rb = srec + ro + u;
+            const B1Bin r{rb[0], rb[wcap], rb[2 * wcap], rb[3 * wcap]};
+            const float conv = b1_conv(fi, fj, r);
+            if (conv > kConvEps) csum = fmaf(conv, ssino[so + u], csum);
+            ++u;
+        }
+        acc += (double)csum;
+    }
+    if (c < nchunks) {
+        // a staged chunk never arrived: wait (bounded) for the copies still in
+        // flight into this CTA's shared memory, then leave the tile unwritten
+        if (tid == 0) {
+            mbar_wait_bounded(&bars[c & 1], parity(c), kWaitLimit);
+            if (c + 1 < nchunks) mbar_wait_bounded(&bars[(c + 1) & 1], parity(c + 1), kWaitLimit);
+        }
+        return false;
+    }
+    use0 += (uint32_t)((nchunks + 1) >> 1);
+    use1 += (uint32_t)(nchunks >> 1);
+    if (i < nx && j < ny) img[(size_t)i * ny + j] = (float)acc * dxdy;
+    return true;
+}
+
+}  // namespace sgd

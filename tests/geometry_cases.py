@@ -50,7 +50,7 @@ def cone_case(name):
     if name == "tiny":    # 16^3 at 2 mm, 8 views, 24 x 20 detector at 3 mm (golden vectors)
         return 16, 16, 16, 24, 20, 2.0, 2.0, 2.0, 3.0, 3.0, LSD, LSO, 2 * np.pi * np.arange(8) / 8
     if name == "tallz":   # 80 slices (two 64-slice chunks) past both detector edges, narrow detector
-        return 12, 10, 80, 16, 20, 2.0, 2.0, 2.0, 3.0, 3.0, LSD, LSO, np.array([0.1, 1.3, np.pi / 4, 2.9, 4.4, 5.7])
+        return 16, 8, 80, 16, 20, 2.0, 2.0, 2.0, 3.0, 3.0, LSD, LSO, np.array([0.1, 1.3, np.pi / 4, 2.9, 4.4, 5.7])
     if name == "c5":      # 256^3 at 1 mm, 360 views over 2 pi, 384 x 384 at 1.5 mm
         return 256, 256, 256, 384, 384, 1.0, 1.0, 1.0, 1.5, 1.5, LSD, LSO, 2 * np.pi * np.arange(360) / 360
     raise KeyError(name)

@@ -142,6 +142,7 @@ class RefSF3D:
         L.ref_sf3d_backward.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.ref_sf3d_destroy.argtypes = [ctypes.c_void_p]
         self.n = nx * ny * nz
+        self.nx, self.ny = nx, ny
         self.m = len(angles) * nu * nv
         self._ang = np.ascontiguousarray(angles, dtype=np.float64)
         self.h = L.ref_sf3d_init(nx, ny, nz, len(angles), nu, nv, dx, dy, dz, du, dv, lsd, lso,
@@ -160,6 +161,12 @@ class RefSF3D:
         return b
 
     def backward(self, y):
+        # SF_backproject has no bounds check on ix, iy (layers/SF_projector.cu:
+        # 237-356): with nx or ny not a multiple of its 8 x 8 blocks, threads
+        # past the edge add into other voxels and, in the last slice, past the
+        # end of the volume.  Only whole blocks are run here.
+        if self.nx % 8 or self.ny % 8:
+            raise ValueError("the reference SF back projection writes out of bounds unless nx, ny are multiples of 8")
         y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
         x = np.zeros(self.n)
         assert lib().ref_sf3d_backward(self.h, y.ctypes.data_as(_dp), x.ctypes.data_as(_dp)) == 0

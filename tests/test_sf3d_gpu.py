@@ -46,8 +46,10 @@ def test_forward_matches_reference_library(case, trap):
     assert rel_l2(A.matvec(x), b_ref) < TOL_REF
 
 
-@pytest.mark.parametrize("case", ["small", "rect", "tallz"])
+@pytest.mark.parametrize("case", ["small", "tallz"])
 def test_backward_matches_reference_library(case):
+    """Whole 8 x 8 blocks only: the reference's back kernel has no bounds
+    check (reflib.RefSF3D.backward)."""
     A, g, x = make(case, 0)
     rng = np.random.default_rng(5)
     y = rng.random(A.shape[0])
