@@ -1,17 +1,13 @@
 """Warm-start CNN kernels (sgd_b200/csrc/cnn.cu) against the FP64 CPU oracle:
 convolution forward, input and weight gradients, the whole network's
 parameter gradients, and a training loop that lowers the loss."""
-import os
-import sys
-
 import numpy as np
 import pytest
 
+from oracle import cnn_oracle
+
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
-
-sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle"))
-import cnn_oracle  # noqa: E402
 
 
 @pytest.fixture(scope="module", autouse=True)
