@@ -122,6 +122,12 @@ int sgd_b0_forward_dev(void* layer, const float* d_img, float* d_sino, void* str
 int sgd_b0_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
 unsigned long long sgd_b0_count(void* layer);
 
+/* New (the reference has only point-source geometry, utils/geo.cu:234): B0 in
+ * parallel-beam geometry.  View angle beta: rays along (cos beta, sin beta),
+ * detector axis (-sin beta, cos beta) through the isocentre, nu bins of pitch
+ * du centred on it.  The handle takes the b0_* and sgd_b0_* calls above. */
+void* sgd_b0_parallel_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double* angles);
+
 /* ---- H0 / Hl hexagonal lattices, 2D fan beam --------------------------------- */
 
 /* Replace h0_init / hl_init (layers/A_H0.cu:555-563, layers/A_Hl.cu:569-577):

@@ -38,6 +38,7 @@ def lib():
         L.oracle_b1_3d_backward.restype = None
         L.oracle_sf3d_forward.restype = None
         L.oracle_exact_fan2d_matrix.restype = None
+        L.oracle_exact_parallel_matrix.restype = None
         L.oracle_matrix_generation.restype = ctypes.c_longlong
         L.oracle_ref_simpson_3d.restype = None
         L.oracle_sf3d_backward.restype = None
@@ -276,3 +277,14 @@ def matrix_generation(kind, np_, nu, nx, ny, dx, dy, du, lsd, lso, precision=1):
                                rows.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
                                cols.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), _p(vals))
     return rows, cols, vals
+
+
+def exact_parallel_matrix(kind, nx, ny, nu, dx, dy, du, angles, tol=1e-10):
+    """Dense exact FP64 parallel-beam system matrix (np*nu, nx*ny) of the
+    pixel-indicator ("b0") or bilinear ("b1") basis, columns ix*ny + iy."""
+    angles = _c(angles)
+    M = np.zeros(len(angles) * nu * nx * ny)
+    d = ctypes.c_double
+    lib().oracle_exact_parallel_matrix({"b0": 0, "b1": 1}[kind], nx, ny, len(angles), nu, d(dx), d(dy), d(du),
+                                       _p(angles), d(tol), _p(M))
+    return M.reshape(len(angles) * nu, nx * ny)

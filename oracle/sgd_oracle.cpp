@@ -1170,6 +1170,43 @@ void oracle_exact_fan2d_matrix(int kind, int nx, int ny, int np, int nu, double 
         }
 }
 
+// Exact parallel-beam system matrix of the pixel-indicator (kind 0) or
+// bilinear (kind 1) basis, dense, M[(p*nu + u)*(nx*ny) + ix*ny + iy]: for
+// view angle beta the rays run along (cos beta, sin beta) and bin u covers
+// the lateral coordinate s in [(u - nu/2) du, (u - nu/2 + 1) du] along
+// (-sin beta, cos beta); the line integral of the basis function averaged
+// over the bin by adaptive Simpson (tolerance `tol` relative).  The
+// reference has no parallel geometry; this is the checker of the
+// parallel-beam B0 layer.
+void oracle_exact_parallel_matrix(int kind, int nx, int ny, int np, int nu, double dx, double dy, double du,
+                                  const double* angles, double tol, double* M) {
+    const size_t ncol = (size_t)nx * ny;
+    std::memset(M, 0, sizeof(double) * ncol * np * nu);
+    const double reach = kind == 0 ? 0.5 * std::hypot(dx, dy) : std::hypot(dx, dy);
+    const double far = 1e4 * (nx * dx + ny * dy);
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int p = 0; p < np; ++p)
+        for (int u = 0; u < nu; ++u) {
+            const double rx = std::cos(angles[p]), ry = std::sin(angles[p]), ex = -ry, ey = rx;
+            const double s0 = (u - 0.5 * nu) * du, s1 = s0 + du;
+            double* row = M + ((size_t)p * nu + u) * ncol;
+            for (int ix = 0; ix < nx; ++ix)
+                for (int iy = 0; iy < ny; ++iy) {
+                    const double o[2] = {(ix - 0.5 * (nx - 1)) * dx, (iy - 0.5 * (ny - 1)) * dy};
+                    const double so = o[0] * ex + o[1] * ey;
+                    if (so + reach < s0 || so - reach > s1) continue;
+                    auto f = [&](double t) {
+                        const double s = s0 + t * du;
+                        const double a[2] = {s * ex - far * rx, s * ey - far * ry};
+                        const double b[2] = {s * ex + far * rx, s * ey + far * ry};
+                        return pixel_line_integral(kind, a, b, o, dx, dy);
+                    };
+                    const double scale = kind == 0 ? std::hypot(dx, dy) : std::max(dx, dy);
+                    row[(size_t)ix * ny + iy] = integrate(f, 0.0, 1.0, tol * scale);
+                }
+        }
+}
+
 // Ref_project_Simpson (layers/Ref_projector.cu:217-367) over a whole volume:
 // for every non-zero voxel (x[(iz*ny + iy)*nx + ix]) and view, the detector
 // cells its eight corners project onto (ranges ceil(u - 1/2), as SF) receive

@@ -61,6 +61,8 @@ def lib() -> ctypes.CDLL:
     for n in ("sgd_sf3d_forward_dev", "sgd_sf3d_backward_dev"):
         getattr(L, n).restype = _i
         getattr(L, n).argtypes = [_vp, _vp, _vp, _vp]
+    L.sgd_b0_parallel_init.restype = _vp
+    L.sgd_b0_parallel_init.argtypes = [_i, _i, _i, _i, _d, _d, _d, _dp]
     L.sgd_b1_batch_create.restype = _vp
     L.sgd_b1_batch_create.argtypes = [_i] + [_vp] * 10
     L.sgd_b1_batch_destroy.restype = None

@@ -87,10 +87,13 @@ def simulate(geo, seeds, i0=1e5, sub=8, noise_seed=0):
 
 
 class ASDPOCS:
-    """ASD-POCS over `count` slices of one geometry (Sidky and Pan 2008
-    parameters by default)."""
+    """ASD-POCS over `count` slices of one geometry.  The TV step per descent
+    step is alpha * |dx_SART| (alpha = 0.002: twenty steps then move the
+    image by 4% of the SART change, so the data step leads; Sidky and Pan's
+    alpha = 0.2 applies to a full ART sweep, a much larger change than one
+    SART step)."""
 
-    def __init__(self, geo, count, beta=1.0, beta_red=0.995, alpha=0.2, alpha_red=0.95, r_max=0.95, eps=0.0,
+    def __init__(self, geo, count, beta=1.0, beta_red=0.995, alpha=0.002, alpha_red=0.95, r_max=0.94, eps=0.0,
                  ng=20):
         self.L = _lib.lib()
         _declare(self.L)

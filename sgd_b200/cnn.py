@@ -50,8 +50,8 @@ class WarmStartCNN:
         self.w32, self.b = [], []
         for cin, cout in zip(self.channels[:-1], self.channels[1:]):
             std = np.sqrt(2.0 / (9 * cin))
-            w = rng.standard_normal((cout, cin, 3, 3)).astype(np.float32) * std
-            self.w32.append(torch.tensor(w, device=self.device))
+            w = (rng.standard_normal((cout, cin, 3, 3)) * std).astype(np.float32)
+            self.w32.append(torch.tensor(w, dtype=torch.float32, device=self.device))
             self.b.append(torch.zeros(cout, dtype=torch.float32, device=self.device))
         self.w32[-1].zero_()
         self.w16 = [w.to(torch.bfloat16) for w in self.w32]

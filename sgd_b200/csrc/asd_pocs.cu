@@ -29,7 +29,7 @@
 namespace sgd {
 
 struct AsdParams {
-    float beta = 1.0f, beta_red = 0.995f, alpha = 0.2f, alpha_red = 0.95f, r_max = 0.95f, eps = 0.0f;
+    float beta = 1.0f, beta_red = 0.995f, alpha = 0.002f, alpha_red = 0.95f, r_max = 0.94f, eps = 0.0f;
     int ng = 20;
 };
 

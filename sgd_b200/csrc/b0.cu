@@ -125,6 +125,44 @@ struct B0Basis {
     }
 };
 
+// B0 in parallel-beam geometry (no counterpart in the reference, whose
+// geometry always has a point source, utils/geo.cu:234).  View angle beta:
+// rays along (cos beta, sin beta), detector axis e = (-sin beta, cos beta)
+// through the isocentre (the limit of the fan geometry as the source
+// recedes), bin u covering s in [(u - nu/2) du, (u - nu/2 + 1) du].  A pixel
+// indicator of dx x dy projects onto e as the convolution of boxes of widths
+// a = dx |e.x| and b = dy |e.y|; averaged over a bin it is dx dy times the
+// unit-area 3-direction box spline of widths (a, b, du) at the distance of the
+// pixel centre's projection from the bin centre (exact, not a model).
+struct B0ParBasis {
+    static constexpr int kViewFloats = 12;
+    // [0] e.x [1] e.y [2] a [3] b [4] du [5] x0 [6] y0 [7] dx [8] dy [9] nu/2
+    struct View {
+        float ex, ey, a, b, du, x0, y0, dx, dy, hnu;
+    };
+    struct Cell {
+        float s;
+        int lo, hi;
+    };
+    __device__ static void load_view(const float* v, View& V) {
+        V = View{__ldg(v), __ldg(v + 1), __ldg(v + 2), __ldg(v + 3), __ldg(v + 4),
+                 __ldg(v + 5), __ldg(v + 6), __ldg(v + 7), __ldg(v + 8), __ldg(v + 9)};
+    }
+    __device__ static bool valid(int, int, const Fan2DParams&) { return true; }
+    __device__ static void setup(const View& V, int i, int j, const Fan2DParams& P, Cell& c) {
+        const float ox = fmaf((float)i, V.dx, V.x0), oy = fmaf((float)j, V.dy, V.y0);
+        c.s = fmaf(ox, V.ex, oy * V.ey);
+        const float h = 0.5f * (V.a + V.b);
+        c.lo = max(0, (int)floorf((c.s - h) / V.du + V.hnu));
+        c.hi = min(P.nu - 1, (int)floorf((c.s + h) / V.du + V.hnu));
+    }
+    __device__ static float value(const View& V, const Cell& c, int u, int, const Fan2DParams&) {
+        const float t = c.s - ((float)u - V.hnu + 0.5f) * V.du;
+        const float conv = B0Basis::conv1d(t + 0.5f * (V.a + V.b + V.du), V.a, V.b, V.du);
+        return (conv > 1e-7f && conv == conv) ? conv : 0.f;
+    }
+};
+
 namespace {
 
 class B0Layer final : public Proj2D {
@@ -181,6 +219,65 @@ public:
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
         fan2d_back<B0Basis>(P, sino, img, out_scale, s);
     }
+};
+
+class B0ParallelLayer final : public Proj2D {
+public:
+    B0ParallelLayer(int nx, int ny, int np, int nu, double dx, double dy, double du, const double* angles) {
+        if (nx < 1 || ny < 1 || np < 1 || nu < 1 || !(dx > 0) || !(dy > 0) || !(du > 0) || !angles)
+            fail("b0 parallel: invalid arguments");
+        geo.nx = nx; geo.ny = ny; geo.np = np; geo.nu = nu;
+        geo.dx = dx; geo.dy = dy; geo.du = du;
+        P.ni = nx;
+        P.nj = ny;
+        ex_.resize(np);
+        ey_.resize(np);
+        std::vector<float> view((size_t)np * B0ParBasis::kViewFloats, 0.f);
+        for (int p = 0; p < np; ++p) {
+            ex_[p] = -std::sin(angles[p]);
+            ey_[p] = std::cos(angles[p]);
+            float* v = &view[(size_t)p * B0ParBasis::kViewFloats];
+            v[0] = (float)ex_[p]; v[1] = (float)ey_[p];
+            v[2] = (float)(dx * std::fabs(ex_[p])); v[3] = (float)(dy * std::fabs(ey_[p]));
+            v[4] = (float)du;
+            v[5] = (float)(-0.5 * (nx - 1) * dx); v[6] = (float)(-0.5 * (ny - 1) * dy);
+            v[7] = (float)dx; v[8] = (float)dy; v[9] = 0.5f * nu;
+        }
+        const double hx = 0.5 * dx, hy = 0.5 * dy, x0 = -0.5 * (nx - 1) * dx, y0 = -0.5 * (ny - 1) * dy;
+        finish_init(view, B0ParBasis::kViewFloats, {}, [&](int i0, int i1, int j0, int j1) {
+            return Box2{x0 + i0 * dx - hx, x0 + i1 * dx + hx, y0 + j0 * dy - hy, y0 + j1 * dy + hy};
+        });
+        out_scale = (float)dx * (float)dy;
+        count = fan2d_count<B0ParBasis>(P, stream);
+    }
+    void forward_dev(const float* img, float* sino, cudaStream_t s) override {
+        fan2d_forward<B0ParBasis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
+    }
+    long long csr(const CsrOut& out) override { return fan2d_csr<B0ParBasis>(P, out_scale, out, stream); }
+    void backward_dev(const float* sino, float* img, cudaStream_t s) override {
+        fan2d_back<B0ParBasis>(P, sino, img, out_scale, s);
+    }
+
+protected:
+    void window(int p, const Box2& b, int& lo, int& hi) const override {
+        double smin = 1e300, smax = -1e300;
+        for (double x : {b.x0, b.x1})
+            for (double y : {b.y0, b.y1}) {
+                const double s = x * ex_[p] + y * ey_[p];
+                smin = std::min(smin, s);
+                smax = std::max(smax, s);
+            }
+        const double umin = smin / geo.du + 0.5 * geo.nu, umax = smax / geo.du + 0.5 * geo.nu;
+        lo = std::max(0, (int)std::floor(umin) - 1);
+        hi = std::min(geo.nu - 1, (int)std::floor(umax) + 1);
+        if (umax < -1.0 || umin > geo.nu + 1.0) {
+            lo = 0;
+            hi = -1;
+        }
+    }
+
+private:
+    std::vector<double> ex_, ey_;
 };
 
 
@@ -299,6 +396,11 @@ long long b0_generator(int np, int nu, int nx, int ny, double dx, double dy, dou
 Proj2D* make_b0_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
                       const double* angles, const double* dz, const double* drho) {
     return new B0Layer(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, dz, drho);
+}
+
+Proj2D* make_b0_parallel_layer(int nx, int ny, int np, int nu, double dx, double dy, double du,
+                               const double* angles) {
+    return new B0ParallelLayer(nx, ny, np, nu, dx, dy, du, angles);
 }
 
 }  // namespace sgd

@@ -10,6 +10,8 @@ Proj2D* make_sf_layer(int nx, int ny, int np, int nu, double dx, double dy, doub
                       const double* angles);
 Proj2D* make_b0_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
                       const double* angles, const double* dz, const double* drho);
+Proj2D* make_b0_parallel_layer(int nx, int ny, int np, int nu, double dx, double dy, double du,
+                               const double* angles);
 Proj2D* make_hex_layer(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
                        const double* angles, const double* dz, const double* drho);
 }
@@ -137,6 +139,13 @@ int sgd_hl_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
 }
 unsigned long long sgd_h0_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
 unsigned long long sgd_hl_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
+
+// B0 in parallel-beam geometry; the handle takes the b0_* / sgd_b0_* calls.
+void* sgd_b0_parallel_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double* angles) {
+    return sgd::guarded<void*>(nullptr, [&]() -> void* {
+        return sgd::make_b0_parallel_layer(nx, ny, np, nu, dx, dy, du, angles);
+    });
+}
 
 long long sgd_SF_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap) {
     return matrix_csr(layer, rowptr, cols, vals, cap, "sgd_SF_matrix_csr");

@@ -40,6 +40,8 @@ void box_window(const FanGeometry& g, int p, const Box2& b, int& lo, int& hi) {
     }
 }
 
+void Proj2D::window(int p, const Box2& b, int& lo, int& hi) const { box_window(geo, p, b, lo, hi); }
+
 Proj2D::~Proj2D() {
     if (stream) cudaStreamSynchronize(stream);
     cudaFree(d_view_);

@@ -48,6 +48,9 @@ public:
 
 protected:
     Proj2D() = default;
+    // Bin window [lo, hi] of world box b in view p for the forward tiles
+    // (fan geometry by default; hi < lo when it misses).
+    virtual void window(int p, const Box2& b, int& lo, int& hi) const;
     // Uploads tables, computes tile windows from `box`, allocates staging.
     template <class BoxFn>
     void finish_init(const std::vector<float>& view, int view_floats, const std::vector<float4>& bins, BoxFn box);

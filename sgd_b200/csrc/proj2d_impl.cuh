@@ -36,7 +36,7 @@ void Proj2D::finish_init(const std::vector<float>& view, int view_floats, const 
                                 std::min(P.nj, (b + 1) * kF2TileJ) - 1);
             for (int p = 0; p < geo.np; ++p) {
                 int lo, hi;
-                box_window(geo, p, bx, lo, hi);
+                window(p, bx, lo, hi);
                 wins[((size_t)a * tj + b) * geo.np + p] = make_int2(lo, hi);
                 wmax = std::max(wmax, hi - lo + 1);
             }

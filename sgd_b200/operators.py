@@ -128,6 +128,36 @@ class A_B0_operator(_Fan2DOperator):
     _prefix = "b0"
 
 
+class A_B0_parallel_operator(_Fan2DOperator):
+    """Pixel-indicator projector in parallel-beam geometry (no counterpart in
+    the reference, whose geometry always has a point source): view angle
+    beta, rays along (cos beta, sin beta), nu bins of pitch du on the axis
+    (-sin beta, cos beta) through the isocentre.  Layouts as A_B0_operator."""
+
+    _prefix = "b0"
+
+    def __init__(self, nx, ny, nnp, nu, dx, dy, du, angles, dtype=np.float64):
+        LinearOperator.__init__(self, dtype=dtype, shape=(nnp * nu, nx * ny))
+        self.vol_shape = (nx, ny)
+        self.proj_shape = (nnp, nu)
+        self.dimension = (dx, dy)
+        self.blur = du
+        self.angles = angles
+        angles = np.ascontiguousarray(angles, dtype=np.float64)
+        if angles.shape != (nnp,):
+            raise ValueError(f"angles must have shape ({nnp},), got {angles.shape}")
+        self._angles = angles
+        L = _lib.lib()
+        self._L = L
+        self.cpointer = L.sgd_b0_parallel_init(nx, ny, nnp, nu, dx, dy, du, _ptr(angles))
+        if not self.cpointer:
+            raise _lib.ProjectorError(f"sgd_b0_parallel_init: {_lib.last_error()}")
+        self._fwd = L.b0_forward_projection
+        self._bwd = L.sgd_b0_backward_projection
+        self._destroy = L.b0_destroy
+        self.conv_count = int(L.sgd_b0_count(self.cpointer))
+
+
 class _HexOperator(_Fan2DOperator):
     """Common body of the hexagonal-lattice operators.  The reference names
     the lattice sizes (nx, ny) in Python and (nl, nc) in C: nx rows of ny

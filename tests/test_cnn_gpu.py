@@ -64,10 +64,10 @@ def test_network_gradients_match_oracle_and_finite_differences():
     net = WarmStartCNN(channels=(1, 8, 8, 1), seed=3)
     rng = np.random.default_rng(0)
     for w in net.w32:  # a non-trivial last layer
-        w.copy_(torch.tensor(rng.standard_normal(tuple(w.shape)).astype(np.float32) * 0.3))
+        w.copy_(torch.tensor((rng.standard_normal(tuple(w.shape)) * 0.3).astype(np.float32)))
     net.w16 = [w.to(torch.bfloat16) for w in net.w32]
     for b in net.b:
-        b.copy_(torch.tensor(rng.standard_normal(b.numel()).astype(np.float32) * 0.1))
+        b.copy_(torch.tensor((rng.standard_normal(b.numel()) * 0.1).astype(np.float32)))
     x = rng.standard_normal((2, 1, 12, 10)).astype(np.float32)
     gy = rng.standard_normal((2, 1, 12, 10)).astype(np.float32)
     y = net.forward(torch.tensor(x, device="cuda"), keep=True)
