@@ -715,6 +715,41 @@ long long b1_3d_voxel_view(const Geo& g, const float* vecs_p, int mode, int p, i
     return cnt;
 }
 
+// Index-space projection matrices built directly from the ray geometry in
+// FP64 (detector plane through dtv spanned by puv, pvv; u = offset/du + nu/2),
+// replacing pmi: equal to it except on the views where utils/geo.cu:36-41
+// degenerates (puv.x == puv.y).  Used by the corrected SF_projector mode.
+void exact_pmi_geo(Geo& g) {
+    auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    for (int p = 0; p < g.np; ++p) {
+        const double *S = &g.src[3 * p], *D = &g.dtv[3 * p], *eu = &g.puv[3 * p], *ev = &g.pvv[3 * p];
+        const double n[3] = {eu[1] * ev[2] - eu[2] * ev[1], eu[2] * ev[0] - eu[0] * ev[2], eu[0] * ev[1] - eu[1] * ev[0]};
+        double SD[3], DS[3];
+        for (int k = 0; k < 3; ++k) { SD[k] = S[k] - D[k]; DS[k] = D[k] - S[k]; }
+        const double uu = dot(eu, eu), vv = dot(ev, ev);
+        double rows[3][4];
+        for (int k = 0; k < 3; ++k) {
+            rows[0][k] = dot(eu, SD) / uu * n[k] + dot(n, DS) * eu[k] / uu;
+            rows[1][k] = dot(ev, SD) / vv * n[k] + dot(n, DS) * ev[k] / vv;
+            rows[2][k] = n[k];
+        }
+        for (int r = 0; r < 3; ++r) rows[r][3] = -(rows[r][0] * S[0] + rows[r][1] * S[1] + rows[r][2] * S[2]);
+        for (int k = 0; k < 4; ++k) {
+            rows[0][k] += 0.5 * g.nu * rows[2][k];
+            rows[1][k] += 0.5 * g.nv * rows[2][k];
+        }
+        const double x0 = -0.5 * (g.nx - 1) * g.dx, y0 = -0.5 * (g.ny - 1) * g.dy, z0 = -0.5 * (g.nz - 1) * g.dz;
+        double m[12];
+        for (int r = 0; r < 3; ++r) {
+            m[4 * r] = rows[r][0] * g.dx;
+            m[4 * r + 1] = rows[r][1] * g.dy;
+            m[4 * r + 2] = rows[r][2] * g.dz;
+            m[4 * r + 3] = rows[r][3] + rows[r][0] * x0 + rows[r][1] * y0 + rows[r][2] * z0;
+        }
+        for (int k = 0; k < 12; ++k) g.pmi[12 * p + k] = (float)(m[k] / m[11]);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // SF_projector 3D separable footprint: layers/SF_projector.cu
 // ---------------------------------------------------------------------------
@@ -769,6 +804,8 @@ int sf3d_voxel_view(const Geo& g, double lsd, int mode, bool fwd, bool trap, int
     sort4(uf);
     const float min_u = std::ceil(uf[0] - 0.5f), max_u = std::ceil(uf[3] - 0.5f);
     if (max_u < 0 || min_u >= nu) return 0;
+    // spans wider than twice the detector (degenerate projections): skipped, as the kernels do
+    if (!(max_u - min_u <= 2.f * nu + 4.f) || !(max_v - min_v <= 2.f * nv + 4.f)) return 0;
     T us[4] = {uf[0], uf[1], uf[2], uf[3]};
     // :173 / :300 with the integer halves of :104-105
     const double ddx = g.dx * (ix - g.nx / 2) - g.src[3 * p], ddy = g.dy * (iy - g.ny / 2) - g.src[3 * p + 1];
@@ -1081,6 +1118,7 @@ void oracle_sf3d_forward(int mode, int trap, int nx, int ny, int nz, int np, int
                          const double* x, double* b) {
     Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
     build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    if (mode == 1) exact_pmi_geo(g);
     std::memset(b, 0, sizeof(double) * (size_t)np * nu * nv);
 #pragma omp parallel for schedule(dynamic)
     for (int p = 0; p < np; ++p) {
@@ -1105,6 +1143,7 @@ void oracle_sf3d_backward(int mode, int trap, int nx, int ny, int nz, int np, in
                           const double* b, double* x) {
     Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
     build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    if (mode == 1) exact_pmi_geo(g);
     std::memset(x, 0, sizeof(double) * (size_t)nx * ny * nz);
 #pragma omp parallel for schedule(dynamic) collapse(2)
     for (int iy = 0; iy < ny; ++iy)

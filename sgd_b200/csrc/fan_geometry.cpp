@@ -237,4 +237,40 @@ void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>
     }
 }
 
+void exact_pmi(const ViewFrame& f, double uc, double vc, int nx, int ny, int nz, double dx, double dy, double dz,
+               float pmi[12]) {
+    const double* S = f.src;
+    const double* D = f.dtv;
+    const double* eu = f.puv;
+    const double* ev = f.pvv;
+    const double n[3] = {eu[1] * ev[2] - eu[2] * ev[1], eu[2] * ev[0] - eu[0] * ev[2], eu[0] * ev[1] - eu[1] * ev[0]};
+    auto dot = [](const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    const double uu = dot(eu, eu), vv = dot(ev, ev);
+    double SD[3], DS[3];
+    for (int k = 0; k < 3; ++k) { SD[k] = S[k] - D[k]; DS[k] = -SD[k]; }
+    // ray S -> X meets the detector at P = S + t (X - S), t = n.(D - S) / n.(X - S):
+    // (P - D).e/|e|^2 times w = n.(X - S) is linear in X
+    double rows[3][4];
+    for (int k = 0; k < 3; ++k) {
+        rows[0][k] = dot(eu, SD) / uu * n[k] + dot(n, DS) * eu[k] / uu;
+        rows[1][k] = dot(ev, SD) / vv * n[k] + dot(n, DS) * ev[k] / vv;
+        rows[2][k] = n[k];
+    }
+    for (int r = 0; r < 3; ++r) rows[r][3] = -(rows[r][0] * S[0] + rows[r][1] * S[1] + rows[r][2] * S[2]);
+    for (int k = 0; k < 4; ++k) {
+        rows[0][k] += uc * rows[2][k];
+        rows[1][k] += vc * rows[2][k];
+    }
+    // voxel indices -> world: x = (i - (nx-1)/2) dx, ...
+    const double x0 = -0.5 * (nx - 1) * dx, y0 = -0.5 * (ny - 1) * dy, z0 = -0.5 * (nz - 1) * dz;
+    double m[12];
+    for (int r = 0; r < 3; ++r) {
+        m[4 * r + 0] = rows[r][0] * dx;
+        m[4 * r + 1] = rows[r][1] * dy;
+        m[4 * r + 2] = rows[r][2] * dz;
+        m[4 * r + 3] = rows[r][3] + rows[r][0] * x0 + rows[r][1] * y0 + rows[r][2] * z0;
+    }
+    for (int k = 0; k < 12; ++k) pmi[k] = (float)(m[k] / m[11]);
+}
+
 }  // namespace sgd

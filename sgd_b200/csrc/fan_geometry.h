@@ -33,6 +33,15 @@ std::vector<ViewFrame> view_frames(int np, double lsd, double lso, double du, do
 void reference_pmi(const ViewFrame& f, double uc, double vc, int nx, int ny, int nz, double dx, double dy,
                    double dz, double pm[12], float pmi[12]);
 
+// The same index-space map built directly from the ray geometry in FP64 (the
+// detector plane through dtv spanned by puv and pvv, uc = nu/2, vc = nv/2).
+// It equals reference_pmi up to rounding except on the views where the
+// reference's detector-alignment matrix is singular (puv.x == puv.y, the
+// snapped 3pi/4 and -pi/4 views), where reference_pmi degenerates
+// (utils/geo.cu:36-41 returns the identity) and this one does not.
+void exact_pmi(const ViewFrame& f, double uc, double vc, int nx, int ny, int nz, double dx, double dy, double dz,
+               float pmi[12]);
+
 struct FanGeometry {
     int nx = 0, ny = 0, np = 0, nu = 0;
     double dx = 1, dy = 1, du = 1, lsd = 0, lso = 0;

@@ -20,8 +20,13 @@
 //     indicator of the non-zero voxels;
 //   * bin indices are not clamped, j * nu + i is only bounds-checked, so bins
 //     beyond the u edges wrap into neighbouring rows (:216, :336).
-// Mode 1 ("fixed"): the forward scales by the voxel value and amplitude and
-// drops out-of-detector bins; the back projection is its exact transpose.
+//   * on the snapped 3pi/4 and -pi/4 views its index-space matrices degenerate
+//     (utils/geo.cu:36-41) and voxels project onto spans of hundreds of bins;
+//     here a voxel whose span exceeds twice the detector is skipped (the one
+//     deviation: the reference visits those spans).
+// Mode 1 ("fixed"): exact projection matrices on every view, the forward
+// scales by the voxel value and amplitude and drops out-of-detector bins; the
+// back projection is its exact transpose.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -136,6 +141,10 @@ __device__ int sf_voxel(const SFGeo& G, const float* pm, const double* src, doub
         o.C = (float)(weight * factor * tw * (2 / ((o.vs[3] - o.vs[0]) + (o.vs[2] - o.vs[1]))));
     else
         o.C = (float)(weight * factor * tw * (1 / (o.vs[1] - o.vs[0])));
+    // a voxel whose projection spans more bins than twice the detector (near
+    // the source plane, or through a degenerate matrix) is skipped: its
+    // footprint is meaningless and the loops below would run unbounded
+    if (!(max_u - min_u <= 2.f * G.nu + 4.f) || !(max_v - min_v <= 2.f * G.nv + 4.f)) return 1;
     o.min_u = (int)min_u; o.max_u = (int)max_u; o.min_v = (int)min_v; o.max_v = (int)max_v;
     return 0;
 }
@@ -161,9 +170,11 @@ __global__ void __launch_bounds__(128) sf3d_forward_kernel(SFGeo G, const float*
         const float C0 = vol[((size_t)iz * G.ny + iy) * G.nx + ix];
         SFVoxel o;
         const int r = sf_voxel(G, pm, src, G.fwdf[p], true, ix, iy, iz, o);
-        if (r == 2 && G.mode == 0) break;
-        if (r == 1 || C0 == 0.f) continue;
-        const float amp = (G.mode == 0) ? 1.0f : o.C * C0;
+        if (r == 2 && G.mode == 0) break;  // the reference leaves its z chunk (:150)
+        if (r != 0 || C0 == 0.f) continue;  // o is only filled when r == 0
+        // mode 1 multiplies in FP64 so that the back kernel's terms are the
+        // same real numbers (an adjoint pair to FP64 accumulation)
+        const double amp = (G.mode == 0) ? 1.0 : (double)o.C * (double)C0;
         for (int i = o.min_u; i <= o.max_u; ++i) {
             const float g = sf_gamma(i - 0.5f, i + 0.5f, o.us);
             if (G.mode == 1 && (i < 0 || i >= G.nu)) continue;
@@ -171,7 +182,7 @@ __global__ void __launch_bounds__(128) sf3d_forward_kernel(SFGeo G, const float*
                 const float f2 = g * sf_fv(G, trap, o, j);
                 const int idxv = j * G.nu + i;
                 if (G.mode == 1 && (j < 0 || j >= G.nv)) continue;
-                if (idxv < nuv && idxv >= 0 && f2 == f2 && f2 != 0.f) atomicAdd(pp + idxv, (double)(f2 * amp));
+                if (idxv < nuv && idxv >= 0 && f2 == f2 && f2 != 0.f) atomicAdd(pp + idxv, (double)f2 * amp);
             }
         }
     }
@@ -203,7 +214,7 @@ __global__ void __launch_bounds__(128) sf3d_back_kernel(SFGeo G, const float* __
         const int r = sf_voxel(G, pm, src, G.mode == 0 ? G.backf : G.fwdf[p], G.mode == 1, ix, iy, iz, o);
         if (r != 0) continue;
         const float* pp = proj + (size_t)p * nuv;
-        float sumV = 0.0f;
+        double sumV = 0.0;
         for (int i = o.min_u; i <= o.max_u; ++i) {
             if (G.mode == 1 && (i < 0 || i >= G.nu)) continue;
             const float g = sf_gamma(i - 0.5f, i + 0.5f, o.us);
@@ -211,11 +222,12 @@ __global__ void __launch_bounds__(128) sf3d_back_kernel(SFGeo G, const float* __
                 if (G.mode == 1 && (j < 0 || j >= G.nv)) continue;
                 const float f = g * sf_fv(G, trap, o, j);
                 const int idxv = j * G.nu + i;
-                if (idxv < nuv && idxv >= 0 && (G.mode == 0 || (f == f && f != 0.f))) sumV += pp[idxv] * f;
+                if (idxv < nuv && idxv >= 0 && (G.mode == 0 || (f == f && f != 0.f)))
+                    sumV += (double)pp[idxv] * (double)f;
             }
         }
-        sumV *= o.C;
-        if (sumV == sumV) acc += (double)sumV;
+        sumV *= (double)o.C;
+        if (sumV == sumV) acc += sumV;
     }
     vol[((size_t)iz * G.ny + iy) * G.nx + ix] = (float)acc;
 }
@@ -244,7 +256,10 @@ public:
         std::vector<double> src((size_t)np * 3), fwdf(np);
         for (int p = 0; p < np; ++p) {
             double pm[12];
-            reference_pmi(fr[p], nu / 2.0, nv / 2.0, nx, ny, nz, dx, dy, dz, pm, &pmi[12 * (size_t)p]);
+            // mode 0 keeps the reference's matrices, degenerate views included;
+            // the corrected pair projects through the exact ones
+            if (mode == 0) reference_pmi(fr[p], nu / 2.0, nv / 2.0, nx, ny, nz, dx, dy, dz, pm, &pmi[12 * (size_t)p]);
+            else exact_pmi(fr[p], nu / 2.0, nv / 2.0, nx, ny, nz, dx, dy, dz, &pmi[12 * (size_t)p]);
             for (int k = 0; k < 3; ++k) src[3 * p + k] = fr[p].src[k];
             const float flsd = (float)lsd;  // SF::project: float lsd (:362)
             fwdf[p] = flsd * flsd * dy * dz / (du * dv);
