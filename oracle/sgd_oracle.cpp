@@ -926,6 +926,38 @@ double integrate(F f, double a, double b, double eps) {
     return adaptive_simpson(f, a, b, fa, fm, fb, (b - a) / 6.0 * (fa + 4.0 * fm + fb), eps, 40);
 }
 
+// Integral over [0, 1] of an integrand whose kinks lie at `cuts` (where the
+// ray passes the basis function's breakpoints): each smooth piece is
+// integrated separately, so the adaptive rule never stops early on a
+// coincidental agreement across a kink.
+template <class F>
+double integrate_pieces(F f, std::vector<double> cuts, double eps) {
+    cuts.push_back(0.0);
+    cuts.push_back(1.0);
+    std::sort(cuts.begin(), cuts.end());
+    double sum = 0.0;
+    for (size_t k = 0; k + 1 < cuts.size(); ++k) {
+        const double a = std::max(0.0, cuts[k]), b = std::min(1.0, cuts[k + 1]);
+        if (b > a) sum += integrate(f, a, b, eps * (b - a));
+    }
+    return sum;
+}
+
+// Breakpoints of a pixel basis centred at o: the corners of the indicator
+// (kind 0) or the 3 x 3 grid of the hat's cell corners (kind 1).
+inline void basis_breakpoints(int kind, const double* o, double dx, double dy, std::vector<double>& px,
+                              std::vector<double>& py) {
+    px.clear();
+    py.clear();
+    if (kind == 0) {
+        for (int a = -1; a <= 1; a += 2)
+            for (int b = -1; b <= 1; b += 2) { px.push_back(o[0] + 0.5 * a * dx); py.push_back(o[1] + 0.5 * b * dy); }
+    } else {
+        for (int a = -1; a <= 1; ++a)
+            for (int b = -1; b <= 1; ++b) { px.push_back(o[0] + a * dx); py.push_back(o[1] + b * dy); }
+    }
+}
+
 // geo_init_example (utils/geo.cu:209-230) with the arguments the matrix
 // generators pass (start 0, end 2 pi (np - 1)/np, layers/A_B1.cu:547): uniform
 // angles without the 45-degree snap.  (np = 1 divides 0 by 0 there; it is
@@ -1203,8 +1235,20 @@ void oracle_exact_fan2d_matrix(int kind, int nx, int ny, int np, int nu, double 
                         double q[2] = {dt[0] + pu[0] * (u - 0.5 * nu + t), dt[1] + pu[1] * (u - 0.5 * nu + t)};
                         return pixel_line_integral(kind, s, q, o, dx, dy);
                     };
+                    // bin parameter of the ray through each breakpoint C:
+                    // cross(D - S + e (off + t), C - S) = 0
+                    std::vector<double> bx, by, cuts;
+                    basis_breakpoints(kind, o, dx, dy, bx, by);
+                    const double off = u - 0.5 * nu;
+                    for (size_t k = 0; k < bx.size(); ++k) {
+                        const double cx = bx[k] - s[0], cy = by[k] - s[1];
+                        const double den = pu[0] * cy - pu[1] * cx;
+                        if (den == 0.0) continue;
+                        const double t = -((dt[0] - s[0]) * cy - (dt[1] - s[1]) * cx) / den - off;
+                        if (t > 0.0 && t < 1.0) cuts.push_back(t);
+                    }
                     const double scale = kind == 0 ? std::hypot(dx, dy) : std::max(dx, dy);
-                    row[(size_t)ix * ny + iy] = integrate(f, 0.0, 1.0, tol * scale);
+                    row[(size_t)ix * ny + iy] = integrate_pieces(f, cuts, tol * scale);
                 }
         }
 }
@@ -1240,8 +1284,14 @@ void oracle_exact_parallel_matrix(int kind, int nx, int ny, int np, int nu, doub
                         const double b[2] = {s * ex + far * rx, s * ey + far * ry};
                         return pixel_line_integral(kind, a, b, o, dx, dy);
                     };
+                    std::vector<double> bx, by, cuts;
+                    basis_breakpoints(kind, o, dx, dy, bx, by);
+                    for (size_t k = 0; k < bx.size(); ++k) {
+                        const double t = (bx[k] * ex + by[k] * ey - s0) / du;
+                        if (t > 0.0 && t < 1.0) cuts.push_back(t);
+                    }
                     const double scale = kind == 0 ? std::hypot(dx, dy) : std::max(dx, dy);
-                    row[(size_t)ix * ny + iy] = integrate(f, 0.0, 1.0, tol * scale);
+                    row[(size_t)ix * ny + iy] = integrate_pieces(f, cuts, tol * scale);
                 }
         }
 }
