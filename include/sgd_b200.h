@@ -233,13 +233,13 @@ int sgd_b1_batch_status(void* batch);
 /* ---- ASD-POCS and its phantom simulator ----------------------------------- */
 
 /* New (the reference's optimizer/asd_pocs.cu is empty): ASD-POCS (Sidky and
- * Pan 2008: SART step, positivity, adaptive TV descent) over the slices of a
+ * Pan 2008: SART step, optional positivity, adaptive TV descent) over the slices of a
  * batch, every scalar per image on the device, one CUDA graph per iteration.
  * bind() takes the iterate and data arenas (the batch's layout) and the image
  * shapes and resets the adaptive state; history() returns (|Ax-b|, |dx_SART|,
  * |dx_TV|) per iteration and image for the first hist_cap iterations. */
 void* sgd_asd_create(void* batch, float beta, float beta_red, float alpha, float alpha_red, float r_max, float eps,
-                     int ng);
+                     int ng, int nonneg);
 void sgd_asd_destroy(void* h);
 int sgd_asd_bind(void* h, float* d_x, const float* d_b, const int* nx, const int* ny, int hist_cap);
 int sgd_asd_reset(void* h);

@@ -38,7 +38,7 @@ def _declare(L):
         return
     i, f, d = ctypes.c_int, ctypes.c_float, ctypes.c_double
     L.sgd_asd_create.restype = _vp
-    L.sgd_asd_create.argtypes = [_vp, f, f, f, f, f, f, i]
+    L.sgd_asd_create.argtypes = [_vp, f, f, f, f, f, f, i, i]
     L.sgd_asd_destroy.restype = None
     L.sgd_asd_destroy.argtypes = [_vp]
     L.sgd_asd_bind.restype = i
@@ -91,15 +91,18 @@ class ASDPOCS:
     step is alpha * |dx_SART| (alpha = 0.002: twenty steps then move the
     image by 4% of the SART change, so the data step leads; Sidky and Pan's
     alpha = 0.2 applies to a full ART sweep, a much larger change than one
-    SART step)."""
+    SART step).  ``nonneg`` projects onto x >= 0 after each SART step (the
+    classical constraint for attenuation images; the seeded ellipse family
+    has negative densities, so its experiments turn it off)."""
 
     def __init__(self, geo, count, beta=1.0, beta_red=0.995, alpha=0.002, alpha_red=0.95, r_max=0.94, eps=0.0,
-                 ng=20):
+                 ng=20, nonneg=True):
         self.L = _lib.lib()
         _declare(self.L)
         self.geo, self.count = geo, count
         self.batch = B1Batch([geo.slice()] * count)
-        self.h = self.L.sgd_asd_create(self.batch.handle, beta, beta_red, alpha, alpha_red, r_max, eps, ng)
+        self.h = self.L.sgd_asd_create(self.batch.handle, beta, beta_red, alpha, alpha_red, r_max, eps, ng,
+                                       int(bool(nonneg)))
         if not self.h:
             raise _lib.ProjectorError(f"sgd_asd_create: {_lib.last_error()}")
         self.x = self.batch.image_arena()
@@ -177,10 +180,10 @@ def plain_curve(solver, sino, truth, iters, every=5):
     return curve
 
 
-def make_pairs(geo, seeds, iters, k_in, count=64, noise_seed=0):
+def make_pairs(geo, seeds, iters, k_in, count=64, noise_seed=0, nonneg=False):
     """Training pairs from plain ASD-POCS for the phantoms `seeds`, `count` at
     a time: (iterate after k_in iterations, iterate after `iters`)."""
-    solver = ASDPOCS(geo, count)
+    solver = ASDPOCS(geo, count, nonneg=nonneg)
     xs, ts = [], []
     for s0 in range(0, len(seeds), count):
         chunk = list(seeds[s0:s0 + count])
@@ -221,7 +224,7 @@ def learned_run(solver, net, sino, truth, k_in, target, max_iters, every=1):
     x = solver.images().unsqueeze(1).clone()
     out = {}
     ms += timed(lambda: out.setdefault("y", net.forward(x)))
-    solver.set_data(sino, x0=torch.clamp(out["y"], min=0.0))
+    solver.set_data(sino, x0=out["y"])
     curve = [(0, ms, float(rmse(solver.images(), truth).mean()))]
     done = 0
     while done < max_iters and curve[-1][2] > target:
@@ -254,7 +257,7 @@ def main():
     t_train = time.perf_counter() - t0
     del xs, ts
     truth, sino, _ = simulate(geo, list(range(args.images)), noise_seed=999)
-    solver = ASDPOCS(geo, args.images)
+    solver = ASDPOCS(geo, args.images, nonneg=False)
     plain = plain_curve(solver, sino, truth, args.iters)
     target = plain[-1][2]
     it_l, ms_l, curve_l = learned_run(solver, net, sino, truth, args.k_in, target, args.iters)

@@ -6,7 +6,7 @@
 // 2008), per image:
 //   x_prev = x
 //   x += beta * A^T((b - A x) / R) / C          SART step, R = A 1, C = A^T 1
-//   x = max(x, 0)                               positivity
+//   x = max(x, 0)                               positivity (optional)
 //   dp = |x - x_prev|, x_res = x
 //   dtvg = alpha * dp                           (first iteration only)
 //   ng times: x -= dtvg * g / |g|, g = grad TV(x)
@@ -31,6 +31,7 @@ namespace sgd {
 struct AsdParams {
     float beta = 1.0f, beta_red = 0.995f, alpha = 0.002f, alpha_red = 0.95f, r_max = 0.94f, eps = 0.0f;
     int ng = 20;
+    int nonneg = 1;  // project onto x >= 0 after the SART step
 };
 
 namespace {
@@ -74,13 +75,13 @@ __global__ void __launch_bounds__(kThreads) sart_residual_kernel(const float* __
     if (threadIdx.x == 0) atomicAdd(&acc[kDD * ni + im], s);
 }
 
-// x = max(x + beta g / C, 0); acc[kDP] += |x - x_prev|^2
+// x = x + beta g / C (then max(., 0) when nonneg); acc[kDP] += |x - x_prev|^2
 __global__ void __launch_bounds__(kThreads) sart_update_kernel(float* __restrict__ x, const float* __restrict__ g,
                                                                const float* __restrict__ C,
                                                                const float* __restrict__ x_prev,
                                                                const float* __restrict__ beta,
                                                                const long long* __restrict__ off, int ni,
-                                                               double* __restrict__ acc) {
+                                                               int nonneg, double* __restrict__ acc) {
     const int im = blockIdx.y;
     const long long o0 = off[im], n = off[im + 1] - o0;
     const float bt = beta[im];
@@ -88,7 +89,7 @@ __global__ void __launch_bounds__(kThreads) sart_update_kernel(float* __restrict
     for (long long e = (long long)blockIdx.x * kThreads + threadIdx.x; e < n; e += (long long)gridDim.x * kThreads) {
         const float w = C[o0 + e];
         float v = x[o0 + e] + (w > 1e-6f ? bt * g[o0 + e] / w : 0.f);
-        v = fmaxf(v, 0.f);
+        if (nonneg) v = fmaxf(v, 0.f);
         const float d = v - x_prev[o0 + e];
         s += (double)d * d;
         x[o0 + e] = v;
@@ -346,7 +347,7 @@ private:
         sart_residual_kernel<<<gs, kThreads, 0, s>>>(b_, ax_, R_, r_, off_sino_, ni_, acc_);
         SGD_LAUNCH_CHECK();
         B->backward(r_, g_, s);
-        sart_update_kernel<<<gi, kThreads, 0, s>>>(x_, g_, C_, xprev_, beta_, off_img_, ni_, acc_);
+        sart_update_kernel<<<gi, kThreads, 0, s>>>(x_, g_, C_, xprev_, beta_, off_img_, ni_, prm_.nonneg, acc_);
         SGD_LAUNCH_CHECK();
         SGD_CUDA(cudaMemcpyAsync(xres_, x_, nimg * sizeof(float), cudaMemcpyDeviceToDevice, s));
         for (int k = 0; k < prm_.ng; ++k) {
@@ -389,13 +390,13 @@ private:
 extern "C" {
 
 void* sgd_asd_create(void* batch, float beta, float beta_red, float alpha, float alpha_red, float r_max, float eps,
-                     int ng) {
+                     int ng, int nonneg) {
     return sgd::guarded<void*>(nullptr, [&]() -> void* {
         if (!batch) sgd::fail("sgd_asd_create: null batch");
         if (ng < 0 || ng > 200) sgd::fail("sgd_asd_create: ng must be in [0, 200]");
         sgd::AsdParams p;
         p.beta = beta; p.beta_red = beta_red; p.alpha = alpha; p.alpha_red = alpha_red; p.r_max = r_max;
-        p.eps = eps; p.ng = ng;
+        p.eps = eps; p.ng = ng; p.nonneg = nonneg ? 1 : 0;
         return new sgd::AsdPocs(static_cast<sgd::B1Batch*>(batch), p);
     });
 }
