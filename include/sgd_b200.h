@@ -196,7 +196,10 @@ unsigned long long sgd_b1_3d_count(void* layer);
  * past the u edges wrap into neighbouring detector rows.  mode 1 applies the
  * voxel value and amplitude, drops out-of-detector bins, and its backward is
  * the exact transpose of its forward.  trap_v: SF-TT (trapezoid in v) in the
- * forward (the reference's `tt` argument); mode 1's backward follows it. */
+ * forward (the reference's `tt` argument); mode 1's backward follows it.
+ * The FP64 host entry points of mode 1 stay in FP64 (inputs, accumulation,
+ * outputs), so the pair is an adjoint pair to FP64 rounding; mode 0's round
+ * through FP32 as the reference does; the *_dev entry points are FP32. */
 void* sgd_sf3d_init(int mode, int trap_v, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
                     double dz, double du, double dv, double lsd, double lso, double* angles);
 int sgd_sf3d_forward_projection(double* b, double* x, void* layer);

@@ -56,13 +56,16 @@ def _declare(L):
 
 class Geometry:
     """A square fan-beam slice: n x n pixels over a 256 mm field, `views`
-    angles over 2 pi, ceil(1.44 n) bins of 1 mm (the batched workload's rule)."""
+    angles over 2 pi, ceil(1.44 n) bins of 512/n mm (1 mm at n = 512, the
+    headline slice): the fan covers the field's circumscribed circle
+    (1.44 * 512 mm * SOD / SDD = 404 mm > 362 mm) at every n, so the data are
+    not truncated."""
 
     def __init__(self, n=256, views=120, lsd=LSD, lso=LSO):
         self.n, self.views, self.lsd, self.lso = n, views, lsd, lso
         self.d = 256.0 / n
         self.nu = math.ceil(1.44 * n)
-        self.du = 1.0
+        self.du = 512.0 / n
         self.angles = 2 * np.pi * np.arange(views) / views
 
     def slice(self):

@@ -30,6 +30,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.h"
@@ -154,8 +155,10 @@ __device__ __forceinline__ float sf_fv(const SFGeo& G, bool trap, const SFVoxel&
     return fmaxf(fminf(j + 0.5f, o.vs[1]) - fmaxf(j - 0.5f, o.vs[0]), 0);
 }
 
-// a thread per (ix, iy, z chunk of 64) and view (grid z = views)
-__global__ void __launch_bounds__(128) sf3d_forward_kernel(SFGeo G, const float* __restrict__ vol,
+// a thread per (ix, iy, z chunk of 64) and view (grid z = views); the volume
+// is FP32 (device entry points) or FP64 (mode 1 host entry points)
+template <typename TVol>
+__global__ void __launch_bounds__(128) sf3d_forward_kernel(SFGeo G, const TVol* __restrict__ vol,
                                                            double* __restrict__ proj64) {
     const int ix = blockIdx.x * 16 + threadIdx.x, iy = blockIdx.y * 8 + threadIdx.y;
     const int chunks = (G.nz + kSFZ - 1) / kSFZ;
@@ -167,11 +170,11 @@ __global__ void __launch_bounds__(128) sf3d_forward_kernel(SFGeo G, const float*
     double* pp = proj64 + (size_t)p * nuv;
     const bool trap = G.trap != 0;
     for (int iz = zc * kSFZ; iz < min(G.nz, (zc + 1) * kSFZ); ++iz) {
-        const float C0 = vol[((size_t)iz * G.ny + iy) * G.nx + ix];
+        const TVol C0 = vol[((size_t)iz * G.ny + iy) * G.nx + ix];
         SFVoxel o;
         const int r = sf_voxel(G, pm, src, G.fwdf[p], true, ix, iy, iz, o);
         if (r == 2 && G.mode == 0) break;  // the reference leaves its z chunk (:150)
-        if (r != 0 || C0 == 0.f) continue;  // o is only filled when r == 0
+        if (r != 0 || C0 == TVol(0)) continue;  // o is only filled when r == 0
         // mode 1 multiplies in FP64 so that the back kernel's terms are the
         // same real numbers (an adjoint pair to FP64 accumulation)
         const double amp = (G.mode == 0) ? 1.0 : (double)o.C * (double)C0;
@@ -188,9 +191,12 @@ __global__ void __launch_bounds__(128) sf3d_forward_kernel(SFGeo G, const float*
     }
 }
 
-// mode 0: SF_backproject (rect in v); mode 1: exact transpose of the fixed forward
-__global__ void __launch_bounds__(128) sf3d_back_kernel(SFGeo G, const float* __restrict__ proj,
-                                                        float* __restrict__ vol) {
+// mode 0: SF_backproject (rect in v); mode 1: exact transpose of the fixed
+// forward.  FP32 in and out (device entry points) or FP64 (mode 1 host entry
+// points, so that the pair stays an adjoint pair to FP64 rounding end to end)
+template <typename TProj, typename TVol>
+__global__ void __launch_bounds__(128) sf3d_back_kernel(SFGeo G, const TProj* __restrict__ proj,
+                                                        TVol* __restrict__ vol) {
     const int ix = blockIdx.x * 16 + threadIdx.x, iy = blockIdx.y * 8 + threadIdx.y;
     const int iz = blockIdx.z;
     if (ix >= G.nx || iy >= G.ny) return;
@@ -213,7 +219,7 @@ __global__ void __launch_bounds__(128) sf3d_back_kernel(SFGeo G, const float* __
         }
         const int r = sf_voxel(G, pm, src, G.mode == 0 ? G.backf : G.fwdf[p], G.mode == 1, ix, iy, iz, o);
         if (r != 0) continue;
-        const float* pp = proj + (size_t)p * nuv;
+        const TProj* pp = proj + (size_t)p * nuv;
         double sumV = 0.0;
         for (int i = o.min_u; i <= o.max_u; ++i) {
             if (G.mode == 1 && (i < 0 || i >= G.nu)) continue;
@@ -229,7 +235,7 @@ __global__ void __launch_bounds__(128) sf3d_back_kernel(SFGeo G, const float* __
         sumV *= (double)o.C;
         if (sumV == sumV) acc += sumV;
     }
-    vol[((size_t)iz * G.ny + iy) * G.nx + ix] = (float)acc;
+    vol[((size_t)iz * G.ny + iy) * G.nx + ix] = (TVol)acc;
 }
 
 __global__ void sf3d_finish_kernel(const double* __restrict__ s64, float* __restrict__ s32, long long n) {
@@ -283,11 +289,24 @@ public:
         if (stream) cudaStreamSynchronize(stream);
         cudaFree(d_pmi_); cudaFree(d_src_); cudaFree(d_fwdf_); cudaFree(d_proj64_);
         cudaFree(d_vol_); cudaFree(d_proj_); cudaFreeHost(h_vol_); cudaFreeHost(h_proj_);
+        cudaFree(d_vol64_); cudaFreeHost(h_vol64_); cudaFreeHost(h_proj64_);
         if (stream) cudaStreamDestroy(stream);
     }
-    // FP64 host arrays: x[(iz*ny + iy)*nx + ix], b[(p*nv + v)*nu + u]
+    // FP64 host arrays: x[(iz*ny + iy)*nx + ix], b[(p*nv + v)*nu + u].  Mode 1
+    // keeps FP64 from the host buffers through the kernels and back; mode 0
+    // rounds through FP32 as the reference's SF class does.
     void forward_host(double* b, const double* x) {
         const long long nvol = (long long)G.nx * G.ny * G.nz, nproj = (long long)G.np * G.nu * G.nv;
+        if (G.mode == 1) {
+            ensure_fp64();
+            std::memcpy(h_vol64_, x, nvol * sizeof(double));
+            SGD_CUDA(cudaMemcpyAsync(d_vol64_, h_vol64_, nvol * sizeof(double), cudaMemcpyHostToDevice, stream));
+            forward64(d_vol64_, stream);
+            SGD_CUDA(cudaMemcpyAsync(h_proj64_, d_proj64_, nproj * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            SGD_CUDA(cudaStreamSynchronize(stream));
+            std::memcpy(b, h_proj64_, nproj * sizeof(double));
+            return;
+        }
 #pragma omp parallel for schedule(static)
         for (long long e = 0; e < nvol; ++e) h_vol_[e] = (float)x[e];
         SGD_CUDA(cudaMemcpyAsync(d_vol_, h_vol_, nvol * sizeof(float), cudaMemcpyHostToDevice, stream));
@@ -299,6 +318,18 @@ public:
     }
     void backward_host(const double* b, double* x) {
         const long long nvol = (long long)G.nx * G.ny * G.nz, nproj = (long long)G.np * G.nu * G.nv;
+        if (G.mode == 1) {
+            ensure_fp64();
+            std::memcpy(h_proj64_, b, nproj * sizeof(double));
+            SGD_CUDA(cudaMemcpyAsync(d_proj64_, h_proj64_, nproj * sizeof(double), cudaMemcpyHostToDevice, stream));
+            dim3 grid((G.nx + 15) / 16, (G.ny + 7) / 8, G.nz);
+            sf3d_back_kernel<double, double><<<grid, dim3(16, 8), 0, stream>>>(G, d_proj64_, d_vol64_);
+            SGD_LAUNCH_CHECK();
+            SGD_CUDA(cudaMemcpyAsync(h_vol64_, d_vol64_, nvol * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            SGD_CUDA(cudaStreamSynchronize(stream));
+            std::memcpy(x, h_vol64_, nvol * sizeof(double));
+            return;
+        }
 #pragma omp parallel for schedule(static)
         for (long long e = 0; e < nproj; ++e) h_proj_[e] = (float)b[e];
         SGD_CUDA(cudaMemcpyAsync(d_proj_, h_proj_, nproj * sizeof(float), cudaMemcpyHostToDevice, stream));
@@ -308,23 +339,39 @@ public:
 #pragma omp parallel for schedule(static)
         for (long long e = 0; e < nvol; ++e) x[e] = (double)h_vol_[e];
     }
-    void forward_dev(const float* vol, float* proj, cudaStream_t s) {
+    // d_proj64_ = A vol (FP64 accumulation)
+    template <typename TVol>
+    void forward64(const TVol* vol, cudaStream_t s) {
         const long long n = (long long)G.np * G.nu * G.nv;
         SGD_CUDA(cudaMemsetAsync(d_proj64_, 0, n * sizeof(double), s));
         const int chunks = (G.nz + kSFZ - 1) / kSFZ;
         dim3 grid((G.nx + 15) / 16, (G.ny + 7) / 8, G.np * chunks);
-        sf3d_forward_kernel<<<grid, dim3(16, 8), 0, s>>>(G, vol, d_proj64_);
+        sf3d_forward_kernel<TVol><<<grid, dim3(16, 8), 0, s>>>(G, vol, d_proj64_);
         SGD_LAUNCH_CHECK();
+    }
+    void forward_dev(const float* vol, float* proj, cudaStream_t s) {
+        const long long n = (long long)G.np * G.nu * G.nv;
+        forward64(vol, s);
         sf3d_finish_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(d_proj64_, proj, n);
         SGD_LAUNCH_CHECK();
     }
     void backward_dev(const float* proj, float* vol, cudaStream_t s) {
         dim3 grid((G.nx + 15) / 16, (G.ny + 7) / 8, G.nz);
-        sf3d_back_kernel<<<grid, dim3(16, 8), 0, s>>>(G, proj, vol);
+        sf3d_back_kernel<float, float><<<grid, dim3(16, 8), 0, s>>>(G, proj, vol);
         SGD_LAUNCH_CHECK();
     }
 
 private:
+    void ensure_fp64() {
+        if (d_vol64_) return;
+        const size_t nvol = (size_t)G.nx * G.ny * G.nz, nproj = (size_t)G.np * G.nu * G.nv;
+        SGD_CUDA(cudaMalloc(&d_vol64_, nvol * sizeof(double)));
+        SGD_CUDA(cudaMallocHost(&h_vol64_, nvol * sizeof(double)));
+        SGD_CUDA(cudaMallocHost(&h_proj64_, nproj * sizeof(double)));
+    }
+    double* d_vol64_ = nullptr;
+    double* h_vol64_ = nullptr;
+    double* h_proj64_ = nullptr;
     float* d_pmi_ = nullptr;
     double* d_src_ = nullptr;
     double* d_fwdf_ = nullptr;

@@ -51,11 +51,15 @@ def test_gradients_are_the_other_projector(kind):
     # the generic forward kernels sum with atomics: equal up to summation order
     fw = P.forward(w.contiguous()).double()
     assert float((s.grad.double() - fw).norm() / fw.norm()) < 1e-6
-    # the pair is an adjoint pair (FP64 dot products)
-    ax = P.forward(x.detach().contiguous()).double()
-    aty = P.backward(y.contiguous()).double()
+    # the pair is an adjoint pair (FP64 dot products) on N(0, 1) vectors of
+    # seed 1234
+    rng = np.random.default_rng(1234)
+    x = torch.tensor(rng.standard_normal(P.image_shape), dtype=torch.float32, device="cuda")
+    y = torch.tensor(rng.standard_normal(P.sino_shape), dtype=torch.float32, device="cuda")
+    ax = P.forward(x).double()
+    aty = P.backward(y).double()
     lhs = float((ax * y.double()).sum())
-    rhs = float((x.detach().double() * aty).sum())
+    rhs = float((x.double() * aty).sum())
     assert abs(lhs - rhs) / abs(lhs) < 1e-6
 
 

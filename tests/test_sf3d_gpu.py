@@ -131,13 +131,20 @@ def test_bad_arguments_raise():
         SF_projector_operator(4, 4, 4, 1, 4, 4, 1, 1, 1, 1, 1, 1085.6, 595.0, np.zeros(1), mode=3)
 
 
-def test_corrected_mode_handles_degenerate_views():
+def test_corrected_mode_handles_degenerate_views(oracle_mod):
     """On the snapped 3pi/4 view the reference's index-space matrix degenerates
-    (utils/geo.cu:36-41); the corrected mode projects through the exact one: a
-    uniform cube seen at pi/4 and 3pi/4 carries the same total."""
+    (utils/geo.cu:36-41); the corrected mode projects through the exact one.
+    Its projection of a uniform cube at pi/4 and 3pi/4 matches the FP64
+    replica, and the total is continuous across the snapped view (the SF
+    footprint model itself is not invariant under a 90-degree turn: the
+    totals at pi/4 and 3pi/4 differ by 0.24 % in the FP64 replica too)."""
     from sgd_b200.operators import SF_projector_operator
     n = 16
-    ang = np.array([np.pi / 4, 3 * np.pi / 4])
-    A = SF_projector_operator(n, n, n, 2, 64, 64, 1.0, 1.0, 1.0, 1.0, 1.0, 1085.6, 595.0, ang, mode=1)
-    b = A.matvec(np.ones(n ** 3)).reshape(2, -1)
-    assert abs(b[0].sum() - b[1].sum()) / b[0].sum() < 1e-3
+    g = (n, n, n, 64, 64, 1.0, 1.0, 1.0, 1.0, 1.0, 1085.6, 595.0)
+    ang = np.array([np.pi / 4, 3 * np.pi / 4, 3 * np.pi / 4 + 1e-3])
+    A = SF_projector_operator(n, n, n, 3, 64, 64, 1.0, 1.0, 1.0, 1.0, 1.0, 1085.6, 595.0, ang, mode=1)
+    x = np.ones(n ** 3)
+    b = A.matvec(x)
+    assert rel_l2(b, oracle_mod.sf3d_forward(x, *g, ang, mode=1)) < TOL_ORACLE
+    t = b.reshape(3, -1).sum(axis=1)
+    assert t[1] > 0 and abs(t[1] - t[2]) / t[1] < 1e-4
