@@ -69,14 +69,6 @@ __device__ __forceinline__ void strip_span(const float4& st, float aa, float ab,
     nhi = min(nmin - 1, (int)floorf(hi));
 }
 
-template <int N>
-__device__ __forceinline__ int pick(const int (&a)[N], int v) {
-    int r = a[0];
-#pragma unroll
-    for (int k = 1; k < N; ++k) r = (v == k) ? a[k] : r;
-    return r;
-}
-
 // Sinogram value of row gw = p * nu + u.  img (i, j) at img[i * ny + j];
 // imgT (i, j) at imgT[j * nx + i].
 __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, const float* __restrict__ strip,
@@ -211,40 +203,29 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             continue;
         }
         if (i >= nx || j >= ny) continue;
-        // this pixel's bins in each view of the chunk, then one flat loop over
-        // all of them: lanes run nearly equal trip counts
-        int ulo[VC], uhi[VC], roff[VC], soff[VC];
-        int total = 0;
+        // per view, this pixel's bins: trip counts differ by at most one bin
+        // between the lanes of a warp.  (A single flat loop over all the
+        // chunk's (view, bin) pairs, switching views per lane, measured 1.38x
+        // slower at 512^2 x 720 views: the warp ran the switch on most
+        // iterations.)  The bin loop is not unrolled: unrolled, it spills at
+        // the 48 registers five CTAs per SM allow.
+        float csum = 0.f;
 #pragma unroll
         for (int v = 0; v < VC; ++v) {
             const int lo = win[(slot * VC + v) * 2], hi = win[(slot * VC + v) * 2 + 1];
-            int a = 0, b = -1;
-            if (hi >= lo) {
-                box_bins(hs + (slot * VC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, a, b);
-                a = max(a, lo);
-                b = min(b, hi);
+            if (hi < lo) continue;
+            int a, b;
+            box_bins(hs + (slot * VC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, a, b);
+            a = max(a, lo);
+            b = min(b, hi);
+            const float4* rb = srec + (st * VC + v) * 4 * wcap - lo;
+            const float* sb = ssino + (st * VC + v) * wcap - lo;
+#pragma unroll 1
+            for (int u = a; u <= b; ++u) {
+                const B1Bin r{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]};
+                const float conv = b1_conv(fi, fj, r);
+                if (conv > kConvEps) csum = fmaf(conv, sb[u], csum);
             }
-            ulo[v] = a;
-            uhi[v] = b;
-            roff[v] = (st * VC + v) * 4 * wcap - lo;
-            soff[v] = (st * VC + v) * wcap - lo;
-            total += max(0, b - a + 1);
-        }
-        float csum = 0.f;
-        int v = 0, u = ulo[0], ue = uhi[0], ro = roff[0], so = soff[0];
-        for (int k = 0; k < total; ++k) {
-            while (u > ue) {
-                ++v;
-                u = pick(ulo, v);
-                ue = pick(uhi, v);
-                ro = pick(roff, v);
-                so = pick(soff, v);
-            }
-            const float4* rb = srec + ro + u;
-            const B1Bin r{rb[0], rb[wcap], rb[2 * wcap], rb[3 * wcap]};
-            const float conv = b1_conv(fi, fj, r);
-            if (conv > kConvEps) csum = fmaf(conv, ssino[so + u], csum);
-            ++u;
         }
         acc += (double)csum;
     }
