@@ -10,7 +10,14 @@
 //                         input tile and the COB x 9 weights are staged in
 //                         shared memory, each thread accumulates COB outputs
 //                         in registers; bias and ReLU fused.
-//   backward data         the same kernel on weights flipped in space and
+//   conv3x3_c32_kernel    32 output channels, input channels in groups of 8
+//                         (the network's middle layers): a CTA per 32x8
+//                         output tile and image, each thread 4 consecutive
+//                         pixels x 8 output channels in registers, the 8
+//                         input tiles and their 32x8x9 weights staged in
+//                         shared memory per group.  Same summation order per
+//                         output as conv3x3_fwd_kernel: bit-identical.
+//   backward data         the same kernels on weights flipped in space and
 //                         transposed in channels (flip_weights_kernel).
 //   conv3x3_wgrad_kernel  a CTA per (output channel, input channel, image
 //                         chunk): 9 + 1 sums per thread in registers over its
@@ -72,6 +79,80 @@ __global__ void __launch_bounds__(kT * kT) conv3x3_fwd_kernel(const float* __res
         float o = acc[c] + (bias ? bias[co] : 0.f);
         if (relu) o = fmaxf(o, 0.f);
         out[((size_t)n * Cout + co) * plane + (size_t)y * W + x] = o;
+    }
+}
+
+constexpr int kCW = 32, kCH = 8;  // output tile of conv3x3_c32_kernel
+constexpr int kCS = 35;            // staged row stride: lanes (row r, 4-pixel group g) read banks 3r + 4g + q
+constexpr int kCG = 8;             // input channels per staged group
+
+__global__ void __launch_bounds__(256, 2) conv3x3_c32_kernel(const float* __restrict__ in,
+                                                             const __nv_bfloat16* __restrict__ w,
+                                                             const float* __restrict__ bias, float* __restrict__ out,
+                                                             int Cin, int H, int W, int relu) {
+    __shared__ float tile[kCG][kCH + 2][kCS];
+    __shared__ __align__(16) float ws[kCG][9][32];
+    const int t = threadIdx.x;
+    const int cg = t >> 6;                     // output channels 8 cg .. 8 cg + 7 (warp-uniform)
+    const int ty = (t >> 3) & 7, tx4 = t & 7;  // output row, 4-pixel group
+    const int n = blockIdx.z;
+    const int x0 = blockIdx.x * kCW, y0 = blockIdx.y * kCH;
+    const size_t plane = (size_t)H * W;
+    float acc[4][8];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int c = 0; c < 8; ++c) acc[p][c] = 0.f;
+    for (int c0 = 0; c0 < Cin; c0 += kCG) {
+        constexpr int kRow = kCW + 2, kPlane = (kCH + 2) * kRow;
+        for (int e = t; e < kCG * kPlane; e += 256) {
+            const int c = e / kPlane, r = (e - c * kPlane) / kRow, q = e - c * kPlane - r * kRow;
+            const int yy = y0 + r - 1, xx = x0 + q - 1;
+            tile[c][r][q] = (yy >= 0 && yy < H && xx >= 0 && xx < W)
+                                ? __ldg(in + ((size_t)n * Cin + c0 + c) * plane + (size_t)yy * W + xx)
+                                : 0.f;
+        }
+        for (int e = t; e < 32 * kCG * 9; e += 256) {
+            const int co = e / (kCG * 9), c = (e / 9) % kCG, k = e % 9;
+            ws[c][k][co] = __bfloat162float(w[((size_t)co * Cin + c0 + c) * 9 + k]);
+        }
+        __syncthreads();
+#pragma unroll 1
+        for (int c = 0; c < kCG; ++c) {
+            float v[3][6];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) v[r][q] = tile[c][ty + r][4 * tx4 + q];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const float4 wa = *reinterpret_cast<const float4*>(&ws[c][k][8 * cg]);
+                const float4 wb = *reinterpret_cast<const float4*>(&ws[c][k][8 * cg + 4]);
+                const float wk[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const float a = v[k / 3][p + k % 3];
+#pragma unroll
+                    for (int co = 0; co < 8; ++co) acc[p][co] = fmaf(wk[co], a, acc[p][co]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    const int y = y0 + ty;
+    if (y >= H) return;
+#pragma unroll
+    for (int co = 0; co < 8; ++co) {
+        const int oc = 8 * cg + co;
+        const float bv = bias ? bias[oc] : 0.f;
+        float* dst = out + ((size_t)n * 32 + oc) * plane + (size_t)y * W;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int x = x0 + 4 * tx4 + p;
+            float o = acc[p][co] + bv;
+            if (relu) o = fmaxf(o, 0.f);
+            if (x < W) dst[x] = o;
+        }
     }
 }
 
@@ -171,7 +252,10 @@ __global__ void adam_kernel(float* __restrict__ w, __nv_bfloat16* __restrict__ w
 void conv_fwd(const float* in, const __nv_bfloat16* w, const float* bias, float* out, int N, int Cin, int Cout, int H,
               int W, int relu, cudaStream_t s) {
     if (N < 1 || Cin < 1 || Cout < 1 || H < 1 || W < 1) fail("conv3x3: invalid sizes");
-    if (Cout >= 8) {
+    if (Cout == 32 && Cin % kCG == 0) {
+        dim3 g((W + kCW - 1) / kCW, (H + kCH - 1) / kCH, N);
+        conv3x3_c32_kernel<<<g, 256, 0, s>>>(in, w, bias, out, Cin, H, W, relu);
+    } else if (Cout >= 8) {
         dim3 g((W + kT - 1) / kT, (H + kT - 1) / kT, N * ((Cout + 7) / 8));
         conv3x3_fwd_kernel<8><<<g, kT * kT, 0, s>>>(in, w, bias, out, Cin, Cout, H, W, relu);
     } else {

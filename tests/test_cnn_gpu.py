@@ -24,7 +24,8 @@ def rel(a, b):
     return float(np.linalg.norm(np.ravel(a) - np.ravel(b)) / max(np.linalg.norm(np.ravel(b)), 1e-300))
 
 
-@pytest.mark.parametrize("ci,co,h,w", [(1, 32, 19, 23), (32, 32, 16, 16), (32, 1, 33, 17), (3, 5, 8, 40)])
+@pytest.mark.parametrize("ci,co,h,w", [(1, 32, 19, 23), (32, 32, 16, 16), (32, 32, 37, 45), (16, 32, 9, 70),
+                                       (32, 1, 33, 17), (3, 5, 8, 40)])
 def test_conv_forward_and_gradients(ci, co, h, w):
     from sgd_b200 import _lib
     from sgd_b200.cnn import _declare, _stream
