@@ -124,6 +124,31 @@ def test_b1_zero_and_impulse():
     assert col.min() >= 0 and col.max() > 0
 
 
+@pytest.mark.parametrize("case", ["rect", "snap"])
+def test_b1_forward_and_back_evaluate_identical_entries(case):
+    """Each matrix entry A[r, c] read off the forward (column of an impulse
+    image) equals, bit for bit, the one read off the back projection (pixel c
+    of an impulse sinogram): the two kernels evaluate the same footprint with
+    the same rounding, whichever of their code paths (row- or column-major
+    strip, staged records) reaches the pair."""
+    from sgd_b200.torch_ops import FanProjector
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case(case)
+    P = FanProjector("b1", nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    rng = np.random.default_rng(0)
+    pixels = [(nx // 2, ny // 2), (3, ny - 5), (int(rng.integers(nx)), int(rng.integers(ny)))]
+    for ci, cj in pixels:
+        e = torch.zeros((nx, ny), device="cuda")
+        e[ci, cj] = 1.0
+        col = P.forward(e).flatten()
+        rows = torch.nonzero(col).flatten().tolist()
+        assert rows
+        for r in rows[:: max(1, len(rows) // 40)]:
+            y = torch.zeros(len(ang) * nu, device="cuda")
+            y[r] = 1.0
+            img = P.backward(y.view(len(ang), nu))
+            assert img[ci, cj].item() == col[r].item()
+
+
 def test_b1_autograd_finite_differences():
     """torch.autograd path on a 64x64 crop of the 512^2, 720-view geometry:
     central differences (step 1e-3) of L(x) = <w, A x> match <A^T w, v>."""
