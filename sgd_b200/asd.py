@@ -203,12 +203,16 @@ def make_pairs(geo, seeds, iters, k_in, count=64, noise_seed=0, nonneg=False):
     return torch.cat(xs)[:n], torch.cat(ts)[:n]
 
 
-def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0):
-    """Mean per-sample loss per epoch."""
+def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0, lr_final=None):
+    """Mean per-sample loss per epoch.  With lr_final the step size follows a
+    cosine from lr down to lr_final over the epochs."""
     gen = torch.Generator().manual_seed(seed)
     n = x.shape[0]
     losses = []
-    for _ in range(epochs):
+    lr0 = lr
+    for ep in range(epochs):
+        if lr_final is not None and epochs > 1:
+            lr = lr_final + 0.5 * (lr0 - lr_final) * (1.0 + math.cos(math.pi * ep / (epochs - 1)))
         perm = torch.randperm(n, generator=gen)
         tot = 0.0
         for k in range(0, n - batch + 1, batch):
@@ -249,9 +253,10 @@ def main():
     ap.add_argument("--train", type=int, default=2000)
     ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--k-in", type=int, default=5)
-    ap.add_argument("--epochs", type=int, default=20)
+    ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-final", type=float, default=1e-4)
     args = ap.parse_args()
     from .cnn import WarmStartCNN
     geo = Geometry(args.n, args.views)
@@ -260,11 +265,15 @@ def main():
     t_pairs = time.perf_counter() - t0
     net = WarmStartCNN(seed=0)
     t0 = time.perf_counter()
-    losses = train(net, xs, ts, epochs=args.epochs, batch=args.batch, lr=args.lr)
+    losses = train(net, xs, ts, epochs=args.epochs, batch=args.batch, lr=args.lr, lr_final=args.lr_final)
     t_train = time.perf_counter() - t0
     del xs, ts
     truth, sino, _ = simulate(geo, list(range(args.images)), noise_seed=999)
     solver = ASDPOCS(geo, args.images, nonneg=False)
+    # one untimed pass of the network at the reconstruction's shape: a
+    # deployed network is loaded and its kernels initialised once
+    net.forward(torch.zeros((args.images, 1, args.n, args.n), device="cuda"))
+    torch.cuda.synchronize()
     plain = plain_curve(solver, sino, truth, args.iters)
     target = plain[-1][2]
     info = {}

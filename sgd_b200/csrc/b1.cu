@@ -128,6 +128,9 @@ size_t b1_back_smem_bytes(int wcap) { return b1_back_smem<kVC>(wcap); }
 
 void b1_prepare_device() {
     SGD_CUDA(cudaFuncSetAttribute(b1_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    // the whole unified L1 as shared memory: five CTAs of staged windows per SM
+    SGD_CUDA(cudaFuncSetAttribute(b1_back_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
 }
 
 void b1_forward_launch(const B1Device& d, const float* img, float* imgT, float* sino, cudaStream_t s) {

@@ -201,6 +201,12 @@ B1Batch::B1Batch(int ns, const int* nx, const int* ny, const int* np, const int*
     SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<4>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<8>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
     set_variant(8, 4);
 }
 

@@ -4,11 +4,12 @@
 //   b1_forward_row   detector-driven: one warp per (view, bin).  Lanes split
 //                    the lines (major axis) the bin's ray strip crosses; each
 //                    lane evaluates the footprint of the few pixels of its line
-//                    inside the strip, and the warp reduces with shuffles.  The
-//                    sinogram value is written once, no atomics.
+//                    inside the strip (packed-pair form, b1_kernels.cuh), and
+//                    the warp reduces with shuffles.  The sinogram value is
+//                    written once, no atomics.
 //   b1_back_tile     voxel-driven: one thread per pixel of a 32x8 tile.  Per
 //                    chunk of VC views the CTA stages the bin window its tile
-//                    projects onto in shared memory: the 96-byte footprint
+//                    projects onto in shared memory: the 64-byte footprint
 //                    records by TMA bulk copies completed on an mbarrier
 //                    (double-buffered, the next chunk in flight while this one
 //                    is evaluated), the sinogram values by plain loads.  Each
@@ -50,16 +51,11 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-constexpr int kBinF4 = sizeof(B1Bin) / sizeof(float4);  // float4 per record
-static_assert(sizeof(B1Bin) == kB1Rec * sizeof(float), "record layout");
-
-// Records are laid out [view][bin][6 float4] (fan_geometry.h).
+// Records are float4 chunks laid out [view][chunk][bin] (fan_geometry.h).
 __device__ __forceinline__ B1Bin load_bin(const float4* rec, int p, int u, int nu) {
-    const float4* q = rec + ((size_t)p * nu + u) * kBinF4;
-    return B1Bin{__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), __ldg(q + 4), __ldg(q + 5)};
+    const float4* q = rec + (size_t)p * 4 * nu + u;
+    return B1Bin{__ldg(q), __ldg(q + nu), __ldg(q + 2 * nu), __ldg(q + 3 * nu)};
 }
-
-__device__ __forceinline__ B1Bin smem_bin(const float4* q) { return B1Bin{q[0], q[1], q[2], q[3], q[4], q[5]}; }
 
 // Candidate minor indices of major line m: the strip between the edge rays over
 // the lines m-1..m+1 a pixel's support covers, widened by the +-1 pixel support
@@ -81,7 +77,7 @@ __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, c
                                                float* __restrict__ sino, int nx, int ny, int nu, float dxdy,
                                                long long gw, int lane) {
     const int p = (int)(gw / nu), u = (int)(gw - (long long)p * nu);
-    const B1Bin r = load_bin(rec, p, u, nu);
+    const B1Pair k = b1_pair(load_bin(rec, p, u, nu));
     const float4 st = __ldg(reinterpret_cast<const float4*>(strip + gw * kStripRec));
     const bool ydom = __ldg(strip + gw * kStripRec + 4) > 0.5f;
     const float aa = fabsf(st.y), ab = fabsf(st.w);
@@ -96,12 +92,12 @@ __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, c
             const float fm = (float)m;
             int nlo, nhi;
             strip_span(st, aa, ab, fm, nx, nlo, nhi);
-            const float2 inner = b1_inner(pair(fm), r);
+            const float2 inner = b1_inner2(pair(fm), k);
             float row = 0.f;
             float2 fn = pair((float)nlo);
             const float* sp = img + (size_t)nlo * ny + m;
             for (int n = nlo; n <= nhi; ++n, fn = __fadd2_rn(fn, pair(1.0f)), sp += ny) {
-                const float conv = b1_conv_x(b1_edges(fn, inner, r), r);
+                const float conv = b1_conv_pair(b1_edges2(fn, inner, k), k);
                 if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
             }
             acc += (double)row;
@@ -116,7 +112,7 @@ __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, c
             float2 fn = pair((float)nlo);
             const float* sp = imgT + (size_t)nlo * nx + m;
             for (int n = nlo; n <= nhi; ++n, fn = __fadd2_rn(fn, pair(1.0f)), sp += nx) {
-                const float conv = b1_conv_x(b1_edges(fm, b1_inner(fn, r), r), r);
+                const float conv = b1_conv_pair(b1_edges2(fm, b1_inner2(fn, k), k), k);
                 if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
             }
             acc += (double)row;
@@ -144,15 +140,14 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);           // [2]
     int* win = reinterpret_cast<int*>(smem + 16);                   // [3][VC][2]
     float* hs = reinterpret_cast<float*>(smem + 16 + 3 * VC * 8);  // [3][VC][8]
-    float4* srec = reinterpret_cast<float4*>(smem + kHeader);      // [2][VC][wcap][6]
-    float* ssino = reinterpret_cast<float*>(srec + 2 * VC * wcap * kBinF4);  // [2][VC][wcap]
+    float4* srec = reinterpret_cast<float4*>(smem + kHeader);      // [2][VC][4 chunks][wcap]
+    float* ssino = reinterpret_cast<float*>(srec + 2 * VC * 4 * wcap);  // [2][VC][wcap]
 
     // each warp covers an 8 (j) x 4 (i) block of the 32 x 8 tile, so that its
     // lanes read few distinct bins of a view
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
     const int i = i0 + 4 * (w >> 2) + (l >> 3), j = j0 + 8 * (w & 3) + (l & 7);
     const float fi = (float)i, fj = (float)j;
-    const float2 fi2 = pair(fi), fj2 = pair(fj);
     const int nchunks = (np + VC - 1) / VC;
     auto parity = [&](int c) { return (((c & 1) ? use1 : use0) + (uint32_t)(c >> 1)) & 1u; };
 
@@ -180,9 +175,9 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             for (int v = 0; v < VC; ++v) {
                 const int lo = win[(slot * VC + v) * 2], W = win[(slot * VC + v) * 2 + 1] - lo + 1;
                 if (W > 0)
-                    bulk_copy_g2s(srec + (size_t)(st * VC + v) * wcap * kBinF4,
-                                  rec + ((size_t)(c * VC + v) * nu + lo) * kBinF4, (uint32_t)W * sizeof(B1Bin),
-                                  &bars[st]);
+                    for (int q = 0; q < 4; ++q)
+                        bulk_copy_g2s(srec + ((st * VC + v) * 4 + q) * wcap,
+                                      rec + ((size_t)(c * VC + v) * 4 + q) * nu + lo, (uint32_t)W * 16u, &bars[st]);
             }
         }
         for (int v = 0; v < VC; ++v) {
@@ -226,12 +221,12 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             box_bins(hs + (slot * VC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, a, b);
             a = max(a, lo);
             b = min(b, hi);
-            const float4* rb = srec + ((st * VC + v) * wcap - lo) * kBinF4;
+            const float4* rb = srec + (st * VC + v) * 4 * wcap - lo;
             const float* sb = ssino + (st * VC + v) * wcap - lo;
 #pragma unroll 1
             for (int u = a; u <= b; ++u) {
-                const B1Bin r = smem_bin(rb + u * kBinF4);
-                const float conv = b1_conv_x(b1_edges(fi2, b1_inner(fj2, r), r), r);
+                const B1Bin r{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]};
+                const float conv = b1_conv(fi, fj, r);
                 if (conv > kConvEps) csum = fmaf(conv, sb[u], csum);
             }
         }

@@ -31,8 +31,8 @@ namespace sgd {
 namespace {
 
 __device__ __forceinline__ B1Bin bin_record(const float4* rec, int p, int u, int nu) {
-    const float4* q = rec + ((size_t)p * nu + u) * (sizeof(B1Bin) / sizeof(float4));
-    return B1Bin{__ldg(q), __ldg(q + 1), __ldg(q + 2), __ldg(q + 3), __ldg(q + 4), __ldg(q + 5)};
+    const float4* q = rec + (size_t)p * 4 * nu + u;
+    return B1Bin{__ldg(q), __ldg(q + nu), __ldg(q + 2 * nu), __ldg(q + 3 * nu)};
 }
 
 __device__ __forceinline__ void hom_of(const BinHomography* hom, int p, float* h) {
@@ -82,12 +82,11 @@ struct B1GenVisit {
         for (int u = lo; u <= hi; ++u) {
             const B1Bin r = bin_record(rec, p, u, nu);
             const float4 g = __ldg(gen + (size_t)p * nu + u);
-            const float2 e = b1_edges(pair(fi), b1_inner(pair(fj), r), r);
-            const float xa = e.x, xb = e.y;
+            const float xa = b1_xa(fi, b1_xa_inner(fj, r), r), xb = b1_xb(fi, b1_xb_inner(fj, r), r);
             const float w = fabsf(xb - xa), m = fminf(fabsf(xa), fabsf(xb));
             if (m * g.x > dx && m * g.y > dy) continue;
             if (fabsf(xa) > g.z + w) continue;
-            const float conv = b1_conv_x(make_float2(-xa, -xa + w), r);
+            const float conv = b1_conv_x(-xa, -xa + w, r);
             if (conv > 0.f) f(u, conv);
         }
     }

@@ -36,6 +36,8 @@ __global__ void __launch_bounds__(256) fan2d_back_kernel(Fan2DParams P, const fl
         img[idx] = 0.f;
         return;
     }
+    // FP64 products and sums, as the forward kernel: the pair is an adjoint
+    // pair to FP64 rounding, whatever the cancellation in the inputs
     double acc = 0.0;
     for (int p = 0; p < P.np; ++p) {
         typename B::View V;
@@ -43,12 +45,10 @@ __global__ void __launch_bounds__(256) fan2d_back_kernel(Fan2DParams P, const fl
         typename B::Cell c;
         B::setup(V, i, j, P, c);
         const float* sp = sino + (size_t)p * P.nu;
-        float vs = 0.f;
         for (int u = c.lo; u <= c.hi; ++u) {
             const float val = B::value(V, c, u, p, P);
-            if (val != 0.f) vs = fmaf(val, __ldg(sp + u), vs);
+            if (val != 0.f) acc = fma((double)val, (double)__ldg(sp + u), acc);
         }
-        acc += (double)vs;
     }
     img[idx] = (float)acc;
 }
@@ -56,7 +56,8 @@ __global__ void __launch_bounds__(256) fan2d_back_kernel(Fan2DParams P, const fl
 template <class B>
 __global__ void __launch_bounds__(kF2Threads) fan2d_forward_kernel(Fan2DParams P, const float* __restrict__ img,
                                                                   double* __restrict__ sino64) {
-    extern __shared__ float s_acc[];  // [kF2Views][wcap]
+    extern __shared__ __align__(8) unsigned char f2_smem[];
+    double* s_acc = reinterpret_cast<double*>(f2_smem);  // [kF2Views][wcap], FP64: see the back kernel
     const int tid = threadIdx.x;
     const int i = blockIdx.y * kF2TileI + (tid >> 5), j = blockIdx.x * kF2TileJ + (tid & 31);
     const int2* twin = P.wins + (size_t)(blockIdx.y * P.tiles_j + blockIdx.x) * P.np;
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(kF2Threads) fan2d_forward_kernel(Fan2DParams P
     const float C = mine ? __ldg(img + (size_t)i * P.nj + j) : 0.f;
     for (int p0 = 0; p0 < P.np; p0 += kF2Views) {
         __syncthreads();  // previous chunk's windows flushed
-        for (int e = tid; e < kF2Views * P.wcap; e += kF2Threads) s_acc[e] = 0.f;
+        for (int e = tid; e < kF2Views * P.wcap; e += kF2Threads) s_acc[e] = 0.0;
         __syncthreads();
         if (C != 0.f) {
             for (int v = 0; v < kF2Views && p0 + v < P.np; ++v) {
@@ -75,10 +76,10 @@ __global__ void __launch_bounds__(kF2Threads) fan2d_forward_kernel(Fan2DParams P
                 typename B::Cell c;
                 B::setup(V, i, j, P, c);
                 const int lo = max(c.lo, w.x), hi = min(c.hi, w.y);
-                float* acc = s_acc + v * P.wcap - w.x;
+                double* acc = s_acc + v * P.wcap - w.x;
                 for (int u = lo; u <= hi; ++u) {
                     const float val = B::value(V, c, u, p, P);
-                    if (val != 0.f) atomicAdd(acc + u, val * C);
+                    if (val != 0.f) atomicAdd(acc + u, (double)val * (double)C);
                 }
             }
         }
@@ -86,8 +87,8 @@ __global__ void __launch_bounds__(kF2Threads) fan2d_forward_kernel(Fan2DParams P
         for (int v = 0; v < kF2Views && p0 + v < P.np; ++v) {
             const int2 w = __ldg(twin + p0 + v);
             for (int k = tid; k <= w.y - w.x; k += kF2Threads) {
-                const float a = s_acc[v * P.wcap + k];
-                if (a != 0.f) atomicAdd(sino64 + (size_t)(p0 + v) * P.nu + w.x + k, (double)a);
+                const double a = s_acc[v * P.wcap + k];
+                if (a != 0.0) atomicAdd(sino64 + (size_t)(p0 + v) * P.nu + w.x + k, a);
             }
         }
     }

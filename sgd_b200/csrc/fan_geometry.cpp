@@ -165,18 +165,16 @@ void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out) {
 
 void b1_profile_constants(double a, double b, float* r) {
     if (b <= 1e-7) b = 0.0;  // single-triangle limit
-    const float c[9] = {(float)b,
-                        (float)(a + b),
-                        (float)a,
-                        (float)(1.0 / (2.0 * a * a)),
-                        (float)(1.0 / a),
-                        -(float)(b * b / (12.0 * a * a)),
-                        b > 0 ? (float)(1.0 / (12.0 * a * a * b * b)) : 0.f,
-                        b > 0 ? -(float)(1.0 / (24.0 * a * a * b * b)) : 0.f,
-                        (float)(a - b)};
-    for (int k = 0; k < 8; ++k) r[6 + 2 * k] = r[7 + 2 * k] = c[k];
-    r[22] = c[8];
-    r[23] = 0.f;
+    r[6] = (float)a;
+    r[7] = (float)b;
+    r[8] = (float)(a + b);
+    r[9] = (float)(a - b);
+    r[10] = (float)(1.0 / a);
+    r[11] = (float)(1.0 / (2.0 * a * a));
+    r[12] = (float)(b * b / (12.0 * a * a));
+    r[13] = b > 0 ? (float)(1.0 / (12.0 * a * a * b * b)) : 0.f;
+    r[14] = b > 0 ? (float)(1.0 / (24.0 * a * a * b * b)) : 0.f;
+    r[15] = 0.f;
 }
 
 void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>& strip) {
@@ -205,16 +203,17 @@ void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>
             const double mBx = kb * tx - nxv, mBy = kb * ty - nyv;
             float r[kB1Rec];
             r[0] = (float)(mAx * g.dx);
-            r[1] = (float)(mBx * g.dx);
-            r[2] = (float)(mAy * g.dy);
-            r[3] = (float)(mBy * g.dy);
-            r[4] = (float)((x0 - px) * mAx + (y0 - py) * mAy);
+            r[1] = (float)(mAy * g.dy);
+            r[2] = (float)((x0 - px) * mAx + (y0 - py) * mAy);
+            r[3] = (float)(mBx * g.dx);
+            r[4] = (float)(mBy * g.dy);
             r[5] = (float)((x0 - px) * mBx + (y0 - py) * mBy);
             // profile half-widths (layers/A_B1.cu:429-478): vx = |dx cos(theta)|,
             // vy = |dy sin(theta)| with theta = atan2(|px - sx|, |py - sy|)
             const double vx = std::fabs(g.dx * ty), vy = std::fabs(g.dy * tx);
             b1_profile_constants(std::max(vx, vy), std::min(vx, vy), r);
-            std::copy(r, r + kB1Rec, rec.begin() + ((size_t)p * nu + u) * kB1Rec);
+            for (int q = 0; q < 4; ++q)
+                for (int k = 0; k < 4; ++k) rec[(((size_t)p * 4 + q) * nu + u) * 4 + k] = r[4 * q + k];
 
             // strip of the bin in index space for the forward kernel
             float* s = &strip[((size_t)p * nu + u) * kStripRec];

@@ -83,19 +83,16 @@ void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out);
 //     S(x) = 1/2 - (p^4 - 2q^4 - 2w^4)/(24a^2b^2)               for x >  a - b
 // Every power is of a distance to a nearby knot, so FP32 keeps its accuracy as
 // b -> 0; b <= 1e-7 uses the single-triangle limit as the reference does
-// (layers/A_B1.cu:52-55).  One 96-byte record per (view, bin), laid out
-// [view][bin][24 floats] so that one bulk copy stages a view's bin window.
-// The constants come in pairs, the operands of the packed-FP32 instructions
-// that evaluate the bin's two edges at once (b1_kernels.cuh):
-//   [0..1]   i coefficients of (xa, xb)     xa = i*r[0] + (j*r[2] + r[4])
-//   [2..3]   j coefficients of (xa, xb)     xb = i*r[1] + (j*r[3] + r[5])
-//   [4..5]   constant terms of (xa, xb)
-//   [6..7]   b, b          [8..9]   a+b, a+b      [10..11] a, a
-//   [12..13] 1/(2a^2) x2   [14..15] 1/a x2
-//   [16..17] -b^2/(12a^2) x2                      [18..19] 1/(12a^2b^2) x2
-//   [20..21] -1/(24a^2b^2) x2                     [22] a-b   [23] unused (0)
+// (layers/A_B1.cu:52-55).  One 64-byte record per (view, bin), stored as four
+// float4 chunks in the layout [view][chunk][bin] so that consecutive bins of
+// one chunk are consecutive 16-byte words (shared-memory bank groups):
+//   [0..2]  xa = i*r[0] + j*r[1] + r[2]
+//   [3..5]  xb = i*r[3] + j*r[4] + r[5]
+//   [6] a   [7] b   [8] a+b   [9] a-b
+//   [10] 1/a   [11] 1/(2a^2)   [12] b^2/(12a^2)   [13] 1/(12a^2b^2)   [14] 1/(24a^2b^2)
+//   [15] unused (0)
 // ---------------------------------------------------------------------------
-constexpr int kB1Rec = 24;
+constexpr int kB1Rec = 16;
 
 // Strip parameters for the detector-driven forward kernel: along the major
 // axis index m, the two edge rays cross the minor axis at
@@ -103,7 +100,7 @@ constexpr int kB1Rec = 24;
 // [4] = 1 when the major axis is y (rows), 0 when it is x (columns).
 constexpr int kStripRec = 8;
 
-// Fills r[6..23] for profile half-widths a >= b.
+// Fills r[6..15] for profile half-widths a >= b.
 void b1_profile_constants(double a, double b, float* r);
 
 void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>& strip);

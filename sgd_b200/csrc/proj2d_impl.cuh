@@ -43,7 +43,7 @@ void Proj2D::finish_init(const std::vector<float>& view, int view_floats, const 
         }
     P.tiles_j = tj;
     P.wcap = wmax;
-    smem_fwd_ = (size_t)kF2Views * wmax * sizeof(float);
+    smem_fwd_ = (size_t)kF2Views * wmax * sizeof(double);
     if (smem_fwd_ > 48 * 1024) fail("forward tile window of %d bins does not fit in shared memory", wmax);
     SGD_CUDA(cudaMalloc(&d_wins_, wins.size() * sizeof(int2)));
     SGD_CUDA(cudaMemcpy(d_wins_, wins.data(), wins.size() * sizeof(int2), cudaMemcpyHostToDevice));
