@@ -151,33 +151,36 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     const int nchunks = (np + VC - 1) / VC;
     auto parity = [&](int c) { return (((c & 1) ? use1 : use0) + (uint32_t)(c >> 1)) & 1u; };
 
-    // stage chunk c: windows and homographies (thread 0, read after the next
-    // barrier), footprint records by TMA (thread 0), sinogram values (all)
+    // stage chunk c: windows and homographies (read after the next barrier)
+    // and footprint records by TMA, lane v of warp 0 taking view v; sinogram
+    // values by all threads
     auto stage = [&](int c) {
         const int st = c & 1, slot = c % 3;
-        if (tid == 0) {
+        if (w == 0) {
+            const int p = c * VC + l;
+            int2 lh = make_int2(0, -1);
             uint32_t bytes = 0;
-            for (int v = 0; v < VC; ++v) {
-                const int p = c * VC + v;
-                int2 lh = make_int2(0, -1);
+            if (l < VC) {
                 if (p < np) {
                     lh = __ldg(twin + p);
                     const BinHomography H = hom[p];
-                    float* h = hs + (slot * VC + v) * 8;
+                    float* h = hs + (slot * VC + l) * 8;
                     h[0] = H.n0; h[1] = H.n1; h[2] = H.n2; h[3] = H.d0; h[4] = H.d1; h[5] = H.d2;
                 }
-                win[(slot * VC + v) * 2] = lh.x;
-                win[(slot * VC + v) * 2 + 1] = lh.y;
-                if (lh.y >= lh.x) bytes += (uint32_t)(lh.y - lh.x + 1) * sizeof(B1Bin);
+                win[(slot * VC + l) * 2] = lh.x;
+                win[(slot * VC + l) * 2 + 1] = lh.y;
+                if (lh.y >= lh.x) bytes = (uint32_t)(lh.y - lh.x + 1) * sizeof(B1Bin);
             }
-            fence_proxy_async_smem();
-            mbar_arrive_expect_tx(&bars[st], bytes);
-            for (int v = 0; v < VC; ++v) {
-                const int lo = win[(slot * VC + v) * 2], W = win[(slot * VC + v) * 2 + 1] - lo + 1;
-                if (W > 0)
-                    for (int q = 0; q < 4; ++q)
-                        bulk_copy_g2s(srec + ((st * VC + v) * 4 + q) * wcap,
-                                      rec + ((size_t)(c * VC + v) * 4 + q) * nu + lo, (uint32_t)W * 16u, &bars[st]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+            if (l == 0) mbar_arrive_expect_tx(&bars[st], bytes);
+            __syncwarp();
+            if (l < VC && lh.y >= lh.x) {
+                fence_proxy_async_smem();
+                const uint32_t n = (uint32_t)(lh.y - lh.x + 1) * 16u;
+                for (int q = 0; q < 4; ++q)
+                    bulk_copy_g2s(srec + ((st * VC + l) * 4 + q) * wcap, rec + ((size_t)p * 4 + q) * nu + lh.x, n,
+                                  &bars[st]);
             }
         }
         for (int v = 0; v < VC; ++v) {
