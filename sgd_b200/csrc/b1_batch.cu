@@ -76,10 +76,13 @@ b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict
     __shared__ int s_abort;
     __shared__ long long s_item;
     if (threadIdx.x == 0) {
-        b1_back_init(smem);
+        uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
         s_abort = 0;
     }
-    uint32_t gseq = 0;
+    uint32_t use0 = 0, use1 = 0;
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_item = (long long)atomicAdd(counter, 1ull);
@@ -92,7 +95,7 @@ b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict
         const int bx = t % S.tiles_x, by = t / S.tiles_x;
         if (!b1_back_tile<VC>(S.rec, S.hom, S.wins + (size_t)t * S.np, sino + S.sino_off, img + S.img_off, S.nx,
                               S.ny, S.np, S.nu, S.wcap, S.dxdy, err, by * kBackTI, bx * kBackTJ, smem, s_abort,
-                              gseq))
+                              use0, use1))
             return;
     }
 }
