@@ -49,15 +49,71 @@ CONFIG = {
 FLUSH_BYTES = 256 << 20
 
 
+def max_over_ranks(x, world, device):
+    """The largest of every rank's x (all ranks call it, in the same order):
+    a multi-rank time is the slowest rank's."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _families():
+    """name -> (description, constructor of a sgd_b200.torch_ops projector,
+    voxel-views per direction, seeded input maker)."""
+    C3_ANG = 2 * np.pi * np.arange(360) / 360
+    C5_ANG = 2 * np.pi * np.arange(360) / 360
+
+    def fan(kind):
+        from sgd_b200.torch_ops import FanProjector
+        return FanProjector(kind, NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES)
+
+    def par():
+        from sgd_b200.torch_ops import ParallelB0Projector
+        return ParallelB0Projector(128, 128, 185, 1.0, 1.0, 1.0, np.pi * np.arange(180) / 180)
+
+    def hexp(mode, nl, nc, dt):
+        from sgd_b200.torch_ops import HexProjector
+        return HexProjector(nl, nc, NU, dt, DU, LSD, LSO, C3_ANG, mode=mode)
+
+    def cone(kind):
+        from sgd_b200.torch_ops import ConeProjector
+        return ConeProjector(kind, 256, 256, 256, 384, 384, 1.0, 1.0, 1.0, 1.5, 1.5, LSD, LSO, C5_ANG)
+
+    return {
+        "sf_c2": ("A_SF separable footprint fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
+                  lambda: fan("SF"), NX * NY * NP),
+        "b0_c2": ("A_B0 pixel basis fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
+                  lambda: fan("b0"), NX * NY * NP),
+        "b0_parallel_c1": ("B0 parallel beam, 128x128 @1mm, 180 views over pi, 185 bins @1mm",
+                           par, 128 * 128 * 180),
+        "h0_c3": ("H0 hexagonal lattice (true hexagon bounds), 550 rows x 477 sites, dt 0.62 mm, 360 views, "
+                  "736 bins @1mm", lambda: hexp("h0c", 550, 477, 0.62), 550 * 477 * 360),
+        "hl_c3": ("Hl hexagonal lattice, 953 rows x 275 sites, dt 1.075 mm, 360 views, 736 bins @1mm",
+                  lambda: hexp("hl", 953, 275, 1.075), 953 * 275 * 360),
+        "b1_3d_c5": ("A_B1_3D cone beam (exact-transpose pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
+                     lambda: cone("b1_3d"), 256 ** 3 * 360),
+        "sf3d_c5": ("SF_projector cone beam (corrected pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
+                    lambda: cone("sf3d"), 256 ** 3 * 360),
+    }
+
+
+FAMILIES = ("sf_c2", "b0_c2", "b0_parallel_c1", "h0_c3", "hl_c3", "b1_3d_c5", "sf3d_c5")
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["c2", "batch48"], default="c2",
+    ap.add_argument("--workload", choices=["c2", "batch48"] + sorted(FAMILIES), default="c2",
                     help="c2: the headline single-slice workload; batch48: 48 uneven slices in one "
-                         "graph-replayed persistent launch per direction")
+                         "graph-replayed persistent launch per direction; the others: the other projector "
+                         "families at their configurations (device-resident fwd+adj)")
     return ap.parse_args()
 
 
@@ -246,10 +302,7 @@ def run_ours(args, rank, world, local_rank):
     fwd_ms = [ev[k][0].elapsed_time(ev[k][1]) for k in range(K)]
     bwd_ms = [ev[k][1].elapsed_time(ev[k][2]) for k in range(K)]
     step_ms = sum(f + b for f, b in zip(fwd_ms, bwd_ms)) / K
-    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms = float(t.item())
+    step_ms = max_over_ranks(step_ms, world, dev)
     units = 2.0 * NX * NY * NP
     value = world * units / (step_ms * 1e-3)
 
@@ -265,10 +318,7 @@ def run_ours(args, rank, world, local_rank):
         yh = A.matvec(xh)
         A.rmatvec(yh)
     e2e_s = (time.perf_counter() - t0) / ke
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * units / float(te.item())
+    e2e_value = world * units / max_over_ranks(e2e_s, world, dev)
 
     if rank != 0:
         return
@@ -362,11 +412,7 @@ def run_batch48(args, rank, world, local_rank):
     clocks = sampler.stop()
     B.status()
     step_ms = sum(e[0].elapsed_time(e[1]) for e in ev) / K
-    t = torch.tensor([step_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms = float(t.item())
+    step_ms = max_over_ranks(step_ms, world, dev)
     units = 2.0 * sum(s[0] * s[1] * len(s[8]) for s in slices)
     if rank != 0:
         return
@@ -381,6 +427,57 @@ def run_batch48(args, rank, world, local_rank):
                    "voxel_views": units / 2, "variant": {"fw": fw, "vc": vc, "from_cache": loaded},
                    "l2": "flushed between steps (256 MiB write outside the timed events)"},
         "gpu_launches": 3 * K, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_family(args, rank, world, local_rank):
+    """Device-resident forward + adjoint of one of the other projector
+    families (FAMILIES), timed like the headline workload."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    desc, make, vv = _families()[args.workload]
+    P = make()
+    g = torch.Generator(device=dev).manual_seed(rank)
+    x = torch.rand(P.image_shape, device=dev, generator=g)
+    y = torch.empty(P.sino_shape, device=dev)
+    b = torch.empty(P.image_shape, device=dev)
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        P.forward(x, out=y)
+        P.backward(y, out=b)
+    torch.cuda.synchronize(dev)
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(K)]
+    sampler = ClockSampler("GPU-" + str(torch.cuda.get_device_properties(dev).uuid))
+    time.sleep(0.3)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    for k in range(K):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        P.forward(x, out=y)
+        ev[k][1].record(stream)
+        P.backward(y, out=b)
+        ev[k][2].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    fwd = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    bwd = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    step_ms = max_over_ranks(fwd + bwd, world, dev)
+    if rank != 0:
+        return
+    line = {
+        "metric": f"fwd+adj voxel-view updates/s ({args.workload})", "value": world * 2.0 * vv / (step_ms * 1e-3),
+        "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": step_ms,
+        "fwd_ms": fwd, "bwd_ms": bwd, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (uniform random image)",
+        "config": {"workload": desc, "voxel_views": vv,
+                   "l2": "flushed between steps (256 MiB write outside the timed events)"},
+        "gpu_launches": None, "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
 
@@ -402,6 +499,8 @@ def main():
     try:
         if args.workload == "batch48":
             run_batch48(args, rank, world, local_rank)
+        elif args.workload in FAMILIES:
+            run_family(args, rank, world, local_rank)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

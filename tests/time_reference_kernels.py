@@ -1,0 +1,108 @@
+"""Times the reference's own CUDA projector kernels (oracle/_ref/libnetwork.so,
+built from the reference's sources) beside this library's, on the same GPU
+and the headline geometry (512x512 @0.5 mm, 720 views over 2 pi, 736 bins @1 mm,
+SOD 595 mm, SDD 1085.6 mm).  Test infrastructure: a measurement of the
+reference, not part of the product.
+
+    python tests/time_reference_kernels.py [--reps 5]
+
+Per projector kind (b1, SF, b0) one JSON line: kernel-only milliseconds per
+direction for both (device-resident buffers; the reference's through the
+layer's project/back_project, its per-view launches included) and the
+end-to-end milliseconds of one forward + one backward through the FP64 host
+C ABI (host copies and conversions included)."""
+import argparse
+import ctypes
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [HERE, os.path.dirname(HERE)]
+
+import reflib  # noqa: E402
+
+NX = NY = 512
+DX = DY = 0.5
+NP, NU, DU = 720, 736, 1.0
+LSD, LSO = 1085.6, 595.0
+ANGLES = 2 * np.pi * np.arange(NP) / NP
+
+
+def ours(kind, reps):
+    import torch
+    from sgd_b200 import operators as ops
+    from sgd_b200.phantom import ellipse_phantom
+    from sgd_b200.torch_ops import FanProjector
+    P = FanProjector(kind, NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES)
+    x = torch.tensor(ellipse_phantom(NX, NY, DX, DY, seed=0), dtype=torch.float32, device="cuda")
+    y = P.forward(x)
+    b = P.backward(y)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    e[0].record()
+    for _ in range(reps):
+        P.forward(x, out=y)
+    e[1].record()
+    for _ in range(reps):
+        P.backward(y, out=b)
+    e[2].record()
+    torch.cuda.synchronize()
+    cls = {"b1": ops.A_B1_operator, "SF": ops.A_SF_operator, "b0": ops.A_B0_operator}[kind]
+    A = cls(NX, NY, NP, NU, DX, DY, DU, LSD, LSO, ANGLES)
+    xh = ellipse_phantom(NX, NY, DX, DY, seed=0).ravel()
+    A.rmatvec(A.matvec(xh))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        A.rmatvec(A.matvec(xh))
+    e2e = (time.perf_counter() - t0) / reps * 1e3
+    return e[0].elapsed_time(e[1]) / reps, e[1].elapsed_time(e[2]) / reps, e2e
+
+
+def reference(kind, reps):
+    from sgd_b200.phantom import ellipse_phantom
+    L = reflib.lib()
+    R = reflib.RefFan2D(kind, NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES)
+    fn = getattr(L, f"ref_{kind.lower()}_kernel_ms")
+    fn.restype = ctypes.c_float
+    fn.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    back = ctypes.c_float(0.0)
+    fwd = fn(R.h, reps, ctypes.byref(back))
+    xh = ellipse_phantom(NX, NY, DX, DY, seed=0).ravel()
+    yh, _ = R.forward(xh)
+    R.backward(yh)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        yh, _ = R.forward(xh)
+        R.backward(yh)
+    e2e = (time.perf_counter() - t0) / reps * 1e3
+    return fwd, back.value, e2e
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--kinds", default="b1,SF,b0")
+    args = ap.parse_args()
+    if not reflib.available():
+        print(json.dumps({"unavailable": "oracle/_ref/libnetwork.so not built (make -C oracle ref)"}))
+        return
+    units = 2.0 * NX * NY * NP
+    for kind in args.kinds.split(","):
+        rf, rb, re = reference(kind, args.reps)
+        of, ob, oe = ours(kind, args.reps)
+        print(json.dumps({
+            "kind": kind, "geometry": "512x512 @0.5mm, 720 views, 736 bins @1mm, SOD 595, SDD 1085.6",
+            "reference_ms": {"fwd": rf, "back": rb, "e2e_fwd_back": re},
+            "ours_ms": {"fwd": of, "back": ob, "e2e_fwd_back": oe},
+            "kernel_speedup": (rf + rb) / (of + ob), "e2e_speedup": re / oe,
+            "ours_updates_per_s": units / ((of + ob) * 1e-3),
+            "reference_updates_per_s": units / ((rf + rb) * 1e-3),
+        }), flush=True)
+
+
+if __name__ == "__main__":
+    main()
