@@ -177,7 +177,34 @@ struct HexBasis {
         }
         return m == 2 ? v[0] : (m == 3 ? v[0] / 2.0 : v[0] / 6.0);
     }
-    // bins: [view][bin][va, vb, vc, 0] doubles
+    // conv4 when all four directions are kept (every bin but those whose ray
+    // makes a lattice direction vanish): the same corners and nesting, the
+    // divisions by h_k as products with host-computed FP64 reciprocals (1/vblur
+    // once per call), unrolled so that the 16 corner values stay in registers
+    __device__ static double conv4_full(double y, double h1, double h2, double h3, double h4, double r2, double r3,
+                                        double r4) {
+        const double hs[4] = {h1, h2, h3, h4};
+        const double rs[4] = {1.0 / h1, r2, r3, r4};
+        double v[16];
+#pragma unroll
+        for (int s = 0; s < 16; ++s) {
+            double yy = y;
+#pragma unroll
+            for (int k = 3; k >= 0; --k)
+                if (s & (1 << (3 - k))) yy = yy - hs[k];
+            v[s] = yy > 0 ? yy * yy * yy : 0.0;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int bit = 1 << (3 - k);
+#pragma unroll
+            for (int s = 0; s < 16; ++s)
+                if (!(s & bit)) v[s] = (v[s] - v[s | bit]) * rs[k];
+        }
+        return v[0] * (1.0 / 6.0);
+    }
+    // bins: [view][bin][va, vb, vc, 0, 1/va, 1/vb, 1/vc, 0] doubles (a zero
+    // reciprocal where the direction is dropped)
     __device__ static float value(const View& V, const Cell& c, int u, int p, const Fan2DParams& P) {
         float sx = c.sx0, sy = c.sy0;
         for (int t = c.lo; t < u; ++t) {  // the reference's FP32 stepping
@@ -198,14 +225,17 @@ struct HexBasis {
             if (da > V.dt && db > V.dt && (ax1 - ox) * (bx1 - ox) >= 0.0f && (ay1 - oy) * (by1 - oy) >= 0.0f)
                 return 0.f;
         }
-        const double* b = reinterpret_cast<const double*>(P.bins) + ((size_t)p * P.nu + u) * 4;
+        const double* b = reinterpret_cast<const double*>(P.bins) + ((size_t)p * P.nu + u) * 8;
         const double va = __ldg(b), vb = __ldg(b + 1), vc = __ldg(b + 2);
         const double vblur = -sqrt((double)(bx1 - ax1) * (bx1 - ax1) + (double)(by1 - ay1) * (by1 - ay1));
         double y = sqrt((double)(ax1 - ox) * (ax1 - ox) + (double)(ay1 - oy) * (ay1 - oy));
         if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) y = -y;
         double conv;
         if (V.mode == kHl) {
-            conv = conv4(y, vblur, va, vb, vc);
+            if (fabs(vblur) > 1e-8 && fabs(va) > 1e-8 && fabs(vb) > 1e-8 && fabs(vc) > 1e-8)
+                conv = conv4_full(y, vblur, va, vb, vc, __ldg(b + 4), __ldg(b + 5), __ldg(b + 6));
+            else
+                conv = conv4(y, vblur, va, vb, vc);
         } else {
             const float fy = (float)y, fb = (float)vblur, fa = (float)va, fv = (float)vb, fc = (float)vc;
             conv = (double)conv3(fy, fb, fa, fv) + (double)conv3(fy, fb, fv, fc) + (double)conv3(fy, fb, fc, fa);
@@ -234,7 +264,7 @@ public:
         const float fdx = fdt * (float)kSqrt3;
         const float fdy = fdt * (mode == kHl ? 0.5f : 1.5f);
         std::vector<float> view((size_t)np * HexBasis::kViewFloats, 0.f);
-        std::vector<float4> bins((size_t)np * nu * 2);
+        std::vector<float4> bins((size_t)np * nu * 4);
         double* bd = reinterpret_cast<double*>(bins.data());
         std::vector<BinHomography> hom;
         bin_homographies(geo, hom);
@@ -262,11 +292,13 @@ public:
                 const float sx = (float)f.dtv[0] + (float)f.puv[0] * (u - 0.5f * nu + 0.5f);
                 const float sy = (float)f.dtv[1] + (float)f.puv[1] * (u - 0.5f * nu + 0.5f);
                 const float th = std::atan2(sx - px, sy - py);
-                double* o = bd + ((size_t)p * nu + u) * 4;
+                double* o = bd + ((size_t)p * nu + u) * 8;
                 o[0] = (double)fdt * std::sin((double)th);
                 o[1] = (double)fdt * std::sin((double)th + 2.0 * kPi / 3.0);
                 o[2] = (double)fdt * std::sin((double)th + 4.0 * kPi / 3.0);
                 o[3] = 0.0;
+                for (int k = 0; k < 3; ++k) o[4 + k] = std::fabs(o[k]) > 1e-8 ? 1.0 / o[k] : 0.0;
+                o[7] = 0.0;
             }
         }
         back_view_ = view;
