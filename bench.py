@@ -79,9 +79,10 @@ def _families():
         from sgd_b200.torch_ops import HexProjector
         return HexProjector(nl, nc, NU, dt, DU, LSD, LSO, C3_ANG, mode=mode)
 
-    def cone(kind):
+    def cone(kind, n=256, views=360, nd=384, d=1.0, dd=1.5):
         from sgd_b200.torch_ops import ConeProjector
-        return ConeProjector(kind, 256, 256, 256, 384, 384, 1.0, 1.0, 1.0, 1.5, 1.5, LSD, LSO, C5_ANG)
+        ang = 2 * np.pi * np.arange(views) / views
+        return ConeProjector(kind, n, n, n, nd, nd, d, d, d, dd, dd, LSD, LSO, ang)
 
     return {
         "sf_c2": ("A_SF separable footprint fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
@@ -98,10 +99,12 @@ def _families():
                      lambda: cone("b1_3d"), 256 ** 3 * 360),
         "sf3d_c5": ("SF_projector cone beam (corrected pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
                     lambda: cone("sf3d"), 256 ** 3 * 360),
+        "b1_3d_small": ("A_B1_3D cone beam, the C5 geometry at half resolution for profiling: 128^3 @2mm, "
+                        "180 views, 192x192 @3mm", lambda: cone("b1_3d", 128, 180, 192, 2.0, 3.0), 128 ** 3 * 180),
     }
 
 
-FAMILIES = ("sf_c2", "b0_c2", "b0_parallel_c1", "h0_c3", "hl_c3", "b1_3d_c5", "sf3d_c5")
+FAMILIES = ("sf_c2", "b0_c2", "b0_parallel_c1", "h0_c3", "hl_c3", "b1_3d_c5", "sf3d_c5", "b1_3d_small")
 
 
 def parse():

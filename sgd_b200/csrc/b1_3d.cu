@@ -40,8 +40,9 @@ namespace {
 constexpr int kZChunk = 32;      // the reference's Z_SIZE (layers/A_B1_3D.cu:25)
 constexpr int kTile = 16;        // forward: 16 x 16 columns per CTA
 constexpr int kWinCap = 6144;    // forward: shared (u, v) window, floats
-constexpr int kBackZ = 8;        // back: voxels of a chunk per thread
+constexpr int kBackZ = 16;       // back: voxels of a chunk per thread
 constexpr int kMaxConv = 8;      // cached in-plane footprints per column
+constexpr int kMaxRows = 4;      // cached axial integrals per voxel (v rows)
 constexpr float kEps = 1e-7f;
 
 struct View3 {
@@ -148,6 +149,14 @@ __device__ __forceinline__ float gamma_trap(float s1, float s2, const float* us)
     tmp = (b2 > b1) ? (1 / (2 * (us[3] - us[2]))) * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3])) : 0.0f;
     if (tmp == tmp) g += tmp;
     return g;
+}
+
+// gamma_trap of rows minv .. minv + kMaxRows - 1 (those up to maxv), once per
+// voxel: the (u, v) loops below reuse them for every u.  Unrolled so that
+// they stay in registers.
+__device__ __forceinline__ void voxel_rows(const float* vs, int minv, int maxv, float* g) {
+#pragma unroll
+    for (int r = 0; r < kMaxRows; ++r) g[r] = (minv + r <= maxv) ? gamma_trap((float)(minv + r), minv + r + 1.0f, vs) : 0.f;
 }
 
 struct Column {
@@ -324,19 +333,31 @@ __global__ void __launch_bounds__(kTile* kTile) b1_3d_forward_kernel(Geo3 G, con
                 const float weight = sqrtf(((c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py) + (oz - pz) * (oz - pz)) /
                                            ((c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py)));
                 const float C = C0 * weight * (2 / (((vs[3] - vs[0]) + (vs[2] - vs[1]))));
-                for (int ti = 0; ti < ncv; ++ti) {
-                    const float val = conv_of(V, c, vecs, G.nu, conv, ti) * C;
-                    if (!(val == val)) continue;
-                    const int u = c.minu + ti;
-                    for (int j = minv; j <= maxv; ++j) {
-                        const float g = gamma_trap((float)j, j + 1.0f, vs);
-                        if (!(g > kEps)) continue;
-                        if (in_smem) {
-                            dp = s_acc + (j - wvl) * wu + (u - wul);
-                            atomicAdd(dp, val * g);
-                        } else {
-                            atomicAdd(gp + (size_t)j * G.nu + u, (double)(val * g));
-                        }
+                auto add = [&](int u, int j, float val, float g) {
+                    if (!(g > kEps)) return;
+                    if (in_smem) {
+                        dp = s_acc + (j - wvl) * wu + (u - wul);
+                        atomicAdd(dp, val * g);
+                    } else {
+                        atomicAdd(gp + (size_t)j * G.nu + u, (double)(val * g));
+                    }
+                };
+                if (maxv - minv < kMaxRows) {
+                    float gr[kMaxRows];
+                    voxel_rows(vs, minv, maxv, gr);
+                    for (int ti = 0; ti < ncv; ++ti) {
+                        const float val = conv_of(V, c, vecs, G.nu, conv, ti) * C;
+                        if (!(val == val)) continue;
+#pragma unroll
+                        for (int r = 0; r < kMaxRows; ++r)
+                            if (minv + r <= maxv) add(c.minu + ti, minv + r, val, gr[r]);
+                    }
+                } else {
+                    for (int ti = 0; ti < ncv; ++ti) {
+                        const float val = conv_of(V, c, vecs, G.nu, conv, ti) * C;
+                        if (!(val == val)) continue;
+                        for (int j = minv; j <= maxv; ++j)
+                            add(c.minu + ti, j, val, gamma_trap((float)j, j + 1.0f, vs));
                     }
                 }
             }
@@ -396,13 +417,26 @@ __global__ void __launch_bounds__(256) b1_3d_back_kernel(Geo3 G, const float* __
             float C = weight;
             if (mode == 1) C = weight * (2 / (((vs[3] - vs[0]) + (vs[2] - vs[1]))));
             float val = 0.f;
-            for (int ti = 0; ti < ncv; ++ti) {
-                const float cv = conv_of(V, c, vecs, G.nu, conv, ti);
-                if (mode == 0 ? !(cv == cv && cv > kEps) : !(cv * C == cv * C)) continue;
-                const int u = c.minu + ti;
-                for (int j = minv; j <= maxv; ++j) {
-                    const float g = gamma_trap((float)j, j + 1.0f, vs);
-                    if (g > kEps) val = fmaf(__ldg(pp + (size_t)j * G.nu + u), g * cv, val);
+            if (maxv - minv < kMaxRows) {
+                float gr[kMaxRows];
+                voxel_rows(vs, minv, maxv, gr);
+                for (int ti = 0; ti < ncv; ++ti) {
+                    const float cv = conv_of(V, c, vecs, G.nu, conv, ti);
+                    if (mode == 0 ? !(cv == cv && cv > kEps) : !(cv * C == cv * C)) continue;
+                    const float* pu = pp + (size_t)minv * G.nu + c.minu + ti;
+#pragma unroll
+                    for (int r = 0; r < kMaxRows; ++r)
+                        if (minv + r <= maxv && gr[r] > kEps) val = fmaf(__ldg(pu + (size_t)r * G.nu), gr[r] * cv, val);
+                }
+            } else {
+                for (int ti = 0; ti < ncv; ++ti) {
+                    const float cv = conv_of(V, c, vecs, G.nu, conv, ti);
+                    if (mode == 0 ? !(cv == cv && cv > kEps) : !(cv * C == cv * C)) continue;
+                    const int u = c.minu + ti;
+                    for (int j = minv; j <= maxv; ++j) {
+                        const float g = gamma_trap((float)j, j + 1.0f, vs);
+                        if (g > kEps) val = fmaf(__ldg(pp + (size_t)j * G.nu + u), g * cv, val);
+                    }
                 }
             }
 #pragma unroll
