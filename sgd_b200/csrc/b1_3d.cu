@@ -22,7 +22,7 @@
 //                         ranges) is accumulated in shared memory and flushed
 //                         to an FP64 sinogram, or added directly when a window
 //                         is larger than the shared buffer.
-//   b1_3d_back_kernel     gather: a thread per column and 8 voxels of a chunk,
+//   b1_3d_back_kernel     gather: a thread per column and 16 voxels of a chunk,
 //                         FP64 accumulators, each voxel written once.
 #include <cuda_runtime.h>
 

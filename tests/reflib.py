@@ -56,15 +56,17 @@ def lib():
 class RefFan2D:
     """The reference's 2D fan projector `kind` (b0, b1, SF) on one geometry."""
 
-    def __init__(self, kind, nx, ny, nu, dx, dy, du, lsd, lso, angles):
+    def __init__(self, kind, nx, ny, nu, dx, dy, du, lsd, lso, angles, dz=None, drho=None):
         L = lib()
         self.kind, self.nx, self.ny, self.nu, self.np = kind, nx, ny, nu, len(angles)
         self._ang = np.ascontiguousarray(angles, dtype=np.float64)
+        self._off = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (dz, drho)]
         p = self._ang.ctypes.data_as(_dp)
+        offs = [None if a is None else a.ctypes.data_as(_dp) for a in self._off]
         if kind == "SF":
             self.h = L.SF_init(nx, ny, self.np, nu, dx, dy, du, lsd, lso, p)
         else:
-            self.h = getattr(L, f"{kind}_init")(nx, ny, self.np, nu, dx, dy, du, lsd, lso, p, None, None)
+            self.h = getattr(L, f"{kind}_init")(nx, ny, self.np, nu, dx, dy, du, lsd, lso, p, *offs)
         assert self.h
 
     def forward(self, x):

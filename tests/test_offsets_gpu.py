@@ -1,0 +1,74 @@
+"""Per-view source offsets (dz, drho) of the fan-beam inits (utils/geo.cu:232-269:
+drho shifts the source along the central ray, dz lifts it; the 2D kernels
+ignore z): the B1 and B0 projectors against the FP64 replica and the
+reference library on the same offset geometry, and the adjoint test."""
+import numpy as np
+import pytest
+
+from geometry_cases import fan_case, rel_l2
+from sgd_b200.phantom import ellipse_phantom
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+
+
+def offsets(n, seed=0):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-3.0, 3.0, n), rng.uniform(-8.0, 8.0, n)  # dz, drho in mm
+
+
+@pytest.mark.parametrize("kind", ["b1", "b0"])
+@pytest.mark.parametrize("case", ["small", "rect"])
+def test_offset_geometry_matches_replica_and_reference(oracle_mod, kind, case):
+    import reflib
+    from sgd_b200 import operators as ops
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case(case)
+    dz, drho = offsets(len(ang))
+    cls = {"b1": ops.A_B1_operator, "b0": ops.A_B0_operator}[kind]
+    A = cls(nx, ny, len(ang), nu, dx, dy, du, lsd, lso, ang, dz=dz, drho=drho)
+    A0 = cls(nx, ny, len(ang), nu, dx, dy, du, lsd, lso, ang)
+    x = ellipse_phantom(nx, ny, dx, dy, seed=4).ravel()
+    b = A.matvec(x)
+    assert rel_l2(b, A0.matvec(x)) > 1e-3  # the offsets change the projection
+    fwd = {"b1": oracle_mod.b1_forward, "b0": oracle_mod.b0_forward}[kind]
+    b_rep = fwd(x, nx, ny, nu, dx, dy, du, lsd, lso, ang, dzs=dz, drho=drho)
+    b_rep = b_rep[0] if isinstance(b_rep, tuple) else b_rep
+    # B0 keeps the reference's FP32 bin stepping, which sits up to ~2e-5 from
+    # the FP64 replica (as the reference itself does)
+    assert rel_l2(b, b_rep) < {"b1": 1e-5, "b0": 5e-5}[kind]
+    if not reflib.available():
+        pytest.fail("reference library oracle/_ref/libnetwork.so not built (make -C oracle ref)")
+    if nx == ny:  # the reference's C wrappers take ny = nx (layers/A_B1.cu:607)
+        R = reflib.RefFan2D(kind, nx, ny, nu, dx, dy, du, lsd, lso, ang, dz=dz, drho=drho)
+        b_ref, _ = R.forward(x)
+        e = rel_l2(b, b_ref)
+        if kind == "b1" and e >= 1e-5:
+            # the reference's FP32 bin stepping (layers/A_B1.cu:160): the gap
+            # must be the reference's own distance from its FP64 formula
+            ours, theirs = rel_l2(b, b_rep), rel_l2(b_ref, b_rep)
+            assert ours < 1e-6 and e <= theirs + ours, (e, ours, theirs)
+        else:
+            assert e < 1e-5
+        y = np.random.default_rng(2).random(A.shape[0])
+        assert rel_l2(A.rmatvec(y), R.backward(y)) < 1e-5
+
+
+@pytest.mark.parametrize("kind", ["b1", "b0"])
+def test_offset_geometry_adjoint(kind):
+    from sgd_b200 import operators as ops
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case("small")
+    dz, drho = offsets(len(ang), seed=1)
+    cls = {"b1": ops.A_B1_operator, "b0": ops.A_B0_operator}[kind]
+    A = cls(nx, ny, len(ang), nu, dx, dy, du, lsd, lso, ang, dz=dz, drho=drho)
+    rng = np.random.default_rng(1234)
+    x = rng.standard_normal(A.shape[1])
+    y = rng.standard_normal(A.shape[0])
+    lhs = float(np.dot(A.matvec(x), y))
+    rhs = float(np.dot(x, A.rmatvec(y)))
+    assert abs(lhs - rhs) / abs(lhs) < 1e-6
