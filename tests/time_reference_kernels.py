@@ -10,7 +10,10 @@ Per projector kind (b1, SF, b0) one JSON line: kernel-only milliseconds per
 direction for both (device-resident buffers; the reference's through the
 layer's project/back_project, its per-view launches included) and the
 end-to-end milliseconds of one forward + one backward through the FP64 host
-C ABI (host copies and conversions included)."""
+C ABI (host copies and conversions included).  With --e2e-only h0,hl,b1_3d
+the hexagonal (about 2^18 sites, 360 views) and cone-beam (256^3, 360 views,
+384^2 detector) layers are compared end to end through the same C ABI, in
+the reference's own modes."""
 import argparse
 import ctypes
 import json
@@ -82,16 +85,52 @@ def reference(kind, reps):
     return fwd, back.value, e2e
 
 
+def e2e_pair(kind, reps):
+    """(reference ms, ours ms) of one forward + one backward through the C ABI."""
+    from sgd_b200 import operators as ops
+    rng = np.random.default_rng(0)
+    if kind in ("h0", "hl"):
+        nl, nc, dt = (550, 477, 0.62) if kind == "h0" else (953, 275, 1.075)
+        ang = 2 * np.pi * np.arange(360) / 360
+        R = reflib.RefHex(kind, nl, nc, NU, dt, DU, LSD, LSO, ang)
+        cls = ops.A_H0_operator if kind == "h0" else ops.A_Hl_operator
+        A = cls(nl, nc, len(ang), NU, dt, DU, LSD, LSO, ang)
+        x = rng.random(nl * nc)
+    else:
+        n, ang = 256, 2 * np.pi * np.arange(360) / 360
+        R = reflib.RefCone(n, n, n, 384, 384, 1.0, 1.0, 1.0, 1.5, 1.5, LSD, LSO, ang)
+        A = ops.A_B1_3D_operator(n, n, n, len(ang), 384, 384, 1.0, 1.0, 1.0, 1.5, 1.5, LSD, LSO, ang)
+        x = rng.random(n ** 3)
+
+    def run(f, b):
+        y = f(x)
+        y = y[0] if isinstance(y, tuple) else y
+        b(y)
+
+    run(R.forward, R.backward)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        run(R.forward, R.backward)
+    tr = (time.perf_counter() - t0) / reps * 1e3
+    run(A.matvec, A.rmatvec)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        run(A.matvec, A.rmatvec)
+    to = (time.perf_counter() - t0) / reps * 1e3
+    return tr, to
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--kinds", default="b1,SF,b0")
+    ap.add_argument("--e2e-only", default="")
     args = ap.parse_args()
     if not reflib.available():
         print(json.dumps({"unavailable": "oracle/_ref/libnetwork.so not built (make -C oracle ref)"}))
         return
     units = 2.0 * NX * NY * NP
-    for kind in args.kinds.split(","):
+    for kind in [k for k in args.kinds.split(",") if k]:
         rf, rb, re = reference(kind, args.reps)
         of, ob, oe = ours(kind, args.reps)
         print(json.dumps({
@@ -102,6 +141,11 @@ def main():
             "ours_updates_per_s": units / ((of + ob) * 1e-3),
             "reference_updates_per_s": units / ((rf + rb) * 1e-3),
         }), flush=True)
+    for kind in [k for k in args.e2e_only.split(",") if k]:
+        tr, to = e2e_pair(kind, max(1, args.reps // 2))
+        print(json.dumps({"kind": kind, "reference_e2e_fwd_back_ms": tr, "ours_e2e_fwd_back_ms": to,
+                          "e2e_speedup": tr / to, "modes": "the reference's own (H0 bounds, A_B1_3D pair as "
+                          "the reference: its backward returns zeros, timed all the same)"}), flush=True)
 
 
 if __name__ == "__main__":
