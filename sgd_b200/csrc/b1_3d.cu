@@ -269,7 +269,7 @@ struct Geo3 {
     const float2* vecs;   // [np][nu]
 };
 
-__global__ void __launch_bounds__(kTile* kTile) b1_3d_forward_kernel(Geo3 G, const float* __restrict__ vol,
+__global__ void __launch_bounds__(kTile * kTile, 4) b1_3d_forward_kernel(Geo3 G, const float* __restrict__ vol,
                                                                      double* __restrict__ proj64) {
     __shared__ float s_acc[kWinCap];
     __shared__ int s_win[4];
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kTile* kTile) b1_3d_forward_kernel(Geo3 G, con
 
 // mode 0: the reference's backward (no 2/width factor, conv > 1e-7 kept,
 // single-bin u or v ranges skipped); mode 1: the exact transpose of the forward
-__global__ void __launch_bounds__(256) b1_3d_back_kernel(Geo3 G, const float* __restrict__ proj,
+__global__ void __launch_bounds__(256, 4) b1_3d_back_kernel(Geo3 G, const float* __restrict__ proj,
                                                          float* __restrict__ vol, int mode) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int per_col = (G.nz + kBackZ - 1) / kBackZ;
