@@ -269,7 +269,7 @@ struct Geo3 {
     const float2* vecs;   // [np][nu]
 };
 
-__global__ void __launch_bounds__(kTile * kTile, 4) b1_3d_forward_kernel(Geo3 G, const float* __restrict__ vol,
+__global__ void __launch_bounds__(kTile * kTile, 6) b1_3d_forward_kernel(Geo3 G, const float* __restrict__ vol,
                                                                      double* __restrict__ proj64) {
     __shared__ float s_acc[kWinCap];
     __shared__ int s_win[4];
