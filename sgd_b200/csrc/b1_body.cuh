@@ -13,8 +13,10 @@
 //                    records by TMA bulk copies completed on an mbarrier
 //                    (double-buffered, the next chunk in flight while this one
 //                    is evaluated), the sinogram values by plain loads.  Each
-//                    thread accumulates over all views in registers and writes
-//                    its pixel once, no atomics.
+//                    thread evaluates a bin's two edges as one packed-FP32
+//                    pair (the constant pairs built from the staged record),
+//                    accumulates over all views in registers and writes its
+//                    pixel once, no atomics.
 //
 // Reference: layers/A_B1.cu:62-208 (forward, one launch per view, FP64
 // atomics) and :211-353 (backward).
@@ -148,6 +150,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
     const int i = i0 + 4 * (w >> 2) + (l >> 3), j = j0 + 8 * (w & 3) + (l & 7);
     const float fi = (float)i, fj = (float)j;
+    const float2 fi2 = pair(fi), fj2 = pair(fj);
     const int nchunks = (np + VC - 1) / VC;
     auto parity = [&](int c) { return (((c & 1) ? use1 : use0) + (uint32_t)(c >> 1)) & 1u; };
 
@@ -228,8 +231,8 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             const float* sb = ssino + (st * VC + v) * wcap - lo;
 #pragma unroll 1
             for (int u = a; u <= b; ++u) {
-                const B1Bin r{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]};
-                const float conv = b1_conv(fi, fj, r);
+                const B1Pair k = b1_pair(B1Bin{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]});
+                const float conv = b1_conv_pair(b1_edges2(fi2, b1_inner2(fj2, k), k), k);
                 if (conv > kConvEps) csum = fmaf(conv, sb[u], csum);
             }
         }

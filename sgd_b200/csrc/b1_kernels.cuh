@@ -4,15 +4,17 @@
 // All arithmetic is written with explicit round-to-nearest intrinsics: the
 // compiler may not contract or reorder it differently in the two kernels, so
 // conv(i, j, p, u) is bit-identical wherever it is computed.  Two forms:
-//   scalar (b1_conv)       the two edges one after the other, on the record
-//                          as staged (the back kernel);
+//   scalar (b1_conv)       the two edges one after the other (the system-
+//                          matrix builder);
 //   packed (b1_conv_pair)  both edges at once on the sm_100 packed-FP32
 //                          instructions (__ffma2_rn, __fadd2_rn, __fmul2_rn),
-//                          on constant pairs built once per bin (the forward
-//                          kernel, which reuses a bin's record for dozens of
-//                          pixels).  Each half of a packed operation rounds
-//                          exactly as the scalar operation does, so the two
-//                          forms give the same bits.
+//                          on constant pairs built from the record (once per
+//                          bin in the forward kernel, which reuses a bin for
+//                          dozens of pixels; per evaluation in the back
+//                          kernel, where the register moves still cost less
+//                          than the scalar form).  Each half of a packed
+//                          operation rounds exactly as the scalar operation
+//                          does, so the two forms give the same bits.
 #pragma once
 
 #include <cuda_runtime.h>
