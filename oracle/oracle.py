@@ -39,6 +39,7 @@ def lib():
         L.oracle_sf3d_forward.restype = None
         L.oracle_exact_fan2d_matrix.restype = None
         L.oracle_exact_parallel_matrix.restype = None
+        L.oracle_exact_hex_matrix.restype = None
         L.oracle_matrix_generation.restype = ctypes.c_longlong
         L.oracle_ref_simpson_3d.restype = None
         L.oracle_sf3d_backward.restype = None
@@ -246,6 +247,17 @@ def exact_fan2d_matrix(kind, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None,
     lib().oracle_exact_fan2d_matrix({"b0": 0, "b1": 1}[kind], nx, ny, len(angles), nu, d(dx), d(dy), d(du), d(lsd),
                                     d(lso), _p(angles), _p(_c(dzs)), _p(_c(drho)), d(tol), _p(M))
     return M.reshape(len(angles) * nu, nx * ny)
+
+
+def exact_hex_matrix(nl, nc, nu, dt, du, lsd, lso, angles, tol=1e-10):
+    """Dense exact FP64 system matrix (np*nu, nc*nl) of the hexagon indicator
+    (the H0 basis, layers/A_H0.cu:158-256): bin-averaged chord lengths;
+    columns in the host layout ic*nl + il, absent sites zero."""
+    angles = _c(angles)
+    M = np.zeros(len(angles) * nu * nc * nl)
+    d = ctypes.c_double
+    lib().oracle_exact_hex_matrix(nl, nc, len(angles), nu, d(dt), d(du), d(lsd), d(lso), _p(angles), d(tol), _p(M))
+    return M.reshape(len(angles) * nu, nc * nl)
 
 
 def ref_simpson_3d(x, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, angles, adaptive=False, max_depth=6,

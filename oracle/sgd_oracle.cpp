@@ -1253,6 +1253,90 @@ void oracle_exact_fan2d_matrix(int kind, int nx, int ny, int np, int nu, double 
         }
 }
 
+// Exact fan-beam system matrix of the hexagon indicator, the basis of H0
+// (layers/A_H0.cu:158-256): site (ic, il) of the lattice at
+// ((ic - (nc-1)/2 [odd rows: (nc-2)/2]) sqrt(3) dt, (il - (nl-1)/2) 1.5 dt)
+// (:174-183; odd rows hold nc - 1 sites), a regular hexagon of circumradius dt
+// with vertices at 30 + 60 k degrees (the union of the three rhombi spanned
+// by the directions at -90, 30 and 150 degrees whose X-rays the kernel sums,
+// :229-245).  Entry: the chord length through the hexagon along the ray from
+// the source to each point of bin u, averaged over the bin, exact per piece
+// between the rays through the vertices (the chord is linear in between).
+// Dense, M[(p*nu + u)*(nc*nl) + ic*nl + il]; absent sites stay 0.
+void oracle_exact_hex_matrix(int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                             const double* angles, double tol, double* M) {
+    Geo g = make_geo(nc, nl, 1, np, nu, 1, dt * std::sqrt(3.0), dt * 0.5, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    const size_t ncol = (size_t)nc * nl;
+    std::memset(M, 0, sizeof(double) * ncol * np * nu);
+    const double sdx = dt * std::sqrt(3.0), sdy = 1.5 * dt;
+    double vx[6], vy[6];
+    for (int k = 0; k < 6; ++k) {
+        vx[k] = dt * std::cos(kPI / 6 + k * kPI / 3);
+        vy[k] = dt * std::sin(kPI / 6 + k * kPI / 3);
+    }
+    // chord of the hexagon at o along the line s -> q (Cyrus-Beck clipping
+    // against its six edges, counter-clockwise)
+    auto chord = [&](const double* s, const double* q, const double* o) {
+        double d[2] = {q[0] - s[0], q[1] - s[1]};
+        const double len = std::hypot(d[0], d[1]);
+        d[0] /= len; d[1] /= len;
+        double t0 = -1e300, t1 = 1e300;
+        for (int k = 0; k < 6; ++k) {
+            const double ax = o[0] + vx[k], ay = o[1] + vy[k];
+            const double ex = vx[(k + 1) % 6] - vx[k], ey = vy[(k + 1) % 6] - vy[k];
+            // inside: cross(e, X - A) >= 0
+            const double num = ex * (s[1] - ay) - ey * (s[0] - ax);
+            const double den = ex * d[1] - ey * d[0];
+            if (den == 0.0) {
+                if (num < 0) return 0.0;
+                continue;
+            }
+            const double t = -num / den;
+            if (den > 0) t0 = std::max(t0, t);
+            else t1 = std::min(t1, t);
+        }
+        return t1 > t0 ? t1 - t0 : 0.0;
+    };
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int p = 0; p < np; ++p)
+        for (int u = 0; u < nu; ++u) {
+            const double* s = &g.src[3 * p];
+            const double* dtv = &g.dtv[3 * p];
+            const double* pu = &g.puv[3 * p];
+            double* row = M + ((size_t)p * nu + u) * ncol;
+            double e0[2], e1[2];
+            for (int k = 0; k < 2; ++k) {
+                e0[k] = dtv[k] + pu[k] * (u - 0.5 * nu) - s[k];
+                e1[k] = dtv[k] + pu[k] * (u - 0.5 * nu + 1.0) - s[k];
+            }
+            const double n0 = std::hypot(e0[0], e0[1]), n1 = std::hypot(e1[0], e1[1]);
+            for (int ic = 0; ic < nc; ++ic)
+                for (int il = 0; il < nl; ++il) {
+                    if ((il & 1) && ic == nc - 1) continue;
+                    const double o[2] = {(ic - ((il & 1) ? 0.5 * (nc - 2) : 0.5 * (nc - 1))) * sdx,
+                                         (il - 0.5 * (nl - 1)) * sdy};
+                    const double r[2] = {o[0] - s[0], o[1] - s[1]};
+                    const double c0 = (e0[0] * r[1] - e0[1] * r[0]) / n0, c1 = (e1[0] * r[1] - e1[1] * r[0]) / n1;
+                    if ((c0 > dt && c1 > dt) || (c0 < -dt && c1 < -dt)) continue;
+                    auto f = [&](double t) {
+                        const double q[2] = {dtv[0] + pu[0] * (u - 0.5 * nu + t), dtv[1] + pu[1] * (u - 0.5 * nu + t)};
+                        return chord(s, q, o);
+                    };
+                    std::vector<double> cuts;
+                    const double off = u - 0.5 * nu;
+                    for (int k = 0; k < 6; ++k) {
+                        const double cx = o[0] + vx[k] - s[0], cy = o[1] + vy[k] - s[1];
+                        const double den = pu[0] * cy - pu[1] * cx;
+                        if (den == 0.0) continue;
+                        const double t = -((dtv[0] - s[0]) * cy - (dtv[1] - s[1]) * cx) / den - off;
+                        if (t > 0.0 && t < 1.0) cuts.push_back(t);
+                    }
+                    row[(size_t)ic * nl + il] = integrate_pieces(f, cuts, tol * 2.0 * dt);
+                }
+        }
+}
+
 // Exact parallel-beam system matrix of the pixel-indicator (kind 0) or
 // bilinear (kind 1) basis, dense, M[(p*nu + u)*(nx*ny) + ix*ny + iy]: for
 // view angle beta the rays run along (cos beta, sin beta) and bin u covers

@@ -89,3 +89,18 @@ def test_h0_reference_mode_loses_mass_the_corrected_mode_keeps(oracle_mod):
     ones.reshape(nc, nl)[nc - 1, 1::2] = 0.0
     sr, sc = Ar.matvec(ones).sum(), Ac.matvec(ones).sum()
     assert sc > 2.0 * sr
+
+
+def test_h0_corrected_against_exact_hexagon_projection(oracle_mod):
+    """The GPU H0 with the true hexagon bounds against the exact FP64
+    bin-averaged chords of the hexagon indicator (three times, the H0 basis's
+    normalisation): the model error of the footprint formula."""
+    from sgd_b200.operators import A_H0_operator
+    nl, nc, nu, dt, du, lsd, lso = 16, 12, 60, 2.0, 1.5, 1085.6, 595.0
+    ang = np.array([0.3, 1.1, np.pi / 4, 2.5])
+    M = oracle_mod.exact_hex_matrix(nl, nc, nu, dt, du, lsd, lso, ang)
+    A = A_H0_operator(nl, nc, len(ang), nu, dt, du, lsd, lso, ang, exact_bounds=True)
+    x = np.random.default_rng(0).random(nc * nl)
+    odd_last = [(nc - 1) * nl + il for il in range(1, nl, 2)]
+    x[odd_last] = 0.0  # absent sites of the odd rows
+    assert rel_l2(A.matvec(x), 3.0 * (M @ x)) < 1e-4

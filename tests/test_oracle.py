@@ -215,6 +215,52 @@ def test_formula_replica_model_error_vs_exact(oracle_mod, kind, case):
     assert err < {"b0": 1e-3, "b1": 5e-4}[kind]
 
 
+@pytest.mark.parametrize("case", ["tiny", "snap"])
+def test_sf_model_error_vs_exact_pixel_indicator(oracle_mod, case):
+    """A_SF approximates the pixel indicator's projection (trapezoid
+    footprint): its FP64 replica against the exact bin-averaged chords."""
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case(case)
+    x = ellipse_phantom(nx, ny, dx, dy, seed=3).ravel()
+    M = oracle_mod.exact_fan2d_matrix("b0", nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    b, _ = oracle_mod.sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    assert rel_l2(b, M @ x) < 1e-3
+
+
+def test_exact_hex_matrix_carries_the_hexagon_area(oracle_mod):
+    """Nearly parallel rays (source 50 m away): a site's bin-averaged chords
+    summed over the bins times the bin width at the site give the area of
+    the regular hexagon of circumradius dt, (3 sqrt 3 / 2) dt^2."""
+    nl, nc, nu, dt, du = 5, 4, 80, 2.0, 0.25
+    lsd, lso = 1.0e5, 5.0e4
+    ang = np.array([0.0, 0.37, np.pi / 6, 1.9])
+    M = oracle_mod.exact_hex_matrix(nl, nc, nu, dt, du, lsd, lso, ang)
+    site = 1 * nl + 2  # ic = 1, il = 2 (an even row)
+    col = M[:, site].reshape(len(ang), nu).sum(axis=1)
+    area = 1.5 * np.sqrt(3.0) * dt * dt
+    # the site sits 1.7 mm off the isocentre: its magnification differs from
+    # lsd / lso by ~4e-5 depending on the view
+    assert np.allclose(col * du * lso / lsd, area, rtol=1e-4)
+    assert not M[:, (nc - 1) * nl + 1].any()  # odd rows hold nc - 1 sites
+
+
+def test_h0_model_error_vs_exact_hexagon(oracle_mod):
+    """H0's value is three times the hexagon indicator's chord (the sum of
+    the three unit-integral rhombus splines scaled by the hexagon area,
+    layers/A_H0.cu:245); with the true hexagon bounds its FP64 replica sits
+    within 1e-4 of the exact bin-averaged chords, while the reference's
+    bounds (at the 0.5 dt row pitch, layers/A_H0.cu:556) lose mass away from
+    the centre row."""
+    nl, nc, nu, dt, du, lsd, lso = 16, 12, 60, 2.0, 1.5, 1085.6, 595.0
+    ang = np.array([0.3, 1.1, np.pi / 4, 2.5])
+    M = oracle_mod.exact_hex_matrix(nl, nc, nu, dt, du, lsd, lso, ang)
+    x = np.random.default_rng(0).random(nc * nl)
+    exact = 3.0 * (M @ x)
+    b, _ = oracle_mod.hex_forward("h0c", x, nl, nc, nu, dt, du, lsd, lso, ang)
+    assert rel_l2(b, exact) < 1e-4
+    b_ref, _ = oracle_mod.hex_forward("h0", x, nl, nc, nu, dt, du, lsd, lso, ang)
+    assert rel_l2(b_ref, exact) > 0.1
+
+
 def test_chord_simpson_3d(oracle_mod):
     """Ref_project_Simpson restated: a uniform odd-sized cube seen along +x
     carries its length on the central cell (the nine samples avoid voxel
