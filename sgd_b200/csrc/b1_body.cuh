@@ -169,6 +169,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
                     const BinHomography H = hom[p];
                     float* h = hs + (slot * VC + l) * 8;
                     h[0] = H.n0; h[1] = H.n1; h[2] = H.n2; h[3] = H.d0; h[4] = H.d1; h[5] = H.d2;
+                    h[6] = fabsf(H.d0) + fabsf(H.d1);
                 }
                 win[(slot * VC + l) * 2] = lh.x;
                 win[(slot * VC + l) * 2 + 1] = lh.y;
@@ -224,7 +225,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             const int lo = win[(slot * VC + v) * 2], hi = win[(slot * VC + v) * 2 + 1];
             if (hi < lo) continue;
             int a, b;
-            box_bins(hs + (slot * VC + v) * 8, fi - 1.f, fi + 1.f, fj - 1.f, fj + 1.f, nu, a, b);
+            box_bins_bound(hs + (slot * VC + v) * 8, fi, fj, nu, a, b);
             a = max(a, lo);
             b = min(b, hi);
             const float4* rb = srec + (st * VC + v) * 4 * wcap - lo;

@@ -20,4 +20,20 @@ __device__ __forceinline__ void box_bins(const float* h, float i0, float i1, flo
     hi = min(nu - 1, (int)floorf(fmaxf(fmaxf(u00, u01), fmaxf(u10, u11))));
 }
 
+// Bin range of the box [fi-1, fi+1] x [fj-1, fj+1] from its centre: with
+// u = N / D linear-fractional, |u - u_c| <= (|n0 - u_c d0| + |n1 - u_c d1|) /
+// (|D_c| - |d0| - |d1|) over the box (h[6] = |d0| + |d1|); a range at least as
+// wide as the corners', from one division instead of four.  A box reaching
+// the source plane gets every bin.
+__device__ __forceinline__ void box_bins_bound(const float* h, float fi, float fj, int nu, int& lo, int& hi) {
+    const float N = fmaf(h[0], fi, fmaf(h[1], fj, h[2]));
+    const float D = fmaf(h[3], fi, fmaf(h[4], fj, h[5]));
+    const float uc = __fdividef(N, D);
+    const float spread = fabsf(fmaf(-uc, h[3], h[0])) + fabsf(fmaf(-uc, h[4], h[1]));
+    const float dmin = fabsf(D) - h[6];
+    const float w = dmin > 0.f ? __fdividef(spread, dmin) : 1e30f;
+    lo = max(0, (int)floorf(uc - w));
+    hi = min(nu - 1, (int)floorf(uc + w));
+}
+
 }  // namespace sgd
