@@ -27,6 +27,7 @@ struct SFBasis {
     struct Cell {
         float us[4];
         float weight;
+        float k01, k23;  // the trapezoid's ramp factors 1 / (2 (us1 - us0)), 1 / (2 (us3 - us2))
         int lo, hi;
     };
     __device__ static void load_view(const float* v, View& V) {
@@ -62,17 +63,21 @@ struct SFBasis {
         sort2(us[1], us[2]);
         c.lo = min(max(0, (int)floorf(us[0])), P.nu - 1);
         c.hi = min(max(0, (int)floorf(us[3])), P.nu - 1);
-        const float theta = atan2f((V.dx * (ix - V.nx2) - V.srcx), (V.dy * (iy - V.ny2) - V.srcy));
-        const float st = fabsf(sinf(theta)), ct = fabsf(cosf(theta));
-        c.weight = V.dx / fmaxf(st, ct);
+        // dx / max(|sin t|, |cos t|) for t = atan2(X, Y) (:174-177) without
+        // the trigonometry: |sin t| = |X| / r, |cos t| = |Y| / r
+        const float X = V.dx * (ix - V.nx2) - V.srcx, Y = V.dy * (iy - V.ny2) - V.srcy;
+        c.weight = V.dx * sqrtf(X * X + Y * Y) / fmaxf(fabsf(X), fabsf(Y));
+        // per-bin constants of gamma_calculate (:48-84), once per cell and view
+        c.k01 = 1 / (2 * (us[1] - us[0]));
+        c.k23 = 1 / (2 * (us[3] - us[2]));
     }
     // layers/A_SF.cu:48-84
-    __device__ static float gamma(float s1, float s2, const float* us) {
+    __device__ static float gamma(float s1, float s2, const Cell& c) {
+        const float* us = c.us;
         float g = 0.0f, tmp, b1, b2;
         b1 = fmaxf(s1, us[0]);
         b2 = fminf(s2, us[1]);
-        tmp = (b2 > b1) ? (1 / (2 * (us[1] - us[0]))) * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0]))
-                        : 0.0f;
+        tmp = (b2 > b1) ? c.k01 * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0])) : 0.0f;
         if (tmp == tmp) g += tmp;
         b1 = fmaxf(s1, us[1]);
         b2 = fminf(s2, us[2]);
@@ -80,13 +85,12 @@ struct SFBasis {
         if (tmp == tmp) g += tmp;
         b1 = fmaxf(s1, us[2]);
         b2 = fminf(s2, us[3]);
-        tmp = (b2 > b1) ? (1 / (2 * (us[3] - us[2]))) * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3]))
-                        : 0.0f;
+        tmp = (b2 > b1) ? c.k23 * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3])) : 0.0f;
         if (tmp == tmp) g += tmp;
         return g;
     }
     __device__ static float value(const View&, const Cell& c, int u, int, const Fan2DParams&) {
-        const float g = gamma((float)u, u + 1.0f, c.us);
+        const float g = gamma((float)u, u + 1.0f, c);
         const float val = c.weight * g;
         return (g > 1e-7f && val == val) ? val : 0.f;
     }
