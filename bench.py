@@ -99,7 +99,7 @@ def _families():
                      lambda: cone("b1_3d"), 256 ** 3 * 360),
         "sf3d_c5": ("SF_projector cone beam (corrected pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
                     lambda: cone("sf3d"), 256 ** 3 * 360),
-        "b1_3d_small": ("A_B1_3D cone beam, the C5 geometry at half resolution for profiling: 128^3 @2mm, "
+        "b1_3d_small": ("A_B1_3D cone beam, the 256^3 cone geometry at half resolution for profiling: 128^3 @2mm, "
                         "180 views, 192x192 @3mm", lambda: cone("b1_3d", 128, 180, 192, 2.0, 3.0), 128 ** 3 * 180),
     }
 
