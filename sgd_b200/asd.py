@@ -170,16 +170,20 @@ def timed(fn):
     return e0.elapsed_time(e1)
 
 
-def plain_curve(solver, sino, truth, iters, every=5):
+def plain_curve(solver, sino, truth, iters, every=5, info=None):
     """(iterations, GPU ms of the iterations alone, mean RMSE) after each block
-    of `every` iterations; the RMSE evaluation is outside the timed region."""
-    solver.set_data(sino)
+    of `every` iterations; the RMSE evaluation is outside the timed region.
+    With info a dict, info["residual"] = mean |Ax - b| entering each
+    iteration's SART step."""
+    solver.set_data(sino, hist_cap=iters if info is not None else 0)
     curve, ms, done = [], 0.0, 0
     while done < iters:
         k = min(every, iters - done)
         ms += timed(lambda: solver.run(k))
         done += k
         curve.append((done, ms, float(rmse(solver.images(), truth).mean())))
+    if info is not None:
+        info["residual"] = [float(r) for r in solver.history(iters)[:, :, 0].mean(axis=1)]
     return curve
 
 
@@ -226,14 +230,15 @@ def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0, lr_final=None):
 def learned_run(solver, net, sino, truth, k_in, target, max_iters, every=1, info=None):
     """k_in plain iterations, the network, then ASD-POCS until the mean RMSE
     reaches `target`: (iterations after the network, GPU ms, curve); the
-    network's own GPU ms goes to info["net_ms"] when info is a dict."""
+    network's own GPU ms goes to info["net_ms"] and the mean |Ax - b|
+    entering each later SART step to info["residual"] when info is a dict."""
     solver.set_data(sino)
     ms = timed(lambda: solver.run(k_in))
     x = solver.images().unsqueeze(1).clone()
     out = {}
     ms_net = timed(lambda: out.setdefault("y", net.forward(x)))
     ms += ms_net
-    solver.set_data(sino, x0=out["y"])
+    solver.set_data(sino, x0=out["y"], hist_cap=max_iters if info is not None else 0)
     curve = [(0, ms, float(rmse(solver.images(), truth).mean()))]
     if info is not None:
         info["net_ms"] = ms_net
@@ -242,6 +247,8 @@ def learned_run(solver, net, sino, truth, k_in, target, max_iters, every=1, info
         ms += timed(lambda: solver.run(every))
         done += every
         curve.append((done, ms, float(rmse(solver.images(), truth).mean())))
+    if info is not None and done:
+        info["residual"] = [float(r) for r in solver.history(done)[:, :, 0].mean(axis=1)]
     return done, ms, curve
 
 
@@ -274,7 +281,8 @@ def main():
     # deployed network is loaded and its kernels initialised once
     net.forward(torch.zeros((args.images, 1, args.n, args.n), device="cuda"))
     torch.cuda.synchronize()
-    plain = plain_curve(solver, sino, truth, args.iters)
+    pinfo = {}
+    plain = plain_curve(solver, sino, truth, args.iters, info=pinfo)
     target = plain[-1][2]
     info = {}
     it_l, ms_l, curve_l = learned_run(solver, net, sino, truth, args.k_in, target, args.iters, info=info)
@@ -282,8 +290,10 @@ def main():
     line = {
         "workload": f"{args.images} fan-beam phantoms {args.n}^2 at {geo.d} mm, {args.views} views, {geo.nu} bins, "
                     f"Poisson I0=1e5; plain ASD-POCS {args.iters} iterations vs CNN warm start after {args.k_in}",
-        "plain": {"iters": args.iters, "gpu_ms": plain[-1][1], "rmse": target, "curve": plain},
-        "learned": {"iters_after_net": it_l, "gpu_ms": ms_l, "net_ms": info["net_ms"], "rmse": curve_l[-1][2],
+        "plain": {"iters": args.iters, "gpu_ms": plain[-1][1], "rmse": target, "curve": plain,
+                  "data_residual": pinfo["residual"]},
+        "learned": {"iters_after_net": it_l, "gpu_ms": ms_l, "net_ms": info["net_ms"],
+                    "data_residual": info.get("residual", []), "rmse": curve_l[-1][2],
                     "curve": curve_l, "reached": curve_l[-1][2] <= target},
         "time_ratio": ms_l / plain[-1][1],
         "training": {"pairs": args.train, "epochs": args.epochs, "loss": losses, "pairs_s": t_pairs,

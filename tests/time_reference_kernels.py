@@ -13,7 +13,9 @@ end-to-end milliseconds of one forward + one backward through the FP64 host
 C ABI (host copies and conversions included).  With --e2e-only h0,hl,b1_3d
 the hexagonal (about 2^18 sites, 360 views) and cone-beam (256^3, 360 views,
 384^2 detector) layers are compared end to end through the same C ABI, in
-the reference's own modes."""
+the reference's own modes.  With --matrix the system-matrix generators
+(bilinear_matrix_generation, pixel_matrix_generation) are timed on both
+libraries at 128^2 x 180 views and 256^2 x 90 views."""
 import argparse
 import ctypes
 import json
@@ -120,8 +122,25 @@ def e2e_pair(kind, reps):
     return tr, to
 
 
+def matrix_pair(kind, n, views):
+    """(reference s, ours s, nnz) of one call of the generator at n^2 pixels of
+    (256/n) mm, `views` views, ceil(1.44 n) bins of (512/n) mm."""
+    from sgd_b200.operators import matrix_generation
+    d, nu, du = 256.0 / n, int(np.ceil(1.44 * n)), 512.0 / n
+    cap = int(5 * n * n * views)
+    t0 = time.perf_counter()
+    nr, _ = reflib.matrix_generation(kind, views, nu, n, n, d, d, du, LSD, LSO, cap)
+    tr = time.perf_counter() - t0
+    matrix_generation(kind, n, n, views, nu, d, d, du, LSD, LSO, buffer_size=cap)  # first call: setup
+    t0 = time.perf_counter()
+    no, _ = matrix_generation(kind, n, n, views, nu, d, d, du, LSD, LSO, buffer_size=cap)
+    to = time.perf_counter() - t0
+    return tr, to, nr, no
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--matrix", action="store_true")
     ap.add_argument("--reps", type=int, default=5)
     ap.add_argument("--kinds", default="b1,SF,b0")
     ap.add_argument("--e2e-only", default="")
@@ -146,6 +165,12 @@ def main():
         print(json.dumps({"kind": kind, "reference_e2e_fwd_back_ms": tr, "ours_e2e_fwd_back_ms": to,
                           "e2e_speedup": tr / to, "modes": "the reference's own (H0 bounds, A_B1_3D pair as "
                           "the reference: its backward returns zeros, timed all the same)"}), flush=True)
+    if args.matrix:
+        for kind in ("b1", "b0"):
+            for n, views in ((128, 180), (256, 90)):
+                tr, to, nr, no = matrix_pair(kind, n, views)
+                print(json.dumps({"generator": kind, "pixels": n, "views": views, "reference_s": tr, "ours_s": to,
+                                  "speedup": tr / to, "nnz_reference": nr, "nnz_ours": no}), flush=True)
 
 
 if __name__ == "__main__":
