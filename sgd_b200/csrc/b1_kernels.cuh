@@ -29,33 +29,37 @@ struct B1Bin {
     float4 q0, q1, q2, q3;
 };
 
+// Derived constants, formed identically in both forms: a - b and
+// -1/(24a^2b^2) = -0.5 * 1/(12a^2b^2) (exact).
+__device__ __forceinline__ float b1_amb(const B1Bin& r) { return __fsub_rn(r.q2.x, r.q1.z); }
+
 // G(x) = sign(x) S(|x|); S in closed form (fan_geometry.h).
 __device__ __forceinline__ float b1_G(float x, const B1Bin& r) {
-    const float a = r.q1.z, b = r.q1.w, apb = r.q2.x, amb = r.q2.y;
-    const float c1 = r.q2.z, c2 = r.q2.w, c3 = r.q3.x, c4 = r.q3.y, c5 = r.q3.z;
+    const float b = r.q1.z, a = r.q2.x, apb = r.q2.z, amb = b1_amb(r);
+    const float c1 = r.q3.x, c2 = r.q3.y, nc3 = r.q3.z, c4 = r.q3.w, nc5 = __fmul_rn(-0.5f, c4);
     const float ax = fabsf(x);
     const float w = fmaxf(__fsub_rn(b, ax), 0.f);
     const float w2 = __fmul_rn(w, w);
     const float w4 = __fmul_rn(w2, w2);
     // inner: x/a - x^2/(2a^2) - b^2/(12a^2) + w^4/(12a^2b^2)
-    float sin_ = __fmaf_rn(ax, __fmaf_rn(-ax, c2, c1), -c3);
+    float sin_ = __fmaf_rn(ax, __fmaf_rn(-ax, c2, c1), nc3);
     sin_ = __fmaf_rn(c4, w4, sin_);
     // outer: 1/2 - (p^4 - 2q^4 - 2w^4)/(24a^2b^2)
     const float p = fmaxf(__fsub_rn(apb, ax), 0.f);
     const float q = fmaxf(__fsub_rn(a, ax), 0.f);
     const float p2 = __fmul_rn(p, p), q2 = __fmul_rn(q, q);
-    float t = __fmaf_rn(p2, p2, -__fadd_rn(w4, w4));
+    float t = __fmaf_rn(p2, p2, __fmul_rn(w4, -2.f));  // -(w4 + w4) exactly
     t = __fmaf_rn(__fmul_rn(-2.f, q2), q2, t);
-    const float sout = __fmaf_rn(-c5, t, 0.5f);
+    const float sout = __fmaf_rn(nc5, t, 0.5f);
     return copysignf(ax <= amb ? sin_ : sout, x);
 }
 
-// Edge offsets of pixel (fi, fj): xa = fi*c0 + (fj*c1 + c2), rounded in that
+// Edge offsets of pixel (fi, fj): xa = fi*ci + (fj*cj + c0), rounded in that
 // order (the forward kernel hoists the bracket out of its row loop).
-__device__ __forceinline__ float b1_xa_inner(float fj, const B1Bin& r) { return __fmaf_rn(fj, r.q0.y, r.q0.z); }
-__device__ __forceinline__ float b1_xb_inner(float fj, const B1Bin& r) { return __fmaf_rn(fj, r.q1.x, r.q1.y); }
+__device__ __forceinline__ float b1_xa_inner(float fj, const B1Bin& r) { return __fmaf_rn(fj, r.q0.z, r.q1.x); }
+__device__ __forceinline__ float b1_xb_inner(float fj, const B1Bin& r) { return __fmaf_rn(fj, r.q0.w, r.q1.y); }
 __device__ __forceinline__ float b1_xa(float fi, float inner, const B1Bin& r) { return __fmaf_rn(fi, r.q0.x, inner); }
-__device__ __forceinline__ float b1_xb(float fi, float inner, const B1Bin& r) { return __fmaf_rn(fi, r.q0.w, inner); }
+__device__ __forceinline__ float b1_xb(float fi, float inner, const B1Bin& r) { return __fmaf_rn(fi, r.q0.y, inner); }
 
 // One MUFU reciprocal (|x| >= 2^-126 here: xb - xa is a bin width at the
 // pixel, ~0.1..10 mm).
@@ -88,20 +92,22 @@ struct B1Pair {
     float amb;                                  // a - b
 };
 
+// The record's first three chunks are already operand pairs; the four
+// single constants of the last are duplicated.
 __device__ __forceinline__ B1Pair b1_pair(const B1Bin& r) {
     B1Pair k;
-    k.ci = make_float2(r.q0.x, r.q0.w);
-    k.cj = make_float2(r.q0.y, r.q1.x);
-    k.c0 = make_float2(r.q0.z, r.q1.y);
-    k.a = pair(r.q1.z);
-    k.b = pair(r.q1.w);
-    k.apb = pair(r.q2.x);
-    k.amb = r.q2.y;
-    k.k1 = pair(r.q2.z);
-    k.k2 = pair(r.q2.w);
-    k.nk3 = pair(-r.q3.x);
-    k.k4 = pair(r.q3.y);
-    k.nk5 = pair(-r.q3.z);
+    k.ci = make_float2(r.q0.x, r.q0.y);
+    k.cj = make_float2(r.q0.z, r.q0.w);
+    k.c0 = make_float2(r.q1.x, r.q1.y);
+    k.b = make_float2(r.q1.z, r.q1.w);
+    k.a = make_float2(r.q2.x, r.q2.y);
+    k.apb = make_float2(r.q2.z, r.q2.w);
+    k.amb = b1_amb(r);
+    k.k1 = pair(r.q3.x);
+    k.k2 = pair(r.q3.y);
+    k.nk3 = pair(r.q3.z);
+    k.k4 = pair(r.q3.w);
+    k.nk5 = __fmul2_rn(k.k4, pair(-0.5f));
     return k;
 }
 

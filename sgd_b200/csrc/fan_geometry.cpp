@@ -165,16 +165,13 @@ void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out) {
 
 void b1_profile_constants(double a, double b, float* r) {
     if (b <= 1e-7) b = 0.0;  // single-triangle limit
-    r[6] = (float)a;
-    r[7] = (float)b;
-    r[8] = (float)(a + b);
-    r[9] = (float)(a - b);
-    r[10] = (float)(1.0 / a);
-    r[11] = (float)(1.0 / (2.0 * a * a));
-    r[12] = (float)(b * b / (12.0 * a * a));
-    r[13] = b > 0 ? (float)(1.0 / (12.0 * a * a * b * b)) : 0.f;
-    r[14] = b > 0 ? (float)(1.0 / (24.0 * a * a * b * b)) : 0.f;
-    r[15] = 0.f;
+    r[6] = r[7] = (float)b;
+    r[8] = r[9] = (float)a;
+    r[10] = r[11] = (float)(a + b);
+    r[12] = (float)(1.0 / a);
+    r[13] = (float)(1.0 / (2.0 * a * a));
+    r[14] = -(float)(b * b / (12.0 * a * a));
+    r[15] = b > 0 ? (float)(1.0 / (12.0 * a * a * b * b)) : 0.f;
 }
 
 void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>& strip) {
@@ -203,10 +200,10 @@ void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>
             const double mBx = kb * tx - nxv, mBy = kb * ty - nyv;
             float r[kB1Rec];
             r[0] = (float)(mAx * g.dx);
-            r[1] = (float)(mAy * g.dy);
-            r[2] = (float)((x0 - px) * mAx + (y0 - py) * mAy);
-            r[3] = (float)(mBx * g.dx);
-            r[4] = (float)(mBy * g.dy);
+            r[1] = (float)(mBx * g.dx);
+            r[2] = (float)(mAy * g.dy);
+            r[3] = (float)(mBy * g.dy);
+            r[4] = (float)((x0 - px) * mAx + (y0 - py) * mAy);
             r[5] = (float)((x0 - px) * mBx + (y0 - py) * mBy);
             // profile half-widths (layers/A_B1.cu:429-478): vx = |dx cos(theta)|,
             // vy = |dy sin(theta)| with theta = atan2(|px - sx|, |py - sy|)

@@ -85,12 +85,15 @@ void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out);
 // b -> 0; b <= 1e-7 uses the single-triangle limit as the reference does
 // (layers/A_B1.cu:52-55).  One 64-byte record per (view, bin), stored as four
 // float4 chunks in the layout [view][chunk][bin] so that consecutive bins of
-// one chunk are consecutive 16-byte words (shared-memory bank groups):
-//   [0..2]  xa = i*r[0] + j*r[1] + r[2]
-//   [3..5]  xb = i*r[3] + j*r[4] + r[5]
-//   [6] a   [7] b   [8] a+b   [9] a-b
-//   [10] 1/a   [11] 1/(2a^2)   [12] b^2/(12a^2)   [13] 1/(12a^2b^2)   [14] 1/(24a^2b^2)
-//   [15] unused (0)
+// one chunk are consecutive 16-byte words (shared-memory bank groups).  The
+// fields come in the pairs that the packed-FP32 form of the footprint takes as
+// operands (b1_kernels.cuh):
+//   [0] [1]  i coefficients of xa, xb        xa = i*r[0] + (j*r[2] + r[4])
+//   [2] [3]  j coefficients of xa, xb        xb = i*r[1] + (j*r[3] + r[5])
+//   [4] [5]  constant terms of xa, xb
+//   [6] [7]  b, b      [8] [9]  a, a      [10] [11]  a+b, a+b
+//   [12] 1/a   [13] 1/(2a^2)   [14] -b^2/(12a^2)   [15] 1/(12a^2b^2)
+// (a-b and 1/(24a^2b^2) = [15]/2 are formed in the kernels.)
 // ---------------------------------------------------------------------------
 constexpr int kB1Rec = 16;
 
