@@ -30,7 +30,7 @@ b1_forward_kernel(const float4* __restrict__ rec, const float* __restrict__ stri
 }
 
 // One CTA per 32x8 tile; wins[tile * np + p] = (lo, hi), the tile's bins in view p.
-__global__ void __launch_bounds__(kBackThreads, 5)
+__global__ void __launch_bounds__(kBackThreads, 8)
 b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__ hom, const int2* __restrict__ wins,
                const float* __restrict__ sino, float* __restrict__ img, int nx, int ny, int np, int nu, int wcap,
                float dxdy, int* __restrict__ err) {

@@ -68,7 +68,7 @@ b1_forward_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restr
 }
 
 template <int VC>
-__global__ void __launch_bounds__(kBackThreads, 4)
+__global__ void __launch_bounds__(kBackThreads, 8)
 b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict__ start, int ns, long long total,
                      const float* __restrict__ sino, float* __restrict__ img, unsigned long long* __restrict__ counter,
                      int* __restrict__ err) {

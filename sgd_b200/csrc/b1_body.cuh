@@ -7,7 +7,8 @@
 //                    inside the strip (packed-pair form, b1_kernels.cuh), and
 //                    the warp reduces with shuffles.  The sinogram value is
 //                    written once, no atomics.
-//   b1_back_tile     voxel-driven: one thread per pixel of a 32x8 tile.  Per
+//   b1_back_tile     voxel-driven: two pixels per thread (rows i and i + 4)
+//                    of a 32x8 tile, 128 threads.  Per
 //                    chunk of VC views the CTA stages the bin window its tile
 //                    projects onto in shared memory: the 64-byte footprint
 //                    records by TMA bulk copies completed on an mbarrier
@@ -33,7 +34,7 @@ namespace sgd {
 
 constexpr int kBackTI = 8;    // tile extent along i (x)
 constexpr int kBackTJ = 32;   // tile extent along j (y): contiguous in memory
-constexpr int kBackThreads = kBackTI * kBackTJ;
+constexpr int kBackThreads = kBackTI * kBackTJ / 2;  // two pixels per thread
 constexpr uint32_t kWaitLimit = 1u << 22;
 
 // 2 mbarriers | 3 x VC windows | 3 x VC homographies, then the staged records
@@ -145,12 +146,13 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     float4* srec = reinterpret_cast<float4*>(smem + kHeader);      // [2][VC][4 chunks][wcap]
     float* ssino = reinterpret_cast<float*>(srec + 2 * VC * 4 * wcap);  // [2][VC][wcap]
 
-    // each warp covers an 8 (j) x 4 (i) block of the 32 x 8 tile, so that its
-    // lanes read few distinct bins of a view
+    // warp w covers columns j0 + 8w .. + 7 of rows i0 .. i0 + 3 (pixel A) and
+    // of rows i0 + 4 .. i0 + 7 (pixel B): 8 x 4 blocks whose lanes read few
+    // distinct bins of a view
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const int i = i0 + 4 * (w >> 2) + (l >> 3), j = j0 + 8 * (w & 3) + (l & 7);
-    const float fi = (float)i, fj = (float)j;
-    const float2 fi2 = pair(fi), fj2 = pair(fj);
+    const int i = i0 + (l >> 3), j = j0 + 8 * w + (l & 7), iB = i + 4;
+    const float fi = (float)i, fj = (float)j, fiB = (float)iB;
+    const float2 fi2 = pair(fi), fj2 = pair(fj), fiB2 = pair(fiB);
     const int nchunks = (np + VC - 1) / VC;
     auto parity = [&](int c) { return (((c & 1) ? use1 : use0) + (uint32_t)(c >> 1)) & 1u; };
 
@@ -200,7 +202,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     __syncthreads();  // the previous tile's last chunk is fully consumed
     stage(0);
 
-    double acc = 0.0;  // FP32 within a chunk (a few tens of terms), FP64 across chunks
+    double acc = 0.0, accB = 0.0;  // FP32 within a chunk (a few tens of terms), FP64 across chunks
     int c = 0;
     for (; c < nchunks; ++c) {
         __syncthreads();  // chunk c's windows and sinogram visible; chunk c-1 fully consumed
@@ -212,32 +214,44 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             atomicExch(err, 1);
             continue;
         }
-        if (i >= nx || j >= ny) continue;
-        // per view, this pixel's bins: trip counts differ by at most one bin
-        // between the lanes of a warp.  (A single flat loop over all the
-        // chunk's (view, bin) pairs, switching views per lane, measured 1.38x
-        // slower at 512^2 x 720 views: the warp ran the switch on most
-        // iterations.)  The bin loop is not unrolled: unrolled, it spills at
-        // the 48 registers five CTAs per SM allow.
-        float csum = 0.f;
+        if (j >= ny || i >= nx) continue;
+        const bool hasB = iB < nx;
+        float csum = 0.f, csumB = 0.f;
 #pragma unroll
         for (int v = 0; v < VC; ++v) {
             const int lo = win[(slot * VC + v) * 2], hi = win[(slot * VC + v) * 2 + 1];
             if (hi < lo) continue;
-            int a, b;
+            int a, b, aB, bB;
             box_bins_bound(hs + (slot * VC + v) * 8, fi, fj, nu, a, b);
+            box_bins_bound(hs + (slot * VC + v) * 8, fiB, fj, nu, aB, bB);
             a = max(a, lo);
             b = min(b, hi);
+            aB = max(aB, lo);
+            bB = hasB ? min(bB, hi) : aB - 1;
             const float4* rb = srec + (st * VC + v) * 4 * wcap - lo;
             const float* sb = ssino + (st * VC + v) * wcap - lo;
+            // per view, each pixel's bins in one loop: trip counts differ by
+            // at most one bin between the lanes of a warp.  (A single flat
+            // loop over all the chunk's (view, bin) pairs, switching views
+            // per lane, measured 1.38x slower at 512^2 x 720 views: the warp
+            // ran the switch on most iterations.)  The two pixels' k-th bins
+            // are evaluated side by side, clamped into their ranges with the
+            // surplus evaluation discarded: two independent chains per
+            // iteration (one pixel per thread measured 3.4 % slower).
+            const int n = max(b - a, bB - aB) + 1;
 #pragma unroll 1
-            for (int u = a; u <= b; ++u) {
-                const B1Pair k = b1_pair(B1Bin{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]});
-                const float conv = b1_conv_pair(b1_edges2(fi2, b1_inner2(fj2, k), k), k);
-                if (conv > kConvEps) csum = fmaf(conv, sb[u], csum);
+            for (int k = 0; k < n; ++k) {
+                const int u = a <= b ? min(a + k, b) : lo, uB = aB <= bB ? min(aB + k, bB) : lo;
+                const B1Pair kA = b1_pair(B1Bin{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]});
+                const B1Pair kB = b1_pair(B1Bin{rb[uB], rb[uB + wcap], rb[uB + 2 * wcap], rb[uB + 3 * wcap]});
+                const float convA = b1_conv_pair(b1_edges2(fi2, b1_inner2(fj2, kA), kA), kA);
+                const float convB = b1_conv_pair(b1_edges2(fiB2, b1_inner2(fj2, kB), kB), kB);
+                if (a + k <= b && convA > kConvEps) csum = fmaf(convA, sb[u], csum);
+                if (aB + k <= bB && convB > kConvEps) csumB = fmaf(convB, sb[uB], csumB);
             }
         }
         acc += (double)csum;
+        accB += (double)csumB;
     }
     if (c < nchunks) {
         // a staged chunk never arrived: wait (bounded) for the copies still in
@@ -251,6 +265,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     use0 += (uint32_t)((nchunks + 1) >> 1);
     use1 += (uint32_t)(nchunks >> 1);
     if (i < nx && j < ny) img[(size_t)i * ny + j] = (float)acc * dxdy;
+    if (iB < nx && j < ny) img[(size_t)iB * ny + j] = (float)accB * dxdy;
     return true;
 }
 
