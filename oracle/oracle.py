@@ -40,6 +40,7 @@ def lib():
         L.oracle_exact_fan2d_matrix.restype = None
         L.oracle_exact_parallel_matrix.restype = None
         L.oracle_exact_hex_matrix.restype = None
+        L.oracle_exact_hl_matrix.restype = None
         L.oracle_matrix_generation.restype = ctypes.c_longlong
         L.oracle_ref_simpson_3d.restype = None
         L.oracle_sf3d_backward.restype = None
@@ -257,6 +258,18 @@ def exact_hex_matrix(nl, nc, nu, dt, du, lsd, lso, angles, tol=1e-10):
     M = np.zeros(len(angles) * nu * nc * nl)
     d = ctypes.c_double
     lib().oracle_exact_hex_matrix(nl, nc, len(angles), nu, d(dt), d(du), d(lsd), d(lso), _p(angles), d(tol), _p(M))
+    return M.reshape(len(angles) * nu, nc * nl)
+
+
+def exact_hl_matrix(nl, nc, nu, dt, du, lsd, lso, angles, tol=1e-10):
+    """Dense exact FP64 system matrix (np*nu, nc*nl) of the hexagonal linear
+    element (the Hl basis, layers/A_Hl.cu:168-266: the Courant hat of the
+    triangular lattice, rows 0.5 dt apart): bin-averaged line integrals;
+    columns in the host layout ic*nl + il, absent sites zero."""
+    angles = _c(angles)
+    M = np.zeros(len(angles) * nu * nc * nl)
+    d = ctypes.c_double
+    lib().oracle_exact_hl_matrix(nl, nc, len(angles), nu, d(dt), d(du), d(lsd), d(lso), _p(angles), d(tol), _p(M))
     return M.reshape(len(angles) * nu, nc * nl)
 
 

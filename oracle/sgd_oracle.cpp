@@ -1337,6 +1337,117 @@ void oracle_exact_hex_matrix(int nl, int nc, int np, int nu, double dt, double d
         }
 }
 
+// Exact fan-beam system matrix of the hexagonal linear element, the basis of
+// Hl (layers/A_Hl.cu:168-266): sites on the lattice of H0 with rows 0.5 dt
+// apart (:184-193), each carrying the Courant hat of the triangular lattice
+// (value 1 at the site, 0 at its six neighbours at distance dt, linear on the
+// six triangles): h(X) = max(0, 1 - |X - o|_hex) with |.|_hex the gauge of the
+// hexagon of circumradius dt and vertices at 30 + 60 k degrees.  The kernel
+// evaluates its X-ray as the univariate box spline of the three lattice
+// directions (:21-46).  Entry: the line integral of h along the ray from the
+// source to each point of bin u, averaged over the bin; along a ray h is
+// linear between the crossings of the six spokes and six edges, across the
+// bin the integral is smooth between the rays through the centre and the
+// vertices, so each piece is integrated exactly.
+// Dense, M[(p*nu + u)*(nc*nl) + ic*nl + il]; absent sites stay 0.
+void oracle_exact_hl_matrix(int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
+                            const double* angles, double tol, double* M) {
+    Geo g = make_geo(nc, nl, 1, np, nu, 1, dt * std::sqrt(3.0), dt * 0.5, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    const size_t ncol = (size_t)nc * nl;
+    std::memset(M, 0, sizeof(double) * ncol * np * nu);
+    const double sdx = dt * std::sqrt(3.0), sdy = 0.5 * dt, apo = 0.5 * std::sqrt(3.0) * dt;
+    double vx[7], vy[7], mx[6], my[6];
+    for (int k = 0; k < 6; ++k) {
+        vx[k] = dt * std::cos(kPI / 6 + k * kPI / 3);
+        vy[k] = dt * std::sin(kPI / 6 + k * kPI / 3);
+        mx[k] = std::cos(k * kPI / 3);  // edge normals, between the vertices
+        my[k] = std::sin(k * kPI / 3);
+    }
+    vx[6] = vy[6] = 0.0;  // the centre
+    auto hat = [&](double x, double y) {
+        double gauge = 0.0;
+        for (int k = 0; k < 6; ++k) gauge = std::max(gauge, (x * mx[k] + y * my[k]) / apo);
+        return std::max(0.0, 1.0 - gauge);
+    };
+    // line integral of the hat at o along s -> q: Simpson on the pieces
+    // between the crossings of the spokes (centre to vertex) and edges
+    auto line = [&](const double* s, const double* q, const double* o) {
+        double d[2] = {q[0] - s[0], q[1] - s[1]};
+        const double len = std::hypot(d[0], d[1]);
+        d[0] /= len; d[1] /= len;
+        const double ax = s[0] - o[0], ay = s[1] - o[1];
+        // the hexagon's extent along the ray
+        double t0 = -1e300, t1 = 1e300;
+        for (int k = 0; k < 6; ++k) {
+            const double num = apo - (ax * mx[k] + ay * my[k]), den = d[0] * mx[k] + d[1] * my[k];
+            if (den == 0.0) {
+                if (num < 0) return 0.0;
+                continue;
+            }
+            const double t = num / den;
+            if (den > 0) t1 = std::min(t1, t);
+            else t0 = std::max(t0, t);
+        }
+        if (!(t1 > t0)) return 0.0;
+        double cut[8];
+        int nc2 = 0;
+        cut[nc2++] = t0;
+        for (int k = 0; k < 6; ++k) {  // spoke k: o + r (vx, vy), r in [0, 1]
+            const double den = d[0] * vy[k] - d[1] * vx[k];
+            if (den == 0.0) continue;
+            const double t = (ay * vx[k] - ax * vy[k]) / den;
+            if (t > t0 && t < t1 && nc2 < 7) cut[nc2++] = t;
+        }
+        cut[nc2++] = t1;
+        std::sort(cut, cut + nc2);
+        double sum = 0.0;
+        for (int k = 0; k + 1 < nc2; ++k) {
+            const double a = cut[k], b = cut[k + 1], m = 0.5 * (a + b);
+            sum += (b - a) / 6.0 * (hat(ax + a * d[0], ay + a * d[1]) + 4.0 * hat(ax + m * d[0], ay + m * d[1]) +
+                                    hat(ax + b * d[0], ay + b * d[1]));
+        }
+        return sum;
+    };
+#pragma omp parallel for schedule(dynamic) collapse(2)
+    for (int p = 0; p < np; ++p)
+        for (int u = 0; u < nu; ++u) {
+            const double* s = &g.src[3 * p];
+            const double* dtv = &g.dtv[3 * p];
+            const double* pu = &g.puv[3 * p];
+            double* row = M + ((size_t)p * nu + u) * ncol;
+            double e0[2], e1[2];
+            for (int k = 0; k < 2; ++k) {
+                e0[k] = dtv[k] + pu[k] * (u - 0.5 * nu) - s[k];
+                e1[k] = dtv[k] + pu[k] * (u - 0.5 * nu + 1.0) - s[k];
+            }
+            const double n0 = std::hypot(e0[0], e0[1]), n1 = std::hypot(e1[0], e1[1]);
+            for (int ic = 0; ic < nc; ++ic)
+                for (int il = 0; il < nl; ++il) {
+                    if ((il & 1) && ic == nc - 1) continue;
+                    const double o[2] = {(ic - ((il & 1) ? 0.5 * (nc - 2) : 0.5 * (nc - 1))) * sdx,
+                                         (il - 0.5 * (nl - 1)) * sdy};
+                    const double r[2] = {o[0] - s[0], o[1] - s[1]};
+                    const double c0 = (e0[0] * r[1] - e0[1] * r[0]) / n0, c1 = (e1[0] * r[1] - e1[1] * r[0]) / n1;
+                    if ((c0 > dt && c1 > dt) || (c0 < -dt && c1 < -dt)) continue;
+                    auto f = [&](double t) {
+                        const double q[2] = {dtv[0] + pu[0] * (u - 0.5 * nu + t), dtv[1] + pu[1] * (u - 0.5 * nu + t)};
+                        return line(s, q, o);
+                    };
+                    std::vector<double> cuts;
+                    const double off = u - 0.5 * nu;
+                    for (int k = 0; k < 7; ++k) {
+                        const double cx = o[0] + vx[k] - s[0], cy = o[1] + vy[k] - s[1];
+                        const double den = pu[0] * cy - pu[1] * cx;
+                        if (den == 0.0) continue;
+                        const double t = -((dtv[0] - s[0]) * cy - (dtv[1] - s[1]) * cx) / den - off;
+                        if (t > 0.0 && t < 1.0) cuts.push_back(t);
+                    }
+                    row[(size_t)ic * nl + il] = integrate_pieces(f, cuts, tol * dt);
+                }
+        }
+}
+
 // Exact parallel-beam system matrix of the pixel-indicator (kind 0) or
 // bilinear (kind 1) basis, dense, M[(p*nu + u)*(nx*ny) + ix*ny + iy]: for
 // view angle beta the rays run along (cos beta, sin beta) and bin u covers

@@ -104,3 +104,16 @@ def test_h0_corrected_against_exact_hexagon_projection(oracle_mod):
     odd_last = [(nc - 1) * nl + il for il in range(1, nl, 2)]
     x[odd_last] = 0.0  # absent sites of the odd rows
     assert rel_l2(A.matvec(x), 3.0 * (M @ x)) < 1e-4
+
+
+def test_hl_against_exact_linear_element_projection(oracle_mod):
+    """The GPU Hl against the exact FP64 bin-averaged line integrals of the
+    Courant hat on the lattice (its FP64 formula sits 7.5e-6 from them)."""
+    from sgd_b200.operators import A_Hl_operator
+    nl, nc, nu, dt, du, lsd, lso = 24, 12, 60, 2.0, 1.5, 1085.6, 595.0
+    ang = np.array([0.3, 1.1, np.pi / 4, 2.5])
+    M = oracle_mod.exact_hl_matrix(nl, nc, nu, dt, du, lsd, lso, ang)
+    A = A_Hl_operator(nl, nc, len(ang), nu, dt, du, lsd, lso, ang)
+    x = np.random.default_rng(0).random(nc * nl)
+    x[[(nc - 1) * nl + il for il in range(1, nl, 2)]] = 0.0  # absent sites of the odd rows
+    assert rel_l2(A.matvec(x), M @ x) < 2e-4

@@ -261,6 +261,31 @@ def test_h0_model_error_vs_exact_hexagon(oracle_mod):
     assert rel_l2(b_ref, exact) > 0.1
 
 
+def test_exact_hl_matrix_carries_the_hat_integral(oracle_mod):
+    """Nearly parallel rays: a site's bin-averaged line integrals of the
+    Courant hat summed over the bins times the bin width at the site give
+    the hat's integral, (sqrt 3 / 2) dt^2 (the triangular lattice's cell)."""
+    nl, nc, nu, dt, du = 5, 4, 80, 2.0, 0.25
+    lsd, lso = 1.0e5, 5.0e4
+    ang = np.array([0.0, 0.37, np.pi / 6, 1.9])
+    M = oracle_mod.exact_hl_matrix(nl, nc, nu, dt, du, lsd, lso, ang)
+    col = M[:, 1 * nl + 2].reshape(len(ang), nu).sum(axis=1)
+    # the site sits 1.7 mm off the isocentre (magnification off by ~4e-5)
+    assert np.allclose(col * du * lso / lsd, 0.5 * np.sqrt(3.0) * dt * dt, rtol=1e-4)
+
+
+def test_hl_model_error_vs_exact_linear_element(oracle_mod):
+    """Hl's formula (the X-ray of the three-direction box spline convolved
+    with the bin's width, layers/A_Hl.cu:21-46) against the exact bin-averaged
+    line integrals of the Courant hat: the model error of its bin blur."""
+    nl, nc, nu, dt, du, lsd, lso = 24, 12, 60, 2.0, 1.5, 1085.6, 595.0
+    ang = np.array([0.3, 1.1, np.pi / 4, 2.5])
+    M = oracle_mod.exact_hl_matrix(nl, nc, nu, dt, du, lsd, lso, ang)
+    x = np.random.default_rng(0).random(nc * nl)
+    b, _ = oracle_mod.hex_forward("hl", x, nl, nc, nu, dt, du, lsd, lso, ang)
+    assert rel_l2(b, M @ x) < 5e-5
+
+
 def test_chord_simpson_3d(oracle_mod):
     """Ref_project_Simpson restated: a uniform odd-sized cube seen along +x
     carries its length on the central cell (the nine samples avoid voxel
