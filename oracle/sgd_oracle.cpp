@@ -815,7 +815,9 @@ int sf3d_voxel_view(const Geo& g, double lsd, int mode, bool fwd, bool trap, int
     T C;
     const T tw = T(2) / ((us[3] - us[0]) + (us[2] - us[1]));
     if (fwd) {
-        const double factor = (double)((float)flsd * (float)flsd) * g.dy * g.dz / (g.du * g.dv);
+        // :364; the corrected pair (mode 1) multiplies in the missing dx
+        const double factor =
+            (double)((float)flsd * (float)flsd) * g.dy * g.dz / (g.du * g.dv) * (mode == 1 ? g.dx : 1.0);
         C = w * w * T(factor) * tw * (trap ? T(2) / ((vs[3] - vs[0]) + (vs[2] - vs[1])) : T(1) / (vs[1] - vs[0]));
     } else {
         C = w * T(flsd * g.dx / g.np) * tw * (T(1) / (vs[1] - vs[0]));

@@ -47,7 +47,7 @@ struct SFGeo {
     double dx, dy, dz;
     const float* pmi;    // [np][12]
     const double* src;   // [np][3]
-    const double* fwdf;  // [np] forward factor lsd^2 dy dz / (du dv)
+    const double* fwdf;  // [np] forward factor lsd^2 dy dz / (du dv) (times dx in mode 1)
     double backf;        // lsd dx / np
 };
 
@@ -268,7 +268,10 @@ public:
             else exact_pmi(fr[p], nu / 2.0, nv / 2.0, nx, ny, nz, dx, dy, dz, &pmi[12 * (size_t)p]);
             for (int k = 0; k < 3; ++k) src[3 * p + k] = fr[p].src[k];
             const float flsd = (float)lsd;  // SF::project: float lsd (:362)
-            fwdf[p] = flsd * flsd * dy * dz / (du * dv);
+            // the reference's factor lsd^2 dy dz / (du dv) (:364) lacks the
+            // voxel's third side: the corrected pair multiplies it in, so
+            // that its forward carries the voxel's line integrals for any dx
+            fwdf[p] = flsd * flsd * dy * dz / (du * dv) * (mode == 1 ? dx : 1.0);
         }
         SGD_CUDA(cudaMalloc(&d_pmi_, pmi.size() * sizeof(float)));
         SGD_CUDA(cudaMemcpy(d_pmi_, pmi.data(), pmi.size() * sizeof(float), cudaMemcpyHostToDevice));

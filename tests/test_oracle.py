@@ -7,7 +7,7 @@ import pytest
 
 from conftest import ROOT
 from geometry_cases import cone_case, fan_case, rel_l2
-from sgd_b200.phantom import ellipse_phantom, ellipse_chords, random_ellipses
+from sgd_b200.phantom import ellipse_chords, ellipse_phantom, ellipsoid_phantom, random_ellipses
 
 
 def test_geometry_snaps_45_degree_views(oracle_mod):
@@ -284,6 +284,22 @@ def test_hl_model_error_vs_exact_linear_element(oracle_mod):
     x = np.random.default_rng(0).random(nc * nl)
     b, _ = oracle_mod.hex_forward("hl", x, nl, nc, nu, dt, du, lsd, lso, ang)
     assert rel_l2(b, M @ x) < 5e-5
+
+
+def test_sf3d_corrected_against_voxel_chords(oracle_mod):
+    """The corrected SF_projector forward (FP64 replica) against the voxel
+    indicator's chord lengths averaged over the detector cells (the Simpson
+    restatement of Ref_project_Simpson, adaptive): unit scale for 2 mm voxels
+    (the reference's amplitude would give half), model error below 1e-3."""
+    nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, ang = cone_case("small")
+    ang = ang[:3] + 0.013
+    x = ellipsoid_phantom(nx, ny, nz, dx, dy, dz, seed=0).ravel()
+    g = (nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, ang)
+    r = oracle_mod.ref_simpson_3d(x, *g, adaptive=True)
+    b = oracle_mod.sf3d_forward(x, *g, mode=1)
+    alpha = float(b @ r) / float(r @ r)
+    assert abs(alpha - 1.0) < 2e-3
+    assert rel_l2(b, r) < 2e-3
 
 
 def test_chord_simpson_3d(oracle_mod):

@@ -94,11 +94,13 @@ def test_reference_forward_sees_support_only():
     assert np.array_equal(b, A.matvec((x != 0).astype(np.float64)))
 
 
-def test_corrected_forward_line_integral():
-    """Mode 1 on a uniform slab: a central ray through a 16 mm-thick cube of
-    ones, perpendicular to it, carries about its length."""
+@pytest.mark.parametrize("d", [1.0, 2.0])
+def test_corrected_forward_line_integral(d):
+    """Mode 1 on a uniform slab: a central ray through a cube of ones, 16
+    voxels of d mm, perpendicular to it, carries about its length (the
+    reference's amplitude lacks the factor dx, right only for 1 mm voxels)."""
     from sgd_b200.operators import SF_projector_operator
-    n, d = 16, 1.0
+    n = 16
     ang = np.array([0.0])
     A = SF_projector_operator(n, n, n, 1, 32, 32, d, d, d, 0.5, 0.5, 1085.6, 595.0, ang, mode=1)
     b = A.matvec(np.ones(n ** 3)).reshape(32, 32)
