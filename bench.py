@@ -64,8 +64,7 @@ def max_over_ranks(x, world, device):
 def _families():
     """name -> (description, constructor of a sgd_b200.torch_ops projector,
     voxel-views per direction, seeded input maker)."""
-    C3_ANG = 2 * np.pi * np.arange(360) / 360
-    C5_ANG = 2 * np.pi * np.arange(360) / 360
+    HEX_ANG = 2 * np.pi * np.arange(360) / 360
 
     def fan(kind):
         from sgd_b200.torch_ops import FanProjector
@@ -77,7 +76,7 @@ def _families():
 
     def hexp(mode, nl, nc, dt):
         from sgd_b200.torch_ops import HexProjector
-        return HexProjector(nl, nc, NU, dt, DU, LSD, LSO, C3_ANG, mode=mode)
+        return HexProjector(nl, nc, NU, dt, DU, LSD, LSO, HEX_ANG, mode=mode)
 
     def cone(kind, n=256, views=360, nd=384, d=1.0, dd=1.5):
         from sgd_b200.torch_ops import ConeProjector
@@ -85,26 +84,26 @@ def _families():
         return ConeProjector(kind, n, n, n, nd, nd, d, d, d, dd, dd, LSD, LSO, ang)
 
     return {
-        "sf_c2": ("A_SF separable footprint fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
+        "sf_fan512": ("A_SF separable footprint fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
                   lambda: fan("SF"), NX * NY * NP),
-        "b0_c2": ("A_B0 pixel basis fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
+        "b0_fan512": ("A_B0 pixel basis fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
                   lambda: fan("b0"), NX * NY * NP),
-        "b0_parallel_c1": ("B0 parallel beam, 128x128 @1mm, 180 views over pi, 185 bins @1mm",
+        "b0_parallel128": ("B0 parallel beam, 128x128 @1mm, 180 views over pi, 185 bins @1mm",
                            par, 128 * 128 * 180),
-        "h0_c3": ("H0 hexagonal lattice (true hexagon bounds), 550 rows x 477 sites, dt 0.62 mm, 360 views, "
+        "h0_hex2e18": ("H0 hexagonal lattice (true hexagon bounds), 550 rows x 477 sites, dt 0.62 mm, 360 views, "
                   "736 bins @1mm", lambda: hexp("h0c", 550, 477, 0.62), 550 * 477 * 360),
-        "hl_c3": ("Hl hexagonal lattice, 953 rows x 275 sites, dt 1.075 mm, 360 views, 736 bins @1mm",
+        "hl_hex2e18": ("Hl hexagonal lattice, 953 rows x 275 sites, dt 1.075 mm, 360 views, 736 bins @1mm",
                   lambda: hexp("hl", 953, 275, 1.075), 953 * 275 * 360),
-        "b1_3d_c5": ("A_B1_3D cone beam (exact-transpose pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
+        "b1_3d_cone256": ("A_B1_3D cone beam (exact-transpose pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
                      lambda: cone("b1_3d"), 256 ** 3 * 360),
-        "sf3d_c5": ("SF_projector cone beam (corrected pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
+        "sf3d_cone256": ("SF_projector cone beam (corrected pair), 256^3 @1mm, 360 views, 384x384 @1.5mm",
                     lambda: cone("sf3d"), 256 ** 3 * 360),
         "b1_3d_small": ("A_B1_3D cone beam, the 256^3 cone geometry at half resolution for profiling: 128^3 @2mm, "
                         "180 views, 192x192 @3mm", lambda: cone("b1_3d", 128, 180, 192, 2.0, 3.0), 128 ** 3 * 180),
     }
 
 
-FAMILIES = ("sf_c2", "b0_c2", "b0_parallel_c1", "h0_c3", "hl_c3", "b1_3d_c5", "sf3d_c5", "b1_3d_small")
+FAMILIES = ("sf_fan512", "b0_fan512", "b0_parallel128", "h0_hex2e18", "hl_hex2e18", "b1_3d_cone256", "sf3d_cone256", "b1_3d_small")
 
 
 def parse():
@@ -113,8 +112,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["c2", "batch48"] + sorted(FAMILIES), default="c2",
-                    help="c2: the headline single-slice workload; batch48: 48 uneven slices in one "
+    ap.add_argument("--workload", choices=["fan512", "batch48"] + sorted(FAMILIES), default="fan512",
+                    help="fan512: the headline single-slice workload; batch48: 48 uneven slices in one "
                          "graph-replayed persistent launch per direction; the others: the other projector "
                          "families at their configurations (device-resident fwd+adj)")
     return ap.parse_args()
@@ -329,7 +328,7 @@ def run_ours(args, rank, world, local_rank):
     # roofline of the dominant kernel: algorithmic FLOPs of the reference
     # formula per launch over its measured duration, against the FP32 FMA
     # rate measured on this GPU now
-    ops = load_op_counts()["b1_c2"]
+    ops = load_op_counts()["b1_fan512"]
     V = NX * NY * NP
     E = P.conv_count
     flops = ops["range_flops_per_pixel_view"] * V + ops["flops_per_evaluation"] * E

@@ -21,7 +21,7 @@ def main():
     out = {}
     ang = 2 * np.pi * np.arange(720) / 720
     r, f, e = oracle.b1_flops(512, 512, 736, 0.5, 0.5, 1.0, 1085.6, 595.0, ang, nviews=24)
-    out["b1_c2"] = {
+    out["b1_fan512"] = {
         "geometry": "B1 fan 512x512 @0.5mm, 720 views, 736 bins @1mm, SOD 595, SDD 1085.6",
         "range_flops_per_pixel_view": r,
         "flops_per_evaluation": f,

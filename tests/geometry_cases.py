@@ -7,7 +7,7 @@ LSD, LSO = 1085.6, 595.0
 
 def fan_case(name):
     """(nx, ny, nu, dx, dy, du, lsd, lso, angles) of a named fan-beam case."""
-    if name == "c2":      # 512^2 at 0.5 mm, 720 views over 2pi, 736 bins at 1 mm
+    if name == "fan512":  # 512^2 at 0.5 mm, 720 views over 2pi, 736 bins at 1 mm
         return 512, 512, 736, 0.5, 0.5, 1.0, LSD, LSO, 2 * np.pi * np.arange(720) / 720
     if name == "small":   # 128^2 at 2 mm, 180 views, 185 bins at 1 mm
         return 128, 128, 185, 2.0, 2.0, 1.0, LSD, LSO, 2 * np.pi * np.arange(180) / 180
@@ -34,9 +34,9 @@ def hex_case(name):
         return 64, 40, 300, 2.0, 1.5, LSD, LSO, 2 * np.pi * np.arange(90) / 90
     if name == "tall":       # Hl-like row pitch: more rows
         return 128, 40, 300, 2.0, 1.5, LSD, LSO, 2 * np.pi * np.arange(90) / 90
-    if name == "c3_h0":      # ~2^18 sites over 512 mm, 360 views x 736 bins
+    if name == "h0_2e18":    # ~2^18 sites over 512 mm, 360 views x 736 bins
         return 550, 477, 736, 0.62, 1.0, LSD, LSO, 2 * np.pi * np.arange(360) / 360
-    if name == "c3_hl":
+    if name == "hl_2e18":
         return 953, 275, 736, 1.075, 1.0, LSD, LSO, 2 * np.pi * np.arange(360) / 360
     raise KeyError(name)
 
@@ -51,6 +51,6 @@ def cone_case(name):
         return 16, 16, 16, 24, 20, 2.0, 2.0, 2.0, 3.0, 3.0, LSD, LSO, 2 * np.pi * np.arange(8) / 8
     if name == "tallz":   # 80 slices (two 64-slice chunks) past both detector edges, narrow detector
         return 16, 8, 80, 16, 20, 2.0, 2.0, 2.0, 3.0, 3.0, LSD, LSO, np.array([0.1, 1.3, np.pi / 4, 2.9, 4.4, 5.7])
-    if name == "c5":      # 256^3 at 1 mm, 360 views over 2 pi, 384 x 384 at 1.5 mm
+    if name == "cone256": # 256^3 at 1 mm, 360 views over 2 pi, 384 x 384 at 1.5 mm
         return 256, 256, 256, 384, 384, 1.0, 1.0, 1.0, 1.5, 1.5, LSD, LSO, 2 * np.pi * np.arange(360) / 360
     raise KeyError(name)

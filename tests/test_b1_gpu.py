@@ -31,7 +31,7 @@ def make_op(case):
     return A_B1_operator(nx, ny, len(ang), nu, dx, dy, du, lsd, lso, ang), (nx, ny, nu, dx, dy, du, lsd, lso, ang)
 
 
-@pytest.mark.parametrize("case", ["tiny", "small", "rect", "snap", "wide", "c2"])
+@pytest.mark.parametrize("case", ["tiny", "small", "rect", "snap", "wide", "fan512"])
 def test_b1_matches_fp64_oracle(oracle_mod, case):
     A, (nx, ny, nu, dx, dy, du, lsd, lso, ang) = make_op(case)
     x = ellipse_phantom(nx, ny, dx, dy, seed=0).ravel()
@@ -45,7 +45,7 @@ def test_b1_matches_fp64_oracle(oracle_mod, case):
     assert abs(A.conv_count - cnt) <= 1e-4 * cnt + 2
 
 
-@pytest.mark.parametrize("case", ["small", "c2"])
+@pytest.mark.parametrize("case", ["small", "fan512"])
 def test_b1_gaussian_vs_fp64_oracle(oracle_mod, case):
     A, (nx, ny, nu, dx, dy, du, lsd, lso, ang) = make_op(case)
     rng = np.random.default_rng(1234)
@@ -55,7 +55,7 @@ def test_b1_gaussian_vs_fp64_oracle(oracle_mod, case):
     assert rel_l2(A.rmatvec(y), oracle_mod.b1_backward(y, nx, ny, nu, dx, dy, du, lsd, lso, ang)) < TOL_GAUSS
 
 
-@pytest.mark.parametrize("case", ["small", "rect", "snap", "wide", "c2"])
+@pytest.mark.parametrize("case", ["small", "rect", "snap", "wide", "fan512"])
 def test_b1_adjoint_dot_product(case):
     A, (nx, ny, nu, *_ , ang) = make_op(case)
     rng = np.random.default_rng(1234)
@@ -66,7 +66,7 @@ def test_b1_adjoint_dot_product(case):
     assert abs(lhs - rhs) / abs(lhs) < TOL_ADJOINT
 
 
-@pytest.mark.parametrize("case", ["small", "snap", "c2"])
+@pytest.mark.parametrize("case", ["small", "snap", "fan512"])
 def test_b1_matches_reference_library(oracle_mod, case):
     """Against the reference's own CUDA layer (built from its sources).
 
@@ -154,7 +154,7 @@ def test_b1_autograd_finite_differences():
     central differences (step 1e-3) of L(x) = <w, A x> match <A^T w, v>."""
     from sgd_b200.torch_ops import FanProjector, project
     nx = ny = 64
-    _, _, nu, dx, dy, du, lsd, lso, ang = fan_case("c2")
+    _, _, nu, dx, dy, du, lsd, lso, ang = fan_case("fan512")
     P = FanProjector("b1", nx, ny, nu, dx, dy, du, lsd, lso, ang)
     g = torch.Generator(device="cpu").manual_seed(7)
     x = torch.randn(nx, ny, generator=g).cuda().requires_grad_(True)

@@ -42,7 +42,7 @@ def test_matches_fp64_oracle(oracle_mod, case):
     assert abs(A.conv_count - cnt) <= 1e-4 * cnt + 3
 
 
-@pytest.mark.parametrize("case", ["small", "c5"])
+@pytest.mark.parametrize("case", ["small", "cone256"])
 def test_matches_reference_library(case):
     """Forward: parity with the reference's own kernel.  Backward: the
     reference's b1_3d_backward_projection scales each voxel's sum by the output
@@ -62,7 +62,7 @@ def test_matches_reference_library(case):
     assert np.linalg.norm(A.rmatvec(b_ref)) > 0
 
 
-@pytest.mark.parametrize("case", ["small", "rect", "c5"])
+@pytest.mark.parametrize("case", ["small", "rect", "cone256"])
 def test_exact_transpose_adjoint(case):
     A, g, _ = make(case, exact=True)
     rng = np.random.default_rng(1234)

@@ -140,7 +140,7 @@ def test_oracle_matches_reference_golden(oracle_mod, fname):
     assert rel_l2(xt, z["xt"]) < float(z["tol"])
 
 
-@pytest.mark.parametrize("case", ["c2", "snap", "rect"])
+@pytest.mark.parametrize("case", ["fan512", "snap", "rect"])
 def test_product_pmi_bit_identical_to_oracle(oracle_mod, case):
     """The library's projection matrices (host code) equal the restatement of
     utils/geo.cu bit for bit: the separable-footprint and 3D kernels take

@@ -18,7 +18,7 @@ def _cuda():
 
 
 CASES = {
-    "c1": (128, 128, 185, 1.0, 1.0, 1.0, np.pi * np.arange(180) / 180),
+    "par128": (128, 128, 185, 1.0, 1.0, 1.0, np.pi * np.arange(180) / 180),
     "rect": (40, 27, 61, 1.3, 0.8, 0.9, np.array([0.0, 0.2, np.pi / 4, 1.9, 3 * np.pi / 4, 2.8])),
 }
 
@@ -29,12 +29,12 @@ def make(case):
     return A_B0_parallel_operator(nx, ny, len(ang), nu, dx, dy, du, ang), (nx, ny, nu, dx, dy, du, ang)
 
 
-@pytest.mark.parametrize("case", ["c1", "rect"])
+@pytest.mark.parametrize("case", ["par128", "rect"])
 def test_matches_exact_fp64_oracle(oracle_mod, case):
     """For parallel rays the 3-direction box spline is the exact bin-averaged
     line integral of the pixel indicator, so the only error is FP32."""
     A, (nx, ny, nu, dx, dy, du, ang) = make(case)
-    if case == "c1":
+    if case == "par128":
         ang = ang[::15]  # 12 of the 180 views keep the dense oracle small
         from sgd_b200.operators import A_B0_parallel_operator
         A = A_B0_parallel_operator(nx, ny, len(ang), nu, dx, dy, du, ang)
@@ -45,7 +45,7 @@ def test_matches_exact_fp64_oracle(oracle_mod, case):
     assert rel_l2(A.rmatvec(y), M.T @ y) < 1e-5
 
 
-@pytest.mark.parametrize("case", ["c1", "rect"])
+@pytest.mark.parametrize("case", ["par128", "rect"])
 def test_adjoint_dot_product(case):
     A, _ = make(case)
     rng = np.random.default_rng(1234)
@@ -60,7 +60,7 @@ def test_long_source_fan_surrogate_approaches_parallel():
     away and the detector at the isocentre differs from the parallel layer by
     the residual ray divergence only."""
     from sgd_b200.operators import A_B0_operator
-    A, (nx, ny, nu, dx, dy, du, ang) = make("c1")
+    A, (nx, ny, nu, dx, dy, du, ang) = make("par128")
     lso = 1e4 * dx
     F = A_B0_operator(nx, ny, len(ang), nu, dx, dy, du, lso + 1e-3, lso, ang)
     x = ellipse_phantom(nx, ny, dx, dy, seed=5).ravel()

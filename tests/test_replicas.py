@@ -55,7 +55,7 @@ def test_max_over_ranks_single_rank_needs_no_group():
 
 
 def test_reference_arm_under_torchrun_prints_once():
-    """Two ranks launched as the driver launches them: rank 0 times the
+    """Two ranks launched by torchrun on one node: rank 0 times the
     reference's CPU path and prints one line, rank 1 exits 0 without work."""
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
            "127.0.0.1", "--master-port", str(_free_port()), "bench.py", "--impl", "reference", "--gpus", "2",
