@@ -20,6 +20,7 @@ import argparse
 import ctypes
 import json
 import math
+import os
 import time
 
 import numpy as np
@@ -207,23 +208,43 @@ def make_pairs(geo, seeds, iters, k_in, count=64, noise_seed=0, nonneg=False):
     return torch.cat(xs)[:n], torch.cat(ts)[:n]
 
 
-def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0, lr_final=None):
+def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0, lr_final=None, checkpoint=None):
     """Mean per-sample loss per epoch.  With lr_final the step size follows a
-    cosine from lr down to lr_final over the epochs."""
+    cosine from lr down to lr_final over the epochs.
+
+    checkpoint: a file path.  After every epoch the network's state (weights,
+    Adam moments and step), the shuffling generator's state and the losses so
+    far are written there; if the file exists when train() starts, training
+    resumes after its last epoch and continues exactly as the uninterrupted
+    run would (same batches, same step sizes)."""
     gen = torch.Generator().manual_seed(seed)
     n = x.shape[0]
     losses = []
     lr0 = lr
-    for ep in range(epochs):
+    start = 0
+    if checkpoint is not None and os.path.exists(checkpoint):
+        ck = torch.load(checkpoint, map_location="cpu", weights_only=True)
+        if ck["epochs"] != epochs or ck["n"] != n or ck["batch"] != batch or ck["seed"] != seed:
+            raise ValueError(f"checkpoint {checkpoint} was written by another training run")
+        net.load_state_dict(ck["net"])
+        gen.set_state(ck["generator"])
+        losses = list(ck["losses"])
+        start = ck["epoch"]
+    for ep in range(start, epochs):
         if lr_final is not None and epochs > 1:
             lr = lr_final + 0.5 * (lr0 - lr_final) * (1.0 + math.cos(math.pi * ep / (epochs - 1)))
         perm = torch.randperm(n, generator=gen)
         tot = 0.0
         for k in range(0, n - batch + 1, batch):
-            idx = perm[k:k + batch].cuda()
+            idx = perm[k:k + batch].to(x.device)
             loss = net.train_step(x[idx].unsqueeze(1), t[idx].unsqueeze(1), lr=lr)
             tot += float(loss)
         losses.append(tot / n)
+        if checkpoint is not None:
+            tmp = checkpoint + ".tmp"
+            torch.save({"epoch": ep + 1, "epochs": epochs, "n": n, "batch": batch, "seed": seed,
+                        "net": net.state_dict(), "generator": gen.get_state(), "losses": losses}, tmp)
+            os.replace(tmp, checkpoint)
     return losses
 
 
@@ -264,6 +285,8 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--lr-final", type=float, default=1e-4)
+    ap.add_argument("--checkpoint", default=None,
+                    help="file for per-epoch training checkpoints; an existing one is resumed")
     args = ap.parse_args()
     from .cnn import WarmStartCNN
     geo = Geometry(args.n, args.views)
@@ -272,7 +295,8 @@ def main():
     t_pairs = time.perf_counter() - t0
     net = WarmStartCNN(seed=0)
     t0 = time.perf_counter()
-    losses = train(net, xs, ts, epochs=args.epochs, batch=args.batch, lr=args.lr, lr_final=args.lr_final)
+    losses = train(net, xs, ts, epochs=args.epochs, batch=args.batch, lr=args.lr, lr_final=args.lr_final,
+                   checkpoint=args.checkpoint)
     t_train = time.perf_counter() - t0
     del xs, ts
     truth, sino, _ = simulate(geo, list(range(args.images)), noise_seed=999)

@@ -132,3 +132,33 @@ class WarmStartCNN:
         g, loss = self.mse_grad(y, t)
         self.adam(self.backward(g), lr=lr)
         return loss
+
+    # -- checkpoints ---------------------------------------------------------
+
+    def state_dict(self):
+        """Everything training resumes from, as host tensors: the FP32
+        master weights and biases, Adam's moments and its step count (the
+        BF16 weights are derived from the masters)."""
+        host = lambda ts: [p.detach().to("cpu", copy=True) for p in ts]  # noqa: E731
+        return {"channels": list(self.channels), "w32": host(self.w32), "b": host(self.b),
+                "m": host(self.m), "v": host(self.v), "step_count": int(self.step_count)}
+
+    def load_state_dict(self, sd):
+        """Inverse of state_dict(); the architecture must match."""
+        if tuple(sd["channels"]) != self.channels:
+            raise ValueError(f"checkpoint channels {tuple(sd['channels'])} != network channels {self.channels}")
+        for key, dst in (("w32", self.w32), ("b", self.b), ("m", self.m), ("v", self.v)):
+            src = sd[key]
+            if len(src) != len(dst) or any(tuple(s.shape) != tuple(d.shape) for s, d in zip(src, dst)):
+                raise ValueError(f"checkpoint tensor shapes of '{key}' do not match the network")
+            for s, d in zip(src, dst):
+                d.copy_(s)
+        for w16, w32 in zip(self.w16, self.w32):
+            w16.copy_(w32)
+        self.step_count = int(sd["step_count"])
+
+    def save(self, path):
+        torch.save(self.state_dict(), path)
+
+    def load(self, path):
+        self.load_state_dict(torch.load(path, map_location="cpu", weights_only=True))
