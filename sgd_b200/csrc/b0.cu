@@ -224,8 +224,9 @@ public:
 class B0ParallelLayer final : public Proj2D {
 public:
     B0ParallelLayer(int nx, int ny, int np, int nu, double dx, double dy, double du, const double* angles) {
-        if (nx < 1 || ny < 1 || np < 1 || nu < 1 || !(dx > 0) || !(dy > 0) || !(du > 0) || !angles)
-            fail("b0 parallel: invalid arguments");
+        if (nx < 1 || ny < 1 || np < 1 || nu < 1) fail("b0 parallel: invalid sizes");
+        check_pitches({dx, dy, du});
+        check_views(np, angles, nullptr, nullptr);
         geo.nx = nx; geo.ny = ny; geo.np = np; geo.nu = nu;
         geo.dx = dx; geo.dy = dy; geo.du = du;
         P.ni = nx;

@@ -497,8 +497,9 @@ public:
            double du_, double dv_, double lsd, double lso, const double* angles)
         : mode(mode_), nx(nx_), ny(ny_), nz(nz_), np(np_), nu(nu_), nv(nv_), dx(dx_), dy(dy_), dz(dz_), du(du_), dv(dv_) {
         if (nx <= 0 || ny <= 0 || nz <= 0 || np <= 0 || nu <= 0 || nv <= 0) fail("invalid sizes");
-        if (!(lso > 0) || !(lsd > lso)) fail("need 0 < lso < lsd");
-        if (!angles) fail("angles pointer is null");
+        check_pitches({dx, dy, dz, du, dv});
+        check_distances(lsd, lso);
+        check_views(np, angles, nullptr, nullptr);
         SGD_CUDA(cudaGetDevice(&device));
         SGD_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         // GeoData(nx, ny, nz, nu, nv, np, dx, dy, dz, du, dv) + geo_init_angles (layers/A_B1_3D.cu:686-694)

@@ -13,6 +13,24 @@ const double kPI = 3.14159265358979323846;
 inline double cross(double ax, double ay, double bx, double by) { return ax * by - ay * bx; }
 }  // namespace
 
+void check_pitches(std::initializer_list<double> pitches) {
+    for (double d : pitches)
+        if (!(d > 0) || !std::isfinite(d)) fail("pixel, voxel and bin pitches must be positive and finite (got %g)", d);
+}
+
+void check_distances(double lsd, double lso) {
+    if (!(lso > 0) || !(lsd > lso) || !std::isfinite(lsd)) fail("need 0 < lso < lsd (lso=%g lsd=%g)", lso, lsd);
+}
+
+void check_views(int np, const double* angles, const double* dz, const double* drho) {
+    if (!angles) fail("angles pointer is null");
+    for (int p = 0; p < np; ++p) {
+        if (!std::isfinite(angles[p])) fail("angle of view %d is not finite", p);
+        if (dz && !std::isfinite(dz[p])) fail("dz of view %d is not finite", p);
+        if (drho && !std::isfinite(drho[p])) fail("drho of view %d is not finite", p);
+    }
+}
+
 std::vector<ViewFrame> view_frames(int np, double lsd, double lso, double du, double dv, const double* angles,
                                    const double* dz, const double* drho) {
     std::vector<ViewFrame> out(np);
@@ -106,9 +124,9 @@ void reference_pmi(const ViewFrame& f, double uc, double vc, int nx, int ny, int
 void FanGeometry::init(int nx_, int ny_, int np_, int nu_, double dx_, double dy_, double du_, double lsd_,
                        double lso_, const double* angles, const double* dz, const double* drho) {
     if (nx_ <= 0 || ny_ <= 0 || np_ <= 0 || nu_ <= 0) fail("invalid sizes nx=%d ny=%d np=%d nu=%d", nx_, ny_, np_, nu_);
-    if (!(dx_ > 0) || !(dy_ > 0) || !(du_ > 0)) fail("pixel and bin pitches must be positive");
-    if (!(lso_ > 0) || !(lsd_ > lso_)) fail("need 0 < lso < lsd (lso=%g lsd=%g)", lso_, lsd_);
-    if (!angles) fail("angles pointer is null");
+    check_pitches({dx_, dy_, du_});
+    check_distances(lsd_, lso_);
+    check_views(np_, angles, dz, drho);
     nx = nx_; ny = ny_; np = np_; nu = nu_;
     dx = dx_; dy = dy_; du = du_; lsd = lsd_; lso = lso_;
     beta.resize(np); src.resize(2 * np); dtv.resize(2 * np); puv.resize(2 * np);

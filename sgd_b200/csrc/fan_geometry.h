@@ -8,9 +8,20 @@
 // centre D + e (u - nu/2 + 1/2) (layers/A_B1.cu:96-98, :153).
 #pragma once
 
+#include <initializer_list>
 #include <vector>
 
 namespace sgd {
+
+// Argument checks every layer runs before its first CUDA call, so that no
+// NaN or infinity reaches the geometry tables (where it would turn into bin
+// ranges): pitches positive and finite; 0 < lso < lsd, finite; angles present
+// and, with the optional per-view offsets dz and drho, finite.  Each throws
+// through fail() (the C entry points turn that into NULL / -1 and
+// sgd_last_error()).
+void check_pitches(std::initializer_list<double> pitches);
+void check_distances(double lsd, double lso);
+void check_views(int np, const double* angles, const double* dz, const double* drho);
 
 // One view of a circular (fan or cone) geometry in 3D: source, detector
 // centre, detector u step and v step (utils/geo.cu:232-269).

@@ -255,7 +255,8 @@ public:
     HexLayer(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
              const double* angles, const double* dz, const double* drho)
         : mode_(mode) {
-        if (nl <= 0 || nc <= 1 || !(dt > 0)) fail("invalid hexagonal lattice nl=%d nc=%d dt=%g", nl, nc, dt);
+        if (nl <= 0 || nc <= 1) fail("invalid hexagonal lattice nl=%d nc=%d", nl, nc);
+        check_pitches({dt});
         // GeoData(nc, nl, 1, nu, 1, np, dt*sqrt3, dt*0.5, 1, du, 1), A_H0.cu:556 / A_Hl.cu:570
         geo.init(nc, nl, np, nu, dt * kSqrt3, dt * 0.5f, du, lsd, lso, angles, dz, drho);
         P.ni = nc;

@@ -254,7 +254,9 @@ public:
     SF3D(int mode, int trap, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz, double du,
          double dv, double lsd, double lso, const double* angles) {
         if (nx <= 0 || ny <= 0 || nz <= 0 || np <= 0 || nu <= 0 || nv <= 0) fail("invalid sizes");
-        if (!(lso > 0) || !(lsd > lso) || !angles) fail("invalid geometry");
+        check_pitches({dx, dy, dz, du, dv});
+        check_distances(lsd, lso);
+        check_views(np, angles, nullptr, nullptr);
         SGD_CUDA(cudaGetDevice(&device));
         SGD_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         const std::vector<ViewFrame> fr = view_frames(np, lsd, lso, du, dv, angles, nullptr, nullptr);
