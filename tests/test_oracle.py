@@ -322,3 +322,40 @@ def test_chord_simpson_3d(oracle_mod):
     assert abs(b[0, nv // 2, nu // 2] - nx * g[5] / 4) / (nx * g[5] / 4) < 1e-2
     b3 = oracle_mod.ref_simpson_3d(x.ravel(), *g).reshape(len(g[-1]), nv, nu)
     assert b3[0, nv // 2, nu // 2] > 2 * b[0, nv // 2, nu // 2]
+
+
+QUAD = os.path.join(GOLDEN, "quad")
+
+
+def _quad_files():
+    return sorted(f for f in os.listdir(QUAD) if f.endswith(".npz")) if os.path.isdir(QUAD) else []
+
+
+@pytest.mark.parametrize("fname", _quad_files())
+def test_exact_oracle_matches_reference_quad(oracle_mod, fname):
+    """The exact FP64 matrices against the reference's own exact projectors
+    (python/matrix_gen/A_B0_ref_project.py, A_B1_ref_project.py: scipy quad
+    per bin, run unmodified by tests/golden/quad/make_quad_golden.py).
+
+    B0 (chord through the pixel square) agrees for any pixel shape.  The B1
+    script returns the bilinear element's line integral divided by the pixel
+    area dx*dy (the reference's CUDA kernel multiplies it in,
+    layers/A_B1.cu:201, and so do the FP64 replica and this oracle), and it
+    gives each side's pitch the other side's blur (A_B1_ref_project.py:39-40,
+    vx = dx sin(theta) with theta measured from the y axis), which only shows
+    when dx != dy: these fixtures keep square pixels, where the two agree once
+    scaled by dx*dy."""
+    z = np.load(os.path.join(QUAD, fname))
+    kind = str(z["kind"])
+    nx, ny, npv, nu = (int(v) for v in z["sizes"])
+    dx, dy, du, lsd, lso = (float(v) for v in z["params"])
+    ang = np.linspace(0, 2 * np.pi, npv, endpoint=False)
+    Q = np.zeros((npv * nu, nx * ny))
+    Q[z["rows"], z["cols"]] = z["vals"]
+    E = oracle_mod.exact_fan2d_matrix(kind, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    scale = dx * dy if kind == "b1" else 1.0
+    assert rel_l2(E, scale * Q) < 1e-6
+    # every entry the quadrature keeps, to its absolute tolerance (1.49e-8)
+    assert np.abs(E - scale * Q).max() < 5e-6 * np.abs(E).max()
+    if kind == "b1" and dx != 1.0:
+        assert abs(rel_l2(E, Q) - abs(dx * dy - 1.0)) < 1e-6  # E = dx*dy Q: the missing factor, exactly
