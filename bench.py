@@ -378,12 +378,12 @@ def run_batch48(args, rank, world, local_rank):
     """48 uneven slices (sides 256/384/512, 360/540/720 views, ceil(1.44 N)
     bins) forward + adjoint per step, replayed from one CUDA graph."""
     import torch
-    from sgd_b200.batch import B1Batch, c4_slices
+    from sgd_b200.batch import B1Batch, uneven_slices
     from sgd_b200.phantom import ellipse_phantom
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    slices = c4_slices(seed=rank)
+    slices = uneven_slices(seed=rank)
     B = B1Batch(slices)
     fw, vc, loaded = B.tune()
     img = B.image_arena()

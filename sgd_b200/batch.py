@@ -123,7 +123,7 @@ class B1Batch:
         return fw.value, vc.value, bool(r)
 
 
-def c4_slices(seed=0, n=48, lsd=1085.6, lso=595.0):
+def uneven_slices(seed=0, n=48, lsd=1085.6, lso=595.0):
     """Uneven batch of fan-beam slices: side N ~ U{256, 384, 512} at
     0.5 * 512 / N mm (a 256 mm field), views ~ U{360, 540, 720} over 2 pi,
     ceil(1.44 N) bins at 1 mm."""

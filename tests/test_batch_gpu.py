@@ -137,8 +137,8 @@ def test_identical_slices_share_tables_and_stay_independent():
 
 def test_uneven_48_slice_batch_matches_per_slice():
     """The 48-slice uneven workload (sides 256/384/512, 360/540/720 views)."""
-    from sgd_b200.batch import B1Batch, c4_slices
-    slices = c4_slices(seed=0)
+    from sgd_b200.batch import B1Batch, uneven_slices
+    slices = uneven_slices(seed=0)
     B = B1Batch(slices)
     img, sino = fill(B, seed=11)
     out_s = B.forward(img)
