@@ -38,6 +38,17 @@ int sgd_geometry_pmi(int nx, int ny, int nz, int np, int nu, int nv, double dx, 
                      double dv, double lsd, double lso, const double* angles, const double* dz_off,
                      const double* drho, double* pm_out, float* pmi_out);
 
+/* New, host only: the 64-byte B1 footprint record of every (view, bin), as
+ * the B1 kernels read them (np*nu*16 floats, layout [view][chunk][bin][4]):
+ * the edge offsets xa = i*r0 + (j*r2 + r4), xb = i*r1 + (j*r3 + r5) of pixel
+ * (i, j) on the line through its centre across the bin's central ray, and
+ * the constants of the closed-form footprint (b, b, a, a, a+b, a+b, 1/a,
+ * 1/(2a^2), -b^2/(12a^2), 1/(12a^2b^2)) that replaces the reference's
+ * linear_convolution_1d (layers/A_B1.cu:182-197, layers/spline_conv.hh:
+ * 295-405).  Arguments as b1_init.  0 / -1. */
+int sgd_b1_bin_records(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                       const double* angles, const double* dz, const double* drho, float* rec_out);
+
 /* ---- B1 bilinear box-spline, 2D fan beam ---------------------------------- */
 
 /* Replaces b1_init, layers/A_B1.hh:24 / layers/A_B1.cu:595-603.  dz and drho

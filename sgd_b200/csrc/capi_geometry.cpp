@@ -18,3 +18,16 @@ extern "C" int sgd_geometry_pmi(int nx, int ny, int nz, int np, int nu, int nv, 
         }
     });
 }
+
+extern "C" int sgd_b1_bin_records(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd,
+                                  double lso, const double* angles, const double* dz, const double* drho,
+                                  float* rec_out) {
+    return sgd::guarded_status([&] {
+        if (!rec_out) sgd::fail("sgd_b1_bin_records: null output");
+        sgd::FanGeometry g;
+        g.init(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, dz, drho);
+        std::vector<float> rec, strip;
+        sgd::b1_tables(g, rec, strip);
+        std::memcpy(rec_out, rec.data(), rec.size() * sizeof(float));
+    });
+}
