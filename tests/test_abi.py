@@ -165,3 +165,17 @@ def test_valid_geometry_passes_the_checks(name):
     _destroy(L, name, h)
     if not h:
         assert not re.search(_GEOMETRY_CHECKS, err), err
+
+
+def test_bench_without_gpu_fails_loudly():
+    """bench.py's own arm has no CPU fallback: without a GPU it exits non-zero
+    and prints no result line."""
+    import subprocess
+    import sys
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    r = subprocess.run([sys.executable, "bench.py", "--steps", "1", "--warmup", "1"], cwd=ROOT, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode != 0
+    assert not [line for line in r.stdout.splitlines() if line.startswith("{")]
