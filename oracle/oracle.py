@@ -137,9 +137,12 @@ def _fan2d(name, nx, ny, nu, dx, dy, du, lsd, lso, angles, vec, out_len, precisi
     return out
 
 
-def sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):
-    """FP64 replica of SF_forward_projection; returns (b, 0): the reference's SF never counts."""
-    return _fan2d("oracle_sf_forward", nx, ny, nu, dx, dy, du, lsd, lso, angles, x, len(angles) * nu, precision), 0
+def sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0, chord=False):
+    """FP64 replica of SF_forward_projection; returns (b, 0): the reference's SF never counts.
+    chord=True (FP64) replaces the reference's amplitude dx/max(|sin|, |cos|)
+    (layers/A_SF.cu:177) by the pixel's chord min(dx/|sin|, dy/|cos|)."""
+    return _fan2d("oracle_sf_forward", nx, ny, nu, dx, dy, du, lsd, lso, angles, x, len(angles) * nu,
+                  2 if chord else precision), 0
 
 
 def sf_backward(b, nx, ny, nu, dx, dy, du, lsd, lso, angles, dzs=None, drho=None, precision=0):

@@ -415,8 +415,11 @@ template <class T> T sf_gamma(T s1, T s2, const T* us) {
 
 // Per-(pixel, view) body of SF_forward_projection (layers/A_SF.cu:87-225) and
 // SF_backward_projection (:228-334): visit(u, weight*gamma) for kept bins.
+// chord: the amplitude is the pixel's chord along the ray through its centre,
+// min(dx/|sin|, dy/|cos|), instead of the reference's dx/max(|sin|, |cos|)
+// (equal for square pixels).
 template <class T, class Visit>
-void sf_pixel_view(const Geo& g, int p, int ix, int iy, Visit visit) {
+void sf_pixel_view(const Geo& g, int p, int ix, int iy, Visit visit, bool chord = false) {
     int nx = g.nx, ny = g.ny, nu = g.nu;
     float dx = (float)g.dx, dy = (float)g.dy;
     const float* pm = &g.pmi[12 * p];
@@ -430,7 +433,7 @@ void sf_pixel_view(const Geo& g, int p, int ix, int iy, Visit visit) {
     T us[4] = {usf[0], usf[1], usf[2], usf[3]};
     T theta = std::atan2((double)(dx * (ix - nx2) - srcx), (double)(dy * (iy - ny2) - srcy));  // :174
     T st = std::fabs(std::sin((double)theta)), ct = std::fabs(std::cos((double)theta));
-    T weight = T(dx) / max(st, ct);                             // :177
+    T weight = chord ? min(T(dx) / st, T(dy) / ct) : T(dx) / max(st, ct);  // :177
     for (int u = minu; u <= maxu; ++u) {
         T gm = sf_gamma<T>(T(u), T(u) + T(1), us);              // :209
         T val = weight * gm;
@@ -1714,6 +1717,9 @@ void oracle_hex_backward(int mode, int nl, int nc, int np, int nu, double dt, do
 
 // SF_forward_projection / SF_backward_projection (layers/A_SF.cu:406-479),
 // same host layouts as B1.  FP64 replica (precision 0) or FP32 (1).
+// precision: 0 FP64 replica, 1 FP32, 2 FP64 with the chord amplitude
+// (sf_pixel_view), not a reference behaviour: the model-error check of the
+// reference's amplitude on non-square pixels.
 void oracle_sf_forward(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
                        const double* angles, const double* x, double* b, int precision) {
     Geo g = make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
@@ -1726,7 +1732,8 @@ void oracle_sf_forward(int nx, int ny, int np, int nu, double dx, double dy, dou
             for (int ix = 0; ix < nx; ++ix) {
                 double C = x[(size_t)ix * ny + iy];
                 auto visit = [&](int u, double v) { bp[u] += v * C; };
-                if (precision) sf_pixel_view<float>(g, p, ix, iy, visit); else sf_pixel_view<double>(g, p, ix, iy, visit);
+                if (precision == 1) sf_pixel_view<float>(g, p, ix, iy, visit);
+                else sf_pixel_view<double>(g, p, ix, iy, visit, precision == 2);
             }
     }
 }

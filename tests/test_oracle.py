@@ -359,3 +359,28 @@ def test_exact_oracle_matches_reference_quad(oracle_mod, fname):
     assert np.abs(E - scale * Q).max() < 5e-6 * np.abs(E).max()
     if kind == "b1" and dx != 1.0:
         assert abs(rel_l2(E, Q) - abs(dx * dy - 1.0)) < 1e-6  # E = dx*dy Q: the missing factor, exactly
+
+
+def test_formula_model_errors_against_reference_quad_on_non_square_pixels(oracle_mod):
+    """The reference's B0 and A_SF formulas (FP64 replicas) against the
+    reference's own exact pixel-indicator projector on 1.0 x 0.8 mm pixels
+    (tests/golden/quad/quad_b0_aniso.npz).  B0 keeps its model error; A_SF's
+    amplitude dx / max(|sin t|, |cos t|) (layers/A_SF.cu:177, :316) is the
+    pixel's chord along the ray only for square pixels and is 15 % off here,
+    while the chord min(dx / |sin t|, dy / |cos t|) brings it back to the
+    square-pixel model error."""
+    z = np.load(os.path.join(QUAD, "quad_b0_aniso.npz"))
+    nx, ny, npv, nu = (int(v) for v in z["sizes"])
+    dx, dy, du, lsd, lso = (float(v) for v in z["params"])
+    assert dx != dy
+    ang = np.linspace(0, 2 * np.pi, npv, endpoint=False)
+    Q = np.zeros((npv * nu, nx * ny))
+    Q[z["rows"], z["cols"]] = z["vals"]
+    x = ellipse_phantom(nx, ny, dx, dy, seed=3).ravel()
+    y = Q @ x
+    b0, _ = oracle_mod.b0_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    assert rel_l2(b0, y) < 1e-3
+    sf, _ = oracle_mod.sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    assert rel_l2(sf, y) > 0.1
+    chord, _ = oracle_mod.sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, ang, chord=True)
+    assert rel_l2(chord, y) < 2e-3
