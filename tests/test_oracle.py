@@ -302,6 +302,22 @@ def test_sf3d_corrected_against_voxel_chords(oracle_mod):
     assert rel_l2(b, r) < 2e-3
 
 
+@pytest.mark.parametrize("voxel", [(2.0, 1.6, 2.0), (2.0, 2.0, 1.5), (1.5, 2.5, 2.0)])
+def test_sf3d_corrected_against_voxel_chords_non_cubic(oracle_mod, voxel):
+    """As above on non-cubic voxels: the corrected amplitude (the voxel's
+    volume over the squared source distance, times the normalised trapezoid
+    and rectangle) keeps unit scale for any voxel shape."""
+    nx, ny, nz, nu, nv, _, _, _, du, dv, lsd, lso, ang = cone_case("small")
+    dx, dy, dz = voxel
+    ang = ang[:3] + 0.013
+    x = ellipsoid_phantom(nx, ny, nz, dx, dy, dz, seed=0).ravel()
+    g = (nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, ang)
+    r = oracle_mod.ref_simpson_3d(x, *g, adaptive=True)
+    b = oracle_mod.sf3d_forward(x, *g, mode=1)
+    assert abs(float(b @ r) / float(r @ r) - 1.0) < 4e-3
+    assert rel_l2(b, r) < 4e-3
+
+
 def test_chord_simpson_3d(oracle_mod):
     """Ref_project_Simpson restated: a uniform odd-sized cube seen along +x
     carries its length on the central cell (the nine samples avoid voxel
