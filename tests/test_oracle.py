@@ -400,3 +400,26 @@ def test_formula_model_errors_against_reference_quad_on_non_square_pixels(oracle
     assert rel_l2(sf, y) > 0.1
     chord, _ = oracle_mod.sf_forward(x, nx, ny, nu, dx, dy, du, lsd, lso, ang, chord=True)
     assert rel_l2(chord, y) < 2e-3
+
+
+@pytest.mark.parametrize("voxel,dv", [(1.0, 0.75), (2.0, 1.5), (2.0, 3.0)])
+def test_b1_3d_scale_is_the_row_height_at_the_isocentre(oracle_mod, voxel, dv):
+    """A uniform cube's central rays against their path lengths (adaptive
+    Simpson voxel chords).  The reference's A_B1_3D forward (FP64 replica)
+    normalises each voxel's axial trapezoid to unit area
+    (layers/A_B1_3D.cu:210), so a detector row receives a fraction of the
+    voxel instead of a density per mm: its value is the line integral times
+    the row height projected to the isocentre, dv * lso / lsd, whatever the
+    voxel size.  The corrected SF_projector carries the line integral."""
+    from geometry_cases import LSD, LSO
+    n, nd = 16, 24
+    ang = np.array([0.3])
+    g = (n, n, n, nd, nd, voxel, voxel, voxel, 1.5, dv, LSD, LSO, ang)
+    x = np.ones(n ** 3)
+    r = oracle_mod.ref_simpson_3d(x, *g, adaptive=True).reshape(nd, nd)
+    b, _ = oracle_mod.b1_3d_forward(x, *g)
+    s = oracle_mod.sf3d_forward(x, *g, mode=1).reshape(nd, nd)
+    c = (slice(nd // 2 - 2, nd // 2 + 2), slice(nd // 2 - 2, nd // 2 + 2))
+    ratio = b.reshape(nd, nd)[c] / r[c]
+    assert np.all(np.abs(ratio / (dv * LSO / LSD) - 1.0) < 1e-2)
+    assert np.all(np.abs(s[c] / r[c] - 1.0) < 5e-3)
