@@ -86,6 +86,8 @@ def _families():
     return {
         "sf_fan512": ("A_SF separable footprint fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
                   lambda: fan("SF"), NX * NY * NP),
+        "b1ref_fan512": ("A_B1 in the reference layer's FP32 rounding, fan beam, 512x512 @0.5mm, 720 views, "
+                         "736 bins @1mm", lambda: fan("b1ref"), NX * NY * NP),
         "b0_fan512": ("A_B0 pixel basis fan beam, 512x512 @0.5mm, 720 views, 736 bins @1mm",
                   lambda: fan("b0"), NX * NY * NP),
         "b0_parallel128": ("B0 parallel beam, 128x128 @1mm, 180 views over pi, 185 bins @1mm",
@@ -103,7 +105,7 @@ def _families():
     }
 
 
-FAMILIES = ("sf_fan512", "b0_fan512", "b0_parallel128", "h0_hex2e18", "hl_hex2e18", "b1_3d_cone256", "sf3d_cone256", "b1_3d_small")
+FAMILIES = ("sf_fan512", "b1ref_fan512", "b0_fan512", "b0_parallel128", "h0_hex2e18", "hl_hex2e18", "b1_3d_cone256", "sf3d_cone256", "b1_3d_small")
 
 
 def parse():
@@ -251,6 +253,20 @@ def load_traffic():
         return json.load(f)
 
 
+def fp32_peak(dev, stream):
+    """FP32 FMA throughput (FLOP/s, FMA = 2) of this GPU now, from the library's
+    probe kernel: the roofline denominator (MEASURED_PEAKS has no FP32 entry)."""
+    import ctypes
+    import torch
+    from sgd_b200 import _lib
+    L = _lib.lib()
+    L.sgd_fp32_fma_rate.restype = ctypes.c_double
+    L.sgd_fp32_fma_rate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    scratch = torch.empty(nsm * 64, dtype=torch.float32, device=dev)
+    return max(L.sgd_fp32_fma_rate(scratch.data_ptr(), nsm * 8 * 4, 4096, stream.cuda_stream) for _ in range(3))
+
+
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
@@ -334,13 +350,7 @@ def run_ours(args, rank, world, local_rank):
     flops = ops["range_flops_per_pixel_view"] * V + ops["flops_per_evaluation"] * E
     fwd_avg, bwd_avg = statistics.mean(fwd_ms), statistics.mean(bwd_ms)
     dom, dom_ms = ("b1_back_kernel", bwd_avg) if bwd_avg >= fwd_avg else ("b1_forward_kernel", fwd_avg)
-    L = _lib.lib()
-    L.sgd_fp32_fma_rate.restype = __import__("ctypes").c_double
-    L.sgd_fp32_fma_rate.argtypes = [__import__("ctypes").c_void_p, __import__("ctypes").c_int,
-                                    __import__("ctypes").c_int, __import__("ctypes").c_void_p]
-    scratch = torch.empty(148 * 64, dtype=torch.float32, device=dev)
-    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
-    peak = max(L.sgd_fp32_fma_rate(scratch.data_ptr(), nsm * 8 * 4, 4096, stream.cuda_stream) for _ in range(3))
+    peak = fp32_peak(dev, stream)
     achieved = flops / (dom_ms * 1e-3)
     traffic = load_traffic().get(dom)
     roofline = {
@@ -472,6 +482,21 @@ def run_family(args, rank, world, local_rank):
     step_ms = max_over_ranks(fwd + bwd, world, dev)
     if rank != 0:
         return
+    roofline = None
+    ops = load_op_counts().get(args.workload)
+    if ops and "flops_per_cell_view" in ops:
+        # the reference formula's FLOPs per launch (both directions evaluate
+        # every visited (cell, bin) pair once) over the slower direction's time
+        flops = ops["flops_per_cell_view"] * vv
+        dom, dom_ms = ("back", bwd) if bwd >= fwd else ("forward", fwd)
+        peak = fp32_peak(dev, stream)
+        roofline = {"bound": "fp32", "kernel": f"{P.kernels[dom]}", "achieved": flops / (dom_ms * 1e-3) / 1e12,
+                    "peak": peak / 1e12, "unit": "TFLOP/s", "frac": flops / (dom_ms * 1e-3) / peak,
+                    "traffic": load_traffic().get(f"{args.workload}:{dom}"),
+                    "peak_source": "measured now: FP32 FMA probe kernel (sgd_fp32_fma_rate), same clocks",
+                    "flops_per_launch": flops, "flops_model": f"{ops['flops_per_cell_view']:.1f} x cell-views "
+                    f"({ops['source']})", "fwd_ms": fwd, "bwd_ms": bwd,
+                    "fwd_plus_adj_frac": 2 * flops / ((fwd + bwd) * 1e-3) / peak}
     line = {
         "metric": f"fwd+adj voxel-view updates/s ({args.workload})", "value": world * 2.0 * vv / (step_ms * 1e-3),
         "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": step_ms,
@@ -479,7 +504,7 @@ def run_family(args, rank, world, local_rank):
         "dtype": "f32", "data": "synthetic (uniform random image)",
         "config": {"workload": desc, "voxel_views": vv,
                    "l2": "flushed between steps (256 MiB write outside the timed events)"},
-        "gpu_launches": None, "clocks": clocks,
+        "roofline": roofline, "gpu_launches": P.launches_per_step * K, "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
 

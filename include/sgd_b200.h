@@ -87,6 +87,14 @@ unsigned long long sgd_b1_count(void* layer);
  * gave up, and the output of that call was not written. */
 int sgd_b1_status(void* layer);
 
+/* New, for testing the failure path above: the polls each back-projection
+ * staging wait makes before it gives up (default 4194304).  With 0 every
+ * wait gives up at once: the kernel still waits, with the full limit, for the
+ * copies it issued, leaves its tiles unwritten and sets the flag that
+ * sgd_b1_status reports; restoring the default restores normal calls.
+ * Returns 0, or -1 for a null layer. */
+int sgd_b1_set_wait_limit(void* layer, unsigned polls);
+
 /* New, with no counterpart in the reference: the B1 forward projection of
  * sgd_b1_forward_dev without any device allocation during the call, for
  * callers that cannot call cudaMalloc while they run (code under another
@@ -99,6 +107,22 @@ int sgd_b1_status(void* layer);
  * the array: calls that overlap on the GPU race.  The layer's device must be
  * current.  Returns 0 on success, -1 on failure. */
 int sgd_b1_forward_noalloc(void* layer, const float* d_img, float* d_sino, void* stream);
+
+/* New: B1 in the reference layer's FP32 rounding.  Same arguments, layouts
+ * and count as b1_init / b1_forward_projection / b1_backward_projection
+ * (layers/A_B1.cu:595-678), but the bin centres are stepped in FP32 from each
+ * pixel's first bin and the edge-ray offsets come from the reference's FP32
+ * intersections (layers/A_B1.cu:100-197), so the output stays within a few
+ * units in the last place of the reference's own; the b1_* layer evaluates
+ * the exact bin geometry instead.  Runs on the generic 2D kernels. */
+void* sgd_b1ref_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                     double* angles, double* dz, double* drho);
+int sgd_b1ref_forward_projection(double* b, double* x, void* layer);
+int sgd_b1ref_backward_projection(double* b, double* x, void* layer);
+void sgd_b1ref_destroy(void* layer);
+int sgd_b1ref_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream);
+int sgd_b1ref_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream);
+unsigned long long sgd_b1ref_count(void* layer);
 
 /* ---- A_SF separable footprint (SF-TR), 2D fan beam -------------------------- */
 
@@ -173,6 +197,26 @@ int sgd_hl_backward_dev(void* layer, const float* d_sino, float* d_img, void* st
 unsigned long long sgd_h0_count(void* layer);
 unsigned long long sgd_hl_count(void* layer);
 
+/* New, for every layer of the generic 2D kernels (SF, B0, B0 parallel, H0,
+ * Hl, B1 reference rounding): synchronises the layer's stream and reports
+ * (0 / -1 with sgd_last_error, then clears) a back projection whose bounded
+ * wait for its shared-memory staging gave up; those tiles were left
+ * unwritten.  The FP64 host entry points check it themselves. */
+int sgd_proj2d_status(void* layer);
+/* New, for testing that path: as sgd_b1_set_wait_limit, for these layers. */
+int sgd_proj2d_set_wait_limit(void* layer, unsigned polls);
+
+/* New, host only (no GPU needed): the plan of the generic 2D kernels for an
+ * nx x ny grid of cells in the fan geometry of b1_init (np views at angles,
+ * nu bins of pitch du, distances lsd, lso), cell (i, j) at x = x0 + i dx,
+ * y = y0 + j dy, whose bin ranges come from points within ri (along i) and
+ * rj (along j) cells of it: the forward's block strips, 8 floats per (view,
+ * block of 32 bins), and the back projection's bin windows, 2 ints (first,
+ * last) per (tile of 8 x 32 cells, view).  Returns the widest window in bins,
+ * -1 on error. */
+int sgd_fan2d_plan(int nx, int ny, int np, int nu, double x0, double dx, double y0, double dy, double ri, double rj,
+                   double du, double lsd, double lso, const double* angles, float* strips, int* twin);
+
 /* ---- A_B1_3D cone beam ---------------------------------------------------- */
 
 /* Replace b1_3d_init / b1_3d_forward_projection / b1_3d_backward_projection,
@@ -241,8 +285,14 @@ int sgd_b1_batch_backward(void* batch, const float* d_sino, float* d_img, void* 
 int sgd_b1_batch_capture(void* batch, const float* d_img, float* d_sino, const float* d_sino_in, float* d_img_out);
 int sgd_b1_batch_replay(void* batch, void* stream);
 int sgd_b1_batch_tune(void* batch, const char* cache_path, int* fw, int* vc);
+/* set_variant and tune rewrite the work-item table the persistent kernels
+ * read: they synchronise the device first and must not be called while
+ * another thread has batch work in flight. */
 int sgd_b1_batch_set_variant(void* batch, int fw, int vc);
 int sgd_b1_batch_status(void* batch);
+/* New, for testing the failure path: as sgd_b1_set_wait_limit, for the
+ * batch's back projection (drops a captured graph). */
+int sgd_b1_batch_set_wait_limit(void* batch, unsigned polls);
 
 /* ---- ASD-POCS and its phantom simulator ----------------------------------- */
 
@@ -310,6 +360,7 @@ long long sgd_b0_matrix_csr(void* layer, long long* rowptr, int* cols, double* v
 long long sgd_SF_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
 long long sgd_h0_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
 long long sgd_hl_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
+long long sgd_b1ref_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap);
 
 /* ---- measurement ---------------------------------------------------------- */
 

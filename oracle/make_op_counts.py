@@ -29,6 +29,34 @@ def main():
         "source": "oracle/sgd_oracle.cpp oracle_b1_flops: +,-,*,/,sqrt of layers/A_B1.cu:96-206 "
                   "and layers/spline_conv.hh:295-405 counted on the path taken, 24 views",
     }
+    per_view = "FLOPs per cell-view of the reference formula (bin range, per-cell terms, every bin visited)"
+    fan = 2 * np.pi * np.arange(720) / 720
+    hexa = 2 * np.pi * np.arange(360) / 360
+    par = np.pi * np.arange(180) / 180
+    rows = {
+        "sf_fan512": ("sf", 512, 512, 736, 0.5, 0.5, 1.0, 1085.6, 595.0, fan,
+                      "layers/A_SF.cu:96-225 (atan2/sin/cos per pixel-view not counted)"),
+        "b0_fan512": ("b0", 512, 512, 736, 0.5, 0.5, 1.0, 1085.6, 595.0, fan, "layers/A_B0.cu:140-229"),
+        # the reference has no parallel geometry: its B0 formula on a fan with
+        # the source 1e4 pixels away stands in for the count
+        "b0_parallel128": ("b0", 128, 128, 185, 1.0, 1.0, 1.0, 2e4, 1e4, par,
+                           "layers/A_B0.cu:140-229 on a distant-source fan (no parallel geometry in the reference)"),
+        "h0_hex2e18": ("h0", 550, 477, 736, 0.62, 0.62, 1.0, 1085.6, 595.0, hexa,
+                       "layers/A_H0.cu:84-256 (six-vertex bound 6 x 9)"),
+        "hl_hex2e18": ("hl", 953, 275, 736, 1.075, 1.075, 1.0, 1085.6, 595.0, hexa,
+                       "layers/A_Hl.cu:21-46, :84-156, :168-266"),
+    }
+    for name, (kind, a, b, nu, dx, dy, du, lsd, lso, ang, src) in rows.items():
+        f, nb = oracle.fan2d_flops(kind, a, b, nu, dx, dy, du, lsd, lso, ang, nviews=24)
+        out[name] = {"flops_per_cell_view": f, "bins_per_cell_view": nb, "model": per_view,
+                     "source": f"oracle/sgd_oracle.cpp oracle_fan2d_flops: {src}, 24 views"}
+    # the B1 reference-rounding mode evaluates the B1 formula
+    b1 = out["b1_fan512"]
+    out["b1ref_fan512"] = {
+        "flops_per_cell_view": b1["range_flops_per_pixel_view"]
+        + b1["flops_per_evaluation"] * b1["evaluations_per_pixel_view"],
+        "bins_per_cell_view": b1["evaluations_per_pixel_view"], "model": per_view,
+        "source": "the b1_fan512 counts (layers/A_B1.cu:96-206)"}
     with open(OUT, "w") as fh:
         json.dump(out, fh, indent=1)
     print(json.dumps(out, indent=1))

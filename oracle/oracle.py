@@ -46,6 +46,7 @@ def lib():
         L.oracle_sf3d_backward.restype = None
         L.oracle_sf_backward.restype = None
         L.oracle_b1_flops.restype = None
+        L.oracle_fan2d_flops.restype = None
     return _LIB
 
 
@@ -104,6 +105,18 @@ def b1_flops(nx, ny, nu, dx, dy, du, lsd, lso, angles, nviews=8):
     out = np.zeros(3)
     lib().oracle_b1_flops(nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(du),
                           ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), nviews, _p(out))
+    return tuple(out)
+
+
+def fan2d_flops(kind, nx, ny, nu, dx, dy, du, lsd, lso, angles, nviews=8):
+    """(FLOPs per cell-view, bins visited per cell-view) of the reference formula
+    of kind "sf", "b0", "h0" or "hl" (lattices: nx rows x ny sites, dx = dt)."""
+    k = {"sf": 1, "b0": 2, "h0": 3, "hl": 4}[kind]
+    angles = _c(angles)
+    out = np.zeros(2)
+    lib().oracle_fan2d_flops(k, nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy),
+                             ctypes.c_double(du), ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), nviews,
+                             _p(out))
     return tuple(out)
 
 

@@ -540,7 +540,24 @@ long long b0_pixel_view(const Geo& g, const double* vp, int p, int ix, int iy, V
 // ---------------------------------------------------------------------------
 const double kSQRT3 = 1.7320508075688772935274463415;
 
-// layers/A_Hl.cu:21-46 with layers/spline_conv.hh:151-229
+// layers/A_Hl.cu:21-46 with layers/spline_conv.hh:151-229, on any scalar
+// type (the FLOP counter runs it on CountedF)
+template <class T> T hl_conv_t(T y, T h1, T h2, T h3, T h4) {
+    T hs[4];
+    int m = 0;
+    if (std::fabs((double)h1) > 1e-8) hs[m++] = h1;
+    if (std::fabs((double)h2) > 1e-8) hs[m++] = h2;
+    if (std::fabs((double)h3) > 1e-8) hs[m++] = h3;
+    if (std::fabs((double)h4) > 1e-8) hs[m++] = h4;
+    if (m < 2) return T(0);
+    std::function<T(T, int)> D = [&](T yy, int k) -> T {
+        if (k < 0) return yy > T(0) ? (m == 2 ? yy : (m == 3 ? yy * yy : yy * yy * yy)) : T(0);
+        return (D(yy, k - 1) - D(yy - hs[k], k - 1)) / hs[k];
+    };
+    T v = D(y, m - 1);
+    return m == 2 ? v : (m == 3 ? v / T(2) : v / T(6));
+}
+
 double hl_linear_convolution_1d(double y, double h1, double h2, double h3, double h4) {
     double hs[4];
     int m = 0;
@@ -632,7 +649,10 @@ long long hex_site_view(const Geo& g, int mode, bool back, int p, int ic, int il
         if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) y = -y;
         double conv;
         if (mode == 2) {
-            conv = hl_linear_convolution_1d(y, vblur, va, vb, vc);
+            if (std::is_same<T, CountedF>::value)
+                conv = (double)hl_conv_t<T>(T(y), T(vblur), T(va), T(vb), T(vc));
+            else
+                conv = hl_linear_convolution_1d(y, vblur, va, vb, vc);
         } else {
             conv = (double)b0_linear_convolution_1d<T>(T(y), T(vblur), T(va), T(vb)) +
                    (double)b0_linear_convolution_1d<T>(T(y), T(vblur), T(vb), T(vc)) +
@@ -1823,6 +1843,74 @@ void oracle_b1_flops(int nx, int ny, int np, int nu, double dx, double dy, doubl
     out[0] = (double)range_flops / pv;
     out[1] = evals ? (double)eval_flops / evals : 0.0;
     out[2] = (double)evals / pv;
+}
+
+
+// Algorithmic FLOPs of the reference formulas of the other 2D projectors,
+// counted (+, -, *, /, sqrt) on the path taken over `nviews` evenly spread
+// views of every cell: kind 1 A_SF (layers/A_SF.cu:96-225), 2 A_B0
+// (layers/A_B0.cu:140-229), 3 A_H0 (layers/A_H0.cu:158-256, the six-vertex
+// bound of :84-156 counted as 6 x (4 + 4 + 1)), 4 A_Hl (layers/A_Hl.cu:
+// 168-266 with the divided differences of :21-46).  out[0] = FLOPs per
+// cell-view (bin range, per-cell terms and every footprint evaluation),
+// out[1] = bins visited per cell-view.  For the lattices, nx x ny = nl rows x
+// nc sites and dx is the site spacing dt.
+void oracle_fan2d_flops(int kind, int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd,
+                        double lso, const double* angles, int nviews, double* out) {
+    const bool hex = kind == 3 || kind == 4;
+    const int nl = nx, nc = ny;
+    Geo g = hex ? make_geo(nc, nl, 1, np, nu, 1, dx * kSQRT3, dx * 0.5f, 1, du, 1)
+                : make_geo(nx, ny, 1, np, nu, 1, dx, dy, 1, du, 1);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::vector<double> b0v;
+    if (kind == 2) b0_vectors(g, b0v);
+    long long total = 0, bins = 0, cells = 0;
+    for (int k = 0; k < nviews; ++k) {
+        int p = (int)((long long)k * np / nviews);
+        const float* pm = &g.pmi[12 * p];
+        const float puvx = (float)g.puv[3 * p];
+        const bool singular = std::fabs(puvx - (float)g.puv[3 * p + 1]) < 1e-7f;
+        for (int i = 0; i < g.nx; ++i)
+            for (int j = 0; j < g.ny; ++j) {
+                if (hex && (j & 1) && i == g.nx - 1) continue;
+                CountedF::flops = 0;
+                long long n = 0;
+                if (kind == 1 || kind == 2) {
+                    int lo, hi;
+                    bin_range<CountedF>(pm, puvx, singular, i - 0.5f, i + 0.5f, j - 0.5f, j + 0.5f, g.nu, lo, hi);
+                    n = hi - lo + 1;
+                    if (kind == 1)
+                        sf_pixel_view<CountedF>(g, p, i, j, [](int, double) {});
+                    else
+                        b0_pixel_view<CountedF>(g, &b0v[(size_t)p * g.nu * 5], p, i, j, [](int, double) {});
+                } else {
+                    const long long c = hex_site_view<CountedF>(g, kind == 3 ? 1 : 2, false, p, i, j,
+                                                                [](int, double) {});
+                    CountedF::flops += 54;
+                    n = kind == 3 ? c / 3 : 0;
+                    if (kind == 4) {  // Hl does not count: bins of the six-vertex range
+                        float icc = (float)i + ((j & 1) ? 0.5f : 0.0f);
+                        const float oc[6] = {0.0f, 0.5f, 0.5f, 0.0f, -0.5f, -0.5f};
+                        const float ol[6] = {-2.0f, -1.0f, 1.0f, 2.0f, 1.0f, -1.0f};
+                        float umin = 1e30f, umax = -1e30f;
+                        for (int v = 0; v < 6; ++v) {
+                            const float u = std::fmaf(pm[0], icc + oc[v], std::fmaf(pm[1], j + ol[v], pm[3])) /
+                                            std::fmaf(pm[8], icc + oc[v], std::fmaf(pm[9], j + ol[v], pm[11]));
+                            umin = std::min(umin, u);
+                            umax = std::max(umax, u);
+                        }
+                        const int lo = std::min(std::max(0, (int)std::floor(umin)), g.nu - 1);
+                        const int hi = std::min(std::max(0, (int)std::floor(umax)), g.nu - 1);
+                        n = std::max(hi, lo) - lo + 1;
+                    }
+                }
+                total += CountedF::flops;
+                bins += n;
+                ++cells;
+            }
+    }
+    out[0] = cells ? (double)total / cells : 0.0;
+    out[1] = cells ? (double)bins / cells : 0.0;
 }
 
 }  // extern "C"

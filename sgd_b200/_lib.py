@@ -83,6 +83,28 @@ def lib() -> ctypes.CDLL:
         f.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_longlong]
     L.sgd_hex_init.restype = _vp
     L.sgd_hex_init.argtypes = [_i] + _INIT_ARGS["h0"]
+    # B1 in the reference's FP32 rounding (generic kernels)
+    L.sgd_b1ref_init.restype = _vp
+    L.sgd_b1ref_init.argtypes = _INIT_ARGS["b1"]
+    for n in ("sgd_b1ref_forward_projection", "sgd_b1ref_backward_projection"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = [_dp, _dp, _vp]
+    L.sgd_b1ref_destroy.restype = None
+    L.sgd_b1ref_destroy.argtypes = [_vp]
+    for n in ("sgd_b1ref_forward_dev", "sgd_b1ref_backward_dev"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = [_vp, _vp, _vp, _vp]
+    L.sgd_b1ref_count.restype = ctypes.c_ulonglong
+    L.sgd_b1ref_count.argtypes = [_vp]
+    L.sgd_b1ref_matrix_csr.restype = ctypes.c_longlong
+    L.sgd_b1ref_matrix_csr.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_longlong]
+    L.sgd_proj2d_status.restype = _i
+    L.sgd_proj2d_status.argtypes = [_vp]
+    for n in ("sgd_b1_set_wait_limit", "sgd_proj2d_set_wait_limit", "sgd_b1_batch_set_wait_limit"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = [_vp, ctypes.c_uint]
+    L.sgd_b1_status.restype = _i
+    L.sgd_b1_status.argtypes = [_vp]
     L.sgd_geometry_pmi.restype = _i
     L.sgd_b1_forward_noalloc.restype = _i
     L.sgd_b1_forward_noalloc.argtypes = [_vp, _vp, _vp, _vp]

@@ -27,13 +27,15 @@ struct B0Basis {
     struct View {
         float pm0, pm1, pm3, pm8, pm9, pm11, puvx, singular, srcx, srcy, dtvx, dtvy, puvy, dx, dy, nx2, ny2;
     };
+    // per bin: vx, vy, a0s, sb0, 1/lsp, 1/lsp^2 (FP64)
+    static constexpr int kBinF4 = 3;
     struct Cell {
-        float ox, oy, sx0, sy0;
+        float ox, oy, sx, sy;  // pixel centre; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
     };
     __device__ static void load_view(const float* v, View& V) {
         const float4* q = reinterpret_cast<const float4*>(v);
-        const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4);
+        const float4 a = q[0], b = q[1], c = q[2], d = q[3], e = q[4];
         V = View{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w, e.x};
     }
     __device__ static bool valid(int, int, const Fan2DParams&) { return true; }
@@ -75,8 +77,8 @@ struct B0Basis {
         c.lo = min(max(0, (int)floorf(us[0])), P.nu - 1);
         c.hi = min(max(0, (int)floorf(us[3])), P.nu - 1);
         const float fl = (float)c.lo;
-        c.sx0 = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
-        c.sy0 = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
+        c.sx = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
+        c.sy = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
     }
     // layers/spline_conv.hh:244-293 (T = float)
     __device__ static float fast3(float x, const float* xi) {
@@ -104,16 +106,17 @@ struct B0Basis {
         if (vs[2] > 1e-7f) return fast3(y, vs);
         return fmaxf(0.0f, fminf(1.0f / vs[0], ((vs[0] + vs[1]) / 2.0f - y) / (vs[0] * vs[1])));
     }
-    // bins: [view][bin][vx, vy, a0s, sb0, 1/lsp, 1/lsp^2] doubles
-    __device__ static float value(const View& V, const Cell& c, int u, int p, const Fan2DParams& P) {
-        float sx = c.sx0, sy = c.sy0;
-        for (int t = c.lo; t < u; ++t) {  // the reference's FP32 stepping
-            sx += V.puvx;
-            sy += V.puvy;
-        }
-        const double* b = reinterpret_cast<const double*>(P.bins) + ((size_t)p * P.nu + u) * 6;
-        const double vx = __ldg(b), vy = __ldg(b + 1), a0s = __ldg(b + 2), sb0 = __ldg(b + 3);
-        const double ilsp = __ldg(b + 4), ilsp2 = __ldg(b + 5);
+    // the reference's FP32 stepping of the bin centre (layers/A_B0.cu:202)
+    __device__ static void skip(const View& V, Cell& c) {
+        c.sx += V.puvx;
+        c.sy += V.puvy;
+    }
+    __device__ static float value(const View& V, Cell& c, int, const float4* t, const Fan2DParams&) {
+        const float sx = c.sx, sy = c.sy;
+        skip(V, c);
+        const double* b = reinterpret_cast<const double*>(t);
+        const double vx = b[0], vy = b[1], a0s = b[2], sb0 = b[3];
+        const double ilsp = b[4], ilsp2 = b[5];
         const float px = V.srcx, py = V.srcy;
         const double r1 = (double)((c.ox - px) * (sx - px) + (c.oy - py) * (sy - py)) * ilsp2;
         const double vblur = (a0s + sb0) * (-r1);
@@ -140,13 +143,15 @@ struct B0ParBasis {
     struct View {
         float ex, ey, a, b, du, x0, y0, dx, dy, hnu;
     };
+    static constexpr int kBinF4 = 0;
     struct Cell {
         float s;
         int lo, hi;
     };
     __device__ static void load_view(const float* v, View& V) {
-        V = View{__ldg(v), __ldg(v + 1), __ldg(v + 2), __ldg(v + 3), __ldg(v + 4),
-                 __ldg(v + 5), __ldg(v + 6), __ldg(v + 7), __ldg(v + 8), __ldg(v + 9)};
+        const float4* q = reinterpret_cast<const float4*>(v);
+        const float4 a = q[0], b = q[1], c = q[2];
+        V = View{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y};
     }
     __device__ static bool valid(int, int, const Fan2DParams&) { return true; }
     __device__ static void setup(const View& V, int i, int j, const Fan2DParams& P, Cell& c) {
@@ -156,11 +161,12 @@ struct B0ParBasis {
         c.lo = max(0, (int)floorf((c.s - h) / V.du + V.hnu));
         c.hi = min(P.nu - 1, (int)floorf((c.s + h) / V.du + V.hnu));
     }
-    __device__ static float value(const View& V, const Cell& c, int u, int, const Fan2DParams&) {
+    __device__ static float value(const View& V, Cell& c, int u, const float4*, const Fan2DParams&) {
         const float t = c.s - ((float)u - V.hnu + 0.5f) * V.du;
         const float conv = B0Basis::conv1d(t + 0.5f * (V.a + V.b + V.du), V.a, V.b, V.du);
         return (conv > 1e-7f && conv == conv) ? conv : 0.f;
     }
+    __device__ static void skip(const View&, Cell&) {}
 };
 
 namespace {
@@ -205,19 +211,24 @@ public:
                 o[0] = vx; o[1] = vy; o[2] = a0s; o[3] = sb0; o[4] = 1.0 / lsp; o[5] = 1.0 / (lsp * lsp);
             }
         }
-        const double hx = 0.5 * dx, hy = 0.5 * dy, x0 = geo.x0(), y0 = geo.y0();
-        finish_init(view, B0Basis::kViewFloats, bins, [&](int i0, int i1, int j0, int j1) {
-            return Box2{x0 + i0 * dx - hx, x0 + i1 * dx + hx, y0 + j0 * dy - hy, y0 + j1 * dy + hy};
-        });
+        finish_init(view, bins);
         out_scale = (float)dx * (float)dy;
         count = fan2d_count<B0Basis>(P, stream);
     }
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
-        fan2d_forward<B0Basis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
+        fan2d_forward<B0Basis>(P, img, sino, out_scale, s);
     }
     long long csr(const CsrOut& out) override { return fan2d_csr<B0Basis>(P, out_scale, out, stream); }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
         fan2d_back<B0Basis>(P, sino, img, out_scale, s);
+    }
+
+protected:
+    // ranges from the corners at +-1/2
+    RangeMap range_map(int p) const override {
+        double hw[6];
+        fan_world_hom(geo, p, hw);
+        return grid_range_map(hw, geo.x0(), geo.dx, geo.y0(), geo.dy, 0.5, 0.5);
     }
 };
 
@@ -244,15 +255,12 @@ public:
             v[5] = (float)(-0.5 * (nx - 1) * dx); v[6] = (float)(-0.5 * (ny - 1) * dy);
             v[7] = (float)dx; v[8] = (float)dy; v[9] = 0.5f * nu;
         }
-        const double hx = 0.5 * dx, hy = 0.5 * dy, x0 = -0.5 * (nx - 1) * dx, y0 = -0.5 * (ny - 1) * dy;
-        finish_init(view, B0ParBasis::kViewFloats, {}, [&](int i0, int i1, int j0, int j1) {
-            return Box2{x0 + i0 * dx - hx, x0 + i1 * dx + hx, y0 + j0 * dy - hy, y0 + j1 * dy + hy};
-        });
+        finish_init(view, {});
         out_scale = (float)dx * (float)dy;
         count = fan2d_count<B0ParBasis>(P, stream);
     }
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
-        fan2d_forward<B0ParBasis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
+        fan2d_forward<B0ParBasis>(P, img, sino, out_scale, s);
     }
     long long csr(const CsrOut& out) override { return fan2d_csr<B0ParBasis>(P, out_scale, out, stream); }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
@@ -260,21 +268,12 @@ public:
     }
 
 protected:
-    void window(int p, const Box2& b, int& lo, int& hi) const override {
-        double smin = 1e300, smax = -1e300;
-        for (double x : {b.x0, b.x1})
-            for (double y : {b.y0, b.y1}) {
-                const double s = x * ex_[p] + y * ey_[p];
-                smin = std::min(smin, s);
-                smax = std::max(smax, s);
-            }
-        const double umin = smin / geo.du + 0.5 * geo.nu, umax = smax / geo.du + 0.5 * geo.nu;
-        lo = std::max(0, (int)std::floor(umin) - 1);
-        hi = std::min(geo.nu - 1, (int)std::floor(umax) + 1);
-        if (umax < -1.0 || umin > geo.nu + 1.0) {
-            lo = 0;
-            hi = -1;
-        }
+    // u = s / du + nu/2 with s = x e.x + y e.y: a map without a pole; ranges
+    // from the corners at +-1/2
+    RangeMap range_map(int p) const override {
+        const double hw[6] = {ex_[p] / geo.du, ey_[p] / geo.du, 0.5 * geo.nu, 0.0, 0.0, 1.0};
+        return grid_range_map(hw, -0.5 * (geo.nx - 1) * geo.dx, geo.dx, -0.5 * (geo.ny - 1) * geo.dy, geo.dy, 0.5,
+                              0.5);
     }
 
 private:

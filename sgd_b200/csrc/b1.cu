@@ -33,7 +33,7 @@ b1_forward_kernel(const float4* __restrict__ rec, const float* __restrict__ stri
 __global__ void __launch_bounds__(kBackThreads, 8)
 b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__ hom, const int2* __restrict__ wins,
                const float* __restrict__ sino, float* __restrict__ img, int nx, int ny, int np, int nu, int wcap,
-               float dxdy, int* __restrict__ err) {
+               float dxdy, int* __restrict__ err, uint32_t wait_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_abort;
     if (threadIdx.x == 0) {
@@ -45,7 +45,7 @@ b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__
     }
     uint32_t use0 = 0, use1 = 0;
     const int2* twin = wins + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * np;
-    b1_back_tile<kVC>(rec, hom, twin, sino, img, nx, ny, np, nu, wcap, dxdy, err, blockIdx.y * kBackTI,
+    b1_back_tile<kVC>(rec, hom, twin, sino, img, nx, ny, np, nu, wcap, dxdy, err, wait_limit, blockIdx.y * kBackTI,
                       blockIdx.x * kBackTJ, smem, s_abort, use0, use1);
 }
 
@@ -148,7 +148,7 @@ void b1_back_launch(const B1Device& d, const float* sino, float* img, cudaStream
     dim3 tg((d.ny + kBackTJ - 1) / kBackTJ, (d.nx + kBackTI - 1) / kBackTI);
     b1_back_kernel<<<tg, kBackThreads, b1_back_smem_bytes(d.wcap), s>>>(
         reinterpret_cast<const float4*>(d.rec), d.hom, reinterpret_cast<const int2*>(d.wins), sino, img, d.nx, d.ny,
-        d.np, d.nu, d.wcap, d.dxdy, d.err);
+        d.np, d.nu, d.wcap, d.dxdy, d.err, d.wait_limit);
     SGD_LAUNCH_CHECK();
 }
 

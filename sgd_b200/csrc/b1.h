@@ -19,6 +19,7 @@ struct B1Device {
     const int* wins = nullptr;           // [tiles][np][2] bin windows of the back kernel's tiles
     int wcap = 4;                        // bins of a staged view window in the back kernel
     int* err = nullptr;                  // device flag: a bounded wait in a kernel gave up
+    unsigned wait_limit = 1u << 22;      // polls of a back-projection staging wait before it gives up
 };
 
 int b1_back_windows(const FanGeometry& g, const std::vector<BinHomography>& hom, std::vector<int>& wins);

@@ -71,7 +71,7 @@ template <int VC>
 __global__ void __launch_bounds__(kBackThreads, 8)
 b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict__ start, int ns, long long total,
                      const float* __restrict__ sino, float* __restrict__ img, unsigned long long* __restrict__ counter,
-                     int* __restrict__ err) {
+                     int* __restrict__ err, uint32_t wait_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_abort;
     __shared__ long long s_item;
@@ -94,7 +94,8 @@ b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict
         const int t = (int)(item - start[k]);
         const int bx = t % S.tiles_x, by = t / S.tiles_x;
         if (!b1_back_tile<VC>(S.rec, S.hom, S.wins + (size_t)t * S.np, sino + S.sino_off, img + S.img_off, S.nx,
-                              S.ny, S.np, S.nu, S.wcap, S.dxdy, err, by * kBackTI, bx * kBackTJ, smem, s_abort,
+                              S.ny, S.np, S.nu, S.wcap, S.dxdy, err, wait_limit, by * kBackTI, bx * kBackTJ, smem,
+                              s_abort,
                               use0, use1))
             return;
     }
@@ -224,6 +225,9 @@ B1Batch::~B1Batch() {
 void B1Batch::set_variant(int fw, int vc) {
     if (fw != 4 && fw != 8 && fw != 16) fail("B1 batch: forward warps %d not in {4, 8, 16}", fw);
     if (vc != 2 && vc != 4 && vc != 8) fail("B1 batch: views per chunk %d not in {2, 4, 8}", vc);
+    // the start table below is read by persistent kernels that may still be
+    // running on the caller's or the batch's stream: let them finish first
+    SGD_CUDA(cudaDeviceSynchronize());
     fw_ = fw;
     vc_ = vc;
     for (int q = 0; q < ns_; ++q) {
@@ -265,7 +269,8 @@ void B1Batch::backward(const float* sino, float* img, cudaStream_t s) {
     const long long* bstart = d_start_ + ns_ + 1;
     auto launch = [&](auto kern, size_t smem) {
         const int grid = sms_ * resident((const void*)kern, kBackThreads, smem);
-        kern<<<grid, kBackThreads, smem, s>>>(d_slices_, bstart, ns_, total, sino, img, d_counter_ + 1, d_err_);
+        kern<<<grid, kBackThreads, smem, s>>>(d_slices_, bstart, ns_, total, sino, img, d_counter_ + 1, d_err_,
+                                              wait_limit_);
     };
     if (vc_ == 2) launch(b1_back_batch_kernel<2>, b1_back_smem<2>(wcap_max_));
     else if (vc_ == 4) launch(b1_back_batch_kernel<4>, b1_back_smem<4>(wcap_max_));
@@ -281,6 +286,11 @@ void B1Batch::check_status() {
         SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
         fail("B1 batch back projection: a staged chunk did not arrive (bounded wait expired)");
     }
+}
+
+void B1Batch::set_wait_limit(unsigned polls) {
+    wait_limit_ = polls;
+    release_graph();  // a captured graph holds the old kernel argument
 }
 
 void B1Batch::release_graph() {
@@ -449,6 +459,13 @@ int sgd_b1_batch_set_variant(void* batch, int fw, int vc) {
     return sgd::guarded_status([&] {
         if (!batch) sgd::fail("sgd_b1_batch_set_variant: null batch");
         static_cast<sgd::B1Batch*>(batch)->set_variant(fw, vc);
+    });
+}
+
+int sgd_b1_batch_set_wait_limit(void* batch, unsigned polls) {
+    return sgd::guarded_status([&] {
+        if (!batch) sgd::fail("sgd_b1_batch_set_wait_limit: null batch");
+        static_cast<sgd::B1Batch*>(batch)->set_wait_limit(polls);
     });
 }
 

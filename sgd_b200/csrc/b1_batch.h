@@ -42,8 +42,14 @@ public:
     // Loads the launch shape for this GPU and geometry from the cache, or
     // measures all variants and appends the best; returns 1 when loaded.
     int tune(const char* cache_path);
+    // Must not overlap batch work in flight on any stream: it rewrites the
+    // work-item table the persistent kernels read (it synchronises the
+    // device first) and drops a captured graph.
     void set_variant(int fw, int vc);
     void check_status();
+    // Polls of each back-projection staging wait before it gives up (the
+    // failure path's test sets 0); drops a captured graph.
+    void set_wait_limit(unsigned polls);
 
     int fw() const { return fw_; }
     int vc() const { return vc_; }
@@ -61,6 +67,7 @@ private:
     std::string signature_, gpu_name_;
     int ns_ = 0, sms_ = 0, device_ = 0, wcap_max_ = 4, max_nx_ = 0, max_ny_ = 0;
     int fw_ = 8, vc_ = 4;
+    unsigned wait_limit_ = 1u << 22;
     cudaStream_t stream_ = nullptr;
     B1Slice* d_slices_ = nullptr;
     long long* d_start_ = nullptr;  // [forward starts | backward starts]

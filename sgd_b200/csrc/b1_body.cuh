@@ -131,13 +131,17 @@ __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, c
 // the caller; use0/use1 count the phases barriers 0/1 completed before this
 // tile, so that a persistent CTA can run many tiles on the same barriers.
 // Returns false, with *err set and the tile unwritten, when a staged chunk
-// never arrived (bounded wait).
+// never arrived (bounded wait); the CTA's barriers are then out of step and it
+// must not run further tiles.
+// wait_limit: polls of each staging wait before it gives up (kWaitLimit in
+// production; a test sets 0 to take the failure path).
 template <int VC>
 __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, const BinHomography* __restrict__ hom,
                                              const int2* __restrict__ twin, const float* __restrict__ sino,
                                              float* __restrict__ img, int nx, int ny, int np, int nu, int wcap,
-                                             float dxdy, int* __restrict__ err, int i0, int j0, unsigned char* smem,
-                                             volatile int& s_abort, uint32_t& use0, uint32_t& use1) {
+                                             float dxdy, int* __restrict__ err, uint32_t wait_limit, int i0, int j0,
+                                             unsigned char* smem, volatile int& s_abort, uint32_t& use0,
+                                             uint32_t& use1) {
     constexpr int kHeader = b1_header_bytes<VC>();
     static_assert(kHeader % 16 == 0, "staged records must start 16-byte aligned");
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);           // [2]
@@ -199,17 +203,29 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
         }
     };
 
+    // chunk f's copies never arrived: wait (bounded, full limit) for them and
+    // for chunk f + 1's, issued before f's wait, so that no bulk copy is still
+    // landing in this CTA's shared memory when it moves on or exits
+    auto drain = [&](int f) {
+        if (tid == 0) {
+            mbar_wait_bounded(&bars[f & 1], parity(f), kWaitLimit);
+            if (f + 1 < nchunks) mbar_wait_bounded(&bars[(f + 1) & 1], parity(f + 1), kWaitLimit);
+        }
+    };
+
     __syncthreads();  // the previous tile's last chunk is fully consumed
     stage(0);
 
     double acc = 0.0, accB = 0.0;  // FP32 within a chunk (a few tens of terms), FP64 across chunks
-    int c = 0;
-    for (; c < nchunks; ++c) {
+    for (int c = 0; c < nchunks; ++c) {
         __syncthreads();  // chunk c's windows and sinogram visible; chunk c-1 fully consumed
-        if (s_abort) break;
+        if (s_abort) {
+            drain(c - 1);
+            return false;
+        }
         if (c + 1 < nchunks) stage(c + 1);
         const int st = c & 1, slot = c % 3;
-        if (!mbar_wait_bounded(&bars[st], parity(c), kWaitLimit)) {
+        if (!mbar_wait_bounded(&bars[st], parity(c), wait_limit)) {
             s_abort = 1;
             atomicExch(err, 1);
             continue;
@@ -253,13 +269,9 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
         acc += (double)csum;
         accB += (double)csumB;
     }
-    if (c < nchunks) {
-        // a staged chunk never arrived: wait (bounded) for the copies still in
-        // flight into this CTA's shared memory, then leave the tile unwritten
-        if (tid == 0) {
-            mbar_wait_bounded(&bars[c & 1], parity(c), kWaitLimit);
-            if (c + 1 < nchunks) mbar_wait_bounded(&bars[(c + 1) & 1], parity(c + 1), kWaitLimit);
-        }
+    __syncthreads();
+    if (s_abort) {  // the last chunk's wait gave up
+        drain(nchunks - 1);
         return false;
     }
     use0 += (uint32_t)((nchunks + 1) >> 1);

@@ -110,7 +110,7 @@ void A_B1::forward_host(double* b, const double* x) {
     forward_dev(st.d_img, st.d_sino, stream);
     SGD_CUDA(cudaMemcpyAsync(st.h_sino, st.d_sino, nsino * sizeof(float), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
-    check_device_status();
+    check_device_status(false);
 #pragma omp parallel for schedule(static) if (nsino > (1 << 16))
     for (long long e = 0; e < nsino; ++e) b[e] = (double)st.h_sino[e];
 }
@@ -123,13 +123,15 @@ void A_B1::backward_host(const double* b, double* x) {
     backward_dev(st.d_sino, st.d_img, stream);
     SGD_CUDA(cudaMemcpyAsync(st.h_img, st.d_img, nimg * sizeof(float), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
-    check_device_status();
+    check_device_status(false);
 #pragma omp parallel for schedule(static) if (nimg > (1 << 16))
     for (long long e = 0; e < nimg; ++e) x[e] = (double)st.h_img[e];
 }
 
-void A_B1::check_device_status() {
+void A_B1::check_device_status(bool sync_device) {
     int e = 0;
+    // the *_dev calls may have run on any of the caller's streams
+    if (sync_device) SGD_CUDA(cudaDeviceSynchronize());
     SGD_CUDA(cudaMemcpy(&e, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) {
         SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
@@ -147,7 +149,7 @@ void A_B1::project(MatrixD& vol, MatrixD& proj, double /*weight*/) {
     add_sino_to_umajor_kernel<<<blocks_for(nsino, 256), 256, 0, stream>>>(st.d_sino, proj(0), dev.np, dev.nu);
     SGD_LAUNCH_CHECK();
     SGD_CUDA(cudaStreamSynchronize(stream));
-    check_device_status();
+    check_device_status(false);
 }
 
 void A_B1::back_project(MatrixD& vol, MatrixD& proj, double /*weight*/) {
@@ -159,7 +161,7 @@ void A_B1::back_project(MatrixD& vol, MatrixD& proj, double /*weight*/) {
     add_img_to_vol_kernel<<<blocks_for(nimg, 256), 256, 0, stream>>>(st.d_img, vol(0), dev.nx, dev.ny);
     SGD_LAUNCH_CHECK();
     SGD_CUDA(cudaStreamSynchronize(stream));
-    check_device_status();
+    check_device_status(false);
 }
 
 }  // namespace sgd

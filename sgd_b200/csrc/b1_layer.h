@@ -50,8 +50,9 @@ public:
     void backward_host(const double* b, double* x);
 
     // Raises (and clears) the device error flag set by a kernel whose bounded
-    // wait gave up.  Synchronous.
-    void check_device_status();
+    // wait gave up.  Synchronous; sync_device = false when the calls in
+    // question ran on the layer's own stream and that was synchronised.
+    void check_device_status(bool sync_device = true);
 
 private:
     int* d_err_ = nullptr;

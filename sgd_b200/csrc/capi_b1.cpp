@@ -64,6 +64,13 @@ int sgd_b1_status(void* layer) {
     });
 }
 
+int sgd_b1_set_wait_limit(void* layer, unsigned polls) {
+    return sgd::guarded_status([&] {
+        if (!layer) sgd::fail("sgd_b1_set_wait_limit: null layer");
+        static_cast<A_B1*>(layer)->dev.wait_limit = polls;
+    });
+}
+
 unsigned long long sgd_b1_count(void* layer) {
     return layer ? static_cast<A_B1*>(layer)->count : 0ull;
 }

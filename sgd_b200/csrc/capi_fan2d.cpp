@@ -2,6 +2,9 @@
 // Names and signatures of the reference ones are kept; see include/sgd_b200.h.
 #include <cuda_runtime.h>
 
+#include <cstring>
+#include <vector>
+
 #include "common.h"
 #include "proj2d.h"
 
@@ -14,6 +17,8 @@ Proj2D* make_b0_parallel_layer(int nx, int ny, int np, int nu, double dx, double
                                const double* angles);
 Proj2D* make_hex_layer(int mode, int nl, int nc, int np, int nu, double dt, double du, double lsd, double lso,
                        const double* angles, const double* dz, const double* drho);
+Proj2D* make_b1ref_layer(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                         const double* angles, const double* dz, const double* drho);
 }
 
 using sgd::Proj2D;
@@ -144,6 +149,73 @@ unsigned long long sgd_hl_count(void* layer) { return layer ? static_cast<Proj2D
 void* sgd_b0_parallel_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double* angles) {
     return sgd::guarded<void*>(nullptr, [&]() -> void* {
         return sgd::make_b0_parallel_layer(nx, ny, np, nu, dx, dy, du, angles);
+    });
+}
+
+// B1 in the reference's FP32 rounding (b1ref.cu).
+void* sgd_b1ref_init(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,
+                     double* angles, double* dz, double* drho) {
+    return sgd::guarded<void*>(nullptr, [&]() -> void* {
+        return sgd::make_b1ref_layer(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, dz, drho);
+    });
+}
+int sgd_b1ref_forward_projection(double* b, double* x, void* layer) {
+    return fwd_host(b, x, layer, "sgd_b1ref_forward_projection");
+}
+int sgd_b1ref_backward_projection(double* b, double* x, void* layer) {
+    return bwd_host(b, x, layer, "sgd_b1ref_backward_projection");
+}
+void sgd_b1ref_destroy(void* layer) { delete static_cast<Proj2D*>(layer); }
+int sgd_b1ref_forward_dev(void* layer, const float* d_img, float* d_sino, void* stream) {
+    return fwd_dev(layer, d_img, d_sino, stream, "sgd_b1ref_forward_dev");
+}
+int sgd_b1ref_backward_dev(void* layer, const float* d_sino, float* d_img, void* stream) {
+    return bwd_dev(layer, d_sino, d_img, stream, "sgd_b1ref_backward_dev");
+}
+unsigned long long sgd_b1ref_count(void* layer) { return layer ? static_cast<Proj2D*>(layer)->count : 0ull; }
+long long sgd_b1ref_matrix_csr(void* layer, long long* rowptr, int* cols, double* vals, long long cap) {
+    return matrix_csr(layer, rowptr, cols, vals, cap, "sgd_b1ref_matrix_csr");
+}
+
+// Host-only plan of the generic kernels for a grid of nx x ny cells in the
+// fan geometry of b1_init (np views at `angles`, nu bins of pitch du, source
+// and detector distances lso, lsd): cell (i, j) at x = x0 + i dx,
+// y = y0 + j dy, with bin ranges from points within ri, rj cells of it.
+// Strips [np][ceil(nu/32)][8] floats, windows [tiles][np][2] ints (tiles of
+// 8 x 32 cells).  Returns the widest window, or -1 (sgd_last_error()).
+int sgd_fan2d_plan(int nx, int ny, int np, int nu, double x0, double dx, double y0, double dy, double ri, double rj,
+                   double du, double lsd, double lso, const double* angles, float* strips, int* twin) {
+    return sgd::guarded<int>(-1, [&]() -> int {
+        if (!angles || !strips || !twin) sgd::fail("sgd_fan2d_plan: null argument");
+        if (!(ri >= 0.0) || !(rj >= 0.0)) sgd::fail("sgd_fan2d_plan: negative reach");
+        sgd::FanGeometry g;
+        g.init(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, nullptr, nullptr);
+        std::vector<float4> st;
+        std::vector<int2> tw;
+        const int w = sgd::plan_fan2d(nx, ny, np, nu, [&](int p) {
+            double hw[6];
+            sgd::fan_world_hom(g, p, hw);
+            return sgd::grid_range_map(hw, x0, dx, y0, dy, ri, rj);
+        }, st, tw);
+        std::memcpy(strips, st.data(), st.size() * sizeof(float4));
+        std::memcpy(twin, tw.data(), tw.size() * sizeof(int2));
+        return w;
+    });
+}
+
+int sgd_proj2d_set_wait_limit(void* layer, unsigned polls) {
+    return sgd::guarded_status([&] {
+        if (!layer) sgd::fail("sgd_proj2d_set_wait_limit: null layer");
+        static_cast<Proj2D*>(layer)->P.wait_limit = polls;
+    });
+}
+
+int sgd_proj2d_status(void* layer) {
+    return sgd::guarded_status([&] {
+        if (!layer) sgd::fail("sgd_proj2d_status: null layer");
+        if (static_cast<Proj2D*>(layer)->status() != 0)
+            sgd::fail("back projection: a staged view chunk did not arrive within the bounded wait; "
+                      "the affected tiles were left unwritten");
     });
 }
 

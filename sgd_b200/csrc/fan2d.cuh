@@ -1,97 +1,257 @@
 // Generic 2D fan-beam projector kernels, parameterised by a footprint basis.
 //
-// A basis B supplies, for cell (i, j) of the image grid and view p:
-//   B::View                 per-view constants (B::kViewFloats floats in global memory)
-//   B::Cell                 per-(cell, view) state: bin range [lo, hi] and whatever
-//                           the footprint needs (projected corners, weights ...)
+// A basis B supplies, for cell (i, j) of the grid and view p:
+//   B::kViewFloats          per-view constants (a multiple of 4 floats)
+//   B::kBinF4               float4 words per (view, bin) in the basis table
+//                           P.bins (0: no table)
+//   B::View, B::Cell        per-view constants; per-(cell, view) state with the
+//                           bin range [lo, hi] (the reference's rule, clamped
+//                           to the detector as the reference clamps it)
+//   B::load_view(v, V)      from shared or global memory
 //   B::valid(i, j, P)       whether (i, j) is a cell of the grid
-//   B::setup(V, i, j, P, c) fills c (c.lo > c.hi: no bins)
-//   B::value(V, c, u, P)    footprint of the cell in bin u, 0 where the reference
-//                           drops it (its thresholds), area factors included
-// Both kernels call the same functions, so the pair is an exact transpose up
-// to summation order.
+//   B::setup(V, i, j, P, c)
+//   B::value(V, c, u, t, P) footprint in bin u (0 where the reference drops
+//                           it), t = the bin's table entry; bins are walked in
+//                           order from c.lo, each by value() or skip(), which
+//                           lets a basis step its bin position as the
+//                           reference does
+//   B::skip(V, c)           steps past a bin without evaluating it
+// The forward's strips and the back's windows come from each cell's true
+// footprint (plan_fan2d, proj2d.h); a bin outside it has footprint exactly 0.
+// So both kernels evaluate every (cell, bin) pair with a non-zero value and
+// u in [lo, hi] (the pairs the reference keeps), through the same functions,
+// with FP64 products and sums: the pair is an exact transpose to FP64
+// rounding.
 //
-//   fan2d_back_kernel     gather: one thread per cell, all views, FP32 within a
-//                         view and FP64 across views, each cell written once.
-//   fan2d_forward_kernel  scatter within a tile: a CTA per tile of cells; per
-//                         chunk of views the tile's bins are accumulated in a
-//                         shared-memory window (FP32 atomics), then each window
-//                         is added to an FP64 sinogram (one atomic per bin per
-//                         tile and view); fan2d_finish converts to FP32.
+//   fan2d_forward_kernel  detector-block driven: a CTA per (view, block of 32
+//                         bins).  The block's ray strip is crossed by the
+//                         lines of the grid's major axis; each lane owns lines
+//                         and walks the few cells of its line inside the strip
+//                         (host-computed strip records), adding each value to
+//                         its own FP64 shared-memory column of the block's
+//                         bins.  The columns are summed across lanes and warps
+//                         and every bin is written once: no atomics.
+//   fan2d_back_kernel     voxel driven: a CTA per tile of cells, a thread per
+//                         cell.  Per chunk of kF2Views views the CTA stages the
+//                         view constants and the tile's window of the basis
+//                         table by bulk asynchronous copies (TMA, completed on
+//                         an mbarrier, double-buffered) and the sinogram
+//                         window by plain loads; each thread accumulates over
+//                         all views in a register and writes its cell once.
 #pragma once
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+
 #include "fan2d_params.h"
+#include "tma.cuh"
 
 namespace sgd {
 
+constexpr uint32_t kF2WaitLimit = 1u << 22;
+
+// Forward block strips (host: plan_fan2d, proj2d.h).  For block k of view p,
+// along the major axis m the block's two bounding rays cross the minor axis
+// at alpha_a + beta_a m and alpha_b + beta_b m; candidate cells lie within
+// `margin` of the span between them.  s0 = (j_major, alpha_a, beta_a,
+// alpha_b), s1 = (beta_b, margin, first line, last line).
 template <class B>
-__global__ void __launch_bounds__(256) fan2d_back_kernel(Fan2DParams P, const float* __restrict__ sino,
-                                                         float* __restrict__ img) {
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)P.ni * P.nj) return;
-    const int i = (int)(idx / P.nj), j = (int)(idx - (long long)i * P.nj);
-    if (!B::valid(i, j, P)) {
-        img[idx] = 0.f;
-        return;
-    }
-    // FP64 products and sums, as the forward kernel: the pair is an adjoint
-    // pair to FP64 rounding, whatever the cancellation in the inputs
-    double acc = 0.0;
-    for (int p = 0; p < P.np; ++p) {
-        typename B::View V;
-        B::load_view(P.view + (size_t)p * B::kViewFloats, V);
-        typename B::Cell c;
-        B::setup(V, i, j, P, c);
-        const float* sp = sino + (size_t)p * P.nu;
-        for (int u = c.lo; u <= c.hi; ++u) {
-            const float val = B::value(V, c, u, p, P);
-            if (val != 0.f) acc = fma((double)val, (double)__ldg(sp + u), acc);
+__global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DParams P, const float* __restrict__ img,
+                                                                         float* __restrict__ sino, float scale) {
+    constexpr int kBF4 = B::kBinF4 > 0 ? B::kBinF4 : 1;
+    __shared__ double s_acc[kF2FwdWarps][kF2Block][33];
+    __shared__ float4 s_bin[kF2Block * kBF4];
+    __shared__ __align__(16) float s_view[B::kViewFloats];
+    const int k = blockIdx.x, p = blockIdx.y;
+    const int u0 = k * kF2Block, nb = min(kF2Block, P.nu - u0);
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    for (int e = tid; e < B::kViewFloats; e += blockDim.x) s_view[e] = __ldg(P.view + (size_t)p * B::kViewFloats + e);
+    if (B::kBinF4 > 0)
+        for (int e = tid; e < nb * B::kBinF4; e += blockDim.x)
+            s_bin[e] = __ldg(P.bins + ((size_t)p * P.nu + u0) * B::kBinF4 + e);
+    for (int e = l; e < kF2Block * 33; e += 32) (&s_acc[w][0][0])[e] = 0.0;
+    __syncthreads();
+
+    typename B::View V;
+    B::load_view(s_view, V);
+    const float4* st = P.strips + ((size_t)p * P.nblk + k) * 2;
+    const float4 s0 = __ldg(st), s1 = __ldg(st + 1);
+    const bool jmaj = s0.x > 0.5f;
+    const int nmin = jmaj ? P.ni : P.nj;
+    const int mlo = (int)s1.z, mhi = (int)s1.w;
+    double* acc = &s_acc[w][0][l];  // bin b at acc[33 b]: this lane's column
+    for (int m = mlo + tid; m <= mhi; m += blockDim.x) {
+        const float fm = (float)m;
+        const float na = fmaf(s0.z, fm, s0.y), nbb = fmaf(s1.x, fm, s0.w);
+        const int nlo = max(0, (int)ceilf(fminf(na, nbb) - s1.y));
+        const int nhi = min(nmin - 1, (int)floorf(fmaxf(na, nbb) + s1.y));
+        for (int n = nlo; n <= nhi; ++n) {
+            const int i = jmaj ? n : m, j = jmaj ? m : n;
+            if (!B::valid(i, j, P)) continue;
+            const float C = __ldg(img + (size_t)i * P.nj + j);
+            if (C == 0.f) continue;
+            typename B::Cell c;
+            B::setup(V, i, j, P, c);
+            if (c.hi < u0 || c.lo >= u0 + nb) continue;
+            const double Cd = (double)C;
+            const int ue = min(c.hi, u0 + nb - 1);
+            int u = c.lo;
+            for (; u < u0; ++u) B::skip(V, c);
+            for (; u <= ue; ++u) {
+                const float v = B::value(V, c, u, s_bin + (u - u0) * B::kBinF4, P);
+                if (v != 0.f) acc[33 * (u - u0)] = fma((double)v, Cd, acc[33 * (u - u0)]);
+            }
         }
     }
-    img[idx] = (float)acc;
+    __syncwarp();
+    if (l < nb) {
+        double t = 0.0;
+        for (int q = 0; q < 32; ++q) t += s_acc[w][l][q];
+        s_acc[w][l][32] = t;
+    }
+    __syncthreads();
+    if (w == 0 && l < nb) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < kF2FwdWarps; ++q) t += s_acc[q][l][32];
+        sino[(size_t)p * P.nu + u0 + l] = (float)t * scale;
+    }
 }
 
-template <class B>
-__global__ void __launch_bounds__(kF2Threads) fan2d_forward_kernel(Fan2DParams P, const float* __restrict__ img,
-                                                                  double* __restrict__ sino64) {
-    extern __shared__ __align__(8) unsigned char f2_smem[];
-    double* s_acc = reinterpret_cast<double*>(f2_smem);  // [kF2Views][wcap], FP64: see the back kernel
-    const int tid = threadIdx.x;
-    const int i = blockIdx.y * kF2TileI + (tid >> 5), j = blockIdx.x * kF2TileJ + (tid & 31);
-    const int2* twin = P.wins + (size_t)(blockIdx.y * P.tiles_j + blockIdx.x) * P.np;
+// Shared memory of the back kernel: 2 mbarriers | windows [2][VC] int2 |
+// view constants [2][VC][kViewFloats] | tables [2][VC][wcap][kBinF4] float4 |
+// sinogram windows [2][VC][wcap] floats.
+template <class B, int VC>
+__host__ __device__ constexpr size_t fan2d_back_header() {
+    return 16 + 2 * VC * 8 + (size_t)2 * VC * B::kViewFloats * 4;
+}
+template <class B, int VC>
+__host__ __device__ constexpr size_t fan2d_back_smem(int wcap) {
+    return fan2d_back_header<B, VC>() + (size_t)2 * VC * wcap * (B::kBinF4 * 16 + 4);
+}
+
+template <class B, int VC>
+__global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams P, const float* __restrict__ sino,
+                                                                    float* __restrict__ img, float scale) {
+    static_assert(B::kViewFloats % 4 == 0, "view rows must be whole 16-byte words");
+    static_assert(fan2d_back_header<B, VC>() % 16 == 0, "staged tables must start 16-byte aligned");
+    extern __shared__ __align__(16) unsigned char f2_smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(f2_smem);
+    int2* win = reinterpret_cast<int2*>(f2_smem + 16);                                   // [2][VC]
+    float* sview = reinterpret_cast<float*>(f2_smem + 16 + 2 * VC * 8);                    // [2][VC][kViewFloats]
+    float4* sbin = reinterpret_cast<float4*>(f2_smem + fan2d_back_header<B, VC>());       // [2][VC][wcap * kBinF4]
+    float* ssino = reinterpret_cast<float*>(sbin + (size_t)2 * VC * P.wcap * B::kBinF4);  // [2][VC][wcap]
+    __shared__ int s_abort;
+
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int tile = blockIdx.y * P.tiles_j + blockIdx.x;
+    const int i = blockIdx.y * kF2TileI + w, j = blockIdx.x * kF2TileJ + l;
     const bool mine = i < P.ni && j < P.nj && B::valid(i, j, P);
-    const float C = mine ? __ldg(img + (size_t)i * P.nj + j) : 0.f;
-    for (int p0 = 0; p0 < P.np; p0 += kF2Views) {
-        __syncthreads();  // previous chunk's windows flushed
-        for (int e = tid; e < kF2Views * P.wcap; e += kF2Threads) s_acc[e] = 0.0;
-        __syncthreads();
-        if (C != 0.f) {
-            for (int v = 0; v < kF2Views && p0 + v < P.np; ++v) {
-                const int p = p0 + v;
-                const int2 w = __ldg(twin + p);
-                typename B::View V;
-                B::load_view(P.view + (size_t)p * B::kViewFloats, V);
-                typename B::Cell c;
-                B::setup(V, i, j, P, c);
-                const int lo = max(c.lo, w.x), hi = min(c.hi, w.y);
-                double* acc = s_acc + v * P.wcap - w.x;
-                for (int u = lo; u <= hi; ++u) {
-                    const float val = B::value(V, c, u, p, P);
-                    if (val != 0.f) atomicAdd(acc + u, (double)val * (double)C);
+    const int2* twin = P.twin + (size_t)tile * P.np;
+    const int nchunks = (P.np + VC - 1) / VC;
+
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+
+    // chunk c: windows (plain stores), view constants and table windows (bulk
+    // copies by lane v of warp 0 for view v), sinogram windows (all threads)
+    auto stage = [&](int c) {
+        const int st = c & 1;
+        if (w == 0) {
+            const int p = c * VC + l;
+            int2 lh = make_int2(0, -1);
+            uint32_t bytes = 0;
+            if (l < VC) {
+                if (p < P.np) {
+                    lh = __ldg(twin + p);
+                    bytes = B::kViewFloats * 4;
+                    if (B::kBinF4 > 0 && lh.y >= lh.x) bytes += (uint32_t)(lh.y - lh.x + 1) * B::kBinF4 * 16;
                 }
+                win[st * VC + l] = lh;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+            if (l == 0) mbar_arrive_expect_tx(&bars[st], bytes);
+            __syncwarp();
+            if (l < VC && p < P.np) {
+                fence_proxy_async_smem();
+                bulk_copy_g2s(sview + (st * VC + l) * B::kViewFloats, P.view + (size_t)p * B::kViewFloats,
+                              B::kViewFloats * 4, &bars[st]);
+                if (B::kBinF4 > 0 && lh.y >= lh.x)
+                    bulk_copy_g2s(sbin + (size_t)(st * VC + l) * P.wcap * B::kBinF4,
+                                  P.bins + ((size_t)p * P.nu + lh.x) * B::kBinF4,
+                                  (uint32_t)(lh.y - lh.x + 1) * B::kBinF4 * 16, &bars[st]);
             }
         }
-        __syncthreads();
-        for (int v = 0; v < kF2Views && p0 + v < P.np; ++v) {
-            const int2 w = __ldg(twin + p0 + v);
-            for (int k = tid; k <= w.y - w.x; k += kF2Threads) {
-                const double a = s_acc[v * P.wcap + k];
-                if (a != 0.0) atomicAdd(sino64 + (size_t)(p0 + v) * P.nu + w.x + k, a);
+        for (int v = 0; v < VC; ++v) {
+            const int p = c * VC + v;
+            if (p >= P.np) break;
+            const int2 lh = __ldg(twin + p);
+            const float* sp = sino + (size_t)p * P.nu + lh.x;
+            float* dp = ssino + (st * VC + v) * P.wcap;
+            for (int e = tid; e <= lh.y - lh.x; e += kF2BackThreads) dp[e] = __ldg(sp + e);
+        }
+    };
+
+    // chunk f's copies never arrived: wait (bounded) for them and for chunk
+    // f + 1's, which were issued before f's wait, so that no bulk copy is
+    // still landing in this CTA's shared memory when it exits; the tile is
+    // left unwritten
+    auto drain = [&](int f) {
+        if (tid == 0) {
+            mbar_wait_bounded(&bars[f & 1], (uint32_t)(f >> 1) & 1u, kF2WaitLimit);
+            if (f + 1 < nchunks) mbar_wait_bounded(&bars[(f + 1) & 1], (uint32_t)((f + 1) >> 1) & 1u, kF2WaitLimit);
+        }
+    };
+
+    stage(0);
+    double acc = 0.0;
+    for (int c = 0; c < nchunks; ++c) {
+        __syncthreads();  // chunk c's windows and sinogram visible; chunk c-1 fully consumed
+        if (s_abort) {
+            drain(c - 1);
+            return;
+        }
+        if (c + 1 < nchunks) stage(c + 1);
+        const int st = c & 1;
+        if (!mbar_wait_bounded(&bars[st], (uint32_t)(c >> 1) & 1u, P.wait_limit)) {
+            s_abort = 1;
+            if (P.err) atomicExch(P.err, 1);
+            continue;
+        }
+        if (!mine) continue;
+#pragma unroll 1
+        for (int v = 0; v < VC; ++v) {
+            const int2 lh = win[st * VC + v];
+            if (lh.y < lh.x) continue;
+            typename B::View V;
+            B::load_view(sview + (st * VC + v) * B::kViewFloats, V);
+            typename B::Cell cl;
+            B::setup(V, i, j, P, cl);
+            if (cl.hi < lh.x || cl.lo > lh.y) continue;
+            const float4* tb = sbin + (size_t)(st * VC + v) * P.wcap * B::kBinF4 - (size_t)lh.x * B::kBinF4;
+            const float* sb = ssino + (st * VC + v) * P.wcap - lh.x;
+            const int ue = min(cl.hi, lh.y);
+            int u = cl.lo;
+            for (; u < lh.x; ++u) B::skip(V, cl);
+            for (; u <= ue; ++u) {
+                const float val = B::value(V, cl, u, tb + (size_t)u * B::kBinF4, P);
+                if (val != 0.f) acc = fma((double)val, (double)sb[u], acc);
             }
         }
     }
+    __syncthreads();
+    if (s_abort) {
+        drain(nchunks - 1);
+        return;
+    }
+    if (i < P.ni && j < P.nj) img[(size_t)i * P.nj + j] = mine ? (float)acc * scale : 0.f;
 }
 
 // The reference's footprint-evaluation count: sum over cells and views of the
@@ -114,7 +274,5 @@ __global__ void fan2d_count_kernel(Fan2DParams P, unsigned long long* out) {
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
     if ((threadIdx.x & 31) == 0 && n) atomicAdd(out, n);
 }
-
-__global__ void fan2d_finish_kernel(const double* __restrict__ s64, float* __restrict__ s32, long long n, float scale);
 
 }  // namespace sgd

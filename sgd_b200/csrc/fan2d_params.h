@@ -9,14 +9,22 @@ namespace sgd {
 struct Fan2DParams {
     int ni = 0, nj = 0;       // cell grid: cell (i, j) at index i * nj + j
     int np = 0, nu = 0;
-    const float* view = nullptr;     // [np][B::kViewFloats]
-    const float4* bins = nullptr;    // basis-specific per-(view, bin) table, or null
-    const int2* wins = nullptr;      // [tiles][np] forward-tile bin windows
-    int wcap = 0;                    // max window width (bins)
-    int tiles_j = 0;                 // tiles along j
-    int aux_i = 0;                   // basis-specific integer (e.g. hex row count)
+    const float* view = nullptr;     // [np][B::kViewFloats], 16-byte rows
+    const float4* bins = nullptr;    // basis-specific per-(view, bin) table [np][nu][B::kBinF4], or null
+    const float4* strips = nullptr;  // [np][nblk][2] forward block strips (fan2d.cuh)
+    int nblk = 0;                    // bin blocks of kF2Block bins per view
+    const int2* twin = nullptr;      // [tiles][np] back-projection tile bin windows
+    int tiles_j = 0;                 // back tiles along j
+    int wcap = 0;                    // widest back window (bins)
+    int aux_i = 0;                   // basis-specific integer
+    int* err = nullptr;              // device status word (bounded waits), 0 = ok
+    unsigned wait_limit = 1u << 22;  // polls of the back kernel's staging wait before it gives up
 };
 
-constexpr int kF2TileI = 8, kF2TileJ = 32, kF2Threads = kF2TileI * kF2TileJ, kF2Views = 4;
+// forward: one CTA per (view, block of kF2Block bins), kF2FwdWarps warps
+constexpr int kF2Block = 32, kF2FwdWarps = 4;
+// back: one CTA per kF2TileI x kF2TileJ cells (one per thread), views staged
+// kF2Views at a time
+constexpr int kF2TileI = 8, kF2TileJ = 32, kF2BackThreads = kF2TileI * kF2TileJ, kF2Views = 4;
 
 }  // namespace sgd

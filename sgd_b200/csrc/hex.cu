@@ -49,14 +49,16 @@ struct HexBasis {
         float h0, h1, h2, h3, h4, h5;
         int mode, back;
     };
+    // per bin: va, vb, vc, 0, 1/va, 1/vb, 1/vc, 0 (FP64; a zero reciprocal
+    // where the direction is dropped)
+    static constexpr int kBinF4 = 4;
     struct Cell {
-        float ox, oy, sx0, sy0;
+        float ox, oy, sx, sy;  // site; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
     };
     __device__ static void load_view(const float* v, View& V) {
         const float4* q = reinterpret_cast<const float4*>(v);
-        const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3), e = __ldg(q + 4),
-                     f = __ldg(q + 5), g = __ldg(q + 6);
+        const float4 a = q[0], b = q[1], c = q[2], d = q[3], e = q[4], f = q[5], g = q[6];
         V = View{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y, d.z, d.w, e.x, e.y,
                  e.z, e.w, f.x, f.y, f.z, f.w, (int)g.x, (int)g.y};
     }
@@ -116,8 +118,8 @@ struct HexBasis {
         else
             pmi_bounds(V, ic, il, P.nu, c.lo, c.hi);
         const float fl = (float)c.lo;
-        c.sx0 = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
-        c.sy0 = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
+        c.sx = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
+        c.sy = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
     }
     __device__ static void sort2d(float& a, float& b) {
         if (a < b) {
@@ -203,14 +205,14 @@ struct HexBasis {
         }
         return v[0] * (1.0 / 6.0);
     }
-    // bins: [view][bin][va, vb, vc, 0, 1/va, 1/vb, 1/vc, 0] doubles (a zero
-    // reciprocal where the direction is dropped)
-    __device__ static float value(const View& V, const Cell& c, int u, int p, const Fan2DParams& P) {
-        float sx = c.sx0, sy = c.sy0;
-        for (int t = c.lo; t < u; ++t) {  // the reference's FP32 stepping
-            sx += V.puvx;
-            sy += V.puvy;
-        }
+    // the reference's FP32 stepping of the bin centre
+    __device__ static void skip(const View& V, Cell& c) {
+        c.sx += V.puvx;
+        c.sy += V.puvy;
+    }
+    __device__ static float value(const View& V, Cell& c, int, const float4* t, const Fan2DParams&) {
+        const float sx = c.sx, sy = c.sy;
+        skip(V, c);
         const float px = V.srcx, py = V.srcy, ox = c.ox, oy = c.oy;
         const float ax = sx - V.puvx * 0.5f, ay = sy - V.puvy * 0.5f;
         const float bx = sx + V.puvx * 0.5f, by = sy + V.puvy * 0.5f;
@@ -225,15 +227,15 @@ struct HexBasis {
             if (da > V.dt && db > V.dt && (ax1 - ox) * (bx1 - ox) >= 0.0f && (ay1 - oy) * (by1 - oy) >= 0.0f)
                 return 0.f;
         }
-        const double* b = reinterpret_cast<const double*>(P.bins) + ((size_t)p * P.nu + u) * 8;
-        const double va = __ldg(b), vb = __ldg(b + 1), vc = __ldg(b + 2);
+        const double* b = reinterpret_cast<const double*>(t);
+        const double va = b[0], vb = b[1], vc = b[2];
         const double vblur = -sqrt((double)(bx1 - ax1) * (bx1 - ax1) + (double)(by1 - ay1) * (by1 - ay1));
         double y = sqrt((double)(ax1 - ox) * (ax1 - ox) + (double)(ay1 - oy) * (ay1 - oy));
         if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) y = -y;
         double conv;
         if (V.mode == kHl) {
             if (fabs(vblur) > 1e-8 && fabs(va) > 1e-8 && fabs(vb) > 1e-8 && fabs(vc) > 1e-8)
-                conv = conv4_full(y, vblur, va, vb, vc, __ldg(b + 4), __ldg(b + 5), __ldg(b + 6));
+                conv = conv4_full(y, vblur, va, vb, vc, b[4], b[5], b[6]);
             else
                 conv = conv4(y, vblur, va, vb, vc);
         } else {
@@ -304,22 +306,8 @@ public:
         }
         back_view_ = view;
         for (int p = 0; p < np; ++p) back_view_[(size_t)p * HexBasis::kViewFloats + 25] = 1.f;
-        // tile boxes: site centres of the tile's rows and columns, plus the
-        // hexagon radius dt (H0) or the linear element's radius dt (Hl); the
-        // reference-compatible H0 bounds are at 0.5 dt row pitch, inside this
-        // box scaled to 1.5 dt only for rows near the centre, so the box also
-        // covers the rows at the pmi positions
-        const double rdt = dt, sdx = dt * kSqrt3;
-        const double ny_pitch = (mode == kHl ? 0.5 : 1.5) * dt;
-        finish_init(view, HexBasis::kViewFloats, bins, [&](int i0, int i1, int j0, int j1) {
-            const double xa = (i0 - 0.5 * (nc - 1)) * sdx - rdt - 0.5 * sdx, xb = (i1 - 0.5 * (nc - 2)) * sdx + rdt;
-            double ya = (j0 - 0.5 * (nl - 1)) * ny_pitch - rdt, yb = (j1 - 0.5 * (nl - 1)) * ny_pitch + rdt;
-            if (mode == kH0Reference) {
-                ya = std::min(ya, (j0 - 0.5 * (nl - 1)) * 0.5 * dt - rdt);
-                yb = std::max(yb, (j1 - 0.5 * (nl - 1)) * 0.5 * dt + rdt);
-            }
-            return Box2{xa, xb, ya, yb};
-        });
+        dt_ = dt;
+        finish_init(view, bins);
         SGD_CUDA(cudaMalloc(&d_back_view_, back_view_.size() * sizeof(float)));
         SGD_CUDA(cudaMemcpy(d_back_view_, back_view_.data(), back_view_.size() * sizeof(float),
                             cudaMemcpyHostToDevice));
@@ -329,7 +317,7 @@ public:
     }
     ~HexLayer() override { cudaFree(d_back_view_); }
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
-        fan2d_forward<HexBasis>(P, img, d_sino64_, sino, out_scale, smem_fwd_, s);
+        fan2d_forward<HexBasis>(P, img, sino, out_scale, s);
     }
     long long csr(const CsrOut& out) override { return fan2d_csr<HexBasis>(P, out_scale, out, stream); }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
@@ -338,8 +326,23 @@ public:
         fan2d_back<HexBasis>(Q, sino, img, out_scale, s);
     }
 
+protected:
+    // The sites' true footprints: the hexagon (H0, rows at 1.5 dt: vertices
+    // within 1/2 + 1/2 site, odd-row shift and vertex, and dt = 2/3 row) or
+    // the linear element (Hl, rows at 0.5 dt: within one site and 2 rows).
+    // The reference-compatible H0 takes its bin ranges from vertices on the
+    // 0.5 dt rows of pmi instead; bins outside the true footprint hold 0, so
+    // planning by the true one keeps every non-zero pair of those ranges.
+    RangeMap range_map(int p) const override {
+        double hw[6];
+        fan_world_hom(geo, p, hw);
+        if (mode_ == kHl) return grid_range_map(hw, geo.x0(), geo.dx, geo.y0(), geo.dy, 1.0, 2.0);
+        return grid_range_map(hw, geo.x0(), geo.dx, -0.5 * (P.nj - 1) * 1.5 * dt_, 1.5 * dt_, 1.0, 1.0);
+    }
+
 private:
     int mode_;
+    double dt_ = 0;
     std::vector<float> back_view_;
     float* d_back_view_ = nullptr;
 };

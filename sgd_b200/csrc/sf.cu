@@ -24,6 +24,7 @@ struct SFBasis {
     struct View {
         float pm0, pm1, pm3, pm8, pm9, pm11, puvx, singular, srcx, srcy, dx, dy, nx2, ny2;
     };
+    static constexpr int kBinF4 = 0;
     struct Cell {
         float us[4];
         float weight;
@@ -32,7 +33,7 @@ struct SFBasis {
     };
     __device__ static void load_view(const float* v, View& V) {
         const float4* q = reinterpret_cast<const float4*>(v);
-        const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+        const float4 a = q[0], b = q[1], c = q[2], d = q[3];
         V = View{a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w, d.x, d.y};
     }
     __device__ static bool valid(int, int, const Fan2DParams&) { return true; }
@@ -89,11 +90,12 @@ struct SFBasis {
         if (tmp == tmp) g += tmp;
         return g;
     }
-    __device__ static float value(const View&, const Cell& c, int u, int, const Fan2DParams&) {
+    __device__ static float value(const View&, Cell& c, int u, const float4*, const Fan2DParams&) {
         const float g = gamma((float)u, u + 1.0f, c);
         const float val = c.weight * g;
         return (g > 1e-7f && val == val) ? val : 0.f;
     }
+    __device__ static void skip(const View&, Cell&) {}
 };
 
 namespace {
@@ -120,19 +122,23 @@ public:
             v[12] = (nx - 1) / 2.0f;
             v[13] = (ny - 1) / 2.0f;
         }
-        const double hx = 0.5 * dx, hy = 0.5 * dy;
-        const double x0 = geo.x0(), y0 = geo.y0();
-        finish_init(view, SFBasis::kViewFloats, {}, [&](int i0, int i1, int j0, int j1) {
-            return Box2{x0 + i0 * dx - hx, x0 + i1 * dx + hx, y0 + j0 * dy - hy, y0 + j1 * dy + hy};
-        });
+        finish_init(view, {});
         count = 0;  // the reference's SF kernels never count (layers/A_SF.cu:19)
     }
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
-        fan2d_forward<SFBasis>(P, img, d_sino64_, sino, 1.f, smem_fwd_, s);
+        fan2d_forward<SFBasis>(P, img, sino, 1.f, s);
     }
     long long csr(const CsrOut& out) override { return fan2d_csr<SFBasis>(P, 1.f, out, stream); }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
         fan2d_back<SFBasis>(P, sino, img, 1.f, s);
+    }
+
+protected:
+    // ranges from the corners at +-1/2
+    RangeMap range_map(int p) const override {
+        double hw[6];
+        fan_world_hom(geo, p, hw);
+        return grid_range_map(hw, geo.x0(), geo.dx, geo.y0(), geo.dy, 0.5, 0.5);
     }
 };
 

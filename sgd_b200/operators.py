@@ -63,18 +63,23 @@ class _Fan2DOperator(LinearOperator):
         self._drho = None if drho is None else np.ascontiguousarray(drho, dtype=np.float64)
         L = _lib.lib()
         self._L = L
-        init = getattr(L, f"{self._prefix}_init")
+        init = getattr(L, self._sym("init"))
         if self._offsets:
             self.cpointer = init(nx, ny, nnp, nu, dx, dy, du, lsd, lso, _ptr(angles), _ptr(self._dz),
                                  _ptr(self._drho))
         else:
             self.cpointer = init(nx, ny, nnp, nu, dx, dy, du, lsd, lso, _ptr(angles))
         if not self.cpointer:
-            raise _lib.ProjectorError(f"{self._prefix}_init: {_lib.last_error()}")
-        self._fwd = getattr(L, f"{self._prefix}_forward_projection")
+            raise _lib.ProjectorError(f"{self._sym('init')}: {_lib.last_error()}")
+        self._fwd = getattr(L, self._sym("forward_projection"))
         self._bwd = getattr(L, f"sgd_{self._prefix}_backward_projection")
-        self._destroy = getattr(L, f"{self._prefix}_destroy")
+        self._destroy = getattr(L, self._sym("destroy"))
         self.conv_count = int(getattr(L, f"sgd_{self._prefix}_count")(self.cpointer))
+
+    def _sym(self, what):
+        # the reference's names (b1_init, ...); modes without a counterpart
+        # in the reference carry the library's sgd_ prefix throughout
+        return f"sgd_{self._prefix}_{what}" if self._prefix == "b1ref" else f"{self._prefix}_{what}"
 
     def __del__(self):
         p = getattr(self, "cpointer", None)
@@ -107,9 +112,21 @@ class _Fan2DOperator(LinearOperator):
 
 
 class A_B1_operator(_Fan2DOperator):
-    """Bilinear box-spline fan-beam projector (python/operators/operators.py:156-219)."""
+    """Bilinear box-spline fan-beam projector (python/operators/operators.py:156-219).
+
+    ``reference_rounding=True`` selects the mode that repeats the reference
+    layer's FP32 bin positioning and edge-ray arithmetic (layers/A_B1.cu:
+    100-197), for results within a few units in the last place of the
+    reference's own; the default evaluates the footprint from exact bin
+    geometry."""
 
     _prefix = "b1"
+
+    def __init__(self, nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dz=None, drho=None, dtype=np.float64,
+                 reference_rounding=False):
+        if reference_rounding:
+            self._prefix = "b1ref"
+        super().__init__(nx, ny, nnp, nu, dx, dy, du, lsd, lso, angles, dz=dz, drho=drho, dtype=dtype)
 
 
 class A_SF_operator(_Fan2DOperator):
@@ -187,11 +204,16 @@ class _HexOperator(_Fan2DOperator):
         self.cpointer = L.sgd_hex_init(self._mode, nx, ny, nnp, nu, dt, du, lsd, lso, _ptr(angles), _ptr(self._dz),
                                        _ptr(self._drho))
         if not self.cpointer:
-            raise _lib.ProjectorError(f"{self._prefix}_init: {_lib.last_error()}")
-        self._fwd = getattr(L, f"{self._prefix}_forward_projection")
+            raise _lib.ProjectorError(f"{self._sym('init')}: {_lib.last_error()}")
+        self._fwd = getattr(L, self._sym("forward_projection"))
         self._bwd = getattr(L, f"sgd_{self._prefix}_backward_projection")
-        self._destroy = getattr(L, f"{self._prefix}_destroy")
+        self._destroy = getattr(L, self._sym("destroy"))
         self.conv_count = int(getattr(L, f"sgd_{self._prefix}_count")(self.cpointer))
+
+    def _sym(self, what):
+        # the reference's names (b1_init, ...); modes without a counterpart
+        # in the reference carry the library's sgd_ prefix throughout
+        return f"sgd_{self._prefix}_{what}" if self._prefix == "b1ref" else f"{self._prefix}_{what}"
 
 
 class A_H0_operator(_HexOperator):

@@ -27,8 +27,9 @@ def _ptr(a):
 class FanProjector:
     """One fan-beam geometry bound to the current CUDA device.
 
-    ``kind`` selects the basis ("b1" bilinear, "SF" separable footprint,
-    "b0" pixel indicator).  Arguments follow the reference's
+    ``kind`` selects the basis ("b1" bilinear, "b1ref" bilinear in the
+    reference layer's FP32 rounding, "SF" separable footprint, "b0" pixel
+    indicator).  Arguments follow the reference's
     ``*_init`` entry points (layers/A_B1.cu:595-603): image nx x ny with pixel
     dx x dy, np views at ``angles`` (radians), nu bins of pitch du,
     source-detector distance lsd, source-isocentre distance lso, optional
@@ -48,7 +49,8 @@ class FanProjector:
         self._L = L
         dz = None if dz is None else np.ascontiguousarray(dz, dtype=np.float64)
         drho = None if drho is None else np.ascontiguousarray(drho, dtype=np.float64)
-        init = getattr(L, f"{kind}_init")
+        pre = "sgd_b1ref" if kind == "b1ref" else kind  # a mode without a reference counterpart
+        init = getattr(L, f"{pre}_init")
         if kind == "SF":
             self.handle = init(self.nx, self.ny, self.np, self.nu, dx, dy, du, lsd, lso, _ptr(angles))
         else:
@@ -56,9 +58,17 @@ class FanProjector:
                                _ptr(drho))
         if not self.handle:
             raise _lib.ProjectorError(f"{kind}_init: {_lib.last_error()}")
+        # the library's kernels behind each direction, and the launches of
+        # one forward + back projection (the B1 forward also transposes)
+        if kind == "b1":
+            self.kernels = {"forward": "b1_forward_kernel", "back": "b1_back_kernel"}
+            self.launches_per_step = 3
+        else:
+            self.kernels = {"forward": "fan2d_forward_kernel", "back": "fan2d_back_kernel"}
+            self.launches_per_step = 2
         self._fwd = getattr(L, f"sgd_{kind}_forward_dev")
         self._bwd = getattr(L, f"sgd_{kind}_backward_dev")
-        self._destroy = getattr(L, f"{kind}_destroy")
+        self._destroy = getattr(L, f"{pre}_destroy")
         self.conv_count = int(getattr(L, f"sgd_{kind}_count")(self.handle))
 
     def __del__(self):
@@ -97,6 +107,11 @@ class FanProjector:
 class _HandleProjector:
     """A layer handle with FP32 device entry points ``fwd(h, in, out, stream)``
     and ``bwd(h, in, out, stream)``: the common body of the projectors below."""
+
+    # the library's kernels behind each direction, and the launches of one
+    # forward + back projection (the generic 2D kernels: one each)
+    kernels = {"forward": "fan2d_forward_kernel", "back": "fan2d_back_kernel"}
+    launches_per_step = 2
 
     def _setup(self, handle, fwd, bwd, destroy, image_shape, sino_shape, what):
         if not handle:
@@ -185,6 +200,9 @@ class ConeProjector(_HandleProjector):
             f, b, d = L.sgd_sf3d_forward_dev, L.sgd_sf3d_backward_dev, L.sgd_sf3d_destroy
         else:
             raise ValueError(f"unknown cone-beam kind {kind!r}")
+        # forward kernel + FP64-to-FP32 finish, back kernel
+        self.kernels = {"forward": f"{kind}_forward_kernel", "back": f"{kind}_back_kernel"}
+        self.launches_per_step = 3
         self._keep = angles
         self._setup(h, f, b, d, (nz, ny, nx), (len(angles), nv, nu), kind)
 
