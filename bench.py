@@ -11,9 +11,12 @@ projection (A x, A^T y).  Metric: fwd+adj voxel-view updates per second,
 
 `--impl reference` times the reference's CPU path for this operator (its
 sparse system matrix applied as python/operators/operators.py:31-49 does) on
-a bounded sample of views: scipy CSR SpMV (single-threaded, the reference's
-own call) and the same CSR product on every host core (torch.sparse_csr,
-MKL); the faster is the line's value.
+a bounded sample of views, the same CSR product on every host core
+(torch.sparse_csr, MKL), W warm-up and K timed steps as our arm; the
+single-threaded scipy figure (the reference's own call) is reported beside
+it.  Our arm's line also carries, measured after its timed region, the same
+CPU path (`cpu_baseline`) and the reference's own CUDA layer built from its
+sources (`reference_gpu`).
 Each rank of a multi-GPU run projects its own phantom (independent replicas,
 weak scaling); there is no collective on the data path.
 """
@@ -114,85 +117,146 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["fan512", "batch48"] + sorted(FAMILIES), default="fan512",
+    ap.add_argument("--workload", choices=["fan512", "batch48", "asd_c5"] + sorted(FAMILIES), default="fan512",
                     help="fan512: the headline single-slice workload; batch48: 48 uneven slices in one "
-                         "graph-replayed persistent launch per direction; the others: the other projector "
-                         "families at their configurations (device-resident fwd+adj)")
+                         "graph-replayed persistent launch per direction; asd_c5: learned vs plain ASD-POCS "
+                         "(several minutes: pair generation and training included); the others: the other "
+                         "projector families at their configurations (device-resident fwd+adj)")
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------------------
 # reference arm / CPU baseline: scipy CSR SpMV on a bounded sample of views
 # ---------------------------------------------------------------------------
+class CpuSpmv:
+    """The reference's CPU path for this operator: its sparse system matrix
+    applied as python/operators/operators.py:45-49 does (A @ x, A.T @ y), on
+    the rows of `n_views` evenly spaced views (a bounded sample; the entries
+    come from the oracle's FP64 replica of layers/A_B1.cu).  Built once."""
+
+    def __init__(self, n_views=24):
+        import torch
+        from oracle import oracle
+        from sgd_b200.phantom import ellipse_phantom
+        self.views = np.arange(0, NP, NP // n_views)[:n_views]
+        self.A = oracle.b1_matrix(NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES, self.views)
+        self.AT = self.A.T.tocsr()
+        self.x = ellipse_phantom(NX, NY, DX, DY, seed=0).ravel()
+        self.y = self.A @ self.x
+        self.units = 2.0 * NX * NY * len(self.views)
+        self.threads = os.cpu_count() or 1
+        torch.set_num_threads(self.threads)
+
+        def csr(M):
+            return torch.sparse_csr_tensor(torch.from_numpy(M.indptr.astype(np.int64)),
+                                           torch.from_numpy(M.indices.astype(np.int64)), torch.from_numpy(M.data),
+                                           size=M.shape)
+
+        self.At, self.ATt = csr(self.A), csr(self.AT)
+        self.xt, self.yt = torch.from_numpy(self.x), torch.from_numpy(self.y)
+        self.At @ self.xt  # first call initialises the sparse backend
+
+    def step_threads(self):
+        """Seconds of one A@x + A.T@y on every host core (torch CSR, MKL)."""
+        t0 = time.perf_counter()
+        self.At @ self.xt
+        self.ATt @ self.yt
+        return time.perf_counter() - t0
+
+    def step_scipy(self):
+        """Seconds of one A@x + A.T@y in scipy (single-threaded, the reference's own call)."""
+        t0 = time.perf_counter()
+        self.A @ self.x
+        self.AT @ self.y
+        return time.perf_counter() - t0
+
+    def desc(self, v1, vn):
+        return (f"CSR SpMV A@x and A.T@y (python/operators/operators.py:45-49 path), FP64, rows of {len(self.views)} "
+                f"of {NP} views (nnz {self.A.nnz}), entries from the FP64 replica of layers/A_B1.cu; "
+                f"scipy 1 thread {v1:.3e}/s, torch CSR (MKL) {self.threads} threads {vn:.3e}/s")
+
+
 def cpu_spmv_sample(n_views=24, reps=3):
-    """Times A@x and A.T@y of the reference's sparse-matrix CPU path on the rows
-    of `n_views` evenly spaced views, single-threaded (scipy, as the reference)
-    and on all host cores (torch CSR).  Returns a dict: updates/s of each, the
-    faster, the threads it used, a description and the seconds spent."""
-    import scipy.sparse  # noqa: F401
-    import torch
-    from oracle import oracle
-    from sgd_b200.phantom import ellipse_phantom
-    views = np.arange(0, NP, NP // n_views)[:n_views]
-    A = oracle.b1_matrix(NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES, views)
-    AT = A.T.tocsr()
-    x = ellipse_phantom(NX, NY, DX, DY, seed=0).ravel()
-    y = A @ x
-    units = 2.0 * NX * NY * len(views)
+    """Best-of-`reps` updates/s of the sampled CPU path, single-threaded and on
+    every host core; the faster is the value."""
     t_all = time.perf_counter()
-    best1 = float("inf")
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        A @ x
-        AT @ y
-        best1 = min(best1, time.perf_counter() - t0)
-    threads = os.cpu_count() or 1
-    torch.set_num_threads(threads)
-
-    def csr(M):
-        return torch.sparse_csr_tensor(torch.from_numpy(M.indptr.astype(np.int64)),
-                                       torch.from_numpy(M.indices.astype(np.int64)), torch.from_numpy(M.data),
-                                       size=M.shape)
-
-    At, ATt = csr(A), csr(AT)
-    xt, yt = torch.from_numpy(x), torch.from_numpy(y)
-    At @ xt  # first call initialises the sparse backend
-    bestn = float("inf")
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        At @ xt
-        ATt @ yt
-        bestn = min(bestn, time.perf_counter() - t0)
+    S = CpuSpmv(n_views)
+    best1 = min(S.step_scipy() for _ in range(reps))
+    bestn = min(S.step_threads() for _ in range(reps))
+    v1, vn = S.units / best1, S.units / bestn
     spent = time.perf_counter() - t_all
-    v1, vn = units / best1, units / bestn
-    desc = (f"CSR SpMV A@x and A.T@y (python/operators/operators.py:45-49 path), FP64, rows of {len(views)} of "
-            f"{NP} views (nnz {A.nnz}), entries from the FP64 replica of layers/A_B1.cu; best of {reps}; "
-            f"scipy 1 thread {v1:.3e}/s, torch CSR (MKL) {threads} threads {vn:.3e}/s")
     if vn >= v1:
-        return {"value": vn, "cores": threads, "single_thread": v1, "desc": desc, "spent": spent}
-    return {"value": v1, "cores": 1, "single_thread": v1, "desc": desc, "spent": spent}
+        return {"value": vn, "cores": S.threads, "single_thread": v1, "desc": S.desc(v1, vn), "spent": spent}
+    return {"value": v1, "cores": 1, "single_thread": v1, "desc": S.desc(v1, vn), "spent": spent}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU path (CpuSpmv) on the host cores,
+    W warm-up and exactly K timed steps, each one A@x + A.T@y of the sample."""
     if rank != 0:
         return
-    steps = []
-    r = {}
-    for _ in range(max(1, args.warmup // 3)):
-        cpu_spmv_sample(reps=1)
-    for _ in range(max(1, min(args.steps, 5))):
-        r = cpu_spmv_sample(reps=1)
-        steps.append(r["value"])
-    value = statistics.median(steps)
+    S = CpuSpmv()
+    for _ in range(args.warmup):
+        S.step_threads()
+    times = [S.step_threads() for _ in range(args.steps)]
+    single = S.units / min(S.step_scipy() for _ in range(3))
+    value = S.units / statistics.median(times)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-        "steps": len(steps), "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": CONFIG,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": r["desc"],
-                         "single_thread_value": r["single_thread"]},
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": CONFIG, "parallelism": f"host threads x{S.threads}",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": S.threads, "kind": "port",
+                         "sample": S.desc(single, value), "single_thread_value": single},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_layer():
+    """The reference's own B1 CUDA layer (layers/A_B1.cu built from its sources
+    into oracle/_ref/libnetwork.so) on the headline geometry, on this GPU,
+    outside the timed region: its kernels alone (A_B1::project /
+    back_project on resident device buffers, per-view launches) and its C ABI
+    end to end (b1_forward_projection + b1_backward_projection on FP64 host
+    arrays).  None when the library was not built."""
+    import ctypes
+    lib_path = os.path.join(ROOT, "oracle", "_ref", "libnetwork.so")
+    if not os.path.exists(lib_path):
+        return None
+    L = ctypes.CDLL(lib_path)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.b1_init.restype = ctypes.c_void_p
+    L.b1_init.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [dp] * 3
+    L.b1_forward_projection.restype = ctypes.c_int
+    L.b1_forward_projection.argtypes = [dp, dp, ctypes.c_void_p]
+    L.b1_backward_projection.restype = None
+    L.b1_backward_projection.argtypes = [dp, dp, ctypes.c_void_p]
+    L.ref_b1_kernel_ms.restype = ctypes.c_float
+    L.ref_b1_kernel_ms.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    ang = np.ascontiguousarray(ANGLES, dtype=np.float64)
+    h = L.b1_init(NX, NY, NP, NU, DX, DY, DU, LSD, LSO, ang.ctypes.data_as(dp), None, None)
+    back = ctypes.c_float(0.0)
+    fwd = L.ref_b1_kernel_ms(h, 3, ctypes.byref(back))
+    from sgd_b200.phantom import ellipse_phantom
+    x = np.ascontiguousarray(ellipse_phantom(NX, NY, DX, DY, seed=0).ravel(), dtype=np.float64)
+    y = np.zeros(NP * NU)
+    xt = np.zeros(NX * NY)
+    L.b1_forward_projection(y.ctypes.data_as(dp), x.ctypes.data_as(dp), h)
+    t0 = time.perf_counter()
+    reps = 2
+    for _ in range(reps):
+        L.b1_forward_projection(y.ctypes.data_as(dp), x.ctypes.data_as(dp), h)
+        L.b1_backward_projection(y.ctypes.data_as(dp), xt.ctypes.data_as(dp), h)
+    abi_ms = (time.perf_counter() - t0) / reps * 1e3
+    units = 2.0 * NX * NY * NP
+    return {"kernels_fwd_ms": fwd, "kernels_bwd_ms": back.value,
+            "kernels_updates_per_s": units / ((fwd + back.value) * 1e-3),
+            "c_abi_ms_per_step": abi_ms, "c_abi_updates_per_s": units / (abi_ms * 1e-3),
+            "source": "oracle/_ref/libnetwork.so: the reference's layers/A_B1.cu built from its own sources "
+                      "(its per-view launches and FP64 atomics), timed on this GPU outside the timed region; "
+                      "kernels: CUDA events around A_B1::project / back_project (3 calls each); C ABI: "
+                      "b1_forward_projection + b1_backward_projection on FP64 host arrays (2 pairs, wall clock)"}
 
 
 # ---------------------------------------------------------------------------
@@ -363,17 +427,20 @@ def run_ours(args, rank, world, local_rank):
         "fwd_ms": fwd_avg, "bwd_ms": bwd_avg,
     }
 
-    cpu = None
+    # baselines, after the timed region, one GPU only: the reference's CPU
+    # path and the reference's own CUDA layer
+    cpu = ref_gpu = None
     if world == 1:
         r = cpu_spmv_sample(reps=3)
         cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": r["desc"],
                "single_thread_value": r["single_thread"], "seconds": round(r["spent"], 2)}
+        ref_gpu = reference_gpu_layer()
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic", "config": dict(CONFIG, parallelism=f"replicas x{world}"),
-        "roofline": roofline, "cpu_baseline": cpu,
+        "dtype": "f32", "data": "synthetic", "config": CONFIG, "parallelism": f"replicas x{world}",
+        "roofline": roofline, "cpu_baseline": cpu, "reference_gpu": ref_gpu,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 4 * (NX * NY + NP * NU),
                 "d2h_bytes_per_step": 4 * (NP * NU + NX * NY),
                 "path": "A_B1_operator.matvec/rmatvec -> b1_forward_projection / b1_backward_projection, FP64 numpy"},
@@ -509,6 +576,33 @@ def run_family(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_asd(args, rank, world, local_rank):
+    """Learned warm start vs plain ASD-POCS (64 fan-beam
+    phantoms 256^2, 120 views, Poisson I0 = 1e5, the 5-layer 32-channel CNN
+    trained on 2000 plain-ASD-POCS pairs by the library's kernels).  The
+    value is the learned run's GPU time to plain's converged RMSE over
+    plain's GPU time to convergence (lower is better; target <= 1/3)."""
+    import torch
+    from sgd_b200.asd import experiment
+    torch.cuda.set_device(local_rank)
+    r = experiment(log=(lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None)
+    if rank != 0:
+        return
+    line = {
+        "metric": "learned / plain ASD-POCS GPU time to plain's converged RMSE", "value": r["time_ratio"],
+        "unit": "ratio", "n_gpus": world, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded ellipse phantoms, Poisson noise)",
+        "config": {"workload": r["workload"], "rmse_truth": r["rmse_truth"], "convergence_rule": r["convergence_rule"]},
+        "plain": {k: r["plain"][k] for k in ("iters", "gpu_ms", "rmse")},
+        "learned": {k: r["learned"][k] for k in ("plain_iters_before_net", "iters_after_net", "gpu_ms", "net_ms",
+                                                  "rmse", "reached")},
+        "data_residual": {"plain_last": r["plain"]["data_residual"][-1],
+                          "learned_last": (r["learned"]["data_residual"] or [None])[-1]},
+        "training": {k: r["training"][k] for k in ("pairs", "target_iters", "epochs", "pairs_s", "train_s")},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -526,6 +620,8 @@ def main():
     try:
         if args.workload == "batch48":
             run_batch48(args, rank, world, local_rank)
+        elif args.workload == "asd_c5":
+            run_asd(args, rank, world, local_rank)
         elif args.workload in FAMILIES:
             run_family(args, rank, world, local_rank)
         else:

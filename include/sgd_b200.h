@@ -240,6 +240,12 @@ int sgd_b1_3d_forward_dev(void* layer, const float* d_vol, float* d_proj, void* 
 int sgd_b1_3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void* stream);
 unsigned long long sgd_b1_3d_count(void* layer);
 
+/* New: synchronises the device and reports (0 / -1 with sgd_last_error, then
+ * clears) an A_B1_3D back projection on the *_dev entry point whose bounded
+ * wait for its staged projection window gave up; those voxels were left
+ * unwritten.  The FP64 host entry point checks it itself. */
+int sgd_b1_3d_status(void* layer);
+
 /* ---- SF_projector: 3D separable footprint --------------------------------- */
 
 /* New entry points for the class SF of layers/SF_projector.hh:9-23, which the

@@ -28,7 +28,7 @@ import torch
 
 from . import _lib
 from .batch import B1Batch
-from .phantom import ellipse_phantom, random_ellipses
+from .phantom import ellipse_phantom, ellipse_phantom_average, random_ellipses
 
 _vp = ctypes.c_void_p
 LSD, LSO = 1085.6, 595.0
@@ -73,10 +73,12 @@ class Geometry:
         return (self.n, self.n, self.nu, self.d, self.d, self.du, self.lsd, self.lso, self.angles)
 
 
-def simulate(geo, seeds, i0=1e5, sub=8, noise_seed=0):
-    """(truth (N, n, n) float32 on the device, sinograms (N, views, nu) float32
-    on the device, ellipses (N, 10, 6)).  Truth = the phantom sampled at
-    pixel centres, the basis coefficients the reconstruction estimates."""
+def simulate(geo, seeds, i0=1e5, sub=8, noise_seed=0, truth="points"):
+    """(truth (N, n, n) on the device, sinograms (N, views, nu) float32 on the
+    device, ellipses (N, 10, 6)).  truth="points": the phantom sampled at
+    pixel centres, FP32; truth="average": the phantom averaged over each
+    pixel in FP64 (ellipse_phantom_average), the reconstruction experiment's
+    ground truth."""
     L = _lib.lib()
     _declare(L)
     radius = 0.5 * geo.n * geo.d
@@ -86,8 +88,11 @@ def simulate(geo, seeds, i0=1e5, sub=8, noise_seed=0):
     _lib.check(L.sgd_ellipse_sinograms(ell.ctypes.data, 10, len(seeds), geo.views, geo.nu, geo.du, geo.lsd, geo.lso,
                                        ang.ctypes.data, sub, float(i0), int(noise_seed), sino.data_ptr(),
                                        torch.cuda.current_stream().cuda_stream), "sgd_ellipse_sinograms")
-    truth = np.stack([ellipse_phantom(geo.n, geo.n, geo.d, geo.d, seed=s) for s in seeds]).astype(np.float32)
-    return torch.tensor(truth, device="cuda"), sino, ell
+    if truth == "average":
+        t = np.stack([ellipse_phantom_average(geo.n, geo.n, geo.d, geo.d, seed=s) for s in seeds])
+        return torch.tensor(t, dtype=torch.float64, device="cuda"), sino, ell
+    t = np.stack([ellipse_phantom(geo.n, geo.n, geo.d, geo.d, seed=s) for s in seeds]).astype(np.float32)
+    return torch.tensor(t, device="cuda"), sino, ell
 
 
 class ASDPOCS:
@@ -188,6 +193,25 @@ def plain_curve(solver, sino, truth, iters, every=5, info=None):
     return curve
 
 
+def plain_converged(solver, sino, truth, max_iters, every=5, window=10, tol=1e-3):
+    """Plain ASD-POCS until its mean RMSE has changed by less than `tol`
+    (relative) over the last `window` iterations, checked every `every`
+    iterations (window a multiple of every), or `max_iters`: (iterations, GPU
+    ms of the iterations alone, mean RMSE, curve).  The rule fixes "plain's
+    final RMSE" by the method's own convergence instead of an arbitrary
+    iteration count."""
+    solver.set_data(sino)
+    curve, ms, done = [(0, 0.0, float(rmse(solver.images(), truth).mean()))], 0.0, 0
+    back = window // every
+    while done < max_iters:
+        ms += timed(lambda: solver.run(every))
+        done += every
+        curve.append((done, ms, float(rmse(solver.images(), truth).mean())))
+        if len(curve) > back and abs(curve[-1][2] - curve[-1 - back][2]) < tol * curve[-1][2]:
+            break
+    return done, ms, curve[-1][2], curve
+
+
 def make_pairs(geo, seeds, iters, k_in, count=64, noise_seed=0, nonneg=False):
     """Training pairs from plain ASD-POCS for the phantoms `seeds`, `count` at
     a time: (iterate after k_in iterations, iterate after `iters`)."""
@@ -216,7 +240,9 @@ def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0, lr_final=None, checkp
     Adam moments and step), the shuffling generator's state and the losses so
     far are written there; if the file exists when train() starts, training
     resumes after its last epoch and continues exactly as the uninterrupted
-    run would (same batches, same step sizes)."""
+    run would (same batches, same step sizes); a checkpoint of a run with
+    other epochs, sample count, batch, seed or step sizes is refused.  The
+    loss of an epoch is the mean over the samples it trained on."""
     gen = torch.Generator().manual_seed(seed)
     n = x.shape[0]
     losses = []
@@ -224,7 +250,8 @@ def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0, lr_final=None, checkp
     start = 0
     if checkpoint is not None and os.path.exists(checkpoint):
         ck = torch.load(checkpoint, map_location="cpu", weights_only=True)
-        if ck["epochs"] != epochs or ck["n"] != n or ck["batch"] != batch or ck["seed"] != seed:
+        if (ck["epochs"] != epochs or ck["n"] != n or ck["batch"] != batch or ck["seed"] != seed
+                or ck.get("lr") != lr0 or ck.get("lr_final") != lr_final):
             raise ValueError(f"checkpoint {checkpoint} was written by another training run")
         net.load_state_dict(ck["net"])
         gen.set_state(ck["generator"])
@@ -235,15 +262,17 @@ def train(net, x, t, epochs=10, batch=16, lr=1e-3, seed=0, lr_final=None, checkp
             lr = lr_final + 0.5 * (lr0 - lr_final) * (1.0 + math.cos(math.pi * ep / (epochs - 1)))
         perm = torch.randperm(n, generator=gen)
         tot = 0.0
-        for k in range(0, n - batch + 1, batch):
+        used = n - n % batch  # the last n % batch samples of the permutation sit out this epoch
+        for k in range(0, used, batch):
             idx = perm[k:k + batch].to(x.device)
             loss = net.train_step(x[idx].unsqueeze(1), t[idx].unsqueeze(1), lr=lr)
             tot += float(loss)
-        losses.append(tot / n)
+        losses.append(tot / max(used, 1))
         if checkpoint is not None:
             tmp = checkpoint + ".tmp"
-            torch.save({"epoch": ep + 1, "epochs": epochs, "n": n, "batch": batch, "seed": seed,
-                        "net": net.state_dict(), "generator": gen.get_state(), "losses": losses}, tmp)
+            torch.save({"epoch": ep + 1, "epochs": epochs, "n": n, "batch": batch, "seed": seed, "lr": lr0,
+                        "lr_final": lr_final, "net": net.state_dict(), "generator": gen.get_state(),
+                        "losses": losses}, tmp)
             os.replace(tmp, checkpoint)
     return losses
 
@@ -273,56 +302,80 @@ def learned_run(solver, net, sino, truth, k_in, target, max_iters, every=1, info
     return done, ms, curve
 
 
+def experiment(n=256, views=120, images=64, train_pairs=2000, k_in=5, epochs=40, batch=16, lr=1e-3, lr_final=1e-4,
+               max_iters=400, checkpoint=None, log=None):
+    """Learned warm start against plain ASD-POCS (64 fan-beam phantoms 256^2,
+    120 views, Poisson I0 = 1e5 by default).  Plain runs to the convergence
+    rule of plain_converged on a calibration batch: its iteration count K
+    makes the training targets (plain after K iterations) of `train_pairs`
+    seeded phantoms, whose inputs are plain after k_in.  On the evaluation
+    batch plain runs to the same rule; its RMSE there, against the FP64
+    pixel-averaged phantoms, is the target, and the learned run (k_in plain
+    iterations, the network, then ASD-POCS) stops on reaching it.  GPU times
+    are CUDA-event times of the iterations and the network.  Returns a dict."""
+    from .cnn import WarmStartCNN
+    say = log or (lambda *a: None)
+    geo = Geometry(n, views)
+    # calibration batch: plain's iterations to convergence
+    ctruth, csino, _ = simulate(geo, list(range(5000, 5000 + images)), noise_seed=555, truth="average")
+    solver = ASDPOCS(geo, images, nonneg=False)
+    K, _, _, _ = plain_converged(solver, csino, ctruth, max_iters)
+    say(f"calibration: plain converges after {K} iterations")
+    t0 = time.perf_counter()
+    xs, ts = make_pairs(geo, list(range(1000, 1000 + train_pairs)), K, k_in)
+    t_pairs = time.perf_counter() - t0
+    net = WarmStartCNN(seed=0)
+    t0 = time.perf_counter()
+    losses = train(net, xs, ts, epochs=epochs, batch=batch, lr=lr, lr_final=lr_final, checkpoint=checkpoint)
+    t_train = time.perf_counter() - t0
+    say(f"pairs {t_pairs:.1f} s, training {t_train:.1f} s")
+    del xs, ts
+    truth, sino, _ = simulate(geo, list(range(images)), noise_seed=999, truth="average")
+    # one untimed pass of the network at the reconstruction's shape: a
+    # deployed network is loaded and its kernels initialised once
+    net.forward(torch.zeros((images, 1, n, n), device="cuda"))
+    torch.cuda.synchronize()
+    it_p, ms_p, target, curve_p = plain_converged(solver, sino, truth, max_iters)
+    solver.set_data(sino, hist_cap=it_p)
+    solver.run(it_p)
+    res_p = [float(r) for r in solver.history(it_p)[:, :, 0].mean(axis=1)]
+    info = {}
+    it_l, ms_l, curve_l = learned_run(solver, net, sino, truth, k_in, target, max_iters, info=info)
+    solver.status()
+    return {
+        "workload": f"{images} fan-beam phantoms {n}^2 at {geo.d} mm, {views} views, {geo.nu} bins at {geo.du} mm, "
+                    f"SOD {LSO} mm, SDD {LSD} mm, Poisson I0=1e5; plain ASD-POCS to convergence vs the CNN warm "
+                    f"start after {k_in} plain iterations",
+        "rmse_truth": "FP64 pixel averages of the ellipse phantoms (8 x 8 samples per pixel), FP64 RMSE",
+        "convergence_rule": "mean RMSE changed by < 1e-3 (relative) over 10 iterations, checked every 5",
+        "calibration_iters": K,
+        "plain": {"iters": it_p, "gpu_ms": ms_p, "rmse": target, "curve": curve_p, "data_residual": res_p},
+        "learned": {"plain_iters_before_net": k_in, "iters_after_net": it_l, "gpu_ms": ms_l,
+                    "net_ms": info["net_ms"], "data_residual": info.get("residual", []), "rmse": curve_l[-1][2],
+                    "curve": curve_l, "reached": curve_l[-1][2] <= target},
+        "time_ratio": ms_l / ms_p,
+        "training": {"pairs": train_pairs, "target_iters": K, "epochs": epochs, "loss": losses, "pairs_s": t_pairs,
+                     "train_s": t_train},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--views", type=int, default=120)
     ap.add_argument("--images", type=int, default=64)
     ap.add_argument("--train", type=int, default=2000)
-    ap.add_argument("--iters", type=int, default=100)
     ap.add_argument("--k-in", type=int, default=5)
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--lr-final", type=float, default=1e-4)
+    ap.add_argument("--max-iters", type=int, default=400)
     ap.add_argument("--checkpoint", default=None,
                     help="file for per-epoch training checkpoints; an existing one is resumed")
     args = ap.parse_args()
-    from .cnn import WarmStartCNN
-    geo = Geometry(args.n, args.views)
-    t0 = time.perf_counter()
-    xs, ts = make_pairs(geo, list(range(1000, 1000 + args.train)), args.iters, args.k_in)
-    t_pairs = time.perf_counter() - t0
-    net = WarmStartCNN(seed=0)
-    t0 = time.perf_counter()
-    losses = train(net, xs, ts, epochs=args.epochs, batch=args.batch, lr=args.lr, lr_final=args.lr_final,
-                   checkpoint=args.checkpoint)
-    t_train = time.perf_counter() - t0
-    del xs, ts
-    truth, sino, _ = simulate(geo, list(range(args.images)), noise_seed=999)
-    solver = ASDPOCS(geo, args.images, nonneg=False)
-    # one untimed pass of the network at the reconstruction's shape: a
-    # deployed network is loaded and its kernels initialised once
-    net.forward(torch.zeros((args.images, 1, args.n, args.n), device="cuda"))
-    torch.cuda.synchronize()
-    pinfo = {}
-    plain = plain_curve(solver, sino, truth, args.iters, info=pinfo)
-    target = plain[-1][2]
-    info = {}
-    it_l, ms_l, curve_l = learned_run(solver, net, sino, truth, args.k_in, target, args.iters, info=info)
-    solver.status()
-    line = {
-        "workload": f"{args.images} fan-beam phantoms {args.n}^2 at {geo.d} mm, {args.views} views, {geo.nu} bins, "
-                    f"Poisson I0=1e5; plain ASD-POCS {args.iters} iterations vs CNN warm start after {args.k_in}",
-        "plain": {"iters": args.iters, "gpu_ms": plain[-1][1], "rmse": target, "curve": plain,
-                  "data_residual": pinfo["residual"]},
-        "learned": {"iters_after_net": it_l, "gpu_ms": ms_l, "net_ms": info["net_ms"],
-                    "data_residual": info.get("residual", []), "rmse": curve_l[-1][2],
-                    "curve": curve_l, "reached": curve_l[-1][2] <= target},
-        "time_ratio": ms_l / plain[-1][1],
-        "training": {"pairs": args.train, "epochs": args.epochs, "loss": losses, "pairs_s": t_pairs,
-                     "train_s": t_train},
-    }
+    line = experiment(args.n, args.views, args.images, args.train, args.k_in, args.epochs, args.batch, args.lr,
+                      args.lr_final, args.max_iters, args.checkpoint, log=lambda m: print(m, flush=True))
     print(json.dumps(line))
 
 

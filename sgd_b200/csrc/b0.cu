@@ -6,10 +6,12 @@
 // pmi (bit-identical to the reference's); per bin, the footprint is the
 // 3-direction box spline of layers/spline_conv.hh:239-293 with directions
 // (vx, vy, vblur) at an offset y measured from the pixel corner, vblur being
-// the bin's width at the pixel's depth.  The reference's mix of FP32 geometry
-// (including its FP32 stepping of the bin centre, sx += puv.x, :202) and FP64
-// per-bin vectors is kept; the two FP64 divisions by the source-bin distance
-// are multiplications by its FP64 reciprocals.
+// the bin's width at the pixel's depth.  The reference's FP32 geometry is
+// kept (its FP32 stepping of the bin centre, sx += puv.x, :202, and the FP32
+// products it forms); its FP64 per-bin vectors and the FP64 scalings of
+// those products, whose results it rounds to FP32 for the spline, run in
+// FP32 here (a difference of an ulp or two per value), the two divisions by
+// the source-bin distance as products with its reciprocals.
 #include <climits>
 #include <cmath>
 #include <vector>
@@ -17,6 +19,7 @@
 #include "common.h"
 #include "hom.cuh"
 #include "proj2d_impl.cuh"
+#include "spline3.cuh"
 
 namespace sgd {
 
@@ -27,8 +30,10 @@ struct B0Basis {
     struct View {
         float pm0, pm1, pm3, pm8, pm9, pm11, puvx, singular, srcx, srcy, dtvx, dtvy, puvy, dx, dy, nx2, ny2;
     };
-    // per bin: vx, vy, a0s, sb0, 1/lsp, 1/lsp^2 (FP64)
-    static constexpr int kBinF4 = 3;
+    // per bin: vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2, 0, 0 (computed in FP64,
+    // stored in FP32: the reference's FP64 arithmetic on them ends in FP32
+    // arguments of the spline)
+    static constexpr int kBinF4 = 2;
     struct Cell {
         float ox, oy, sx, sy;  // pixel centre; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
@@ -41,13 +46,6 @@ struct B0Basis {
     __device__ static bool valid(int, int, const Fan2DParams&) { return true; }
     __device__ static void sort2(float& a, float& b) {
         if (a > b) {
-            const float t = b;
-            b = a;
-            a = t;
-        }
-    }
-    __device__ static void sort2d(float& a, float& b) {
-        if (a < b) {
             const float t = b;
             b = a;
             a = t;
@@ -80,32 +78,8 @@ struct B0Basis {
         c.sx = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
         c.sy = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
     }
-    // layers/spline_conv.hh:244-293 (T = float)
-    __device__ static float fast3(float x, const float* xi) {
-        const float h = 1.0f / xi[0];
-        const float p = xi[0] * xi[1] * xi[2];
-        const float K0 = (xi[0] - xi[1] - xi[2]) / 2.0f, K1 = (xi[0] - xi[1] + xi[2]) / 2.0f;
-        const float K2 = (xi[0] + xi[1] - xi[2]) / 2.0f, K3 = (xi[0] + xi[1] + xi[2]) / 2.0f;
-        float v;
-        if (x >= K3) v = 0.0f;
-        else if (x >= K2) v = 0.5f * (K3 - x) * (K3 - x) / p;
-        else if (x >= K1) v = ((xi[0] + xi[1]) / 2.0f - x) * xi[2] / p;
-        else if (x < -K0) v = h - (K0 * K0 + x * x) / p;
-        else if (x < K0) v = h;
-        else v = h - 0.5f * (K0 - x) * (K0 - x) / p;
-        return v;
-    }
     // layers/A_B0.cu:20-35
-    __device__ static float conv1d(float y, float v1, float v2, float v3) {
-        float vs[3];
-        y = fabsf(y - (v1 + v2 + v3) / 2.0f);
-        vs[0] = fabsf(v1), vs[1] = fabsf(v2), vs[2] = fabsf(v3);
-        sort2d(vs[1], vs[2]);
-        sort2d(vs[0], vs[1]);
-        sort2d(vs[1], vs[2]);
-        if (vs[2] > 1e-7f) return fast3(y, vs);
-        return fmaxf(0.0f, fminf(1.0f / vs[0], ((vs[0] + vs[1]) / 2.0f - y) / (vs[0] * vs[1])));
-    }
+    __device__ static float conv1d(float y, float v1, float v2, float v3) { return box3(y, v1, v2, v3); }
     // the reference's FP32 stepping of the bin centre (layers/A_B0.cu:202)
     __device__ static void skip(const View& V, Cell& c) {
         c.sx += V.puvx;
@@ -114,16 +88,15 @@ struct B0Basis {
     __device__ static float value(const View& V, Cell& c, int, const float4* t, const Fan2DParams&) {
         const float sx = c.sx, sy = c.sy;
         skip(V, c);
-        const double* b = reinterpret_cast<const double*>(t);
-        const double vx = b[0], vy = b[1], a0s = b[2], sb0 = b[3];
-        const double ilsp = b[4], ilsp2 = b[5];
+        const float4 b0 = t[0], b1 = t[1];  // vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2
         const float px = V.srcx, py = V.srcy;
-        const double r1 = (double)((c.ox - px) * (sx - px) + (c.oy - py) * (sy - py)) * ilsp2;
-        const double vblur = (a0s + sb0) * (-r1);
+        // layers/A_B0.cu:207-219: the FP32 products as the reference forms
+        // them, its FP64 scalings in FP32
+        const float r1 = ((c.ox - px) * (sx - px) + (c.oy - py) * (sy - py)) * b1.y;
+        const float vblur = (b0.z + b0.w) * (-r1);
         const float x1 = sx - px, y1 = sy - py, x2 = c.ox - 0.5f * V.dx - px, y2 = c.oy + 0.5f * V.dy - py;
-        double y = (double)(x1 * y2 - x2 * y1) * ilsp;
-        y += a0s * r1;
-        const float conv = conv1d((float)(-y), (float)vx, (float)vy, (float)vblur);
+        const float y = fmaf(b0.z, r1, (x1 * y2 - x2 * y1) * b1.x);
+        const float conv = conv1d(-y, b0.x, b0.y, vblur);
         return (conv > 1e-7f && conv == conv) ? conv : 0.f;
     }
 };
@@ -179,8 +152,7 @@ public:
         P.ni = nx;
         P.nj = ny;
         std::vector<float> view((size_t)np * B0Basis::kViewFloats, 0.f);
-        std::vector<float4> bins((size_t)np * nu * 3);
-        double* bd = reinterpret_cast<double*>(bins.data());
+        std::vector<float4> bins((size_t)np * nu * B0Basis::kBinF4);
         for (int p = 0; p < np; ++p) {
             const ViewFrame& f = geo.frames[p];
             float* v = &view[(size_t)p * B0Basis::kViewFloats];
@@ -207,8 +179,9 @@ public:
                 double sb0 = std::fabs((sx - px) * (by - py) - (bx - px) * (sy - py)) / lsp;
                 a0s /= ((ax - px) * (sx - px) + (ay - py) * (sy - py)) / (lsp * lsp);
                 sb0 /= ((bx - px) * (sx - px) + (by - py) * (sy - py)) / (lsp * lsp);
-                double* o = bd + ((size_t)p * nu + u) * 6;
-                o[0] = vx; o[1] = vy; o[2] = a0s; o[3] = sb0; o[4] = 1.0 / lsp; o[5] = 1.0 / (lsp * lsp);
+                float4* o = &bins[((size_t)p * nu + u) * B0Basis::kBinF4];
+                o[0] = make_float4((float)vx, (float)vy, (float)a0s, (float)sb0);
+                o[1] = make_float4((float)(1.0 / lsp), (float)(1.0 / (lsp * lsp)), 0.f, 0.f);
             }
         }
         finish_init(view, bins);

@@ -4,7 +4,7 @@
 //
 // Per voxel (ix, iy, iz) and view: the in-plane B1 footprint conv(u) of the
 // column (ix, iy) over the bins u of its +-1 voxel support (the reference's
-// FP32 formula, its FP32 bin stepping included), times the integral gamma(v)
+// FP32 formula, its FP32 bin stepping included), times the integral g(v)
 // of the axial trapezoid (corners ix +- 1 at iy, iz +- 1/2 through pmi) over
 // bin row v, times vol * dx dy dz * sqrt(r3^2 / r2^2).  The reference's
 // forward also multiplies by 2 / (trapezoid width) (:210), its backward does
@@ -12,38 +12,61 @@
 //   mode 0 "reference": both kernels as the reference (parity);
 //   mode 1 "adjoint":   the forward as the reference and the back projector its
 //                       exact transpose (dot-product test, autograd).
-// conv(u) does not depend on z; both kernels compute it once per column and
-// view and reuse it for the column's voxels (the reference recomputes it per
-// voxel).  Voxels are processed in the reference's z chunks of 32 so that the
-// FP32 stepping oz += dz is identical.
 //
-//   b1_3d_forward_kernel  a CTA per 16 x 16 columns x one z chunk; per view the
-//                         CTA's (u, v) window (block min/max of its voxels'
-//                         ranges) is accumulated in shared memory and flushed
-//                         to an FP64 sinogram, or added directly when a window
-//                         is larger than the shared buffer.
-//   b1_3d_back_kernel     gather: a thread per column and 16 voxels of a chunk,
-//                         FP64 accumulators, each voxel written once.
+// conv(u) does not depend on z and g(v) does not depend on u, so per view and
+// column the projection factors through the column's axial profile:
+//   forward   proj(u, v) += conv(u) A(v),  A(v) = sum_z C(z) w(z) g(z, v)
+//   back      vol(z) += w(z) sum_v g(z, v) B(v),  B(v) = sum_u conv(u) proj(u, v)
+// (w the reference's amplitude), evaluated by
+//   b1_3d_fwd_kernel   a CTA per (view, block of 16 u bins).  Its columns are
+//                      the block's in-plane strip (the 2D kernels' plan, B1
+//                      support); a warp takes one column at a time, its lanes
+//                      the column's voxels (z contiguous in a transposed copy
+//                      of the volume, one reference z chunk of 32 per pass),
+//                      and builds A in shared memory; after each batch of one
+//                      column per warp the threads, each owning detector
+//                      rows, add conv(u) A(v) into the block's FP64
+//                      accumulators.  Every bin is written once: no atomics
+//                      in global memory.
+//   b1_3d_back_kernel  a CTA per 4 x 2 columns (a warp each) and 256 voxels
+//                      of z (a lane each owns 8, FP64 accumulators in
+//                      registers).  Per view the CTA's window of 16 u bins
+//                      x all v rows is staged by a TMA tensor load (double
+//                      buffered on mbarriers with bounded waits); each warp
+//                      forms B of its column from it and each lane its
+//                      voxels' sums.  Every voxel is written once.
+// The reference's z chunks of 32 are kept: the FP32 stepping oz += dz from a
+// chunk's start, and its `return` at the first voxel whose trapezoid starts
+// beyond the detector top, which ends the rest of that chunk (a warp ballot
+// here).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "common.h"
 #include "fan_geometry.h"
+#include "proj2d.h"
+#include "tensor_map.h"
+#include "tma.cuh"
 
 namespace sgd {
 
 namespace {
 
 constexpr int kZChunk = 32;      // the reference's Z_SIZE (layers/A_B1_3D.cu:25)
-constexpr int kTile = 16;        // forward: 16 x 16 columns per CTA
-constexpr int kWinCap = 6144;    // forward: shared (u, v) window, floats
-constexpr int kBackZ = 16;       // back: voxels of a chunk per thread
-constexpr int kMaxConv = 8;      // cached in-plane footprints per column
-constexpr int kMaxRows = 4;      // cached axial integrals per voxel (v rows)
 constexpr float kEps = 1e-7f;
+constexpr int kUB = 16;          // forward: u bins per block
+constexpr int kFW = 8;           // forward: warps, columns per batch
+constexpr int kMaxLines = 2048;  // forward: strip lines held in shared memory
+constexpr int kTX = 4, kTY = 2;  // back: columns per CTA (a warp each)
+constexpr int kWin = 16;         // back: staged u window (bins)
+constexpr int kRowBox = 192;     // back: rows per TMA box
+constexpr int kZPer = 8;         // back: voxels per lane (z = l + 32 k)
+constexpr uint32_t kWaitLimit3 = 1u << 22;
 
 struct View3 {
     float pm[12];
@@ -151,14 +174,6 @@ __device__ __forceinline__ float gamma_trap(float s1, float s2, const float* us)
     return g;
 }
 
-// gamma_trap of rows minv .. minv + kMaxRows - 1 (those up to maxv), once per
-// voxel: the (u, v) loops below reuse them for every u.  Unrolled so that
-// they stay in registers.
-__device__ __forceinline__ void voxel_rows(const float* vs, int minv, int maxv, float* g) {
-#pragma unroll
-    for (int r = 0; r < kMaxRows; ++r) g[r] = (minv + r <= maxv) ? gamma_trap((float)(minv + r), minv + r + 1.0f, vs) : 0.f;
-}
-
 struct Column {
     float ox, oy, v1, v2, v3, v4;
     int minu, maxu;
@@ -224,20 +239,6 @@ __device__ __forceinline__ float column_conv_at(const View3& V, const Column& c,
     return lc1d(x1 * sgn, x2, fmaxf(v.x, v.y), fminf(v.x, v.y));
 }
 
-// the first kMaxConv footprints of the column, cached; bins beyond (only the
-// reference's degenerate ranges of odd-45-degree views reach them) are
-// recomputed by column_conv_at
-__device__ __forceinline__ void column_conv(const View3& V, const Column& c, const float2* __restrict__ vecs, int nu,
-                                            float* conv) {
-    const int n = min(c.maxu - c.minu + 1, kMaxConv);
-    for (int ti = 0; ti < n; ++ti) conv[ti] = column_conv_at(V, c, vecs, nu, ti);
-}
-
-__device__ __forceinline__ float conv_of(const View3& V, const Column& c, const float2* __restrict__ vecs, int nu,
-                                         const float* conv, int ti) {
-    return ti < kMaxConv ? conv[ti] : column_conv_at(V, c, vecs, nu, ti);
-}
-
 // axial trapezoid of voxel iz (layers/A_B1_3D.cu:188-205); false: beyond the
 // detector top (the reference returns for the rest of its chunk)
 __device__ __forceinline__ bool voxel_v(const View3& V, const Column& c, int iz, int nv, float* vs, int& minv,
@@ -262,6 +263,7 @@ __device__ __forceinline__ bool voxel_v(const View3& V, const Column& c, int iz,
     return true;
 }
 
+
 struct Geo3 {
     int nx, ny, nz, np, nu, nv;
     float dx, dy, dz;
@@ -269,190 +271,391 @@ struct Geo3 {
     const float2* vecs;   // [np][nu]
 };
 
-__global__ void __launch_bounds__(kTile * kTile, 6) b1_3d_forward_kernel(Geo3 G, const float* __restrict__ vol,
-                                                                     double* __restrict__ proj64) {
-    __shared__ float s_acc[kWinCap];
-    __shared__ int s_win[4];
-    const int ix = blockIdx.x * kTile + threadIdx.x, iy = blockIdx.y * kTile + threadIdx.y;
-    const int z_start = blockIdx.z * kZChunk, z_end = min(G.nz, z_start + kZChunk);
-    const int tid = threadIdx.y * kTile + threadIdx.x;
-    const bool mine = ix < G.nx && iy < G.ny;
-    const size_t plane = (size_t)G.nx * G.ny;
-    for (int p = 0; p < G.np; ++p) {
-        View3 V;
-        load_view3(G.view + (size_t)p * 20, V);
-        Column c;
-        float conv[kMaxConv];
-        int ncv = 0;
-        int ulo = 1 << 30, uhi = -1, vlo = 1 << 30, vhi = -1;
-        const float2* vecs = G.vecs + (size_t)p * G.nu;
-        if (mine) {
-            column_setup(V, ix, iy, G.nx, G.ny, G.nu, G.dx, G.dy, c);
-            column_conv(V, c, vecs, G.nu, conv);
-            ncv = c.maxu - c.minu + 1;
-            // v extent of the chunk: trapezoids at its first and last voxels
-            float vs[4];
-            int a, b;
-            if (voxel_v(V, c, z_start, G.nv, vs, a, b)) {
-                vlo = min(vlo, a); vhi = max(vhi, b);
-            }
-            if (voxel_v(V, c, z_end - 1, G.nv, vs, a, b)) {
-                vlo = min(vlo, a); vhi = max(vhi, b);
-            } else {
-                vhi = G.nv - 1;
-            }
-            ulo = c.minu;
-            uhi = c.minu + ncv - 1;
-        }
-        if (tid == 0) {
-            s_win[0] = 1 << 30; s_win[1] = -1; s_win[2] = 1 << 30; s_win[3] = -1;
-        }
-        __syncthreads();
-        if (mine && vhi >= vlo) {
-            atomicMin(&s_win[0], ulo); atomicMax(&s_win[1], uhi);
-            atomicMin(&s_win[2], vlo); atomicMax(&s_win[3], vhi);
-        }
-        __syncthreads();
-        const int wul = s_win[0], wuh = s_win[1], wvl = s_win[2], wvh = s_win[3];
-        const int wu = wuh - wul + 1, wv = wvh - wvl + 1;
-        const bool in_smem = wu > 0 && wv > 0 && wu * wv <= kWinCap;
-        if (in_smem)
-            for (int e = tid; e < wu * wv; e += kTile * kTile) s_acc[e] = 0.f;
-        __syncthreads();
-        if (mine && wu > 0 && wv > 0) {
-            float* dp = nullptr;
-            double* gp = proj64 + (size_t)p * G.nu * G.nv;
-            float oz = (z_start - 0.5f * (G.nz - 1)) * G.dz;
-            for (int iz = z_start; iz < z_end; ++iz, oz += G.dz) {
-                const float C0 = vol[(size_t)iz * plane + (size_t)iy * G.nx + ix];
-                float vs[4];
-                int minv, maxv;
-                if (!voxel_v(V, c, iz, G.nv, vs, minv, maxv)) break;
-                if (C0 == 0.f) continue;
-                const float px = V.srcx, py = V.srcy, pz = V.srcz;
-                const float weight = sqrtf(((c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py) + (oz - pz) * (oz - pz)) /
-                                           ((c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py)));
-                const float C = C0 * weight * (2 / (((vs[3] - vs[0]) + (vs[2] - vs[1]))));
-                auto add = [&](int u, int j, float val, float g) {
-                    if (!(g > kEps)) return;
-                    if (in_smem) {
-                        dp = s_acc + (j - wvl) * wu + (u - wul);
-                        atomicAdd(dp, val * g);
-                    } else {
-                        atomicAdd(gp + (size_t)j * G.nu + u, (double)(val * g));
-                    }
-                };
-                if (maxv - minv < kMaxRows) {
-                    float gr[kMaxRows];
-                    voxel_rows(vs, minv, maxv, gr);
-                    for (int ti = 0; ti < ncv; ++ti) {
-                        const float val = conv_of(V, c, vecs, G.nu, conv, ti) * C;
-                        if (!(val == val)) continue;
+// Launch tables of the new kernels.
+struct Plan3 {
+    const float4* strips;  // [np][nblk][2]: forward block strips (fan2d.cuh record)
+    int nblk;
+    const int* twin;       // [tiles][np]: back window's first bin (a multiple of 4), -1: read global memory
+    int tiles_x, tiles_y;
+    int* err;              // bounded-wait status, 0 = ok
+};
+
+// Axial footprint of voxel iz of column c (layers/A_B1_3D.cu:188-210): the
+// trapezoid vs[0..3] in v, its first and last rows, the reference's axial
+// normalisation 2 / width and the ramp factors of its row integrals (fast
+// reciprocals: within an ulp or two of the reference's divisions).  Returns
+// false when the trapezoid starts beyond the detector top.
+struct Axial {
+    float vs[4];
+    float k01, k23, width2;
+    int minv, maxv;
+};
+
+__device__ __forceinline__ bool axial(const View3& V, const Column& c, int iz, int nv, Axial& a) {
+    const float* pm = V.pm;
+    const float signz1 = (iz - 0.5f), signz2 = (iz + 0.5f);
+    float* vs = a.vs;
+    vs[0] = __fdividef(c.v1 + pm[6] * signz1, c.v3 + pm[10] * signz1);
+    vs[1] = __fdividef(c.v1 + pm[6] * signz2, c.v3 + pm[10] * signz2);
+    vs[2] = __fdividef(c.v2 + pm[6] * signz1, c.v4 + pm[10] * signz1);
+    vs[3] = __fdividef(c.v2 + pm[6] * signz2, c.v4 + pm[10] * signz2);
+    if (V.singular != 0.f) {
+        const float r = __fdividef(1.0f, V.puvy);
 #pragma unroll
-                        for (int r = 0; r < kMaxRows; ++r)
-                            if (minv + r <= maxv) add(c.minu + ti, minv + r, val, gr[r]);
-                    }
-                } else {
-                    for (int ti = 0; ti < ncv; ++ti) {
-                        const float val = conv_of(V, c, vecs, G.nu, conv, ti) * C;
-                        if (!(val == val)) continue;
-                        for (int j = minv; j <= maxv; ++j)
-                            add(c.minu + ti, j, val, gamma_trap((float)j, j + 1.0f, vs));
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        if (in_smem) {
-            double* gp = proj64 + (size_t)p * G.nu * G.nv;
-            for (int e = tid; e < wu * wv; e += kTile * kTile) {
-                const float a = s_acc[e];
-                if (a != 0.f) {
-                    const int j = wvl + e / wu, u = wul + e % wu;
-                    atomicAdd(gp + (size_t)j * G.nu + u, (double)a);
-                }
-            }
-        }
-        __syncthreads();
+        for (int k = 0; k < 4; ++k) vs[k] = (vs[k] * 1.5f - 1.0f) * r;
     }
+    sort4(vs);
+    if (!(vs[0] < (float)nv)) return false;
+    a.minv = min(max(0, (int)floorf(vs[0])), nv - 1);
+    a.maxv = min(max(0, (int)floorf(vs[3])), nv - 1);
+    a.k01 = __fdividef(0.5f, vs[1] - vs[0]);
+    a.k23 = __fdividef(0.5f, vs[3] - vs[2]);
+    a.width2 = __fdividef(2.0f, (vs[3] - vs[0]) + (vs[2] - vs[1]));
+    return true;
+}
+
+// layers/A_B1_3D.cu:30-66 over row [s1, s1 + 1]
+__device__ __forceinline__ float row_gamma(const Axial& a, float s1) {
+    const float* us = a.vs;
+    const float s2 = s1 + 1.0f;
+    float g = 0.0f, tmp, b1, b2;
+    b1 = fmaxf(s1, us[0]);
+    b2 = fminf(s2, us[1]);
+    tmp = (b2 > b1) ? a.k01 * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0])) : 0.0f;
+    if (tmp == tmp) g += tmp;
+    b1 = fmaxf(s1, us[1]);
+    b2 = fminf(s2, us[2]);
+    tmp = (b2 > b1) ? b2 - b1 : 0.0f;
+    if (tmp == tmp) g += tmp;
+    b1 = fmaxf(s1, us[2]);
+    b2 = fminf(s2, us[3]);
+    tmp = (b2 > b1) ? a.k23 * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3])) : 0.0f;
+    if (tmp == tmp) g += tmp;
+    return g;
+}
+
+// The reference's amplitude sqrt(r3^2 / r2^2) of a voxel at height oz.
+__device__ __forceinline__ float amplitude(float ir2, float dzz) { return sqrtf(fmaf(dzz * dzz, ir2, 1.0f)); }
+
+// Lane l's voxel of a 32-voxel pass is live unless it or an earlier voxel of
+// its reference chunk started beyond the detector top (the reference's
+// `return`, layers/A_B1_3D.cu:202): `beyond` is the pass's ballot.
+__device__ __forceinline__ bool chunk_live(unsigned beyond, int l) { return (beyond & ((2u << l) - 1u)) == 0u; }
+
+// oz of voxel iz: the reference steps it by dz from its 32-voxel chunk's start.
+__device__ __forceinline__ float chunk_oz(int iz, int nz, float dz) {
+    const int z0 = iz & ~(kZChunk - 1);
+    float oz = (z0 - 0.5f * (nz - 1)) * dz;
+    for (int q = z0; q < iz; ++q) oz += dz;
+    return oz;
+}
+
+// vol [z][y][x] -> volT [y][x][z]
+__global__ void to_columns_kernel(const float* __restrict__ vol, float* __restrict__ volT, int nx, int ny, int nz) {
+    __shared__ float t[32][33];
+    const int col0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
+    const int ncol = nx * ny;
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int z = z0 + k, col = col0 + threadIdx.x;
+        if (z < nz && col < ncol) t[k][threadIdx.x] = vol[(size_t)z * ncol + col];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int col = col0 + k, z = z0 + threadIdx.x;
+        if (z < nz && col < ncol) volT[(size_t)col * nz + z] = t[threadIdx.x][k];
+    }
+}
+
+__host__ __device__ constexpr size_t fwd3_smem(int nv, int nz) {
+    return (size_t)kUB * nv * 8 + (size_t)kFW * nv * 4 + kFW * kUB * 4 + (kMaxLines + 1) * 4 + (size_t)nz * 4;
+}
+
+__global__ void __launch_bounds__(kFW * 32, 2) b1_3d_fwd_kernel(Geo3 G, Plan3 K, const float* __restrict__ volT,
+                                                             float* __restrict__ proj, float scale) {
+    extern __shared__ __align__(16) unsigned char f3_smem[];
+    const int nv = G.nv, nz = G.nz;
+    double* acc = reinterpret_cast<double*>(f3_smem);   // [kUB][nv]
+    float* A = reinterpret_cast<float*>(acc + kUB * nv);  // [kFW][nv]: each warp's column profile
+    float* cs = A + kFW * nv;                             // [kFW][kUB]: its conv per block bin
+    int* pref = reinterpret_cast<int*>(cs + kFW * kUB);   // [kMaxLines + 1]: candidates before each line
+    float* soz = reinterpret_cast<float*>(pref + kMaxLines + 1);  // [nz]
+    __shared__ int s_act[kFW][2];
+    const int k = blockIdx.x, p = blockIdx.y, tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int u0 = k * kUB, nb = min(kUB, G.nu - u0);
+
+    for (int e = tid; e < kUB * nv; e += blockDim.x) acc[e] = 0.0;
+    for (int z = tid; z < nz; z += blockDim.x) soz[z] = chunk_oz(z, nz, G.dz);
+    const float4* st = K.strips + ((size_t)p * K.nblk + k) * 2;
+    const float4 s0 = __ldg(st), s1 = __ldg(st + 1);
+    const bool jmaj = s0.x > 0.5f;
+    const int nmin = jmaj ? G.nx : G.ny;
+    const int mlo = (int)s1.z, nlines = (int)s1.w - mlo + 1;
+    auto span = [&](int m, int& nlo, int& nhi) {
+        const float fm = (float)m;
+        const float na = fmaf(s0.z, fm, s0.y), nbb = fmaf(s1.x, fm, s0.w);
+        nlo = max(0, (int)ceilf(fminf(na, nbb) - s1.y));
+        nhi = min(nmin - 1, (int)floorf(fmaxf(na, nbb) + s1.y));
+    };
+    // candidates per line, then their running sum (warp 0)
+    for (int t = tid; t < nlines; t += blockDim.x) {
+        int a, b;
+        span(mlo + t, a, b);
+        pref[t + 1] = max(0, b - a + 1);
+    }
+    __syncthreads();
+    if (w == 0) {
+        int carry = 0;
+        if (l == 0) pref[0] = 0;
+        for (int t0 = 0; t0 < nlines; t0 += 32) {
+            int v = t0 + l < nlines ? pref[t0 + l + 1] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int n = __shfl_up_sync(0xffffffffu, v, o);
+                if (l >= o) v += n;
+            }
+            if (t0 + l < nlines) pref[t0 + l + 1] = v + carry;
+            carry += __shfl_sync(0xffffffffu, v, 31);
+        }
+    }
+    __syncthreads();
+    const int total = nlines > 0 ? pref[nlines] : 0;
+
+    View3 V;
+    load_view3(G.view + (size_t)p * 20, V);
+    const float2* vecs = G.vecs + (size_t)p * G.nu;
+    float* Aw = A + w * nv;
+    for (int base = 0; base < total; base += kFW) {
+        const int idx = base + w;
+        int blo = 1, bhi = 0;
+        if (idx < total) {
+            int lo = 0, hi = nlines;  // pref[lo] <= idx < pref[hi]
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (pref[mid] <= idx) lo = mid;
+                else hi = mid;
+            }
+            int nlo, nhi;
+            span(mlo + lo, nlo, nhi);
+            const int n = nlo + (idx - pref[lo]), m = mlo + lo;
+            const int ix = jmaj ? n : m, iy = jmaj ? m : n;
+            Column c;
+            column_setup(V, ix, iy, G.nx, G.ny, G.nu, G.dx, G.dy, c);
+            const int tlo = max(c.minu, u0), thi = min(c.maxu, u0 + nb - 1);
+            if (tlo <= thi) {
+                blo = tlo - u0;
+                bhi = thi - u0;
+                // the column's footprint in each of its block bins, a lane each
+                if (l < kUB) {
+                    float cv = 0.f;
+                    if (l >= blo && l <= bhi) {
+                        cv = column_conv_at(V, c, vecs, G.nu, u0 + l - c.minu);
+                        if (!(cv == cv)) cv = 0.f;  // the reference skips a NaN product (:283)
+                    }
+                    cs[w * kUB + l] = cv;
+                }
+                for (int v = l; v < nv; v += 32) Aw[v] = 0.f;
+                __syncwarp();
+                const float px = V.srcx, py = V.srcy, pz = V.srcz;
+                const float ir2 = __fdividef(1.0f, (c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py));
+                const float* colv = volT + ((size_t)iy * G.nx + ix) * nz;
+                for (int z0 = 0; z0 < nz; z0 += 32) {
+                    const int iz = z0 + l;
+                    Axial a;
+                    const bool in = iz < nz;
+                    const bool ok = in && axial(V, c, iz, nv, a);
+                    const unsigned beyond = __ballot_sync(0xffffffffu, in && !ok);
+                    if (!ok || !chunk_live(beyond, l)) continue;
+                    const float C0 = __ldg(colv + iz);
+                    if (C0 == 0.f) continue;
+                    const float C = C0 * amplitude(ir2, soz[iz] - pz) * a.width2;
+                    if (!(C == C)) continue;
+                    for (int j = a.minv; j <= a.maxv; ++j) {
+                        const float g = row_gamma(a, (float)j);
+                        if (g > kEps) atomicAdd(Aw + j, C * g);
+                    }
+                }
+            }
+        }
+        if (l == 0) {
+            s_act[w][0] = blo;
+            s_act[w][1] = bhi;
+        }
+        __syncthreads();  // every warp's A and conv of this batch
+        for (int v = tid; v < nv; v += blockDim.x) {
+#pragma unroll 1
+            for (int q = 0; q < kFW; ++q) {
+                const int b0 = s_act[q][0], b1 = s_act[q][1];
+                if (b1 < b0) continue;
+                const float av = A[q * nv + v];
+                if (av == 0.f) continue;
+                for (int b = b0; b <= b1; ++b) {
+                    const float cv = cs[q * kUB + b];
+                    if (cv != 0.f) acc[b * nv + v] = fma((double)cv, (double)av, acc[b * nv + v]);
+                }
+            }
+        }
+        __syncthreads();  // before the warps overwrite A
+    }
+    for (int e = tid; e < nb * nv; e += blockDim.x) {
+        const int v = e / nb, b = e - v * nb;
+        proj[((size_t)p * nv + v) * G.nu + u0 + b] = (float)acc[b * nv + v] * scale;
+    }
+}
+
+__host__ __device__ constexpr int rows_padded(int nv) { return (nv + kRowBox - 1) / kRowBox * kRowBox; }
+
+// 128 bytes of slack: the staging buffer is placed on a 128-byte boundary
+__host__ __device__ constexpr size_t back3_smem(int nv) {
+    return 128 + (size_t)2 * rows_padded(nv) * kWin * 4 + (size_t)kTX * kTY * nv * 4 + 16;
 }
 
 // mode 0: the reference's backward (no 2/width factor, conv > 1e-7 kept,
-// single-bin u or v ranges skipped); mode 1: the exact transpose of the forward
-__global__ void __launch_bounds__(256, 4) b1_3d_back_kernel(Geo3 G, const float* __restrict__ proj,
-                                                         float* __restrict__ vol, int mode) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int per_col = (G.nz + kBackZ - 1) / kBackZ;
-    const long long ncol = (long long)G.nx * G.ny;
-    if (t >= ncol * per_col) return;
-    const int col = (int)(t % ncol), part = (int)(t / ncol);
-    const int ix = col % G.nx, iy = col / G.nx;
-    const int z0 = part * kBackZ, z1 = min(G.nz, z0 + kBackZ);
-    const int z_start = (z0 / kZChunk) * kZChunk;  // the reference's chunk: oz is stepped from its start
-    double acc[kBackZ];
+// single-bin u or v ranges skipped); mode 1: the exact transpose of the
+// forward.  use_tma: the projection is staged through `map` (a tensor map of
+// proj, extents (nu, nv, np)); otherwise read from global memory.
+__global__ void __launch_bounds__(kTX * kTY * 32, 2) b1_3d_back_kernel(const __grid_constant__ CUtensorMap map,
+                                                                    Geo3 G, Plan3 K, const float* __restrict__ proj,
+                                                                    float* __restrict__ vol, int mode, int use_tma) {
+    extern __shared__ __align__(128) unsigned char b3_smem[];
+    const int nv = G.nv, nvp = rows_padded(nv), nboxes = nvp / kRowBox;
+    // [2][nvp][kWin], every TMA box (kRowBox rows of kWin floats, 12 KB) on a
+    // 128-byte boundary
+    float* stage = reinterpret_cast<float*>(b3_smem + ((128 - (smem_addr(b3_smem) & 127u)) & 127u));
+    float* Bs = stage + (size_t)2 * nvp * kWin;                 // [warps][nv]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(Bs + kTX * kTY * nv);
+    __shared__ int s_abort;
+    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
+    const int tile = blockIdx.y * K.tiles_x + blockIdx.x;
+    const int ix = blockIdx.x * kTX + (w % kTX), iy = blockIdx.y * kTY + (w / kTX);
+    const bool col_ok = ix < G.nx && iy < G.ny;
+    const int zbase = blockIdx.z * 32 * kZPer;
+    const int* twin = K.twin + (size_t)tile * G.np;
+    float* Bw = Bs + w * nv;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    __syncthreads();
+    // view p's window into buffer p & 1 (a plain arrival when it is read from
+    // global memory, so that every view completes one phase)
+    auto issue = [&](int p) {
+        const int ulo = use_tma ? __ldg(twin + p) : -1;
+        uint64_t* bar = &bars[p & 1];
+        if (ulo < 0) {
+            mbar_arrive_expect_tx(bar, 0);
+            return;
+        }
+        mbar_arrive_expect_tx(bar, (uint32_t)(nboxes * kRowBox * kWin * 4));
+        fence_proxy_async_smem();
+        for (int r = 0; r < nboxes; ++r)
+            tma_load_3d(stage + ((size_t)(p & 1) * nvp + (size_t)r * kRowBox) * kWin, &map, ulo, r * kRowBox, p, bar);
+    };
+    auto drain = [&](int f) {
+        if (tid == 0) {
+            mbar_wait_bounded(&bars[f & 1], (uint32_t)(f >> 1) & 1u, kWaitLimit3);
+            if (f + 1 < G.np) mbar_wait_bounded(&bars[(f + 1) & 1], (uint32_t)((f + 1) >> 1) & 1u, kWaitLimit3);
+        }
+    };
+    if (tid == 0) {
+        issue(0);
+        if (G.np > 1) issue(1);
+    }
+    double acc[kZPer];
+    float oz[kZPer];
 #pragma unroll
-    for (int k = 0; k < kBackZ; ++k) acc[k] = 0.0;
-    const float dxyz = G.dx * G.dy * G.dz;
+    for (int q = 0; q < kZPer; ++q) {
+        acc[q] = 0.0;
+        oz[q] = chunk_oz(min(zbase + 32 * q + l, G.nz - 1), G.nz, G.dz);
+    }
     for (int p = 0; p < G.np; ++p) {
+        if (!mbar_wait_bounded(&bars[p & 1], (uint32_t)(p >> 1) & 1u, kWaitLimit3)) {
+            s_abort = 1;
+            if (K.err) atomicExch(K.err, 1);
+        }
+        __syncthreads();
+        if (s_abort) {
+            drain(p);
+            return;
+        }
+        const int ulo = use_tma ? __ldg(twin + p) : -1;
+        const float* sp = stage + (size_t)(p & 1) * nvp * kWin;
+        const float* gp = proj + (size_t)p * nv * G.nu;
         View3 V;
         load_view3(G.view + (size_t)p * 20, V);
         Column c;
-        column_setup(V, ix, iy, G.nx, G.ny, G.nu, G.dx, G.dy, c);
-        if (mode == 0 && c.minu >= c.maxu) continue;  // layers/A_B1_3D.cu:404
-        float conv[kMaxConv];
-        const float2* vecs = G.vecs + (size_t)p * G.nu;
-        column_conv(V, c, vecs, G.nu, conv);
-        const int ncv = c.maxu - c.minu + 1;
-        const float* pp = proj + (size_t)p * G.nu * G.nv;
-        float oz = (z_start - 0.5f * (G.nz - 1)) * G.dz;
-        for (int iz = z_start; iz < z0; ++iz) oz += G.dz;
-        for (int iz = z0; iz < z1; ++iz, oz += G.dz) {
-            float vs[4];
-            int minv, maxv;
-            if (!voxel_v(V, c, iz, G.nv, vs, minv, maxv)) break;
-            if (mode == 0 && minv >= maxv) continue;  // :433
-            const float px = V.srcx, py = V.srcy, pz = V.srcz;
-            const float weight = sqrtf(((c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py) + (oz - pz) * (oz - pz)) /
-                                       ((c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py)));
-            float C = weight;
-            if (mode == 1) C = weight * (2 / (((vs[3] - vs[0]) + (vs[2] - vs[1]))));
-            float val = 0.f;
-            if (maxv - minv < kMaxRows) {
-                float gr[kMaxRows];
-                voxel_rows(vs, minv, maxv, gr);
-                for (int ti = 0; ti < ncv; ++ti) {
-                    const float cv = conv_of(V, c, vecs, G.nu, conv, ti);
-                    if (mode == 0 ? !(cv == cv && cv > kEps) : !(cv * C == cv * C)) continue;
-                    const float* pu = pp + (size_t)minv * G.nu + c.minu + ti;
-#pragma unroll
-                    for (int r = 0; r < kMaxRows; ++r)
-                        if (minv + r <= maxv && gr[r] > kEps) val = fmaf(__ldg(pu + (size_t)r * G.nu), gr[r] * cv, val);
+        bool active = col_ok;
+        if (active) {
+            column_setup(V, ix, iy, G.nx, G.ny, G.nu, G.dx, G.dy, c);
+            if (mode == 0 && c.minu >= c.maxu) active = false;  // layers/A_B1_3D.cu:404
+        }
+        if (active) {
+            const int ncv = c.maxu - c.minu + 1;
+            // conv of bin minu + l, then B(v) = sum over kept bins of conv(u) proj(u, v)
+            float cv = 0.f;
+            if (l < ncv) {
+                cv = column_conv_at(V, c, G.vecs + (size_t)p * G.nu, G.nu, l);
+                const bool keep = mode == 0 ? (cv == cv && cv > kEps) : (cv == cv);
+                if (!keep) cv = 0.f;
+            }
+            const int nreg = min(ncv, 32);
+            for (int v0 = 0; v0 < nv; v0 += 32) {  // uniform trip count: the shuffles below need every lane
+                const int v = v0 + l;
+                float b = 0.f;
+                for (int t = 0; t < nreg; ++t) {
+                    const float ct = __shfl_sync(0xffffffffu, cv, t);
+                    if (ct == 0.f || v >= nv) continue;
+                    const int u = c.minu + t, du = u - ulo;
+                    const float pv = (ulo >= 0 && du >= 0 && du < kWin) ? sp[(size_t)v * kWin + du]
+                                                                         : __ldg(gp + (size_t)v * G.nu + u);
+                    b = fmaf(ct, pv, b);
                 }
-            } else {
-                for (int ti = 0; ti < ncv; ++ti) {
-                    const float cv = conv_of(V, c, vecs, G.nu, conv, ti);
-                    if (mode == 0 ? !(cv == cv && cv > kEps) : !(cv * C == cv * C)) continue;
-                    const int u = c.minu + ti;
-                    for (int j = minv; j <= maxv; ++j) {
-                        const float g = gamma_trap((float)j, j + 1.0f, vs);
-                        if (g > kEps) val = fmaf(__ldg(pp + (size_t)j * G.nu + u), g * cv, val);
+                if (v < nv) Bw[v] = b;
+            }
+            if (ncv > 32) {  // the reference's degenerate ranges on snapped views: the rest, lane by lane
+                for (int v = l; v < nv; v += 32) {
+                    float b = Bw[v];
+                    for (int t = 32; t < ncv; ++t) {
+                        float ct = column_conv_at(V, c, G.vecs + (size_t)p * G.nu, G.nu, t);
+                        if (!(mode == 0 ? (ct == ct && ct > kEps) : (ct == ct))) continue;
+                        b = fmaf(ct, __ldg(gp + (size_t)v * G.nu + c.minu + t), b);
                     }
+                    Bw[v] = b;
                 }
             }
+            __syncwarp();
+            const float px = V.srcx, py = V.srcy, pz = V.srcz;
+            const float ir2 = __fdividef(1.0f, (c.ox - px) * (c.ox - px) + (c.oy - py) * (c.oy - py));
 #pragma unroll
-            for (int k = 0; k < kBackZ; ++k)
-                if (k == iz - z0) acc[k] += (double)(val * C);
+            for (int q = 0; q < kZPer; ++q) {
+                const int iz = zbase + 32 * q + l;
+                Axial a;
+                const bool in = iz < G.nz;
+                const bool ok = in && axial(V, c, iz, nv, a);
+                const unsigned beyond = __ballot_sync(0xffffffffu, in && !ok);
+                if (!ok || !chunk_live(beyond, l)) continue;
+                if (mode == 0 && a.minv >= a.maxv) continue;  // :433
+                float val = 0.f;
+                for (int j = a.minv; j <= a.maxv; ++j) {
+                    const float g = row_gamma(a, (float)j);
+                    if (g > kEps) val = fmaf(g, Bw[j], val);
+                }
+                const float C = mode == 0 ? amplitude(ir2, oz[q] - pz) : amplitude(ir2, oz[q] - pz) * a.width2;
+                acc[q] += (double)(val * C);
+            }
         }
+        __syncthreads();  // buffer p & 1 fully read
+        if (tid == 0 && p + 2 < G.np) issue(p + 2);
     }
+    if (!col_ok) return;
+    const float dxyz = G.dx * G.dy * G.dz;
     const size_t plane = (size_t)G.nx * G.ny;
 #pragma unroll
-    for (int k = 0; k < kBackZ; ++k)
-        if (z0 + k < z1) vol[(size_t)(z0 + k) * plane + col] = (float)(acc[k] * (double)dxyz);
-}
-
-__global__ void b1_3d_finish_kernel(const double* __restrict__ s64, float* __restrict__ s32, long long n, float scale) {
-    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e < n) s32[e] = (float)(s64[e] * (double)scale);
+    for (int q = 0; q < kZPer; ++q) {
+        const int iz = zbase + 32 * q + l;
+        if (iz < G.nz) vol[(size_t)iz * plane + (size_t)iy * G.nx + ix] = (float)(acc[q] * (double)dxyz);
+    }
 }
 
 // footprint evaluations the reference counts (:50): one per u bin of each
@@ -528,8 +731,9 @@ public:
         SGD_CUDA(cudaMalloc(&d_vecs_, vecs.size() * sizeof(float2)));
         SGD_CUDA(cudaMemcpy(d_vecs_, vecs.data(), vecs.size() * sizeof(float2), cudaMemcpyHostToDevice));
         G = Geo3{nx, ny, nz, np, nu, nv, (float)dx, (float)dy, (float)dz, d_view_, d_vecs_};
+        plan(lsd, lso, angles);
         const size_t nvol = (size_t)nx * ny * nz, nproj = (size_t)np * nu * nv;
-        SGD_CUDA(cudaMalloc(&d_proj64_, nproj * sizeof(double)));
+        SGD_CUDA(cudaMalloc(&d_volT_, nvol * sizeof(float)));
         SGD_CUDA(cudaMalloc(&d_vol_, nvol * sizeof(float)));
         SGD_CUDA(cudaMalloc(&d_proj_, nproj * sizeof(float)));
         SGD_CUDA(cudaMallocHost(&h_vol_, nvol * sizeof(float)));
@@ -546,25 +750,39 @@ public:
     }
     ~B1Cone() {
         if (stream) cudaStreamSynchronize(stream);
-        cudaFree(d_view_); cudaFree(d_vecs_); cudaFree(d_proj64_); cudaFree(d_vol_); cudaFree(d_proj_);
+        cudaFree(d_view_); cudaFree(d_vecs_); cudaFree(d_volT_); cudaFree(d_vol_); cudaFree(d_proj_);
+        cudaFree(d_strips_); cudaFree(d_twin_); cudaFree(d_err_);
         cudaFreeHost(h_vol_); cudaFreeHost(h_proj_);
         if (stream) cudaStreamDestroy(stream);
     }
     // vol [z][y][x], proj [p][v][u], FP32 device
     void forward_dev(const float* vol, float* proj, cudaStream_t s) {
-        const long long nproj = (long long)np * nu * nv;
-        SGD_CUDA(cudaMemsetAsync(d_proj64_, 0, nproj * sizeof(double), s));
-        dim3 grid((nx + kTile - 1) / kTile, (ny + kTile - 1) / kTile, (nz + kZChunk - 1) / kZChunk);
-        b1_3d_forward_kernel<<<grid, dim3(kTile, kTile), 0, s>>>(G, vol, d_proj64_);
+        const int ncol = nx * ny;
+        to_columns_kernel<<<dim3((ncol + 31) / 32, (nz + 31) / 32), dim3(32, 8), 0, s>>>(vol, d_volT_, nx, ny, nz);
         SGD_LAUNCH_CHECK();
-        b1_3d_finish_kernel<<<(unsigned)((nproj + 255) / 256), 256, 0, s>>>(d_proj64_, proj, nproj,
-                                                                          (float)dx * (float)dy * (float)dz);
+        b1_3d_fwd_kernel<<<dim3(K.nblk, np), kFW * 32, fwd3_smem(nv, nz), s>>>(G, K, d_volT_, proj,
+                                                                             (float)dx * (float)dy * (float)dz);
         SGD_LAUNCH_CHECK();
     }
     void backward_dev(const float* proj, float* vol, cudaStream_t s) {
-        const long long n = (long long)nx * ny * ((nz + kBackZ - 1) / kBackZ);
-        b1_3d_back_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(G, proj, vol, mode);
+        // the projection through TMA tensor loads when its rows are whole
+        // 16-byte words and it is 16-byte aligned; from global memory otherwise
+        const bool tma = (nu % 4) == 0 && (reinterpret_cast<uintptr_t>(proj) % 16) == 0;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        if (tma) map = encode_tensor_3d_f32(proj, (uint64_t)nu, (uint64_t)nv, (uint64_t)np, kWin, kRowBox, 1);
+        const dim3 grid(K.tiles_x, K.tiles_y, (nz + 32 * kZPer - 1) / (32 * kZPer));
+        b1_3d_back_kernel<<<grid, kTX * kTY * 32, back3_smem(nv), s>>>(map, G, K, proj, vol, mode, tma ? 1 : 0);
         SGD_LAUNCH_CHECK();
+    }
+    // 0, or -1 when a back projection's staging wait gave up (those voxels
+    // were left unwritten); synchronises the device and clears the flag
+    int status() {
+        int h = 0;
+        SGD_CUDA(cudaDeviceSynchronize());
+        SGD_CUDA(cudaMemcpy(&h, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
+        SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
+        return h ? -1 : 0;
     }
     void forward_host(double* b, const double* x) {
         const long long nvol = (long long)nx * ny * nz, nproj = (long long)np * nu * nv;
@@ -584,15 +802,85 @@ public:
         SGD_CUDA(cudaMemcpyAsync(d_proj_, h_proj_, nproj * sizeof(float), cudaMemcpyHostToDevice, stream));
         backward_dev(d_proj_, d_vol_, stream);
         SGD_CUDA(cudaMemcpyAsync(h_vol_, d_vol_, nvol * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        int e = 0;
+        SGD_CUDA(cudaMemcpyAsync(&e, d_err_, sizeof(int), cudaMemcpyDeviceToHost, stream));
         SGD_CUDA(cudaStreamSynchronize(stream));
+        if (e) {
+            SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
+            fail("A_B1_3D back projection: a staged view did not arrive within the bounded wait; output incomplete");
+        }
 #pragma omp parallel for schedule(static)
-        for (long long e = 0; e < nvol; ++e) x[e] = (double)h_vol_[e];
+        for (long long e2 = 0; e2 < nvol; ++e2) x[e2] = (double)h_vol_[e2];
     }
 
 private:
+    // The launch tables: the forward's block strips from the in-plane fan
+    // geometry (B1 support +-1 voxel, blocks of kUB bins), and per back tile
+    // of kTX x kTY columns and view the first bin of its staged window (a
+    // multiple of 4 for the TMA box), -1 when its bins span more than kWin.
+    void plan(double lsd, double lso, const double* angles) {
+        if (nx > kMaxLines || ny > kMaxLines) fail("A_B1_3D: %d x %d columns exceed %d per line", nx, ny, kMaxLines);
+        if (fwd3_smem(nv, nz) > 227 * 1024 || back3_smem(nv) > 227 * 1024)
+            fail("A_B1_3D: %d detector rows do not fit the kernels' shared memory", nv);
+        FanGeometry g;
+        g.init(nx, ny, np, nu, dx, dy, du, lsd, lso, angles, nullptr, nullptr);
+        auto map = [&](int p) {
+            double hw[6];
+            fan_world_hom(g, p, hw);
+            return grid_range_map(hw, g.x0(), g.dx, g.y0(), g.dy, 1.0, 1.0);
+        };
+        std::vector<float4> strips;
+        std::vector<int2> unused;
+        plan_fan2d(nx, ny, np, nu, map, strips, unused, kUB);
+        K.nblk = (nu + kUB - 1) / kUB;
+        K.tiles_x = (nx + kTX - 1) / kTX;
+        K.tiles_y = (ny + kTY - 1) / kTY;
+        std::vector<int> twin((size_t)K.tiles_x * K.tiles_y * np, -1);
+        for (int p = 0; p < np; ++p) {
+            const RangeMap m = map(p);
+            for (int ty = 0; ty < K.tiles_y; ++ty)
+                for (int tx = 0; tx < K.tiles_x; ++tx) {
+                    const double i0 = tx * kTX - 1.0, i1 = std::min(nx, (tx + 1) * kTX) - 1 + 1.0;
+                    const double j0 = ty * kTY - 1.0, j1 = std::min(ny, (ty + 1) * kTY) - 1 + 1.0;
+                    double umin = 1e300, umax = -1e300;
+                    int pos = 0, neg = 0;
+                    for (double i : {i0, i1})
+                        for (double j : {j0, j1}) {
+                            const double D = m.h[3] * i + m.h[4] * j + m.h[5];
+                            (D > 0 ? pos : neg)++;
+                            const double u = (m.h[0] * i + m.h[1] * j + m.h[2]) / D;
+                            umin = std::min(umin, u);
+                            umax = std::max(umax, u);
+                        }
+                    if (pos && neg) continue;
+                    const int lo = std::max(0, (int)std::floor(umin) - 1);
+                    const int hi = std::min(nu - 1, (int)std::floor(umax) + 1);
+                    const int ulo = lo & ~3;
+                    if (hi - ulo + 1 <= kWin) twin[((size_t)ty * K.tiles_x + tx) * np + p] = ulo;
+                }
+        }
+        SGD_CUDA(cudaMalloc(&d_strips_, strips.size() * sizeof(float4)));
+        SGD_CUDA(cudaMemcpy(d_strips_, strips.data(), strips.size() * sizeof(float4), cudaMemcpyHostToDevice));
+        SGD_CUDA(cudaMalloc(&d_twin_, twin.size() * sizeof(int)));
+        SGD_CUDA(cudaMemcpy(d_twin_, twin.data(), twin.size() * sizeof(int), cudaMemcpyHostToDevice));
+        SGD_CUDA(cudaMalloc(&d_err_, sizeof(int)));
+        SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
+        K.strips = d_strips_;
+        K.twin = d_twin_;
+        K.err = d_err_;
+        SGD_CUDA(cudaFuncSetAttribute(b1_3d_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)fwd3_smem(nv, nz)));
+        SGD_CUDA(cudaFuncSetAttribute(b1_3d_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)back3_smem(nv)));
+    }
+
+    Plan3 K{};
+    float4* d_strips_ = nullptr;
+    int* d_twin_ = nullptr;
+    int* d_err_ = nullptr;
+    float* d_volT_ = nullptr;
     float* d_view_ = nullptr;
     float2* d_vecs_ = nullptr;
-    double* d_proj64_ = nullptr;
     float* d_vol_ = nullptr;
     float* d_proj_ = nullptr;
     float* h_vol_ = nullptr;
@@ -650,5 +938,13 @@ int sgd_b1_3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void*
     });
 }
 unsigned long long sgd_b1_3d_count(void* layer) { return layer ? static_cast<B1Cone*>(layer)->count : 0ull; }
+int sgd_b1_3d_status(void* layer) {
+    return sgd::guarded_status([&] {
+        if (!layer) sgd::fail("sgd_b1_3d_status: null layer");
+        if (static_cast<B1Cone*>(layer)->status() != 0)
+            sgd::fail("A_B1_3D back projection: a staged view did not arrive within the bounded wait; "
+                      "the affected voxels were left unwritten");
+    });
+}
 
 }  // extern "C"

@@ -19,16 +19,18 @@
 // The forward's strips and the back's windows come from each cell's true
 // footprint (plan_fan2d, proj2d.h); a bin outside it has footprint exactly 0.
 // So both kernels evaluate every (cell, bin) pair with a non-zero value and
-// u in [lo, hi] (the pairs the reference keeps), through the same functions,
-// with FP64 products and sums: the pair is an exact transpose to FP64
-// rounding.
+// u in [lo, hi] (the pairs the reference keeps) through the same functions;
+// sums run in FP32 over the few terms of a lane's lines in one bin (fused
+// multiply-adds) and, in the back projection, compensated over a cell's bins
+// in a chunk of views (exact products), then in FP64, so the pair is an
+// adjoint pair well below 1e-6 even on heavily cancelling Gaussian inputs.
 //
 //   fan2d_forward_kernel  detector-block driven: a CTA per (view, block of 32
 //                         bins).  The block's ray strip is crossed by the
 //                         lines of the grid's major axis; each lane owns lines
 //                         and walks the few cells of its line inside the strip
 //                         (host-computed strip records), adding each value to
-//                         its own FP64 shared-memory column of the block's
+//                         its own FP32 shared-memory column of the block's
 //                         bins.  The columns are summed across lanes and warps
 //                         and every bin is written once: no atomics.
 //   fan2d_back_kernel     voxel driven: a CTA per tile of cells, a thread per
@@ -51,6 +53,27 @@ namespace sgd {
 
 constexpr uint32_t kF2WaitLimit = 1u << 22;
 
+// Compensated (Kahan) FP32 accumulation: s holds the sum, c the part of it
+// that is rounding error (true sum = s - c), four FP32 operations per term
+// and no conversions.  Written with round-to-nearest intrinsics so that the
+// compiler can neither fuse nor reassociate them.
+__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
+    const float y = __fsub_rn(x, c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+}
+
+// s - c += a * b with the product exact: its rounding error (one fused
+// multiply-add) joins the compensation.  Forward and back then round no
+// product differently, and the pair stays an adjoint pair to FP64 level.
+__device__ __forceinline__ void kahan_fma(float& s, float& c, float a, float b) {
+    const float p = __fmul_rn(a, b);
+    const float e = __fmaf_rn(a, b, -p);
+    kahan_add(s, c, p);
+    c = __fsub_rn(c, e);
+}
+
 // Forward block strips (host: plan_fan2d, proj2d.h).  For block k of view p,
 // along the major axis m the block's two bounding rays cross the minor axis
 // at alpha_a + beta_a m and alpha_b + beta_b m; candidate cells lie within
@@ -60,7 +83,10 @@ template <class B>
 __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DParams P, const float* __restrict__ img,
                                                                          float* __restrict__ sino, float scale) {
     constexpr int kBF4 = B::kBinF4 > 0 ? B::kBinF4 : 1;
-    __shared__ double s_acc[kF2FwdWarps][kF2Block][33];
+    // each lane's FP32 column of the block's bins over its lines (a few terms
+    // per bin), summed across lanes and warps in FP64
+    __shared__ float s_acc[kF2FwdWarps][kF2Block][33];
+    __shared__ double s_red[kF2FwdWarps][kF2Block];
     __shared__ float4 s_bin[kF2Block * kBF4];
     __shared__ __align__(16) float s_view[B::kViewFloats];
     const int k = blockIdx.x, p = blockIdx.y;
@@ -70,7 +96,7 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
     if (B::kBinF4 > 0)
         for (int e = tid; e < nb * B::kBinF4; e += blockDim.x)
             s_bin[e] = __ldg(P.bins + ((size_t)p * P.nu + u0) * B::kBinF4 + e);
-    for (int e = l; e < kF2Block * 33; e += 32) (&s_acc[w][0][0])[e] = 0.0;
+    for (int e = l; e < kF2Block * 33; e += 32) (&s_acc[w][0][0])[e] = 0.f;
     __syncthreads();
 
     typename B::View V;
@@ -80,7 +106,7 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
     const bool jmaj = s0.x > 0.5f;
     const int nmin = jmaj ? P.ni : P.nj;
     const int mlo = (int)s1.z, mhi = (int)s1.w;
-    double* acc = &s_acc[w][0][l];  // bin b at acc[33 b]: this lane's column
+    float* acc = &s_acc[w][0][l];  // bin b at acc[33 b]: this lane's column
     for (int m = mlo + tid; m <= mhi; m += blockDim.x) {
         const float fm = (float)m;
         const float na = fmaf(s0.z, fm, s0.y), nbb = fmaf(s1.x, fm, s0.w);
@@ -94,27 +120,26 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
             typename B::Cell c;
             B::setup(V, i, j, P, c);
             if (c.hi < u0 || c.lo >= u0 + nb) continue;
-            const double Cd = (double)C;
             const int ue = min(c.hi, u0 + nb - 1);
             int u = c.lo;
             for (; u < u0; ++u) B::skip(V, c);
             for (; u <= ue; ++u) {
                 const float v = B::value(V, c, u, s_bin + (u - u0) * B::kBinF4, P);
-                if (v != 0.f) acc[33 * (u - u0)] = fma((double)v, Cd, acc[33 * (u - u0)]);
+                if (v != 0.f) acc[33 * (u - u0)] = fmaf(v, C, acc[33 * (u - u0)]);
             }
         }
     }
     __syncwarp();
     if (l < nb) {
         double t = 0.0;
-        for (int q = 0; q < 32; ++q) t += s_acc[w][l][q];
-        s_acc[w][l][32] = t;
+        for (int q = 0; q < 32; ++q) t += (double)s_acc[w][l][q];
+        s_red[w][l] = t;
     }
     __syncthreads();
     if (w == 0 && l < nb) {
         double t = 0.0;
 #pragma unroll
-        for (int q = 0; q < kF2FwdWarps; ++q) t += s_acc[q][l][32];
+        for (int q = 0; q < kF2FwdWarps; ++q) t += s_red[q][l];
         sino[(size_t)p * P.nu + u0 + l] = (float)t * scale;
     }
 }
@@ -226,6 +251,8 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
             continue;
         }
         if (!mine) continue;
+        // a compensated FP32 sum within a chunk of views, FP64 across chunks
+        float csum = 0.f, ccmp = 0.f;
 #pragma unroll 1
         for (int v = 0; v < VC; ++v) {
             const int2 lh = win[st * VC + v];
@@ -242,9 +269,10 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
             for (; u < lh.x; ++u) B::skip(V, cl);
             for (; u <= ue; ++u) {
                 const float val = B::value(V, cl, u, tb + (size_t)u * B::kBinF4, P);
-                if (val != 0.f) acc = fma((double)val, (double)sb[u], acc);
+                if (val != 0.f) kahan_fma(csum, ccmp, val, sb[u]);
             }
         }
+        acc += (double)csum - (double)ccmp;
     }
     __syncthreads();
     if (s_abort) {

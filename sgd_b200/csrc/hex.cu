@@ -33,11 +33,14 @@
 
 #include "common.h"
 #include "proj2d_impl.cuh"
+#include "spline3.cuh"
 
 namespace sgd {
 
 enum HexMode : int { kH0Corrected = 0, kH0Reference = 1, kHl = 2 };
 
+// M: the HexMode, fixed per kernel so that each compiles only its own path
+template <int M>
 struct HexBasis {
     static constexpr int kViewFloats = 28;
     // [0..5] pmi 0,1,3,8,9,11 [6] puv.x [7] puv.y [8] src.x [9] src.y [10] dtv.x [11] dtv.y
@@ -49,8 +52,8 @@ struct HexBasis {
         float h0, h1, h2, h3, h4, h5;
         int mode, back;
     };
-    // per bin: va, vb, vc, 0, 1/va, 1/vb, 1/vc, 0 (FP64; a zero reciprocal
-    // where the direction is dropped)
+    // per bin, eight double words: va, vb, vc | FP32 va, vb | 1/va, 1/vb, 1/vc
+    // (a zero reciprocal where the direction is dropped) | FP32 vc, 0
     static constexpr int kBinF4 = 4;
     struct Cell {
         float ox, oy, sx, sy;  // site; centre of the next bin of the walk (FP32 stepped)
@@ -113,7 +116,7 @@ struct HexBasis {
     __device__ static void setup(const View& V, int ic, int il, const Fan2DParams& P, Cell& c) {
         c.oy = (il - V.nl2) * V.dy;
         c.ox = ((il & 1) ? (ic - V.nc3) : (ic - V.nc2)) * V.dx;
-        if (V.mode == kH0Corrected)
+        if (M == kH0Corrected)
             true_bounds(V, c.ox, c.oy, P.nu, c.lo, c.hi);
         else
             pmi_bounds(V, ic, il, P.nu, c.lo, c.hi);
@@ -121,33 +124,8 @@ struct HexBasis {
         c.sx = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
         c.sy = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
     }
-    __device__ static void sort2d(float& a, float& b) {
-        if (a < b) {
-            const float t = b;
-            b = a;
-            a = t;
-        }
-    }
-    // layers/A_H0.cu:21-36 / spline_conv.hh:244-293 (T = float)
-    __device__ static float conv3(float y, float v1, float v2, float v3) {
-        float vs[3];
-        y = fabsf(y - (v1 + v2 + v3) / 2.0f);
-        vs[0] = fabsf(v1), vs[1] = fabsf(v2), vs[2] = fabsf(v3);
-        sort2d(vs[1], vs[2]);
-        sort2d(vs[0], vs[1]);
-        sort2d(vs[1], vs[2]);
-        if (!(vs[2] > 1e-7f)) return fmaxf(0.0f, fminf(1.0f / vs[0], ((vs[0] + vs[1]) / 2.0f - y) / (vs[0] * vs[1])));
-        const float* xi = vs;
-        const float h = 1.0f / xi[0], p = xi[0] * xi[1] * xi[2];
-        const float K0 = (xi[0] - xi[1] - xi[2]) / 2.0f, K1 = (xi[0] - xi[1] + xi[2]) / 2.0f;
-        const float K2 = (xi[0] + xi[1] - xi[2]) / 2.0f, K3 = (xi[0] + xi[1] + xi[2]) / 2.0f;
-        if (y >= K3) return 0.0f;
-        if (y >= K2) return 0.5f * (K3 - y) * (K3 - y) / p;
-        if (y >= K1) return ((xi[0] + xi[1]) / 2.0f - y) * xi[2] / p;
-        if (y < -K0) return h - (K0 * K0 + y * y) / p;
-        if (y < K0) return h;
-        return h - 0.5f * (K0 - y) * (K0 - y) / p;
-    }
+    // layers/A_H0.cu:21-36 / spline_conv.hh:244-293
+    __device__ static float conv3(float y, float v1, float v2, float v3) { return box3(y, v1, v2, v3); }
     // layers/A_Hl.cu:21-46 with spline_conv.hh:151-229: divided differences of
     // truncated powers y+^(m-1), m = number of kept directions
     __device__ static double tp(double y, int m) {
@@ -222,27 +200,31 @@ struct HexBasis {
         const float ra = num / dena, rb = num / denb;
         const float ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;
         const float bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
-        if (V.mode == kH0Reference && V.back) {  // layers/A_H0.cu:331-334
+        if (M == kH0Reference && V.back) {  // layers/A_H0.cu:331-334
             const float da = hypotf(ax1 - ox, ay1 - oy), db = hypotf(bx1 - ox, by1 - oy);
             if (da > V.dt && db > V.dt && (ax1 - ox) * (bx1 - ox) >= 0.0f && (ay1 - oy) * (by1 - oy) >= 0.0f)
                 return 0.f;
         }
         const double* b = reinterpret_cast<const double*>(t);
-        const double va = b[0], vb = b[1], vc = b[2];
-        const double vblur = -sqrt((double)(bx1 - ax1) * (bx1 - ax1) + (double)(by1 - ay1) * (by1 - ay1));
-        double y = sqrt((double)(ax1 - ox) * (ax1 - ox) + (double)(ay1 - oy) * (ay1 - oy));
-        if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) y = -y;
-        double conv;
-        if (V.mode == kHl) {
+        // the edge rays' separation and the site's offset: the reference takes
+        // FP64 square roots of these FP32 differences; their FP32 roots differ
+        // by at most an ulp, far below the FP32 geometry's own rounding
+        const float dbx = bx1 - ax1, dby = by1 - ay1, dax = ax1 - ox, day = ay1 - oy;
+        const float fblur = -sqrtf(fmaf(dbx, dbx, dby * dby));
+        float fy = sqrtf(fmaf(dax, dax, day * day));
+        if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) fy = -fy;
+        if (M == kHl) {
+            const double va = b[0], vb = b[1], vc = b[2], y = (double)fy, vblur = (double)fblur;
+            double conv;
             if (fabs(vblur) > 1e-8 && fabs(va) > 1e-8 && fabs(vb) > 1e-8 && fabs(vc) > 1e-8)
                 conv = conv4_full(y, vblur, va, vb, vc, b[4], b[5], b[6]);
             else
                 conv = conv4(y, vblur, va, vb, vc);
-        } else {
-            const float fy = (float)y, fb = (float)vblur, fa = (float)va, fv = (float)vb, fc = (float)vc;
-            conv = (double)conv3(fy, fb, fa, fv) + (double)conv3(fy, fb, fv, fc) + (double)conv3(fy, fb, fc, fa);
+            return (conv == conv && conv > 0.0) ? (float)conv : 0.f;
         }
-        return (conv == conv && conv > 0.0) ? (float)conv : 0.f;
+        const float va = t[1].z, vb = t[1].w, vc = t[3].z;  // the FP32 copies
+        const float conv = conv3(fy, fblur, va, vb) + conv3(fy, fblur, vb, vc) + conv3(fy, fblur, vc, va);
+        return (conv == conv && conv > 0.f) ? conv : 0.f;
     }
 };
 
@@ -266,14 +248,15 @@ public:
         const float fdt = (float)(dt * 0.5f) * 2.0f;  // d3xyz.y * 2.0f (A_H0.cu:171)
         const float fdx = fdt * (float)kSqrt3;
         const float fdy = fdt * (mode == kHl ? 0.5f : 1.5f);
-        std::vector<float> view((size_t)np * HexBasis::kViewFloats, 0.f);
+        constexpr int kVF = HexBasis<kHl>::kViewFloats;
+        std::vector<float> view((size_t)np * kVF, 0.f);
         std::vector<float4> bins((size_t)np * nu * 4);
         double* bd = reinterpret_cast<double*>(bins.data());
         std::vector<BinHomography> hom;
         bin_homographies(geo, hom);
         for (int p = 0; p < np; ++p) {
             const ViewFrame& f = geo.frames[p];
-            float* v = &view[(size_t)p * HexBasis::kViewFloats];
+            float* v = &view[(size_t)p * kVF];
             const float* m = &geo.pmi[12 * (size_t)p];
             v[0] = m[0]; v[1] = m[1]; v[2] = m[3]; v[3] = m[8]; v[4] = m[9]; v[5] = m[11];
             v[6] = (float)f.puv[0]; v[7] = (float)f.puv[1];
@@ -299,13 +282,19 @@ public:
                 o[0] = (double)fdt * std::sin((double)th);
                 o[1] = (double)fdt * std::sin((double)th + 2.0 * kPi / 3.0);
                 o[2] = (double)fdt * std::sin((double)th + 4.0 * kPi / 3.0);
-                o[3] = 0.0;
+                // the spare fourth and eighth words hold the FP32 copies the
+                // H0 spline takes
                 for (int k = 0; k < 3; ++k) o[4 + k] = std::fabs(o[k]) > 1e-8 ? 1.0 / o[k] : 0.0;
-                o[7] = 0.0;
+                float* f = reinterpret_cast<float*>(o + 3);
+                f[0] = (float)o[0];
+                f[1] = (float)o[1];
+                float* g = reinterpret_cast<float*>(o + 7);
+                g[0] = (float)o[2];
+                g[1] = 0.f;
             }
         }
         back_view_ = view;
-        for (int p = 0; p < np; ++p) back_view_[(size_t)p * HexBasis::kViewFloats + 25] = 1.f;
+        for (int p = 0; p < np; ++p) back_view_[(size_t)p * kVF + 25] = 1.f;
         dt_ = dt;
         finish_init(view, bins);
         SGD_CUDA(cudaMalloc(&d_back_view_, back_view_.size() * sizeof(float)));
@@ -313,20 +302,29 @@ public:
                             cudaMemcpyHostToDevice));
         out_scale = fdx * fdy;  // area factor (double)dx * (double)dy of the reference
         // the reference's H0 counts footprint evaluations three per bin; Hl never counts
-        count = (mode == kHl) ? 0 : 3 * fan2d_count<HexBasis>(P, stream);
+        count = (mode == kHl) ? 0 : 3 * dispatch([&](auto b) { return fan2d_count<decltype(b)>(P, stream); });
     }
     ~HexLayer() override { cudaFree(d_back_view_); }
     void forward_dev(const float* img, float* sino, cudaStream_t s) override {
-        fan2d_forward<HexBasis>(P, img, sino, out_scale, s);
+        dispatch([&](auto b) { fan2d_forward<decltype(b)>(P, img, sino, out_scale, s); return 0ull; });
     }
-    long long csr(const CsrOut& out) override { return fan2d_csr<HexBasis>(P, out_scale, out, stream); }
+    long long csr(const CsrOut& out) override {
+        return (long long)dispatch([&](auto b) { return (unsigned long long)fan2d_csr<decltype(b)>(P, out_scale, out, stream); });
+    }
     void backward_dev(const float* sino, float* img, cudaStream_t s) override {
         Fan2DParams Q = P;
         Q.view = d_back_view_;
-        fan2d_back<HexBasis>(Q, sino, img, out_scale, s);
+        dispatch([&](auto b) { fan2d_back<decltype(b)>(Q, sino, img, out_scale, s); return 0ull; });
     }
 
 protected:
+    // f(HexBasis<mode>()) for the layer's mode
+    template <class F>
+    unsigned long long dispatch(F&& f) const {
+        if (mode_ == kH0Corrected) return f(HexBasis<kH0Corrected>());
+        if (mode_ == kH0Reference) return f(HexBasis<kH0Reference>());
+        return f(HexBasis<kHl>());
+    }
     // The sites' true footprints: the hexagon (H0, rows at 1.5 dt: vertices
     // within 1/2 + 1/2 site, odd-row shift and vertex, and dt = 2/3 row) or
     // the linear element (Hl, rows at 0.5 dt: within one site and 2 rows).

@@ -1,8 +1,10 @@
 // Host + device FP64 buffer with the interface of the reference's MatrixD
 // (utils/matrix_double.hh:7-36): operator[] is the host pointer, operator()
 // the device pointer.  Kept so C++ callers of project/back_project
-// (SGD.cu:176-187, Bilinear.cu:25-39 in the reference) compile unchanged.
-// Errors throw sgd::Error instead of NNException.
+// (SGD.cu:176-187, Bilinear.cu:25-39 in the reference) compile against this
+// library by including reference_compat.h, which names the classes in the
+// global namespace as the reference does.  Errors throw sgd::Error instead of
+// NNException.
 #pragma once
 
 #include <cuda_runtime.h>

@@ -121,8 +121,8 @@ StripFit fit_strip(const RangeMap& m, double U0, double U1, bool jmaj, int nmajo
 }  // namespace
 
 int plan_fan2d(int ni, int nj, int np, int nu, const std::function<RangeMap(int)>& map, std::vector<float4>& strips,
-               std::vector<int2>& twin) {
-    const int nblk = (nu + kF2Block - 1) / kF2Block;
+               std::vector<int2>& twin, int block) {
+    const int nblk = (nu + block - 1) / block;
     strips.assign((size_t)np * nblk * 2, make_float4(0.f, 0.f, 0.f, 0.f));
     const int ti = (ni + kF2TileI - 1) / kF2TileI, tj = (nj + kF2TileJ - 1) / kF2TileJ;
     twin.assign((size_t)ti * tj * np, make_int2(0, -1));
@@ -133,7 +133,7 @@ int plan_fan2d(int ni, int nj, int np, int nu, const std::function<RangeMap(int)
         // with the fewest candidate cells
         for (int k = 0; k < nblk; ++k) {
             // half a bin of slack for the FP32 rounding of the kernels' ranges
-            const double U0 = k * kF2Block - 0.5, U1 = std::min(nu, (k + 1) * kF2Block) + 0.5;
+            const double U0 = k * block - 0.5, U1 = std::min(nu, (k + 1) * block) + 0.5;
             const StripFit fj = fit_strip(m, U0, U1, true, nj, ni);
             const StripFit fi = fit_strip(m, U0, U1, false, ni, nj);
             if (!fj.ok && !fi.ok) fail("projector geometry: degenerate detector strip in view %d", p);

@@ -88,7 +88,8 @@ RangeMap grid_range_map(const double hw[6], double x0, double dx, double y0, dou
 // footprint (the bins of the points the map's radii cover) meets a block is a
 // candidate of the block's strip, and every cell's footprint lies inside its
 // tile's window.  Returns the widest window.
+// `block`: bins per forward block (kF2Block for the 2D kernels).
 int plan_fan2d(int ni, int nj, int np, int nu, const std::function<RangeMap(int)>& map, std::vector<float4>& strips,
-               std::vector<int2>& twin);
+               std::vector<int2>& twin, int block = kF2Block);
 
 }  // namespace sgd

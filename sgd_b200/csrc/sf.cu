@@ -67,10 +67,13 @@ struct SFBasis {
         // dx / max(|sin t|, |cos t|) for t = atan2(X, Y) (:174-177) without
         // the trigonometry: |sin t| = |X| / r, |cos t| = |Y| / r
         const float X = V.dx * (ix - V.nx2) - V.srcx, Y = V.dy * (iy - V.ny2) - V.srcy;
-        c.weight = V.dx * sqrtf(X * X + Y * Y) / fmaxf(fabsf(X), fabsf(Y));
-        // per-bin constants of gamma_calculate (:48-84), once per cell and view
-        c.k01 = 1 / (2 * (us[1] - us[0]));
-        c.k23 = 1 / (2 * (us[3] - us[2]));
+        c.weight = V.dx * sqrtf(X * X + Y * Y) * __fdividef(1.0f, fmaxf(fabsf(X), fabsf(Y)));
+        // per-bin constants of gamma_calculate (:48-84), once per cell and
+        // view (fast reciprocals: within an ulp or two of the reference's
+        // divisions; a zero-width ramp still gives an infinite factor whose
+        // terms the NaN test drops)
+        c.k01 = __fdividef(0.5f, us[1] - us[0]);
+        c.k23 = __fdividef(0.5f, us[3] - us[2]);
     }
     // layers/A_SF.cu:48-84
     __device__ static float gamma(float s1, float s2, const Cell& c) {

@@ -59,6 +59,22 @@ def ellipse_phantom(nx: int, ny: int, dx: float, dy: float, seed: int = 0, n: in
     return sample_ellipses(ell, x, y)
 
 
+def ellipse_phantom_average(nx: int, ny: int, dx: float, dy: float, seed: int = 0, n: int = 10,
+                            sub: int = 8) -> np.ndarray:
+    """The same phantom averaged over each pixel (FP64, sub x sub samples per
+    pixel at the centres of its sub-cells): the image a perfect reconstruction
+    in pixels would hold, the ground truth of the reconstruction experiments."""
+    radius = 0.5 * min(nx * dx, ny * dy)
+    ell = random_ellipses(seed, n, radius)
+    x, y = pixel_centres(nx, ny, dx, dy)
+    off = (np.arange(sub) + 0.5) / sub - 0.5
+    out = np.zeros((nx, ny), dtype=np.float64)
+    for ox in off:
+        for oy in off:
+            out += sample_ellipses(ell, x + ox * dx, y + oy * dy)
+    return out / (sub * sub)
+
+
 def ellipse_chords(ell: np.ndarray, px, py, qx, qy) -> np.ndarray:
     """Line integrals of the ellipse phantom along the lines through P and Q.
 

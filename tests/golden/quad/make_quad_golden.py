@@ -5,8 +5,8 @@ integral, numba-compiled integrands), unmodified, from the reference tree.
 
     python tests/golden/quad/make_quad_golden.py [REFERENCE_ROOT] [OUTDIR]
 
-REFERENCE_ROOT defaults to /root/reference (read only; Python writes no
-bytecode there).  Each fixture holds the geometry and the reference's COO
+REFERENCE_ROOT defaults to $SGD_REFERENCE, else the reference checkout beside
+the repository (read only; Python writes no bytecode there).  Each fixture holds the geometry and the reference's COO
 triplets (row p*nu + u, column ix*ny + iy, value); views are the scripts'
 own linspace(0, 2 pi, np, endpoint=False).  tests/test_oracle.py checks the
 CPU oracle's exact matrices (oracle_exact_fan2d_matrix) against them.
@@ -47,4 +47,8 @@ def main(ref_root, out):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference", sys.argv[2] if len(sys.argv) > 2 else HERE)
+    default_ref = os.environ.get("SGD_REFERENCE",
+                                 os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(HERE))), "..",
+                                              "reference"))
+    main(sys.argv[1] if len(sys.argv) > 1 else os.path.normpath(default_ref),
+         sys.argv[2] if len(sys.argv) > 2 else HERE)

@@ -39,3 +39,44 @@ def test_c_caller_error_protocol(tmp_path):
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout + r.stderr
+
+
+def test_reference_style_cpp_caller_links(tmp_path):
+    """A C++ caller written as the reference's own (global MatrixD and A_B1,
+    the project/back_project calls of SGD.cu:176-187) compiles against
+    reference_compat.h and links against the library; without a GPU the
+    layer's constructor throws instead of returning."""
+    _need("g++")
+    from sgd_b200 import _lib
+    csrc = os.path.join(ROOT, "sgd_b200", "csrc")
+    cuda_inc = "/usr/local/cuda/include"
+    if not os.path.isdir(cuda_inc):
+        pytest.skip("CUDA headers not installed")
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include <cstdio>
+#include "reference_compat.h"
+int main() {
+    const int nx = 8, ny = 8, np = 4, nu = 12;
+    double ang[np] = {0.0, 0.5, 1.0, 1.5};
+    try {
+        A_B1 layer(nx, ny, np, nu, 1.0, 1.0, 1.0, 100.0, 50.0, ang, nullptr, nullptr);
+        MatrixD vol(nx * ny, 1), proj(np * nu, 1);
+        vol.allocateMemory();
+        proj.allocateMemory();
+        layer.project(vol, proj, 1.0);
+        layer.back_project(vol, proj, 1.0);
+        std::printf("ran\n");
+    } catch (const std::exception& e) {
+        std::printf("threw: %s\n", e.what());
+    }
+    return 0;
+}
+''')
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    exe = tmp_path / "caller"
+    r = subprocess.run(["g++", "-std=c++17", "-I", csrc, "-I", cuda_inc, str(src), "-o", str(exe), "-L", libdir,
+                        "-lnetwork", f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and (r.stdout.startswith("ran") or r.stdout.startswith("threw")), r.stdout + r.stderr
