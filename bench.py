@@ -593,12 +593,13 @@ def run_asd(args, rank, world, local_rank):
         "unit": "ratio", "n_gpus": world, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded ellipse phantoms, Poisson noise)",
         "config": {"workload": r["workload"], "rmse_truth": r["rmse_truth"], "convergence_rule": r["convergence_rule"]},
-        "plain": {k: r["plain"][k] for k in ("iters", "gpu_ms", "rmse")},
+        "plain": {k: r["plain"][k] for k in ("iters", "converged", "gpu_ms", "rmse")},
         "learned": {k: r["learned"][k] for k in ("plain_iters_before_net", "iters_after_net", "gpu_ms", "net_ms",
                                                   "rmse", "reached")},
         "data_residual": {"plain_last": r["plain"]["data_residual"][-1],
                           "learned_last": (r["learned"]["data_residual"] or [None])[-1]},
         "training": {k: r["training"][k] for k in ("pairs", "target_iters", "epochs", "pairs_s", "train_s")},
+        "calibration_converged": r["calibration_converged"],
     }
     print(json.dumps(line), flush=True)
 

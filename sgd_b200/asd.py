@@ -303,7 +303,7 @@ def learned_run(solver, net, sino, truth, k_in, target, max_iters, every=1, info
 
 
 def experiment(n=256, views=120, images=64, train_pairs=2000, k_in=5, epochs=40, batch=16, lr=1e-3, lr_final=1e-4,
-               max_iters=400, checkpoint=None, log=None):
+               max_iters=1000, checkpoint=None, log=None):
     """Learned warm start against plain ASD-POCS (64 fan-beam phantoms 256^2,
     120 views, Poisson I0 = 1e5 by default).  Plain runs to the convergence
     rule of plain_converged on a calibration batch: its iteration count K
@@ -349,7 +349,9 @@ def experiment(n=256, views=120, images=64, train_pairs=2000, k_in=5, epochs=40,
         "rmse_truth": "FP64 pixel averages of the ellipse phantoms (8 x 8 samples per pixel), FP64 RMSE",
         "convergence_rule": "mean RMSE changed by < 1e-3 (relative) over 10 iterations, checked every 5",
         "calibration_iters": K,
-        "plain": {"iters": it_p, "gpu_ms": ms_p, "rmse": target, "curve": curve_p, "data_residual": res_p},
+        "calibration_converged": K < max_iters,
+        "plain": {"iters": it_p, "converged": it_p < max_iters, "gpu_ms": ms_p, "rmse": target, "curve": curve_p,
+                  "data_residual": res_p},
         "learned": {"plain_iters_before_net": k_in, "iters_after_net": it_l, "gpu_ms": ms_l,
                     "net_ms": info["net_ms"], "data_residual": info.get("residual", []), "rmse": curve_l[-1][2],
                     "curve": curve_l, "reached": curve_l[-1][2] <= target},

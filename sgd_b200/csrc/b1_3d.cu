@@ -63,7 +63,7 @@ constexpr int kUB = 16;          // forward: u bins per block
 constexpr int kFW = 8;           // forward: warps, columns per batch
 constexpr int kMaxLines = 2048;  // forward: strip lines held in shared memory
 constexpr int kTX = 4, kTY = 2;  // back: columns per CTA (a warp each)
-constexpr int kWin = 16;         // back: staged u window (bins)
+constexpr int kWin = 20;         // back: staged u window (bins); rows of 80 bytes keep float4 row reads free of bank conflicts
 constexpr int kRowBox = 192;     // back: rows per TMA box
 constexpr int kZPer = 8;         // back: voxels per lane (z = l + 32 k)
 constexpr uint32_t kWaitLimit3 = 1u << 22;
@@ -370,7 +370,7 @@ __host__ __device__ constexpr size_t fwd3_smem(int nv, int nz) {
     return (size_t)kUB * nv * 8 + (size_t)kFW * nv * 4 + kFW * kUB * 4 + (kMaxLines + 1) * 4 + (size_t)nz * 4;
 }
 
-__global__ void __launch_bounds__(kFW * 32, 2) b1_3d_fwd_kernel(Geo3 G, Plan3 K, const float* __restrict__ volT,
+__global__ void __launch_bounds__(kFW * 32, 3) b1_3d_fwd_kernel(Geo3 G, Plan3 K, const float* __restrict__ volT,
                                                              float* __restrict__ proj, float scale) {
     extern __shared__ __align__(16) unsigned char f3_smem[];
     const int nv = G.nv, nz = G.nz;
@@ -513,7 +513,7 @@ __host__ __device__ constexpr size_t back3_smem(int nv) {
 // single-bin u or v ranges skipped); mode 1: the exact transpose of the
 // forward.  use_tma: the projection is staged through `map` (a tensor map of
 // proj, extents (nu, nv, np)); otherwise read from global memory.
-__global__ void __launch_bounds__(kTX * kTY * 32, 2) b1_3d_back_kernel(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(kTX * kTY * 32, 3) b1_3d_back_kernel(const __grid_constant__ CUtensorMap map,
                                                                     Geo3 G, Plan3 K, const float* __restrict__ proj,
                                                                     float* __restrict__ vol, int mode, int use_tma) {
     extern __shared__ __align__(128) unsigned char b3_smem[];
@@ -592,36 +592,60 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 2) b1_3d_back_kernel(const __g
         }
         if (active) {
             const int ncv = c.maxu - c.minu + 1;
-            // conv of bin minu + l, then B(v) = sum over kept bins of conv(u) proj(u, v)
+            // conv of bin minu + l (lane l), then B(v) = sum over kept bins
+            // of conv(u) proj(u, v), a lane per row
             float cv = 0.f;
             if (l < ncv) {
                 cv = column_conv_at(V, c, G.vecs + (size_t)p * G.nu, G.nu, l);
                 const bool keep = mode == 0 ? (cv == cv && cv > kEps) : (cv == cv);
                 if (!keep) cv = 0.f;
             }
-            const int nreg = min(ncv, 32);
-            for (int v0 = 0; v0 < nv; v0 += 32) {  // uniform trip count: the shuffles below need every lane
-                const int v = v0 + l;
-                float b = 0.f;
-                for (int t = 0; t < nreg; ++t) {
-                    const float ct = __shfl_sync(0xffffffffu, cv, t);
-                    if (ct == 0.f || v >= nv) continue;
-                    const int u = c.minu + t, du = u - ulo;
-                    const float pv = (ulo >= 0 && du >= 0 && du < kWin) ? sp[(size_t)v * kWin + du]
-                                                                         : __ldg(gp + (size_t)v * G.nu + u);
-                    b = fmaf(ct, pv, b);
+            const int du0 = c.minu - ulo, q0 = du0 >> 2, sh = du0 & 3;
+            if (ulo >= 0 && du0 >= 0 && ncv + sh <= 8 && 4 * q0 + 8 <= kWin) {
+                // the column's bins lie in two 16-byte words of each staged
+                // row: B(v) = sum_k coef[k] row[4 q0 + k], coef the column's
+                // footprint shifted by sh (the same for every lane)
+                float coef[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const float ck = __shfl_sync(0xffffffffu, cv, max(0, min(31, k - sh)));
+                    coef[k] = (k >= sh && k - sh < ncv) ? ck : 0.f;
                 }
-                if (v < nv) Bw[v] = b;
-            }
-            if (ncv > 32) {  // the reference's degenerate ranges on snapped views: the rest, lane by lane
                 for (int v = l; v < nv; v += 32) {
-                    float b = Bw[v];
-                    for (int t = 32; t < ncv; ++t) {
-                        float ct = column_conv_at(V, c, G.vecs + (size_t)p * G.nu, G.nu, t);
-                        if (!(mode == 0 ? (ct == ct && ct > kEps) : (ct == ct))) continue;
-                        b = fmaf(ct, __ldg(gp + (size_t)v * G.nu + c.minu + t), b);
-                    }
+                    const float4* row = reinterpret_cast<const float4*>(sp + (size_t)v * kWin) + q0;
+                    const float4 a = row[0], b4 = row[1];
+                    float b = coef[0] * a.x;
+                    b = fmaf(coef[1], a.y, b);
+                    b = fmaf(coef[2], a.z, b);
+                    b = fmaf(coef[3], a.w, b);
+                    b = fmaf(coef[4], b4.x, b);
+                    b = fmaf(coef[5], b4.y, b);
+                    b = fmaf(coef[6], b4.z, b);
+                    b = fmaf(coef[7], b4.w, b);
                     Bw[v] = b;
+                }
+            } else {
+                // not in the staged window (or a snapped view's wide range):
+                // global memory, a lane per row
+                for (int v0 = 0; v0 < nv; v0 += 32) {  // uniform trip count: the shuffles need every lane
+                    const int v = v0 + l;
+                    float b = 0.f;
+                    for (int t = 0; t < min(ncv, 32); ++t) {
+                        const float ct = __shfl_sync(0xffffffffu, cv, t);
+                        if (ct != 0.f && v < nv) b = fmaf(ct, __ldg(gp + (size_t)v * G.nu + c.minu + t), b);
+                    }
+                    if (v < nv) Bw[v] = b;
+                }
+                if (ncv > 32) {  // the reference's degenerate ranges on snapped views: the rest
+                    for (int v = l; v < nv; v += 32) {
+                        float b = Bw[v];
+                        for (int t = 32; t < ncv; ++t) {
+                            const float ct = column_conv_at(V, c, G.vecs + (size_t)p * G.nu, G.nu, t);
+                            if (!(mode == 0 ? (ct == ct && ct > kEps) : (ct == ct))) continue;
+                            b = fmaf(ct, __ldg(gp + (size_t)v * G.nu + c.minu + t), b);
+                        }
+                        Bw[v] = b;
+                    }
                 }
             }
             __syncwarp();

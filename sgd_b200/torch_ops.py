@@ -200,8 +200,12 @@ class ConeProjector(_HandleProjector):
             f, b, d = L.sgd_sf3d_forward_dev, L.sgd_sf3d_backward_dev, L.sgd_sf3d_destroy
         else:
             raise ValueError(f"unknown cone-beam kind {kind!r}")
-        # forward kernel + FP64-to-FP32 finish, back kernel
-        self.kernels = {"forward": f"{kind}_forward_kernel", "back": f"{kind}_back_kernel"}
+        if kind == "b1_3d":
+            # column transpose + forward kernel, back kernel
+            self.kernels = {"forward": "b1_3d_fwd_kernel", "back": "b1_3d_back_kernel"}
+        else:
+            # forward kernel + FP64-to-FP32 finish, back kernel
+            self.kernels = {"forward": "sf3d_forward_kernel", "back": "sf3d_back_kernel"}
         self.launches_per_step = 3
         self._keep = angles
         self._setup(h, f, b, d, (nz, ny, nx), (len(angles), nv, nu), kind)

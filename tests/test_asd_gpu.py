@@ -147,27 +147,35 @@ def _asd_reference(A, b, x, iters, beta=1.0, beta_red=0.995, alpha=0.002, alpha_
 
 
 def test_asd_pocs_matches_fp64_restatement(oracle_mod):
-    """Four iterations of the GPU solver on a 32^2 fan-beam slice against the
-    same iterations in NumPy FP64 on the oracle's B1 system matrix (the FP64
-    replica of layers/A_B1.cu, which the GPU projector matches to ~5e-7)."""
+    """The GPU solver on a 32^2 fan-beam slice against the same iterations in
+    NumPy FP64 on the oracle's B1 system matrix (the FP64 replica of
+    layers/A_B1.cu, which the GPU projector matches to ~5e-7).
+
+    Two iterations (one TV descent) agree to 1e-4.  Later iterations drift
+    apart by the TV gradient's own conditioning: with eps = 1e-8 its terms
+    a / sqrt(eps + a^2) turn an FP32 rounding of x (~6e-8 at |x| ~ 1) into a
+    relative change of ~ulp / sqrt(eps) ~ 6e-4.  The same restatement with
+    only its TV gradient rounded to FP32 differs from the FP64 one by 2.5e-4
+    after three iterations and 6.3e-4 after four, so four iterations are held
+    to 2e-3."""
     from sgd_b200.asd import ASDPOCS, Geometry, simulate
     geo = Geometry(32, 24)
     n, _, nu, dx, dy, du, lsd, lso, ang = geo.slice()
     truth, sino, _ = simulate(geo, [5], i0=0.0)
     A = oracle_mod.b1_matrix(n, n, nu, dx, dy, du, lsd, lso, ang, np.arange(len(ang)))
-    iters = 4
-    s = ASDPOCS(geo, 1, nonneg=False)
-    s.set_data(sino, hist_cap=iters)
-    s.run(iters)
-    torch.cuda.synchronize()
-    s.status()
-    x_gpu = s.images()[0].double().cpu().numpy().ravel()
     b = sino[0].double().cpu().numpy().ravel()
-    x_ref, h_ref = _asd_reference(A, b, np.zeros(n * n), iters)
-    assert rel_l2(x_gpu, x_ref) < 1e-4
-    h = s.history(iters)[:, 0, :].astype(np.float64)
-    assert np.allclose(h[:, 0], h_ref[:, 0], rtol=1e-4) and np.allclose(h[:, 1], h_ref[:, 1], rtol=1e-4)
-    assert np.allclose(h[1:, 2], h_ref[1:, 2], rtol=1e-3) and h[0, 2] == 0.0
+    for iters, tol in ((2, 1e-4), (4, 2e-3)):
+        s = ASDPOCS(geo, 1, nonneg=False)
+        s.set_data(sino, hist_cap=iters)
+        s.run(iters)
+        torch.cuda.synchronize()
+        s.status()
+        x_gpu = s.images()[0].double().cpu().numpy().ravel()
+        x_ref, h_ref = _asd_reference(A, b, np.zeros(n * n), iters)
+        assert rel_l2(x_gpu, x_ref) < tol, iters
+        h = s.history(iters)[:, 0, :].astype(np.float64)
+        assert np.allclose(h[:, 0], h_ref[:, 0], rtol=1e-4) and np.allclose(h[:, 1], h_ref[:, 1], rtol=1e-4)
+        assert np.allclose(h[1:, 2], h_ref[1:, 2], rtol=1e-3) and h[0, 2] == 0.0
 
 
 def test_positivity_constraint():
