@@ -105,10 +105,14 @@ def _families():
                     lambda: cone("sf3d"), 256 ** 3 * 360),
         "b1_3d_small": ("A_B1_3D cone beam, the 256^3 cone geometry at half resolution for profiling: 128^3 @2mm, "
                         "180 views, 192x192 @3mm", lambda: cone("b1_3d", 128, 180, 192, 2.0, 3.0), 128 ** 3 * 180),
+        "sf3d_small": ("SF_projector cone beam (corrected pair), the 256^3 cone geometry at half resolution for "
+                       "profiling: 128^3 @2mm, 180 views, 192x192 @3mm",
+                       lambda: cone("sf3d", 128, 180, 192, 2.0, 3.0), 128 ** 3 * 180),
     }
 
 
-FAMILIES = ("sf_fan512", "b1ref_fan512", "b0_fan512", "b0_parallel128", "h0_hex2e18", "hl_hex2e18", "b1_3d_cone256", "sf3d_cone256", "b1_3d_small")
+FAMILIES = ("sf_fan512", "b1ref_fan512", "b0_fan512", "b0_parallel128", "h0_hex2e18", "hl_hex2e18", "b1_3d_cone256", "sf3d_cone256", "b1_3d_small",
+            "sf3d_small")
 
 
 def parse():

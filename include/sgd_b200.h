@@ -103,9 +103,11 @@ int sgd_b1_set_wait_limit(void* layer, unsigned polls);
  * fixed 4 MiB __device__ array that every GPU loading this library holds until
  * exit, so images are limited to 1,048,576 pixels (1024 x 1024); larger ones
  * are rejected with -1 and a message.  The first call on each device looks up
- * the array's address (make it before any stream capture).  All calls share
- * the array: calls that overlap on the GPU race.  The layer's device must be
- * current.  Returns 0 on success, -1 on failure. */
+ * the array's address (make it before any stream capture) and keeps it for
+ * the process: after a cudaDeviceReset, which invalidates both that address
+ * and every layer, this entry point must not be called again.  All calls
+ * share the array: calls that overlap on the GPU race.  The layer's device
+ * must be current.  Returns 0 on success, -1 on failure. */
 int sgd_b1_forward_noalloc(void* layer, const float* d_img, float* d_sino, void* stream);
 
 /* New: B1 in the reference layer's FP32 rounding.  Same arguments, layouts
@@ -245,6 +247,9 @@ unsigned long long sgd_b1_3d_count(void* layer);
  * wait for its staged projection window gave up; those voxels were left
  * unwritten.  The FP64 host entry point checks it itself. */
 int sgd_b1_3d_status(void* layer);
+/* New: the polls an A_B1_3D back projection spends waiting for one staged
+ * view before it gives up (default 4194304); applies to later calls. */
+int sgd_b1_3d_set_wait_limit(void* layer, unsigned limit);
 
 /* ---- SF_projector: 3D separable footprint --------------------------------- */
 
@@ -258,9 +263,10 @@ int sgd_b1_3d_status(void* layer);
  * voxel value and amplitude, drops out-of-detector bins, and its backward is
  * the exact transpose of its forward.  trap_v: SF-TT (trapezoid in v) in the
  * forward (the reference's `tt` argument); mode 1's backward follows it.
- * The FP64 host entry points of mode 1 stay in FP64 (inputs, accumulation,
- * outputs), so the pair is an adjoint pair to FP64 rounding; mode 0's round
- * through FP32 as the reference does; the *_dev entry points are FP32. */
+ * The FP64 host entry points round through the FP32 device path, as the
+ * reference's SF class does; accumulation is FP64 in both modes.  Mode 1
+ * needs a circular orbit (the detector's u row of every projection matrix
+ * free of z, which geo_init_angles geometries are). */
 void* sgd_sf3d_init(int mode, int trap_v, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
                     double dz, double du, double dv, double lsd, double lso, double* angles);
 int sgd_sf3d_forward_projection(double* b, double* x, void* layer);
@@ -268,6 +274,12 @@ int sgd_sf3d_backward_projection(double* b, double* x, void* layer);
 void sgd_sf3d_destroy(void* layer);
 int sgd_sf3d_forward_dev(void* layer, const float* d_vol, float* d_proj, void* stream);
 int sgd_sf3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void* stream);
+/* New: as sgd_b1_3d_status, for mode 1's back projection (mode 0's has no
+ * staged wait and always reports 0). */
+int sgd_sf3d_status(void* layer);
+/* New: the polls a mode-1 back projection spends waiting for one staged view
+ * before it gives up (default 4194304); applies to later calls. */
+int sgd_sf3d_set_wait_limit(void* layer, unsigned limit);
 
 /* ---- batched B1: many slices per launch ----------------------------------- */
 

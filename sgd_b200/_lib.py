@@ -100,11 +100,15 @@ def lib() -> ctypes.CDLL:
     L.sgd_b1ref_matrix_csr.argtypes = [_vp, _vp, _vp, _vp, ctypes.c_longlong]
     L.sgd_proj2d_status.restype = _i
     L.sgd_proj2d_status.argtypes = [_vp]
-    for n in ("sgd_b1_set_wait_limit", "sgd_proj2d_set_wait_limit", "sgd_b1_batch_set_wait_limit"):
+    for n in ("sgd_b1_set_wait_limit", "sgd_proj2d_set_wait_limit", "sgd_b1_batch_set_wait_limit",
+              "sgd_b1_3d_set_wait_limit", "sgd_sf3d_set_wait_limit"):
         getattr(L, n).restype = _i
         getattr(L, n).argtypes = [_vp, ctypes.c_uint]
     L.sgd_b1_status.restype = _i
     L.sgd_b1_status.argtypes = [_vp]
+    for n in ("sgd_b1_3d_status", "sgd_sf3d_status"):
+        getattr(L, n).restype = _i
+        getattr(L, n).argtypes = [_vp]
     L.sgd_geometry_pmi.restype = _i
     L.sgd_b1_forward_noalloc.restype = _i
     L.sgd_b1_forward_noalloc.argtypes = [_vp, _vp, _vp, _vp]

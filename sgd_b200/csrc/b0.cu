@@ -85,17 +85,17 @@ struct B0Basis {
         c.sx += V.puvx;
         c.sy += V.puvy;
     }
-    __device__ static float value(const View& V, Cell& c, int, const float4* t, const Fan2DParams&) {
+    __device__ static float value(const View& V, Cell& c, int, BinRef t, const Fan2DParams&) {
         const float sx = c.sx, sy = c.sy;
         skip(V, c);
         const float4 b0 = t[0], b1 = t[1];  // vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2
         const float px = V.srcx, py = V.srcy;
         // layers/A_B0.cu:207-219: the FP32 products as the reference forms
         // them, its FP64 scalings in FP32
-        const float r1 = ((c.ox - px) * (sx - px) + (c.oy - py) * (sy - py)) * b1.y;
+        const float r1 = dot2f(c.ox - px, sx - px, c.oy - py, sy - py) * b1.y;
         const float vblur = (b0.z + b0.w) * (-r1);
         const float x1 = sx - px, y1 = sy - py, x2 = c.ox - 0.5f * V.dx - px, y2 = c.oy + 0.5f * V.dy - py;
-        const float y = fmaf(b0.z, r1, (x1 * y2 - x2 * y1) * b1.x);
+        const float y = fmaf(b0.z, r1, dot2f(x1, y2, -x2, y1) * b1.x);
         const float conv = conv1d(-y, b0.x, b0.y, vblur);
         return (conv > 1e-7f && conv == conv) ? conv : 0.f;
     }
@@ -134,7 +134,7 @@ struct B0ParBasis {
         c.lo = max(0, (int)floorf((c.s - h) / V.du + V.hnu));
         c.hi = min(P.nu - 1, (int)floorf((c.s + h) / V.du + V.hnu));
     }
-    __device__ static float value(const View& V, Cell& c, int u, const float4*, const Fan2DParams&) {
+    __device__ static float value(const View& V, Cell& c, int u, BinRef, const Fan2DParams&) {
         const float t = c.s - ((float)u - V.hnu + 0.5f) * V.du;
         const float conv = B0Basis::conv1d(t + 0.5f * (V.a + V.b + V.du), V.a, V.b, V.du);
         return (conv > 1e-7f && conv == conv) ? conv : 0.f;
@@ -179,9 +179,9 @@ public:
                 double sb0 = std::fabs((sx - px) * (by - py) - (bx - px) * (sy - py)) / lsp;
                 a0s /= ((ax - px) * (sx - px) + (ay - py) * (sy - py)) / (lsp * lsp);
                 sb0 /= ((bx - px) * (sx - px) + (by - py) * (sy - py)) / (lsp * lsp);
-                float4* o = &bins[((size_t)p * nu + u) * B0Basis::kBinF4];
+                float4* o = &bins[(size_t)p * B0Basis::kBinF4 * nu + u];  // planes of nu words
                 o[0] = make_float4((float)vx, (float)vy, (float)a0s, (float)sb0);
-                o[1] = make_float4((float)(1.0 / lsp), (float)(1.0 / (lsp * lsp)), 0.f, 0.f);
+                o[nu] = make_float4((float)(1.0 / lsp), (float)(1.0 / (lsp * lsp)), 0.f, 0.f);
             }
         }
         finish_init(view, bins);

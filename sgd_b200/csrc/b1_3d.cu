@@ -48,6 +48,7 @@
 #include <vector>
 
 #include "common.h"
+#include "cone_columns.cuh"
 #include "fan_geometry.h"
 #include "proj2d.h"
 #include "tensor_map.h"
@@ -66,7 +67,7 @@ constexpr int kTX = 4, kTY = 2;  // back: columns per CTA (a warp each)
 constexpr int kWin = 20;         // back: staged u window (bins); rows of 80 bytes keep float4 row reads free of bank conflicts
 constexpr int kRowBox = 192;     // back: rows per TMA box
 constexpr int kZPer = 8;         // back: voxels per lane (z = l + 32 k)
-constexpr uint32_t kWaitLimit3 = 1u << 22;
+constexpr uint32_t kDrainLimit = 1u << 22;  // back: polls of the drain after a failed wait
 
 struct View3 {
     float pm[12];
@@ -278,6 +279,7 @@ struct Plan3 {
     const int* twin;       // [tiles][np]: back window's first bin (a multiple of 4), -1: read global memory
     int tiles_x, tiles_y;
     int* err;              // bounded-wait status, 0 = ok
+    unsigned wait_limit;   // polls of one staged view before the back projection gives up
 };
 
 // Axial footprint of voxel iz of column c (layers/A_B1_3D.cu:188-210): the
@@ -348,22 +350,6 @@ __device__ __forceinline__ float chunk_oz(int iz, int nz, float dz) {
     float oz = (z0 - 0.5f * (nz - 1)) * dz;
     for (int q = z0; q < iz; ++q) oz += dz;
     return oz;
-}
-
-// vol [z][y][x] -> volT [y][x][z]
-__global__ void to_columns_kernel(const float* __restrict__ vol, float* __restrict__ volT, int nx, int ny, int nz) {
-    __shared__ float t[32][33];
-    const int col0 = blockIdx.x * 32, z0 = blockIdx.y * 32;
-    const int ncol = nx * ny;
-    for (int k = threadIdx.y; k < 32; k += 8) {
-        const int z = z0 + k, col = col0 + threadIdx.x;
-        if (z < nz && col < ncol) t[k][threadIdx.x] = vol[(size_t)z * ncol + col];
-    }
-    __syncthreads();
-    for (int k = threadIdx.y; k < 32; k += 8) {
-        const int col = col0 + k, z = z0 + threadIdx.x;
-        if (z < nz && col < ncol) volT[(size_t)col * nz + z] = t[threadIdx.x][k];
-    }
 }
 
 __host__ __device__ constexpr size_t fwd3_smem(int nv, int nz) {
@@ -552,10 +538,13 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 3) b1_3d_back_kernel(const __g
         for (int r = 0; r < nboxes; ++r)
             tma_load_3d(stage + ((size_t)(p & 1) * nvp + (size_t)r * kRowBox) * kWin, &map, ulo, r * kRowBox, p, bar);
     };
+    // view f's copies never arrived: wait (bounded, full limit) for them and
+    // for view f + 1's, issued before f's wait, so that no bulk copy is still
+    // landing in this CTA's shared memory when it exits
     auto drain = [&](int f) {
         if (tid == 0) {
-            mbar_wait_bounded(&bars[f & 1], (uint32_t)(f >> 1) & 1u, kWaitLimit3);
-            if (f + 1 < G.np) mbar_wait_bounded(&bars[(f + 1) & 1], (uint32_t)((f + 1) >> 1) & 1u, kWaitLimit3);
+            mbar_wait_bounded(&bars[f & 1], (uint32_t)(f >> 1) & 1u, kDrainLimit);
+            if (f + 1 < G.np) mbar_wait_bounded(&bars[(f + 1) & 1], (uint32_t)((f + 1) >> 1) & 1u, kDrainLimit);
         }
     };
     if (tid == 0) {
@@ -570,7 +559,7 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 3) b1_3d_back_kernel(const __g
         oz[q] = chunk_oz(min(zbase + 32 * q + l, G.nz - 1), G.nz, G.dz);
     }
     for (int p = 0; p < G.np; ++p) {
-        if (!mbar_wait_bounded(&bars[p & 1], (uint32_t)(p >> 1) & 1u, kWaitLimit3)) {
+        if (!mbar_wait_bounded(&bars[p & 1], (uint32_t)(p >> 1) & 1u, K.wait_limit)) {
             s_abort = 1;
             if (K.err) atomicExch(K.err, 1);
         }
@@ -781,8 +770,7 @@ public:
     }
     // vol [z][y][x], proj [p][v][u], FP32 device
     void forward_dev(const float* vol, float* proj, cudaStream_t s) {
-        const int ncol = nx * ny;
-        to_columns_kernel<<<dim3((ncol + 31) / 32, (nz + 31) / 32), dim3(32, 8), 0, s>>>(vol, d_volT_, nx, ny, nz);
+        launch_to_columns(vol, d_volT_, nx, ny, nz, s);
         SGD_LAUNCH_CHECK();
         b1_3d_fwd_kernel<<<dim3(K.nblk, np), kFW * 32, fwd3_smem(nv, nz), s>>>(G, K, d_volT_, proj,
                                                                              (float)dx * (float)dy * (float)dz);
@@ -801,6 +789,10 @@ public:
     }
     // 0, or -1 when a back projection's staging wait gave up (those voxels
     // were left unwritten); synchronises the device and clears the flag
+    void set_wait_limit(unsigned limit) {
+        SGD_CUDA(cudaStreamSynchronize(stream));
+        K.wait_limit = limit;
+    }
     int status() {
         int h = 0;
         SGD_CUDA(cudaDeviceSynchronize());
@@ -892,6 +884,7 @@ private:
         K.strips = d_strips_;
         K.twin = d_twin_;
         K.err = d_err_;
+        K.wait_limit = 1u << 22;
         SGD_CUDA(cudaFuncSetAttribute(b1_3d_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)fwd3_smem(nv, nz)));
         SGD_CUDA(cudaFuncSetAttribute(b1_3d_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -962,6 +955,12 @@ int sgd_b1_3d_backward_dev(void* layer, const float* d_proj, float* d_vol, void*
     });
 }
 unsigned long long sgd_b1_3d_count(void* layer) { return layer ? static_cast<B1Cone*>(layer)->count : 0ull; }
+int sgd_b1_3d_set_wait_limit(void* layer, unsigned limit) {
+    return sgd::guarded_status([&] {
+        if (!layer) sgd::fail("sgd_b1_3d_set_wait_limit: null layer");
+        static_cast<B1Cone*>(layer)->set_wait_limit(limit);
+    });
+}
 int sgd_b1_3d_status(void* layer) {
     return sgd::guarded_status([&] {
         if (!layer) sgd::fail("sgd_b1_3d_status: null layer");

@@ -16,7 +16,10 @@
 // Set-up: the first call on each device looks up the array's device address
 // with cudaGetSymbolAddress (the host-side symbol is only a stand-in, not a
 // device address) and caches it for that device; make that first call before
-// any stream capture.  The image must be at most kNoAllocMaxPixels pixels.
+// any stream capture.  The cache lives as long as the process: a
+// cudaDeviceReset destroys the context that owns the array (and every layer
+// made in it), after which the cached address is stale, so the entry point
+// is not to be called after a reset.  The image must be at most kNoAllocMaxPixels pixels.
 // Every call shares the one array; a call overwrites all of the scratch it
 // reads before reading it, so nothing needs clearing, but calls that overlap
 // on the GPU (concurrent streams, or several host threads) race on it.

@@ -101,7 +101,7 @@ struct B1RefBasis {
         return copysignf(ax <= amb ? sin_ : sout, x);
     }
     // layers/A_B1.cu:182-203 for the bin at the walk's current centre
-    __device__ static float value(const View& V, Cell& c, int, const float4* t, const Fan2DParams&) {
+    __device__ static float value(const View& V, Cell& c, int, BinRef t, const Fan2DParams&) {
         const float sx = c.sx, sy = c.sy;
         skip(V, c);
         const float px = V.srcx, py = V.srcy, ox = c.ox, oy = c.oy;
@@ -109,13 +109,15 @@ struct B1RefBasis {
         const float ay = sy - V.puvy * 0.5f;
         const float bx = sx + V.puvx * 0.5f;
         const float by = sy + V.puvy * 0.5f;
-        const float ra = ((ox - px) * (sx - px) + (oy - py) * (sy - py)) / ((ax - px) * (sx - px) + (ay - py) * (sy - py));
-        const float rb = ((ox - px) * (sx - px) + (oy - py) * (sy - py)) / ((bx - px) * (sx - px) + (by - py) * (sy - py));
+        // the reference's expressions; a*b + c*d as dot2f (first product fused)
+        const float num = dot2f(ox - px, sx - px, oy - py, sy - py);
+        const float ra = num / dot2f(ax - px, sx - px, ay - py, sy - py);
+        const float rb = num / dot2f(bx - px, sx - px, by - py, sy - py);
         const float ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;
         const float bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
-        const float x1 = sqrtf((ax1 - ox) * (ax1 - ox) + (ay1 - oy) * (ay1 - oy));
-        const float x2 = sqrtf((bx1 - ox) * (bx1 - ox) + (by1 - oy) * (by1 - oy));
-        const float sgn = ((ax1 - ox) * (bx1 - ox) + (ay1 - oy) * (by1 - oy) > 0) ? 1.0f : -1.0f;
+        const float x1 = sqrtf(dot2f(ax1 - ox, ax1 - ox, ay1 - oy, ay1 - oy));
+        const float x2 = sqrtf(dot2f(bx1 - ox, bx1 - ox, by1 - oy, by1 - oy));
+        const float sgn = (dot2f(ax1 - ox, bx1 - ox, ay1 - oy, by1 - oy) > 0) ? 1.0f : -1.0f;
         const float xa = x1 * sgn;
         const float4 k0 = t[0], k1 = t[1], k2 = t[2];
         const float conv = fabsf(G(x2, k0, k1, k2) - G(xa, k0, k1, k2)) / fabsf(x2 - xa);
@@ -157,10 +159,10 @@ public:
                 float r[16];
                 b1_profile_constants(std::max(vx, vy), std::min(vx, vy), r);
                 const float b = r[6], a = r[8];
-                float4* o = &bins[((size_t)p * nu + u) * B1RefBasis::kBinF4];
+                float4* o = &bins[(size_t)p * B1RefBasis::kBinF4 * nu + u];  // planes of nu words
                 o[0] = make_float4(b, a, r[10], (float)((double)a - (double)b));
-                o[1] = make_float4(r[12], r[13], r[14], r[15]);
-                o[2] = make_float4(-0.5f * r[15], 0.f, 0.f, 0.f);
+                o[nu] = make_float4(r[12], r[13], r[14], r[15]);
+                o[2 * nu] = make_float4(-0.5f * r[15], 0.f, 0.f, 0.f);
             }
         }
         finish_init(view, bins);

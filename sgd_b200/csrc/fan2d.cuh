@@ -3,7 +3,10 @@
 // A basis B supplies, for cell (i, j) of the grid and view p:
 //   B::kViewFloats          per-view constants (a multiple of 4 floats)
 //   B::kBinF4               float4 words per (view, bin) in the basis table
-//                           P.bins (0: no table)
+//                           P.bins (0: no table), stored as kBinF4 planes of
+//                           nu words per view ([view][word][bin]) so that
+//                           lanes on neighbouring bins read neighbouring
+//                           16-byte words of shared memory
 //   B::View, B::Cell        per-view constants; per-(cell, view) state with the
 //                           bin range [lo, hi] (the reference's rule, clamped
 //                           to the detector as the reference clamps it)
@@ -11,7 +14,8 @@
 //   B::valid(i, j, P)       whether (i, j) is a cell of the grid
 //   B::setup(V, i, j, P, c)
 //   B::value(V, c, u, t, P) footprint in bin u (0 where the reference drops
-//                           it), t = the bin's table entry; bins are walked in
+//                           it), t = the bin's table entry (t[k]: word k, a
+//                           BinRef over the planes); bins are walked in
 //                           order from c.lo, each by value() or skip(), which
 //                           lets a basis step its bin position as the
 //                           reference does
@@ -31,8 +35,11 @@
 //                         and walks the few cells of its line inside the strip
 //                         (host-computed strip records), adding each value to
 //                         its own FP32 shared-memory column of the block's
-//                         bins.  The columns are summed across lanes and warps
-//                         and every bin is written once: no atomics.
+//                         bins.  Neighbouring lanes own neighbouring lines and
+//                         read the image (j-major strips) or its transposed
+//                         copy (i-major) at neighbouring addresses.  The
+//                         columns are summed across lanes and warps and every
+//                         bin is written once: no atomics.
 //   fan2d_back_kernel     voxel driven: a CTA per tile of cells, a thread per
 //                         cell.  Per chunk of kF2Views views the CTA stages the
 //                         view constants and the tile's window of the basis
@@ -52,6 +59,20 @@
 namespace sgd {
 
 constexpr uint32_t kF2WaitLimit = 1u << 22;
+
+// a * b + c * d with the first product fused: the contraction the compiler
+// picks for that source form, written out so that every kernel (and the
+// system-matrix visitor) that inlines a basis forms the same bits.  The
+// forward and back projections are transposes of each other only if they
+// evaluate identical values.
+__device__ __forceinline__ float dot2f(float a, float b, float c, float d) { return __fmaf_rn(a, b, __fmul_rn(c, d)); }
+
+// One bin's entry of a basis table held as planes: word k at p[k * stride].
+struct BinRef {
+    const float4* p;
+    int stride;
+    __device__ __forceinline__ float4 operator[](int k) const { return p[k * stride]; }
+};
 
 // Compensated (Kahan) FP32 accumulation: s holds the sum, c the part of it
 // that is rounding error (true sum = s - c), four FP32 operations per term
@@ -87,15 +108,17 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
     // per bin), summed across lanes and warps in FP64
     __shared__ float s_acc[kF2FwdWarps][kF2Block][33];
     __shared__ double s_red[kF2FwdWarps][kF2Block];
-    __shared__ float4 s_bin[kF2Block * kBF4];
+    __shared__ float4 s_bin[kBF4 * kF2Block];  // [word][bin of the block]
     __shared__ __align__(16) float s_view[B::kViewFloats];
     const int k = blockIdx.x, p = blockIdx.y;
     const int u0 = k * kF2Block, nb = min(kF2Block, P.nu - u0);
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
     for (int e = tid; e < B::kViewFloats; e += blockDim.x) s_view[e] = __ldg(P.view + (size_t)p * B::kViewFloats + e);
     if (B::kBinF4 > 0)
-        for (int e = tid; e < nb * B::kBinF4; e += blockDim.x)
-            s_bin[e] = __ldg(P.bins + ((size_t)p * P.nu + u0) * B::kBinF4 + e);
+        for (int e = tid; e < nb * B::kBinF4; e += blockDim.x) {
+            const int k = e / nb, b = e - k * nb;
+            s_bin[k * kF2Block + b] = __ldg(P.bins + ((size_t)p * B::kBinF4 + k) * P.nu + u0 + b);
+        }
     for (int e = l; e < kF2Block * 33; e += 32) (&s_acc[w][0][0])[e] = 0.f;
     __syncthreads();
 
@@ -106,6 +129,10 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
     const bool jmaj = s0.x > 0.5f;
     const int nmin = jmaj ? P.ni : P.nj;
     const int mlo = (int)s1.z, mhi = (int)s1.w;
+    // cell (m, n) of line m: lanes own consecutive lines, so that j-major
+    // strips read the image and i-major ones its transposed copy coalesced
+    const int nmaj = jmaj ? P.nj : P.ni;
+    const float* src = jmaj ? img : P.imgT;
     float* acc = &s_acc[w][0][l];  // bin b at acc[33 b]: this lane's column
     for (int m = mlo + tid; m <= mhi; m += blockDim.x) {
         const float fm = (float)m;
@@ -115,7 +142,7 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
         for (int n = nlo; n <= nhi; ++n) {
             const int i = jmaj ? n : m, j = jmaj ? m : n;
             if (!B::valid(i, j, P)) continue;
-            const float C = __ldg(img + (size_t)i * P.nj + j);
+            const float C = __ldg(src + (size_t)n * nmaj + m);
             if (C == 0.f) continue;
             typename B::Cell c;
             B::setup(V, i, j, P, c);
@@ -124,7 +151,7 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
             int u = c.lo;
             for (; u < u0; ++u) B::skip(V, c);
             for (; u <= ue; ++u) {
-                const float v = B::value(V, c, u, s_bin + (u - u0) * B::kBinF4, P);
+                const float v = B::value(V, c, u, BinRef{s_bin + (u - u0), kF2Block}, P);
                 if (v != 0.f) acc[33 * (u - u0)] = fmaf(v, C, acc[33 * (u - u0)]);
             }
         }
@@ -144,8 +171,24 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
     }
 }
 
+// in [rows][cols] -> out [cols][rows] (the forward's line-major image copy)
+static __global__ void fan2d_transpose_kernel(const float* __restrict__ in, float* __restrict__ out, int rows,
+                                              int cols) {
+    __shared__ float t[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int r = r0 + k, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) t[k][threadIdx.x] = in[(size_t)r * cols + c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.y; k < 32; k += 8) {
+        const int c = c0 + k, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) out[(size_t)c * rows + r] = t[threadIdx.x][k];
+    }
+}
+
 // Shared memory of the back kernel: 2 mbarriers | windows [2][VC] int2 |
-// view constants [2][VC][kViewFloats] | tables [2][VC][wcap][kBinF4] float4 |
+// view constants [2][VC][kViewFloats] | tables [2][VC][kBinF4][wcap] float4 |
 // sinogram windows [2][VC][wcap] floats.
 template <class B, int VC>
 __host__ __device__ constexpr size_t fan2d_back_header() {
@@ -209,9 +252,10 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
                 bulk_copy_g2s(sview + (st * VC + l) * B::kViewFloats, P.view + (size_t)p * B::kViewFloats,
                               B::kViewFloats * 4, &bars[st]);
                 if (B::kBinF4 > 0 && lh.y >= lh.x)
-                    bulk_copy_g2s(sbin + (size_t)(st * VC + l) * P.wcap * B::kBinF4,
-                                  P.bins + ((size_t)p * P.nu + lh.x) * B::kBinF4,
-                                  (uint32_t)(lh.y - lh.x + 1) * B::kBinF4 * 16, &bars[st]);
+                    for (int k = 0; k < B::kBinF4; ++k)
+                        bulk_copy_g2s(sbin + ((size_t)(st * VC + l) * B::kBinF4 + k) * P.wcap,
+                                      P.bins + ((size_t)p * B::kBinF4 + k) * P.nu + lh.x,
+                                      (uint32_t)(lh.y - lh.x + 1) * 16, &bars[st]);
             }
         }
         for (int v = 0; v < VC; ++v) {
@@ -262,13 +306,13 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
             typename B::Cell cl;
             B::setup(V, i, j, P, cl);
             if (cl.hi < lh.x || cl.lo > lh.y) continue;
-            const float4* tb = sbin + (size_t)(st * VC + v) * P.wcap * B::kBinF4 - (size_t)lh.x * B::kBinF4;
+            const float4* tb = sbin + (size_t)(st * VC + v) * P.wcap * B::kBinF4 - lh.x;
             const float* sb = ssino + (st * VC + v) * P.wcap - lh.x;
             const int ue = min(cl.hi, lh.y);
             int u = cl.lo;
             for (; u < lh.x; ++u) B::skip(V, cl);
             for (; u <= ue; ++u) {
-                const float val = B::value(V, cl, u, tb + (size_t)u * B::kBinF4, P);
+                const float val = B::value(V, cl, u, BinRef{tb + u, P.wcap}, P);
                 if (val != 0.f) kahan_fma(csum, ccmp, val, sb[u]);
             }
         }

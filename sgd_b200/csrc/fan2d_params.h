@@ -10,7 +10,8 @@ struct Fan2DParams {
     int ni = 0, nj = 0;       // cell grid: cell (i, j) at index i * nj + j
     int np = 0, nu = 0;
     const float* view = nullptr;     // [np][B::kViewFloats], 16-byte rows
-    const float4* bins = nullptr;    // basis-specific per-(view, bin) table [np][nu][B::kBinF4], or null
+    const float4* bins = nullptr;    // basis-specific per-(view, bin) table [np][B::kBinF4][nu] (planes), or null
+    float* imgT = nullptr;           // [nj][ni] transposed copy of the image for i-major strips (forward scratch)
     const float4* strips = nullptr;  // [np][nblk][2] forward block strips (fan2d.cuh)
     int nblk = 0;                    // bin blocks of kF2Block bins per view
     const int2* twin = nullptr;      // [tiles][np] back-projection tile bin windows

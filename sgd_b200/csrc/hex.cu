@@ -30,6 +30,7 @@
 // "H0 corrected" bounds the true hexagon of each site and has no skip test:
 // the pair is then an exact transpose.
 #include <cmath>
+#include <cstring>
 
 #include "common.h"
 #include "proj2d_impl.cuh"
@@ -52,9 +53,10 @@ struct HexBasis {
         float h0, h1, h2, h3, h4, h5;
         int mode, back;
     };
-    // per bin, eight double words: va, vb, vc | FP32 va, vb | 1/va, 1/vb, 1/vc
-    // (a zero reciprocal where the direction is dropped) | FP32 vc, 0
-    static constexpr int kBinF4 = 4;
+    // per bin: Hl three 16-byte words of FP64 pairs (va, vb) (vc, 1/va)
+    // (1/vb, 1/vc) (a zero reciprocal where the direction is dropped); H0 one
+    // word of FP32 (va, vb, vc, 0)
+    static constexpr int kBinF4 = M == kHl ? 3 : 1;
     struct Cell {
         float ox, oy, sx, sy;  // site; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
@@ -183,20 +185,25 @@ struct HexBasis {
         }
         return v[0] * (1.0 / 6.0);
     }
+    __device__ static double2 as_double2(float4 f) {
+        double2 d;
+        memcpy(&d, &f, sizeof(d));
+        return d;
+    }
     // the reference's FP32 stepping of the bin centre
     __device__ static void skip(const View& V, Cell& c) {
         c.sx += V.puvx;
         c.sy += V.puvy;
     }
-    __device__ static float value(const View& V, Cell& c, int, const float4* t, const Fan2DParams&) {
+    __device__ static float value(const View& V, Cell& c, int, BinRef t, const Fan2DParams&) {
         const float sx = c.sx, sy = c.sy;
         skip(V, c);
         const float px = V.srcx, py = V.srcy, ox = c.ox, oy = c.oy;
         const float ax = sx - V.puvx * 0.5f, ay = sy - V.puvy * 0.5f;
         const float bx = sx + V.puvx * 0.5f, by = sy + V.puvy * 0.5f;
-        const float num = ((ox - px) * (sx - px) + (oy - py) * (sy - py));
-        const float dena = ((ax - px) * (sx - px) + (ay - py) * (sy - py));
-        const float denb = ((bx - px) * (sx - px) + (by - py) * (sy - py));
+        const float num = dot2f(ox - px, sx - px, oy - py, sy - py);
+        const float dena = dot2f(ax - px, sx - px, ay - py, sy - py);
+        const float denb = dot2f(bx - px, sx - px, by - py, sy - py);
         const float ra = num / dena, rb = num / denb;
         const float ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;
         const float bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
@@ -205,7 +212,6 @@ struct HexBasis {
             if (da > V.dt && db > V.dt && (ax1 - ox) * (bx1 - ox) >= 0.0f && (ay1 - oy) * (by1 - oy) >= 0.0f)
                 return 0.f;
         }
-        const double* b = reinterpret_cast<const double*>(t);
         // the edge rays' separation and the site's offset: the reference takes
         // FP64 square roots of these FP32 differences; their FP32 roots differ
         // by at most an ulp, far below the FP32 geometry's own rounding
@@ -214,15 +220,17 @@ struct HexBasis {
         float fy = sqrtf(fmaf(dax, dax, day * day));
         if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) fy = -fy;
         if (M == kHl) {
-            const double va = b[0], vb = b[1], vc = b[2], y = (double)fy, vblur = (double)fblur;
+            const double2 w0 = as_double2(t[0]), w1 = as_double2(t[1]), w2 = as_double2(t[2]);
+            const double va = w0.x, vb = w0.y, vc = w1.x, y = (double)fy, vblur = (double)fblur;
             double conv;
             if (fabs(vblur) > 1e-8 && fabs(va) > 1e-8 && fabs(vb) > 1e-8 && fabs(vc) > 1e-8)
-                conv = conv4_full(y, vblur, va, vb, vc, b[4], b[5], b[6]);
+                conv = conv4_full(y, vblur, va, vb, vc, w1.y, w2.x, w2.y);
             else
                 conv = conv4(y, vblur, va, vb, vc);
             return (conv == conv && conv > 0.0) ? (float)conv : 0.f;
         }
-        const float va = t[1].z, vb = t[1].w, vc = t[3].z;  // the FP32 copies
+        const float4 w = t[0];
+        const float va = w.x, vb = w.y, vc = w.z;
         const float conv = conv3(fy, fblur, va, vb) + conv3(fy, fblur, vb, vc) + conv3(fy, fblur, vc, va);
         return (conv == conv && conv > 0.f) ? conv : 0.f;
     }
@@ -250,8 +258,8 @@ public:
         const float fdy = fdt * (mode == kHl ? 0.5f : 1.5f);
         constexpr int kVF = HexBasis<kHl>::kViewFloats;
         std::vector<float> view((size_t)np * kVF, 0.f);
-        std::vector<float4> bins((size_t)np * nu * 4);
-        double* bd = reinterpret_cast<double*>(bins.data());
+        const int nw = (mode == kHl) ? HexBasis<kHl>::kBinF4 : HexBasis<kH0Corrected>::kBinF4;
+        std::vector<float4> bins((size_t)np * nu * nw);
         std::vector<BinHomography> hom;
         bin_homographies(geo, hom);
         for (int p = 0; p < np; ++p) {
@@ -278,19 +286,17 @@ public:
                 const float sx = (float)f.dtv[0] + (float)f.puv[0] * (u - 0.5f * nu + 0.5f);
                 const float sy = (float)f.dtv[1] + (float)f.puv[1] * (u - 0.5f * nu + 0.5f);
                 const float th = std::atan2(sx - px, sy - py);
-                double* o = bd + ((size_t)p * nu + u) * 8;
+                double o[6];
                 o[0] = (double)fdt * std::sin((double)th);
                 o[1] = (double)fdt * std::sin((double)th + 2.0 * kPi / 3.0);
                 o[2] = (double)fdt * std::sin((double)th + 4.0 * kPi / 3.0);
-                // the spare fourth and eighth words hold the FP32 copies the
-                // H0 spline takes
-                for (int k = 0; k < 3; ++k) o[4 + k] = std::fabs(o[k]) > 1e-8 ? 1.0 / o[k] : 0.0;
-                float* f = reinterpret_cast<float*>(o + 3);
-                f[0] = (float)o[0];
-                f[1] = (float)o[1];
-                float* g = reinterpret_cast<float*>(o + 7);
-                g[0] = (float)o[2];
-                g[1] = 0.f;
+                for (int k = 0; k < 3; ++k) o[3 + k] = std::fabs(o[k]) > 1e-8 ? 1.0 / o[k] : 0.0;
+                float4* w = &bins[(size_t)p * nw * nu + u];  // planes of nu words
+                if (mode == kHl) {
+                    for (int k = 0; k < 3; ++k) std::memcpy(&w[(size_t)k * nu], &o[2 * k], 16);
+                } else {
+                    w[0] = make_float4((float)o[0], (float)o[1], (float)o[2], 0.f);
+                }
             }
         }
         back_view_ = view;

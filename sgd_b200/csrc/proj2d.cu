@@ -188,6 +188,8 @@ void Proj2D::finish_init(const std::vector<float>& view, const std::vector<float
 
     const size_t nimg = (size_t)P.ni * P.nj, nsino = (size_t)np * nu;
     SGD_CUDA(cudaMalloc(&d_img_, nimg * sizeof(float)));
+    SGD_CUDA(cudaMalloc(&d_imgT_, nimg * sizeof(float)));
+    P.imgT = d_imgT_;
     SGD_CUDA(cudaMalloc(&d_sino_, nsino * sizeof(float)));
     SGD_CUDA(cudaMallocHost(&h_img_, nimg * sizeof(float)));
     SGD_CUDA(cudaMallocHost(&h_sino_, nsino * sizeof(float)));
@@ -201,6 +203,7 @@ Proj2D::~Proj2D() {
     cudaFree(d_twin_);
     cudaFree(d_err_);
     cudaFree(d_img_);
+    cudaFree(d_imgT_);
     cudaFree(d_sino_);
     cudaFreeHost(h_img_);
     cudaFreeHost(h_sino_);

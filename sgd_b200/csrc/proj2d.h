@@ -70,6 +70,7 @@ protected:
     int2* d_twin_ = nullptr;
     int* d_err_ = nullptr;
     float* d_img_ = nullptr;
+    float* d_imgT_ = nullptr;  // the forward's line-major image copy
     float* d_sino_ = nullptr;
     float* h_img_ = nullptr;
     float* h_sino_ = nullptr;

@@ -13,6 +13,8 @@ namespace sgd {
 
 template <class B>
 void fan2d_forward(const Fan2DParams& P, const float* img, float* sino, float scale, cudaStream_t s) {
+    fan2d_transpose_kernel<<<dim3((P.nj + 31) / 32, (P.ni + 31) / 32), dim3(32, 8), 0, s>>>(img, P.imgT, P.ni, P.nj);
+    SGD_LAUNCH_CHECK();
     dim3 grid(P.nblk, P.np);
     fan2d_forward_kernel<B><<<grid, kF2FwdWarps * 32, 0, s>>>(P, img, sino, scale);
     SGD_LAUNCH_CHECK();
@@ -58,7 +60,7 @@ struct Fan2DVisit {
         typename B::Cell c;
         B::setup(V, i, j, P, c);
         for (int u = c.lo; u <= c.hi; ++u) {
-            const float v = B::value(V, c, u, P.bins + ((size_t)p * P.nu + u) * B::kBinF4, P);
+            const float v = B::value(V, c, u, BinRef{P.bins + (size_t)p * B::kBinF4 * P.nu + u, P.nu}, P);
             if (v != 0.f) f(u, v * scale);
         }
     }

@@ -67,7 +67,7 @@ struct SFBasis {
         // dx / max(|sin t|, |cos t|) for t = atan2(X, Y) (:174-177) without
         // the trigonometry: |sin t| = |X| / r, |cos t| = |Y| / r
         const float X = V.dx * (ix - V.nx2) - V.srcx, Y = V.dy * (iy - V.ny2) - V.srcy;
-        c.weight = V.dx * sqrtf(X * X + Y * Y) * __fdividef(1.0f, fmaxf(fabsf(X), fabsf(Y)));
+        c.weight = V.dx * sqrtf(dot2f(X, X, Y, Y)) * __fdividef(1.0f, fmaxf(fabsf(X), fabsf(Y)));
         // per-bin constants of gamma_calculate (:48-84), once per cell and
         // view (fast reciprocals: within an ulp or two of the reference's
         // divisions; a zero-width ramp still gives an infinite factor whose
@@ -93,7 +93,7 @@ struct SFBasis {
         if (tmp == tmp) g += tmp;
         return g;
     }
-    __device__ static float value(const View&, Cell& c, int u, const float4*, const Fan2DParams&) {
+    __device__ static float value(const View&, Cell& c, int u, BinRef, const Fan2DParams&) {
         const float g = gamma((float)u, u + 1.0f, c);
         const float val = c.weight * g;
         return (g > 1e-7f && val == val) ? val : 0.f;

@@ -39,7 +39,7 @@ __device__ __forceinline__ float box3(float y, float v1, float v2, float v3) {
     const float a = K3 - yc, b = K0 - yc;
     const float p_top = 0.5f * a * a * rp;                      // K2 <= y < K3
     const float p_ramp = ((x0 + x1) * 0.5f - yc) * x2 * rp;     // K1 <= y < K2
-    const float p_flat_in = h - (K0 * K0 + yc * yc) * rp;       // y < -K0
+    const float p_flat_in = h - __fmaf_rn(K0, K0, __fmul_rn(yc, yc)) * rp;  // y < -K0 (K0^2 + yc^2, one fixed contraction)
     const float p_shoulder = h - 0.5f * b * b * rp;             // K0 <= y < K1
     float v = yc < K0 ? h : p_shoulder;
     v = yc < -K0 ? p_flat_in : v;

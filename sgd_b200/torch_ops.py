@@ -65,7 +65,8 @@ class FanProjector:
             self.launches_per_step = 3
         else:
             self.kernels = {"forward": "fan2d_forward_kernel", "back": "fan2d_back_kernel"}
-            self.launches_per_step = 2
+            # image transpose + forward kernel, back kernel
+            self.launches_per_step = 3
         self._fwd = getattr(L, f"sgd_{kind}_forward_dev")
         self._bwd = getattr(L, f"sgd_{kind}_backward_dev")
         self._destroy = getattr(L, f"{pre}_destroy")
@@ -109,9 +110,10 @@ class _HandleProjector:
     and ``bwd(h, in, out, stream)``: the common body of the projectors below."""
 
     # the library's kernels behind each direction, and the launches of one
-    # forward + back projection (the generic 2D kernels: one each)
+    # forward + back projection (the generic 2D kernels: the forward's image
+    # transpose and kernel, the back kernel)
     kernels = {"forward": "fan2d_forward_kernel", "back": "fan2d_back_kernel"}
-    launches_per_step = 2
+    launches_per_step = 3
 
     def _setup(self, handle, fwd, bwd, destroy, image_shape, sino_shape, what):
         if not handle:
@@ -203,8 +205,11 @@ class ConeProjector(_HandleProjector):
         if kind == "b1_3d":
             # column transpose + forward kernel, back kernel
             self.kernels = {"forward": "b1_3d_fwd_kernel", "back": "b1_3d_back_kernel"}
+        elif exact:
+            # column transpose + factored forward kernel, back kernel
+            self.kernels = {"forward": "sf3d_fwd_kernel", "back": "sf3d_back1_kernel"}
         else:
-            # forward kernel + FP64-to-FP32 finish, back kernel
+            # the reference's scatter + FP64-to-FP32 finish, its gather
             self.kernels = {"forward": "sf3d_forward_kernel", "back": "sf3d_back_kernel"}
         self.launches_per_step = 3
         self._keep = angles

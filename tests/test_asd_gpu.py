@@ -157,14 +157,16 @@ def test_asd_pocs_matches_fp64_restatement(oracle_mod):
     relative change of ~ulp / sqrt(eps) ~ 6e-4.  The same restatement with
     only its TV gradient rounded to FP32 differs from the FP64 one by 2.5e-4
     after three iterations and 6.3e-4 after four, so four iterations are held
-    to 2e-3."""
+    to 2e-3 (and the TV step lengths, which the same rounding moves by 1e-3,
+    to 5e-3)."""
     from sgd_b200.asd import ASDPOCS, Geometry, simulate
     geo = Geometry(32, 24)
     n, _, nu, dx, dy, du, lsd, lso, ang = geo.slice()
     truth, sino, _ = simulate(geo, [5], i0=0.0)
     A = oracle_mod.b1_matrix(n, n, nu, dx, dy, du, lsd, lso, ang, np.arange(len(ang)))
     b = sino[0].double().cpu().numpy().ravel()
-    for iters, tol in ((2, 1e-4), (4, 2e-3)):
+    # (iterations, image tolerance, tolerance of the TV step lengths)
+    for iters, tol, tol_tv in ((2, 1e-4, 1e-3), (4, 2e-3, 5e-3)):
         s = ASDPOCS(geo, 1, nonneg=False)
         s.set_data(sino, hist_cap=iters)
         s.run(iters)
@@ -175,7 +177,7 @@ def test_asd_pocs_matches_fp64_restatement(oracle_mod):
         assert rel_l2(x_gpu, x_ref) < tol, iters
         h = s.history(iters)[:, 0, :].astype(np.float64)
         assert np.allclose(h[:, 0], h_ref[:, 0], rtol=1e-4) and np.allclose(h[:, 1], h_ref[:, 1], rtol=1e-4)
-        assert np.allclose(h[1:, 2], h_ref[1:, 2], rtol=1e-3) and h[0, 2] == 0.0
+        assert np.allclose(h[1:, 2], h_ref[1:, 2], rtol=tol_tv) and h[0, 2] == 0.0
 
 
 def test_positivity_constraint():

@@ -12,7 +12,7 @@ here faults or hangs a GPU: the copies complete, only the wait is cut short.
 import numpy as np
 import pytest
 
-from geometry_cases import fan_case
+from geometry_cases import cone_case, fan_case
 from sgd_b200 import _lib
 
 torch = pytest.importorskip("torch")
@@ -86,4 +86,32 @@ def test_batch_back_projection_wait_failure_is_reported_and_recoverable():
     B.backward(sino, again)
     torch.cuda.synchronize()
     B.status()
+    assert torch.equal(again, good)
+
+
+@pytest.mark.parametrize("kind", ["b1_3d", "sf3d"])
+def test_cone_back_projection_wait_failure_is_reported_and_recoverable(kind):
+    """The cone-beam back projectors (exact-transpose pairs): a CTA that gives
+    up on its staged view leaves its voxels unwritten and raises the flag."""
+    from sgd_b200.torch_ops import ConeProjector
+    L = _lib.lib()
+    nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, ang = cone_case("small")
+    P = ConeProjector(kind, nx, ny, nz, nu, nv, dx, dy, dz, du, dv, lsd, lso, ang)
+    set_limit = getattr(L, f"sgd_{kind}_set_wait_limit")
+    status = getattr(L, f"sgd_{kind}_status")
+    y = _sino(P)
+    good = P.backward(y).clone()
+    assert status(P.handle) == 0
+    out = torch.full(P.image_shape, SENTINEL, device="cuda")
+    try:
+        assert set_limit(P.handle, 0) == 0
+        P.backward(y, out=out)
+        assert status(P.handle) == -1
+        assert "wait" in _lib.last_error()
+    finally:
+        assert set_limit(P.handle, DEFAULT_POLLS) == 0
+    assert torch.all(out == SENTINEL)
+    assert status(P.handle) == 0
+    again = P.backward(y)
+    assert status(P.handle) == 0
     assert torch.equal(again, good)

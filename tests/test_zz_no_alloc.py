@@ -43,6 +43,42 @@ def test_noalloc_forward_matches_allocating_entry_point_twice():
         assert rel_l2(o, r) < TOL
 
 
+def test_noalloc_call_allocates_nothing():
+    """After the first call (which looks up the scratch array's address), a
+    call changes no device allocation: the free device memory is the same
+    before and after it, and it records into a CUDA graph under the global
+    capture mode, in which cudaMalloc is an error; the replayed graph gives
+    the projection."""
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required")
+    from sgd_b200.torch_ops import FanProjector
+    f = _entry()
+    nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case("small")
+    P = FanProjector("b1", nx, ny, nu, dx, dy, du, lsd, lso, ang)
+    img = torch.tensor(ellipse_phantom(nx, ny, dx, dy, seed=2), dtype=torch.float32, device="cuda")
+    out = torch.zeros(P.sino_shape, dtype=torch.float32, device="cuda")
+    ref = P.forward(img)
+
+    def call():
+        s = torch.cuda.current_stream().cuda_stream
+        return f(P.handle, ctypes.c_void_p(img.data_ptr()), ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s))
+
+    assert call() == 0  # first call: address lookup
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    assert call() == 0
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    out.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, capture_error_mode="global"):
+        assert call() == 0
+    g.replay()
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), ref.cpu().numpy()) < TOL
+    del g
+
+
 def test_noalloc_rejects_images_beyond_its_scratch():
     if not torch.cuda.is_available():
         pytest.fail("CUDA device required")
