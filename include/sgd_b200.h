@@ -263,10 +263,11 @@ int sgd_b1_3d_set_wait_limit(void* layer, unsigned limit);
  * voxel value and amplitude, drops out-of-detector bins, and its backward is
  * the exact transpose of its forward.  trap_v: SF-TT (trapezoid in v) in the
  * forward (the reference's `tt` argument); mode 1's backward follows it.
- * The FP64 host entry points round through the FP32 device path, as the
- * reference's SF class does; accumulation is FP64 in both modes.  Mode 1
- * needs a circular orbit (the detector's u row of every projection matrix
- * free of z, which geo_init_angles geometries are). */
+ * The FP64 host entry points round their inputs to FP32 as the reference's
+ * SF class does; mode 1 returns its FP64 accumulators, mode 0 rounds its
+ * output to FP32 as the reference does; the *_dev entry points are FP32.
+ * Mode 1 needs a circular orbit (the detector's u row of every projection
+ * matrix free of z, which geo_init_angles geometries are). */
 void* sgd_sf3d_init(int mode, int trap_v, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy,
                     double dz, double du, double dv, double lsd, double lso, double* angles);
 int sgd_sf3d_forward_projection(double* b, double* x, void* layer);

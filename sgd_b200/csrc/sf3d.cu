@@ -51,6 +51,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include <cuda.h>
@@ -299,18 +300,24 @@ struct SFPlan {
 // over more than twice its width (sf_voxel's skip).
 struct SFCol {
     float us[4];
-    float tw, pmv2, pmv3, tv1, tv2, tv3, tv4;
-    double ddx, ddy;
+    float tw, pmv2, inv3, tv1, tv2, invt3, invt4;
+    float rho2;  // squared in-plane distance of the column from the source
     int min_u, max_u;
 };
+
+// a * b + c * d + e with fixed contractions, so that every kernel inlining
+// these functions forms the same bits
+__device__ __forceinline__ float lin3(float a, float b, float c, float d, float e) {
+    return __fadd_rn(__fmaf_rn(a, b, __fmul_rn(c, d)), e);
+}
 
 __device__ __forceinline__ bool sf_column(const SFGeo& G, const float* pm, const double* src, int ix, int iy,
                                           SFCol& c) {
     const float signy1 = iy - 0.5f, signy2 = iy + 0.5f, signx1 = ix - 0.5f, signx2 = ix + 0.5f;
-    const float u1 = pm[0] * signx1 + pm[1] * signy1 + pm[3], u2 = pm[8] * signx1 + pm[9] * signy1 + pm[11];
-    const float u3 = pm[0] * signx2 + pm[1] * signy1 + pm[3], u4 = pm[8] * signx2 + pm[9] * signy1 + pm[11];
-    const float u5 = pm[0] * signx1 + pm[1] * signy2 + pm[3], u6 = pm[8] * signx1 + pm[9] * signy2 + pm[11];
-    const float u7 = pm[0] * signx2 + pm[1] * signy2 + pm[3], u8 = pm[8] * signx2 + pm[9] * signy2 + pm[11];
+    const float u1 = lin3(pm[0], signx1, pm[1], signy1, pm[3]), u2 = lin3(pm[8], signx1, pm[9], signy1, pm[11]);
+    const float u3 = lin3(pm[0], signx2, pm[1], signy1, pm[3]), u4 = lin3(pm[8], signx2, pm[9], signy1, pm[11]);
+    const float u5 = lin3(pm[0], signx1, pm[1], signy2, pm[3]), u6 = lin3(pm[8], signx1, pm[9], signy2, pm[11]);
+    const float u7 = lin3(pm[0], signx2, pm[1], signy2, pm[3]), u8 = lin3(pm[8], signx2, pm[9], signy2, pm[11]);
     c.us[0] = u1 / u2;
     c.us[1] = u3 / u4;
     c.us[2] = u5 / u6;
@@ -321,14 +328,17 @@ __device__ __forceinline__ bool sf_column(const SFGeo& G, const float* pm, const
     c.min_u = (int)min_u;
     c.max_u = (int)max_u;
     c.tw = (2 / (((c.us[3] - c.us[0]) + (c.us[2] - c.us[1]))));
-    c.pmv2 = pm[4] * ix + pm[5] * iy + pm[7];
-    c.pmv3 = pm[8] * ix + pm[9] * iy + pm[11];
-    c.tv1 = pm[4] * signx1 + pm[5] * iy + pm[7];
-    c.tv2 = pm[4] * signx2 + pm[5] * iy + pm[7];
-    c.tv3 = pm[8] * signx1 + pm[9] * iy + pm[11];
-    c.tv4 = pm[8] * signx2 + pm[9] * iy + pm[11];
-    c.ddx = G.dx * (ix - G.nx / 2) - src[0];
-    c.ddy = G.dy * (iy - G.ny / 2) - src[1];
+    // the axial rectangle's ends and trapezoid's corners are (n + pm[6] s) /
+    // d with d free of z (pm[10] = 0): one reciprocal per column
+    const float fix = (float)ix, fiy = (float)iy;
+    c.pmv2 = lin3(pm[4], fix, pm[5], fiy, pm[7]);
+    c.inv3 = __frcp_rn(lin3(pm[8], fix, pm[9], fiy, pm[11]));
+    c.tv1 = lin3(pm[4], signx1, pm[5], fiy, pm[7]);
+    c.tv2 = lin3(pm[4], signx2, pm[5], fiy, pm[7]);
+    c.invt3 = __frcp_rn(lin3(pm[8], signx1, pm[9], fiy, pm[11]));
+    c.invt4 = __frcp_rn(lin3(pm[8], signx2, pm[9], fiy, pm[11]));
+    const double ddx = G.dx * (ix - G.nx / 2) - src[0], ddy = G.dy * (iy - G.ny / 2) - src[1];
+    c.rho2 = (float)(ddx * ddx + ddy * ddy);
     return true;
 }
 
@@ -342,35 +352,68 @@ struct SFAx {
     int min_v, max_v;
 };
 
-__device__ __forceinline__ bool sf_axial(const SFGeo& G, const float* pm, const SFCol& c, double srcz, double factor,
-                                         bool trap, int iz, SFAx& a) {
-    const float signz1 = (iz - 0.5f), signz2 = (iz + 0.5f);
+// sf_gamma with its differences of squares contracted one fixed way
+// (a*a - b*b as fma(a, a, -(b*b))), for the corrected pair, whose forward and
+// back kernels must form the same bits.
+__device__ __forceinline__ float sf_gamma1(float s1, float s2, const float* us) {
+    auto sq_diff = [](float a, float b) { return __fmaf_rn(a, a, -__fmul_rn(b, b)); };
+    float g = 0.0f, tmp, b1, b2;
+    b1 = fmaxf(s1, us[0]);
+    b2 = fminf(s2, us[1]);
+    tmp = (b2 > b1) ? (1 / (2 * (us[1] - us[0]))) * sq_diff(b2 - us[0], b1 - us[0]) : 0.0f;
+    if (tmp == tmp) g += tmp;
+    b1 = fmaxf(s1, us[1]);
+    b2 = fminf(s2, us[2]);
+    tmp = (b2 > b1) ? b2 - b1 : 0.0f;
+    if (tmp == tmp) g += tmp;
+    b1 = fmaxf(s1, us[2]);
+    b2 = fminf(s2, us[3]);
+    tmp = (b2 > b1) ? (1 / (2 * (us[3] - us[2]))) * sq_diff(b1 - us[3], b2 - us[3]) : 0.0f;
+    if (tmp == tmp) g += tmp;
+    return g;
+}
+
+// End k of a column's axial rectangles: the image of z = k - 1/2 (consecutive
+// voxels share their ends bit for bit).
+__device__ __forceinline__ float sf_end(const SFCol& c, float pm6, int k) {
+    return __fmul_rn(__fmaf_rn(pm6, k - 0.5f, c.pmv2), c.inv3);
+}
+
+// The forward amplitude of voxel iz without its axial width: the view factor
+// times 2 / (trapezoid width) over the squared distance from the source
+// (FP32, fast reciprocal: the FP64 distance of sf_voxel agrees to ~1e-7).
+__device__ __forceinline__ float sf_amp(const SFGeo& G, const SFCol& c, float dzf, float srcz, float factor, int iz) {
+    const float ddz = __fmaf_rn(dzf, (float)(iz - G.nz / 2), -srcz);
+    return __fdividef(__fmul_rn(factor, c.tw), __fmaf_rn(ddz, ddz, c.rho2));
+}
+
+__device__ __forceinline__ bool sf_axial(const SFGeo& G, const float* pm, const SFCol& c, float dzf, float srcz,
+                                         float factor, bool trap, int iz, SFAx& a) {
     float min_v, max_v;
     if (!trap) {
-        a.vs[0] = (c.pmv2 + pm[6] * signz1) / (c.pmv3 + pm[10] * signz1);
+        a.vs[0] = sf_end(c, pm[6], iz);
         min_v = ceilf(a.vs[0] - 0.5f);
         if (min_v >= G.nv) return false;
-        a.vs[1] = (c.pmv2 + pm[6] * signz2) / (c.pmv3 + pm[10] * signz2);
+        a.vs[1] = sf_end(c, pm[6], iz + 1);
         max_v = ceilf(a.vs[1] - 0.5f);
         if (max_v < 0) return false;
     } else {
-        a.vs[0] = (c.tv1 + pm[6] * signz1) / (c.tv3 + pm[10] * signz1);
-        a.vs[1] = (c.tv1 + pm[6] * signz2) / (c.tv3 + pm[10] * signz2);
-        a.vs[2] = (c.tv2 + pm[6] * signz1) / (c.tv4 + pm[10] * signz1);
-        a.vs[3] = (c.tv2 + pm[6] * signz2) / (c.tv4 + pm[10] * signz2);
+        const float signz1 = (iz - 0.5f), signz2 = (iz + 0.5f);
+        a.vs[0] = __fmul_rn(__fmaf_rn(pm[6], signz1, c.tv1), c.invt3);
+        a.vs[1] = __fmul_rn(__fmaf_rn(pm[6], signz2, c.tv1), c.invt3);
+        a.vs[2] = __fmul_rn(__fmaf_rn(pm[6], signz1, c.tv2), c.invt4);
+        a.vs[3] = __fmul_rn(__fmaf_rn(pm[6], signz2, c.tv2), c.invt4);
         sort4f(a.vs);
         min_v = ceilf(a.vs[0] - 0.5f);
         max_v = ceilf(a.vs[3] - 0.5f);
         if ((max_v < 0) || (min_v >= G.nv)) return false;
     }
     if (!(max_v - min_v <= 2.f * G.nv + 4.f)) return false;
-    const double ddz = G.dz * (iz - G.nz / 2) - srcz;
-    float weight = rsqrtf((float)(c.ddx * c.ddx + c.ddy * c.ddy + ddz * ddz));
-    weight *= weight;
+    const float amp = sf_amp(G, c, dzf, srcz, factor, iz);
     if (trap)
-        a.C = (float)(weight * factor * c.tw * (2 / ((a.vs[3] - a.vs[0]) + (a.vs[2] - a.vs[1]))));
+        a.C = amp * __fdividef(2.f, (a.vs[3] - a.vs[0]) + (a.vs[2] - a.vs[1]));
     else
-        a.C = (float)(weight * factor * c.tw * (1 / (a.vs[1] - a.vs[0])));
+        a.C = amp * __fdividef(1.f, a.vs[1] - a.vs[0]);
     a.min_v = max(0, (int)min_v);
     a.max_v = min(G.nv - 1, (int)max_v);
     return true;
@@ -378,7 +421,7 @@ __device__ __forceinline__ bool sf_axial(const SFGeo& G, const float* pm, const 
 
 // axial footprint of row j (sf_fv)
 __device__ __forceinline__ float sf_row(const SFAx& a, bool trap, int j) {
-    if (trap) return sf_gamma(j - 0.5f, j + 0.5f, a.vs);
+    if (trap) return sf_gamma1(j - 0.5f, j + 0.5f, a.vs);
     return fmaxf(fminf(j + 0.5f, a.vs[1]) - fmaxf(j - 0.5f, a.vs[0]), 0.f);
 }
 
@@ -389,14 +432,11 @@ __host__ __device__ constexpr size_t sf_fwd_smem(int nv) {
 
 // The voxel weight C(z) vol(z) of sf_axial for a rectangle whose ends vs0,
 // vs1 were formed already (the same expressions): 0 where sf_axial skips.
-__device__ __forceinline__ double sf_rect_weight(const SFGeo& G, const SFCol& c, double srcz, double factor, int iz,
-                                                 float vs0, float vs1, float C0) {
+__device__ __forceinline__ double sf_rect_weight(const SFGeo& G, const SFCol& c, float dzf, float srcz, float factor,
+                                                 int iz, float vs0, float vs1, float C0) {
     const float min_v = ceilf(vs0 - 0.5f), max_v = ceilf(vs1 - 0.5f);
     if (min_v >= G.nv || max_v < 0 || !(max_v - min_v <= 2.f * G.nv + 4.f)) return 0.0;
-    const double ddz = G.dz * (iz - G.nz / 2) - srcz;
-    float weight = rsqrtf((float)(c.ddx * c.ddx + c.ddy * c.ddy + ddz * ddz));
-    weight *= weight;
-    const float C = (float)(weight * factor * c.tw * (1 / (vs1 - vs0)));
+    const float C = sf_amp(G, c, dzf, srcz, factor, iz) * __fdividef(1.f, vs1 - vs0);
     return C == C ? (double)C * (double)C0 : 0.0;
 }
 
@@ -407,20 +447,17 @@ __device__ __forceinline__ double sf_rect_weight(const SFGeo& G, const SFCol& c,
 // the few voxels that overlap its row in FP64 (rows at the chunk's edges add
 // to what the previous chunk left).  No atomics; every term as the back
 // projection forms it.
-__device__ __forceinline__ void sf_rect_profile(const SFGeo& G, const float* pm, const SFCol& c, double srcz,
-                                                double factor, const float* __restrict__ colv, int l, float* T,
-                                                double* W, double* Aw) {
+__device__ __forceinline__ void sf_rect_profile(const SFGeo& G, const float* pm, const SFCol& c, float dzf,
+                                                float srcz, float factor, const float* __restrict__ colv, int l,
+                                                float* T, double* W, double* Aw) {
     const int nz = G.nz, nv = G.nv;
     for (int z0 = 0; z0 < nz; z0 += kZC) {
         const int zn = min(kZC, nz - z0);
-        for (int k = l; k <= zn; k += 32) {
-            const float sz = (z0 + k) - 0.5f;
-            T[k] = (c.pmv2 + pm[6] * sz) / (c.pmv3 + pm[10] * sz);
-        }
+        for (int k = l; k <= zn; k += 32) T[k] = sf_end(c, pm[6], z0 + k);
         __syncwarp();
         for (int k = l; k < zn; k += 32) {
             const float C0 = __ldg(colv + z0 + k);
-            W[k] = C0 == 0.f ? 0.0 : sf_rect_weight(G, c, srcz, factor, z0 + k, T[k], T[k + 1], C0);
+            W[k] = C0 == 0.f ? 0.0 : sf_rect_weight(G, c, dzf, srcz, factor, z0 + k, T[k], T[k + 1], C0);
         }
         __syncwarp();
         const float tlo = T[0], thi = T[zn];
@@ -446,8 +483,11 @@ __device__ __forceinline__ void sf_rect_profile(const SFGeo& G, const float* pm,
     }
 }
 
+// TOut: float (device entry points) or double (the FP64 host entry points
+// return the FP64 accumulators as they are)
+template <typename TOut>
 __global__ void __launch_bounds__(kFW * 32, 3) sf3d_fwd_kernel(SFGeo G, SFPlan K, const float* __restrict__ volT,
-                                                            float* __restrict__ proj) {
+                                                            TOut* __restrict__ proj) {
     extern __shared__ __align__(16) unsigned char sf_fsmem[];
     const int nv = G.nv, nz = G.nz;
     double* acc = reinterpret_cast<double*>(sf_fsmem);  // [kUB][nv]
@@ -498,7 +538,7 @@ __global__ void __launch_bounds__(kFW * 32, 3) sf3d_fwd_kernel(SFGeo G, SFPlan K
 
     const float* pm = G.pmi + 12 * (size_t)p;
     const double* src = G.src + 3 * (size_t)p;
-    const double factor = G.fwdf[p];
+    const float factor = (float)G.fwdf[p], srcz = (float)src[2], dzf = (float)G.dz;
     const bool trap = G.trap != 0;
     double* Aw = A + w * nv;
     for (int base = 0; base < total; base += kFW) {
@@ -525,7 +565,7 @@ __global__ void __launch_bounds__(kFW * 32, 3) sf3d_fwd_kernel(SFGeo G, SFPlan K
                         float gv = 0.f;
                         if (l >= blo && l <= bhi) {
                             const int i = u0 + l;
-                            gv = sf_gamma(i - 0.5f, i + 0.5f, c.us);
+                            gv = sf_gamma1(i - 0.5f, i + 0.5f, c.us);
                             if (!(gv == gv)) gv = 0.f;
                         }
                         cs[w * kUB + l] = gv;
@@ -534,7 +574,7 @@ __global__ void __launch_bounds__(kFW * 32, 3) sf3d_fwd_kernel(SFGeo G, SFPlan K
                     __syncwarp();
                     const float* colv = volT + ((size_t)iy * G.nx + ix) * nz;
                     if (!trap) {
-                        sf_rect_profile(G, pm, c, src[2], factor, colv, l, Tz + w * (kZC + 2), Wz + w * kZC, Aw);
+                        sf_rect_profile(G, pm, c, dzf, srcz, factor, colv, l, Tz + w * (kZC + 2), Wz + w * kZC, Aw);
                     } else {
                         // trapezoids of neighbouring voxels overlap: FP64
                         // shared-memory atomics over each voxel's rows
@@ -542,7 +582,7 @@ __global__ void __launch_bounds__(kFW * 32, 3) sf3d_fwd_kernel(SFGeo G, SFPlan K
                             const float C0 = __ldg(colv + iz);
                             if (C0 == 0.f) continue;
                             SFAx a;
-                            if (!sf_axial(G, pm, c, src[2], factor, trap, iz, a)) continue;
+                            if (!sf_axial(G, pm, c, dzf, srcz, factor, trap, iz, a)) continue;
                             const double wv = (double)a.C * (double)C0;
                             for (int j = a.min_v; j <= a.max_v; ++j) {
                                 const float f = sf_row(a, trap, j);
@@ -575,7 +615,7 @@ __global__ void __launch_bounds__(kFW * 32, 3) sf3d_fwd_kernel(SFGeo G, SFPlan K
     }
     for (int e = tid; e < nb * nv; e += blockDim.x) {
         const int v = e / nb, b = e - v * nb;
-        proj[((size_t)p * nv + v) * G.nu + u0 + b] = (float)acc[b * nv + v];
+        proj[((size_t)p * nv + v) * G.nu + u0 + b] = (TOut)acc[b * nv + v];
     }
 }
 
@@ -589,9 +629,10 @@ __host__ __device__ constexpr size_t sf_back_smem(int nv) {
 // The exact transpose of sf3d_fwd_kernel.  use_tma: the projection is staged
 // through `map` (a tensor map of proj, extents (nu, nv, np)); otherwise read
 // from global memory.
+template <typename TOut>
 __global__ void __launch_bounds__(kTX * kTY * 32, 2) sf3d_back1_kernel(const __grid_constant__ CUtensorMap map,
                                                                     SFGeo G, SFPlan K, const float* __restrict__ proj,
-                                                                    float* __restrict__ vol, int use_tma) {
+                                                                    TOut* __restrict__ vol, int use_tma) {
     extern __shared__ __align__(128) unsigned char sf_bsmem[];
     const int nv = G.nv, nu = G.nu, nvp = sf_rows_padded(nv), nboxes = nvp / kRowBox;
     // [2][nvp][kWin], every TMA box (kRowBox rows of kWin floats) on a
@@ -660,6 +701,7 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 2) sf3d_back1_kernel(const __g
         const float* gp = proj + (size_t)p * nv * nu;
         const float* pm = G.pmi + 12 * (size_t)p;
         const double* src = G.src + 3 * (size_t)p;
+        const float srczf = (float)src[2], factorf = (float)G.fwdf[p], dzf = (float)G.dz;
         SFCol c;
         if (col_ok && sf_column(G, pm, src, ix, iy, c)) {
             const int lo = max(c.min_u, 0), ncv = min(c.max_u, nu - 1) - lo + 1;
@@ -668,34 +710,36 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 2) sf3d_back1_kernel(const __g
             float gv = 0.f;
             if (l < ncv) {
                 const int i = lo + l;
-                gv = sf_gamma(i - 0.5f, i + 0.5f, c.us);
+                gv = sf_gamma1(i - 0.5f, i + 0.5f, c.us);
                 if (!(gv == gv)) gv = 0.f;
             }
             const int du0 = lo - ulo, q0 = du0 >> 2, sh = du0 & 3;
             if (ulo >= 0 && du0 >= 0 && ncv + sh <= 8 && 4 * q0 + 8 <= kWin) {
                 // the column's bins lie in two 16-byte words of each staged
-                // row: B(v) = sum_k coef[k] row[4 q0 + k]
-                float coef[8];
+                // row, from word element sh on: B(v) = sum_t g_t row[4 q0 +
+                // sh + t] over its ncv bins, FP64 sums of the FP32 products
+                // (each exact in FP64; only the ncv elements are converted)
+                double gd[8];
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
-                    const float ck = __shfl_sync(0xffffffffu, gv, max(0, min(31, k - sh)));
-                    coef[k] = (k >= sh && k - sh < ncv) ? ck : 0.f;
-                }
-                // FP64 sums of the FP32 products' exact values, as the
-                // forward's profile (each product of two FP32 numbers is exact
-                // in FP64)
-                for (int v = l; v < nv; v += 32) {
-                    const float4* row = reinterpret_cast<const float4*>(sp + (size_t)v * kWin) + q0;
-                    const float4 a = row[0], b4 = row[1];
-                    double b = (double)coef[0] * (double)a.x;
-                    b = fma((double)coef[1], (double)a.y, b);
-                    b = fma((double)coef[2], (double)a.z, b);
-                    b = fma((double)coef[3], (double)a.w, b);
-                    b = fma((double)coef[4], (double)b4.x, b);
-                    b = fma((double)coef[5], (double)b4.y, b);
-                    b = fma((double)coef[6], (double)b4.z, b);
-                    b = fma((double)coef[7], (double)b4.w, b);
-                    Bw[v] = b;
+                for (int t = 0; t < 8; ++t) gd[t] = (double)__shfl_sync(0xffffffffu, gv, t);
+                auto form = [&](auto shc) {
+                    constexpr int SH = decltype(shc)::value;
+                    for (int v = l; v < nv; v += 32) {
+                        const float4* row = reinterpret_cast<const float4*>(sp + (size_t)v * kWin) + q0;
+                        const float4 a = row[0], b4 = row[1];
+                        const float e[8] = {a.x, a.y, a.z, a.w, b4.x, b4.y, b4.z, b4.w};
+                        double b = 0.0;
+#pragma unroll
+                        for (int t = 0; t < 8 - SH; ++t)
+                            if (t < ncv) b = fma(gd[t], (double)e[SH + t], b);
+                        Bw[v] = b;
+                    }
+                };
+                switch (sh) {
+                    case 0: form(std::integral_constant<int, 0>{}); break;
+                    case 1: form(std::integral_constant<int, 1>{}); break;
+                    case 2: form(std::integral_constant<int, 2>{}); break;
+                    default: form(std::integral_constant<int, 3>{}); break;
                 }
             } else {
                 // not in the staged window: global memory, a lane per row
@@ -713,7 +757,7 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 2) sf3d_back1_kernel(const __g
                         double b = Bw[v];
                         for (int t = 32; t < ncv; ++t) {
                             const int i = lo + t;
-                            const float ct = sf_gamma(i - 0.5f, i + 0.5f, c.us);
+                            const float ct = sf_gamma1(i - 0.5f, i + 0.5f, c.us);
                             if (ct == ct && ct != 0.f) b = fma((double)ct, (double)__ldg(gp + (size_t)v * nu + i), b);
                         }
                         Bw[v] = b;
@@ -725,7 +769,7 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 2) sf3d_back1_kernel(const __g
             for (int q = 0; q < kZPer; ++q) {
                 const int iz = zbase + 32 * q + l;
                 SFAx a;
-                if (iz >= G.nz || !sf_axial(G, pm, c, src[2], G.fwdf[p], trap, iz, a)) continue;
+                if (iz >= G.nz || !sf_axial(G, pm, c, dzf, srczf, factorf, trap, iz, a)) continue;
                 double val = 0.0;
                 for (int j = a.min_v; j <= a.max_v; ++j) val = fma((double)sf_row(a, trap, j), Bw[j], val);
                 const double s = val * (double)a.C;
@@ -740,7 +784,7 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 2) sf3d_back1_kernel(const __g
 #pragma unroll
     for (int q = 0; q < kZPer; ++q) {
         const int iz = zbase + 32 * q + l;
-        if (iz < G.nz) vol[(size_t)iz * plane + (size_t)iy * G.nx + ix] = (float)acc[q];
+        if (iz < G.nz) vol[(size_t)iz * plane + (size_t)iy * G.nx + ix] = (TOut)acc[q];
     }
 }
 
@@ -803,18 +847,28 @@ public:
     }
     ~SF3D() {
         if (stream) cudaStreamSynchronize(stream);
-        cudaFree(d_pmi_); cudaFree(d_src_); cudaFree(d_fwdf_); cudaFree(d_proj64_); cudaFree(d_volT_);
+        cudaFree(d_pmi_); cudaFree(d_src_); cudaFree(d_fwdf_); cudaFree(d_proj64_); cudaFree(d_vol64_);
+        cudaFree(d_volT_);
         cudaFree(d_strips_); cudaFree(d_twin_); cudaFree(d_err_);
         cudaFree(d_vol_); cudaFree(d_proj_); cudaFreeHost(h_vol_); cudaFreeHost(h_proj_);
         if (stream) cudaStreamDestroy(stream);
     }
-    // FP64 host arrays x[(iz*ny + iy)*nx + ix], b[(p*nv + v)*nu + u], rounded
-    // through the FP32 device path as the reference's SF class does
+    // FP64 host arrays x[(iz*ny + iy)*nx + ix], b[(p*nv + v)*nu + u]: the
+    // inputs are rounded to FP32 as the reference's SF class does; mode 1
+    // returns its FP64 accumulators, mode 0 rounds its output to FP32 as the
+    // reference does
     void forward_host(double* b, const double* x) {
         const long long nvol = (long long)G.nx * G.ny * G.nz, nproj = (long long)G.np * G.nu * G.nv;
 #pragma omp parallel for schedule(static)
         for (long long e = 0; e < nvol; ++e) h_vol_[e] = (float)x[e];
         SGD_CUDA(cudaMemcpyAsync(d_vol_, h_vol_, nvol * sizeof(float), cudaMemcpyHostToDevice, stream));
+        if (G.mode == 1) {
+            ensure_fp64();
+            forward1(d_vol_, d_proj64_, stream);
+            SGD_CUDA(cudaMemcpyAsync(b, d_proj64_, nproj * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            SGD_CUDA(cudaStreamSynchronize(stream));
+            return;
+        }
         forward_dev(d_vol_, d_proj_, stream);
         SGD_CUDA(cudaMemcpyAsync(h_proj_, d_proj_, nproj * sizeof(float), cudaMemcpyDeviceToHost, stream));
         SGD_CUDA(cudaStreamSynchronize(stream));
@@ -826,8 +880,14 @@ public:
 #pragma omp parallel for schedule(static)
         for (long long e = 0; e < nproj; ++e) h_proj_[e] = (float)b[e];
         SGD_CUDA(cudaMemcpyAsync(d_proj_, h_proj_, nproj * sizeof(float), cudaMemcpyHostToDevice, stream));
-        backward_dev(d_proj_, d_vol_, stream);
-        SGD_CUDA(cudaMemcpyAsync(h_vol_, d_vol_, nvol * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        if (G.mode == 1) {
+            ensure_fp64();
+            back1(d_proj_, d_vol64_, stream);
+            SGD_CUDA(cudaMemcpyAsync(x, d_vol64_, nvol * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        } else {
+            backward_dev(d_proj_, d_vol_, stream);
+            SGD_CUDA(cudaMemcpyAsync(h_vol_, d_vol_, nvol * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        }
         int e = 0;
         SGD_CUDA(cudaMemcpyAsync(&e, d_err_, sizeof(int), cudaMemcpyDeviceToHost, stream));
         SGD_CUDA(cudaStreamSynchronize(stream));
@@ -835,16 +895,14 @@ public:
             SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
             fail("SF_projector back projection: a staged view did not arrive within the bounded wait; output incomplete");
         }
+        if (G.mode == 1) return;
 #pragma omp parallel for schedule(static)
         for (long long e2 = 0; e2 < nvol; ++e2) x[e2] = (double)h_vol_[e2];
     }
     // vol [z][y][x], proj [p][v][u], FP32 device
     void forward_dev(const float* vol, float* proj, cudaStream_t s) {
         if (G.mode == 1) {
-            launch_to_columns(vol, d_volT_, G.nx, G.ny, G.nz, s);
-            SGD_LAUNCH_CHECK();
-            sf3d_fwd_kernel<<<dim3(K.nblk, G.np), kFW * 32, sf_fwd_smem(G.nv), s>>>(G, K, d_volT_, proj);
-            SGD_LAUNCH_CHECK();
+            forward1(vol, proj, s);
             return;
         }
         const long long n = (long long)G.np * G.nu * G.nv;
@@ -858,15 +916,7 @@ public:
     }
     void backward_dev(const float* proj, float* vol, cudaStream_t s) {
         if (G.mode == 1) {
-            // the projection through TMA tensor loads when its rows are whole
-            // 16-byte words and it is 16-byte aligned; from global memory otherwise
-            const bool tma = (G.nu % 4) == 0 && (reinterpret_cast<uintptr_t>(proj) % 16) == 0;
-            CUtensorMap map;
-            std::memset(&map, 0, sizeof(map));
-            if (tma) map = encode_tensor_3d_f32(proj, (uint64_t)G.nu, (uint64_t)G.nv, (uint64_t)G.np, kWin, kRowBox, 1);
-            const dim3 grid(K.tiles_x, K.tiles_y, (G.nz + 32 * kZPer - 1) / (32 * kZPer));
-            sf3d_back1_kernel<<<grid, kTX * kTY * 32, sf_back_smem(G.nv), s>>>(map, G, K, proj, vol, tma ? 1 : 0);
-            SGD_LAUNCH_CHECK();
+            back1(proj, vol, s);
             return;
         }
         dim3 grid((G.nx + 15) / 16, (G.ny + 7) / 8, G.nz);
@@ -888,6 +938,31 @@ public:
     }
 
 private:
+    // mode 1: the column copy and the factored forward
+    template <typename TOut>
+    void forward1(const float* vol, TOut* proj, cudaStream_t s) {
+        launch_to_columns(vol, d_volT_, G.nx, G.ny, G.nz, s);
+        SGD_LAUNCH_CHECK();
+        sf3d_fwd_kernel<TOut><<<dim3(K.nblk, G.np), kFW * 32, sf_fwd_smem(G.nv), s>>>(G, K, d_volT_, proj);
+        SGD_LAUNCH_CHECK();
+    }
+    // mode 1: the projection through TMA tensor loads when its rows are whole
+    // 16-byte words and it is 16-byte aligned; from global memory otherwise
+    template <typename TOut>
+    void back1(const float* proj, TOut* vol, cudaStream_t s) {
+        const bool tma = (G.nu % 4) == 0 && (reinterpret_cast<uintptr_t>(proj) % 16) == 0;
+        CUtensorMap map;
+        std::memset(&map, 0, sizeof(map));
+        if (tma) map = encode_tensor_3d_f32(proj, (uint64_t)G.nu, (uint64_t)G.nv, (uint64_t)G.np, kWin, kRowBox, 1);
+        const dim3 grid(K.tiles_x, K.tiles_y, (G.nz + 32 * kZPer - 1) / (32 * kZPer));
+        sf3d_back1_kernel<TOut><<<grid, kTX * kTY * 32, sf_back_smem(G.nv), s>>>(map, G, K, proj, vol, tma ? 1 : 0);
+        SGD_LAUNCH_CHECK();
+    }
+    void ensure_fp64() {
+        const size_t nvol = (size_t)G.nx * G.ny * G.nz, nproj = (size_t)G.np * G.nu * G.nv;
+        if (!d_proj64_) SGD_CUDA(cudaMalloc(&d_proj64_, nproj * sizeof(double)));
+        if (!d_vol64_) SGD_CUDA(cudaMalloc(&d_vol64_, nvol * sizeof(double)));
+    }
     // Mode 1's launch tables.  The in-plane footprint of column (i, j) in
     // view p spans u' in the image of its corners (i +- 1/2, j +- 1/2) under
     // u' = (pm0 i + pm1 j + pm3) / (pm8 i + pm9 j + pm11), bins are
@@ -954,15 +1029,20 @@ private:
         SGD_CUDA(cudaMemcpy(d_twin_, twin.data(), twin.size() * sizeof(int), cudaMemcpyHostToDevice));
         K.strips = d_strips_;
         K.twin = d_twin_;
-        SGD_CUDA(cudaFuncSetAttribute(sf3d_fwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SGD_CUDA(cudaFuncSetAttribute(sf3d_fwd_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sf_fwd_smem(nv)));
-        SGD_CUDA(cudaFuncSetAttribute(sf3d_back1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SGD_CUDA(cudaFuncSetAttribute(sf3d_fwd_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sf_fwd_smem(nv)));
+        SGD_CUDA(cudaFuncSetAttribute(sf3d_back1_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sf_back_smem(nv)));
+        SGD_CUDA(cudaFuncSetAttribute(sf3d_back1_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)sf_back_smem(nv)));
     }
     float* d_pmi_ = nullptr;
     double* d_src_ = nullptr;
     double* d_fwdf_ = nullptr;
     double* d_proj64_ = nullptr;
+    double* d_vol64_ = nullptr;
     float* d_volT_ = nullptr;
     float4* d_strips_ = nullptr;
     int* d_twin_ = nullptr;

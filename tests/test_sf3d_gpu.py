@@ -74,10 +74,13 @@ def test_matches_fp64_oracle(oracle_mod, case, mode, trap):
 @pytest.mark.parametrize("case", ["small", "rect", "tallz"])
 @pytest.mark.parametrize("trap", [False, True])
 def test_corrected_mode_is_exact_adjoint(case, trap):
+    """<A x, y> = <x, A^T y> on N(0, 1) vectors rounded to FP32 values: the
+    kernels take FP32 inputs, so FP64 inputs would add their own rounding
+    (about 3e-8 times the cancellation of the dot products) to the test."""
     A, _, _ = make(case, 1, trap)
     rng = np.random.default_rng(1234)
-    x = rng.standard_normal(A.shape[1])
-    y = rng.standard_normal(A.shape[0])
+    x = rng.standard_normal(A.shape[1]).astype(np.float32).astype(np.float64)
+    y = rng.standard_normal(A.shape[0]).astype(np.float32).astype(np.float64)
     lhs = float(np.dot(A.matvec(x), y))
     rhs = float(np.dot(x, A.rmatvec(y)))
     assert abs(lhs - rhs) / abs(lhs) < TOL_ADJOINT
