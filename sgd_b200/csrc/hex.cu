@@ -14,10 +14,15 @@
 // the line through the site perpendicular to the bin's central ray: offset y
 // and blur width vblur in FP64) and evaluates
 //   H0: the sum of three 3-direction box splines (vblur, va, vb), (vblur, vb,
-//       vc), (vblur, vc, va), FP32 closed form (layers/spline_conv.hh:244-293);
-//   Hl: the 4-direction box spline (vblur, va, vb, vc) by FP64 divided
-//       differences of truncated cubes, directions below 1e-8 dropped
-//       (A_Hl.cu:21-46);
+//       vc), (vblur, vc, va) (layers/spline_conv.hh:244-293), each the
+//       difference over the blur width of its pair's trapezoid CDF, FP32;
+//   Hl: the 4-direction box spline (vblur, va, vb, vc) (A_Hl.cu:21-46,
+//       FP64 divided differences of truncated cubes there): with all four
+//       directions kept, the difference over the blur width of the
+//       3-direction spline's CDF in closed form, FP32 (box4_by_cum,
+//       spline3.cuh; within 5e-7 of the FP64 form); otherwise, as the
+//       reference, FP64 divided differences with the directions below 1e-8
+//       dropped;
 // va, vb, vc = dt sin(theta + {0, 2pi/3, 4pi/3}) with theta the bin's ray
 // direction (FP64, per view and bin on the host; the reference recomputes them
 // per pair from the stepped FP32 bin centre, a difference far below 1e-6).
@@ -30,7 +35,6 @@
 // "H0 corrected" bounds the true hexagon of each site and has no skip test:
 // the pair is then an exact transpose.
 #include <cmath>
-#include <cstring>
 
 #include "common.h"
 #include "proj2d_impl.cuh"
@@ -53,10 +57,8 @@ struct HexBasis {
         float h0, h1, h2, h3, h4, h5;
         int mode, back;
     };
-    // per bin: Hl three 16-byte words of FP64 pairs (va, vb) (vc, 1/va)
-    // (1/vb, 1/vc) (a zero reciprocal where the direction is dropped); H0 one
-    // word of FP32 (va, vb, vc, 0)
-    static constexpr int kBinF4 = M == kHl ? 3 : 1;
+    // per bin one word of FP32 (va, vb, vc, 0)
+    static constexpr int kBinF4 = 1;
     struct Cell {
         float ox, oy, sx, sy;  // site; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
@@ -126,8 +128,6 @@ struct HexBasis {
         c.sx = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
         c.sy = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
     }
-    // layers/A_H0.cu:21-36 / spline_conv.hh:244-293
-    __device__ static float conv3(float y, float v1, float v2, float v3) { return box3(y, v1, v2, v3); }
     // layers/A_Hl.cu:21-46 with spline_conv.hh:151-229: divided differences of
     // truncated powers y+^(m-1), m = number of kept directions
     __device__ static double tp(double y, int m) {
@@ -159,37 +159,6 @@ struct HexBasis {
         }
         return m == 2 ? v[0] : (m == 3 ? v[0] / 2.0 : v[0] / 6.0);
     }
-    // conv4 when all four directions are kept (every bin but those whose ray
-    // makes a lattice direction vanish): the same corners and nesting, the
-    // divisions by h_k as products with host-computed FP64 reciprocals (1/vblur
-    // once per call), unrolled so that the 16 corner values stay in registers
-    __device__ static double conv4_full(double y, double h1, double h2, double h3, double h4, double r2, double r3,
-                                        double r4) {
-        const double hs[4] = {h1, h2, h3, h4};
-        const double rs[4] = {1.0 / h1, r2, r3, r4};
-        double v[16];
-#pragma unroll
-        for (int s = 0; s < 16; ++s) {
-            double yy = y;
-#pragma unroll
-            for (int k = 3; k >= 0; --k)
-                if (s & (1 << (3 - k))) yy = yy - hs[k];
-            v[s] = yy > 0 ? yy * yy * yy : 0.0;
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int bit = 1 << (3 - k);
-#pragma unroll
-            for (int s = 0; s < 16; ++s)
-                if (!(s & bit)) v[s] = (v[s] - v[s | bit]) * rs[k];
-        }
-        return v[0] * (1.0 / 6.0);
-    }
-    __device__ static double2 as_double2(float4 f) {
-        double2 d;
-        memcpy(&d, &f, sizeof(d));
-        return d;
-    }
     // the reference's FP32 stepping of the bin centre
     __device__ static void skip(const View& V, Cell& c) {
         c.sx += V.puvx;
@@ -219,19 +188,24 @@ struct HexBasis {
         const float fblur = -sqrtf(fmaf(dbx, dbx, dby * dby));
         float fy = sqrtf(fmaf(dax, dax, day * day));
         if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) fy = -fy;
-        if (M == kHl) {
-            const double2 w0 = as_double2(t[0]), w1 = as_double2(t[1]), w2 = as_double2(t[2]);
-            const double va = w0.x, vb = w0.y, vc = w1.x, y = (double)fy, vblur = (double)fblur;
-            double conv;
-            if (fabs(vblur) > 1e-8 && fabs(va) > 1e-8 && fabs(vb) > 1e-8 && fabs(vc) > 1e-8)
-                conv = conv4_full(y, vblur, va, vb, vc, w1.y, w2.x, w2.y);
-            else
-                conv = conv4(y, vblur, va, vb, vc);
-            return (conv == conv && conv > 0.0) ? (float)conv : 0.f;
-        }
         const float4 w = t[0];
         const float va = w.x, vb = w.y, vc = w.z;
-        const float conv = conv3(fy, fblur, va, vb) + conv3(fy, fblur, vb, vc) + conv3(fy, fblur, vc, va);
+        if (M == kHl) {
+            // all four directions kept (every bin but those whose ray makes a
+            // lattice direction vanish): the blur direction integrated in
+            // closed form, FP32; otherwise the reference's FP64 divided
+            // differences with the vanishing directions dropped
+            if (fabsf(fblur) > 1e-8f && fabsf(va) > 1e-8f && fabsf(vb) > 1e-8f && fabsf(vc) > 1e-8f) {
+                const float conv = box4_by_cum(fy, -fblur, va, vb, vc);
+                return (conv == conv && conv > 0.f) ? conv : 0.f;
+            }
+            const double conv = conv4((double)fy, (double)fblur, (double)va, (double)vb, (double)vc);
+            return (conv == conv && conv > 0.0) ? (float)conv : 0.f;
+        }
+        // the three splines as differences of their pairs' trapezoid CDFs
+        // over the blur width (box3_sum3_by_cum; within 1e-6 of the three
+        // closed forms at values up to 3/dt)
+        const float conv = box3_sum3_by_cum(fy, -fblur, va, vb, vc);
         return (conv == conv && conv > 0.f) ? conv : 0.f;
     }
 };
@@ -258,8 +232,7 @@ public:
         const float fdy = fdt * (mode == kHl ? 0.5f : 1.5f);
         constexpr int kVF = HexBasis<kHl>::kViewFloats;
         std::vector<float> view((size_t)np * kVF, 0.f);
-        const int nw = (mode == kHl) ? HexBasis<kHl>::kBinF4 : HexBasis<kH0Corrected>::kBinF4;
-        std::vector<float4> bins((size_t)np * nu * nw);
+        std::vector<float4> bins((size_t)np * nu);
         std::vector<BinHomography> hom;
         bin_homographies(geo, hom);
         for (int p = 0; p < np; ++p) {
@@ -286,17 +259,11 @@ public:
                 const float sx = (float)f.dtv[0] + (float)f.puv[0] * (u - 0.5f * nu + 0.5f);
                 const float sy = (float)f.dtv[1] + (float)f.puv[1] * (u - 0.5f * nu + 0.5f);
                 const float th = std::atan2(sx - px, sy - py);
-                double o[6];
+                double o[3];
                 o[0] = (double)fdt * std::sin((double)th);
                 o[1] = (double)fdt * std::sin((double)th + 2.0 * kPi / 3.0);
                 o[2] = (double)fdt * std::sin((double)th + 4.0 * kPi / 3.0);
-                for (int k = 0; k < 3; ++k) o[3 + k] = std::fabs(o[k]) > 1e-8 ? 1.0 / o[k] : 0.0;
-                float4* w = &bins[(size_t)p * nw * nu + u];  // planes of nu words
-                if (mode == kHl) {
-                    for (int k = 0; k < 3; ++k) std::memcpy(&w[(size_t)k * nu], &o[2 * k], 16);
-                } else {
-                    w[0] = make_float4((float)o[0], (float)o[1], (float)o[2], 0.f);
-                }
+                bins[(size_t)p * nu + u] = make_float4((float)o[0], (float)o[1], (float)o[2], 0.f);
             }
         }
         back_view_ = view;
