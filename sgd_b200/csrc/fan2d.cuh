@@ -167,7 +167,8 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
         double t = 0.0;
 #pragma unroll
         for (int q = 0; q < kF2FwdWarps; ++q) t += s_red[q][l];
-        sino[(size_t)p * P.nu + u0 + l] = (float)t * scale;
+        if (P.out64) P.out64[(size_t)p * P.nu + u0 + l] = t * (double)scale;
+        else sino[(size_t)p * P.nu + u0 + l] = (float)t * scale;
     }
 }
 
@@ -323,7 +324,10 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
         drain(nchunks - 1);
         return;
     }
-    if (i < P.ni && j < P.nj) img[(size_t)i * P.nj + j] = mine ? (float)acc * scale : 0.f;
+    if (i < P.ni && j < P.nj) {
+        if (P.out64) P.out64[(size_t)i * P.nj + j] = mine ? acc * (double)scale : 0.0;
+        else img[(size_t)i * P.nj + j] = mine ? (float)acc * scale : 0.f;
+    }
 }
 
 // The reference's footprint-evaluation count: sum over cells and views of the

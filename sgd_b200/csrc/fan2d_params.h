@@ -20,6 +20,7 @@ struct Fan2DParams {
     int aux_i = 0;                   // basis-specific integer
     int* err = nullptr;              // device status word (bounded waits), 0 = ok
     unsigned wait_limit = 1u << 22;  // polls of the back kernel's staging wait before it gives up
+    double* out64 = nullptr;         // when set, the kernels write their FP64 sums here instead of the FP32 output
 };
 
 // forward: one CTA per (view, block of kF2Block bins), kF2FwdWarps warps

@@ -173,7 +173,9 @@ struct HexBasis {
         const float num = dot2f(ox - px, sx - px, oy - py, sy - py);
         const float dena = dot2f(ax - px, sx - px, ay - py, sy - py);
         const float denb = dot2f(bx - px, sx - px, by - py, sy - py);
-        const float ra = num / dena, rb = num / denb;
+        // fast divisions: within two ulps of the reference's, on positions
+        // whose own FP32 rounding is larger
+        const float ra = __fdividef(num, dena), rb = __fdividef(num, denb);
         const float ax1 = px + (ax - px) * ra, ay1 = py + (ay - py) * ra;
         const float bx1 = px + (bx - px) * rb, by1 = py + (by - py) * rb;
         if (M == kH0Reference && V.back) {  // layers/A_H0.cu:331-334

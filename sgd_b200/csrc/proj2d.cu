@@ -204,6 +204,7 @@ Proj2D::~Proj2D() {
     cudaFree(d_err_);
     cudaFree(d_img_);
     cudaFree(d_imgT_);
+    cudaFree(d_out64_);
     cudaFree(d_sino_);
     cudaFreeHost(h_img_);
     cudaFreeHost(h_sino_);
@@ -220,16 +221,20 @@ int Proj2D::status(bool sync_device) {
     return h ? -1 : 0;
 }
 
+// The FP64 host entry points: inputs rounded to FP32 (the kernels' input
+// type, as the reference's layers round them), outputs the kernels' FP64 sums
+// (the FP32 *_dev outputs round them once more).
 void Proj2D::forward_host(double* b, const double* x) {
     const long long nimg = (long long)P.ni * P.nj, nsino = (long long)P.np * P.nu;
 #pragma omp parallel for schedule(static) if (nimg > (1 << 16))
     for (long long e = 0; e < nimg; ++e) h_img_[e] = (float)x[e];
     SGD_CUDA(cudaMemcpyAsync(d_img_, h_img_, nimg * sizeof(float), cudaMemcpyHostToDevice, stream));
+    ensure_out64();
+    P.out64 = d_out64_;
     forward_dev(d_img_, d_sino_, stream);
-    SGD_CUDA(cudaMemcpyAsync(h_sino_, d_sino_, nsino * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    P.out64 = nullptr;
+    SGD_CUDA(cudaMemcpyAsync(b, d_out64_, nsino * sizeof(double), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
-#pragma omp parallel for schedule(static) if (nsino > (1 << 16))
-    for (long long e = 0; e < nsino; ++e) b[e] = (double)h_sino_[e];
 }
 
 void Proj2D::backward_host(const double* b, double* x) {
@@ -237,12 +242,19 @@ void Proj2D::backward_host(const double* b, double* x) {
 #pragma omp parallel for schedule(static) if (nsino > (1 << 16))
     for (long long e = 0; e < nsino; ++e) h_sino_[e] = (float)b[e];
     SGD_CUDA(cudaMemcpyAsync(d_sino_, h_sino_, nsino * sizeof(float), cudaMemcpyHostToDevice, stream));
+    ensure_out64();
+    P.out64 = d_out64_;
     backward_dev(d_sino_, d_img_, stream);
-    SGD_CUDA(cudaMemcpyAsync(h_img_, d_img_, nimg * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    P.out64 = nullptr;
+    SGD_CUDA(cudaMemcpyAsync(x, d_out64_, nimg * sizeof(double), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
     if (status(false) != 0) fail("back projection: a staged view chunk did not arrive (bounded wait); output incomplete");
-#pragma omp parallel for schedule(static) if (nimg > (1 << 16))
-    for (long long e = 0; e < nimg; ++e) x[e] = (double)h_img_[e];
+}
+
+void Proj2D::ensure_out64() {
+    if (d_out64_) return;
+    const size_t n = std::max((size_t)P.ni * P.nj, (size_t)P.np * P.nu);
+    SGD_CUDA(cudaMalloc(&d_out64_, n * sizeof(double)));
 }
 
 }  // namespace sgd

@@ -71,6 +71,8 @@ protected:
     int* d_err_ = nullptr;
     float* d_img_ = nullptr;
     float* d_imgT_ = nullptr;  // the forward's line-major image copy
+    double* d_out64_ = nullptr;  // the FP64 host entry points' output (allocated at their first call)
+    void ensure_out64();
     float* d_sino_ = nullptr;
     float* h_img_ = nullptr;
     float* h_sino_ = nullptr;
