@@ -57,8 +57,11 @@ struct HexBasis {
         float h0, h1, h2, h3, h4, h5;
         int mode, back;
     };
-    // per bin one word of FP32 (va, vb, vc, 0)
-    static constexpr int kBinF4 = 1;
+    // per bin FP32 (va, vb, vc, ...); H0 with the true bounds adds the exact
+    // edge-ray maps: (va, vb, vc, beta_a) (alpha_a, alpha_b) (beta_b, 0, 0, 0),
+    // the signed offset of edge ray e from site O along the line through O
+    // perpendicular to the bin's central ray being alpha_e . O + beta_e
+    static constexpr int kBinF4 = M == kH0Corrected ? 3 : 1;
     struct Cell {
         float ox, oy, sx, sy;  // site; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
@@ -110,7 +113,9 @@ struct HexBasis {
         float umin = 1e30f, umax = -1e30f;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
-            const float u = fmaf(V.h0, xs[k], fmaf(V.h1, ys[k], V.h2)) / fmaf(V.h3, xs[k], fmaf(V.h4, ys[k], V.h5));
+            // fast division: a range end it moves by an ulp across a bin edge
+            // adds or drops a bin the hexagon barely touches (value ~ 0)
+            const float u = __fdividef(fmaf(V.h0, xs[k], fmaf(V.h1, ys[k], V.h2)), fmaf(V.h3, xs[k], fmaf(V.h4, ys[k], V.h5)));
             umin = fminf(umin, u);
             umax = fmaxf(umax, u);
         }
@@ -165,6 +170,16 @@ struct HexBasis {
         c.sy += V.puvy;
     }
     __device__ static float value(const View& V, Cell& c, int, BinRef t, const Fan2DParams&) {
+        if (M == kH0Corrected) {
+            // the exact bin geometry (this mode is held to the FP64 replica,
+            // not to the reference's FP32 rounding): two affine maps in place
+            // of the edge-ray intersections, divisions and square roots
+            const float4 w0 = t[0], w1 = t[1], w2 = t[2];
+            const float xa = __fmaf_rn(w1.x, c.ox, __fmaf_rn(w1.y, c.oy, w0.w));
+            const float xb = __fmaf_rn(w1.z, c.ox, __fmaf_rn(w1.w, c.oy, w2.x));
+            const float conv = box3_sum3_by_cum(xa, fabsf(xb - xa), w0.x, w0.y, w0.z);
+            return (conv == conv && conv > 0.f) ? conv : 0.f;
+        }
         const float sx = c.sx, sy = c.sy;
         skip(V, c);
         const float px = V.srcx, py = V.srcy, ox = c.ox, oy = c.oy;
@@ -234,7 +249,8 @@ public:
         const float fdy = fdt * (mode == kHl ? 0.5f : 1.5f);
         constexpr int kVF = HexBasis<kHl>::kViewFloats;
         std::vector<float> view((size_t)np * kVF, 0.f);
-        std::vector<float4> bins((size_t)np * nu);
+        const int nw = mode == kH0Corrected ? HexBasis<kH0Corrected>::kBinF4 : HexBasis<kHl>::kBinF4;
+        std::vector<float4> bins((size_t)np * nu * nw);
         std::vector<BinHomography> hom;
         bin_homographies(geo, hom);
         for (int p = 0; p < np; ++p) {
@@ -265,7 +281,32 @@ public:
                 o[0] = (double)fdt * std::sin((double)th);
                 o[1] = (double)fdt * std::sin((double)th + 2.0 * kPi / 3.0);
                 o[2] = (double)fdt * std::sin((double)th + 4.0 * kPi / 3.0);
-                bins[(size_t)p * nu + u] = make_float4((float)o[0], (float)o[1], (float)o[2], 0.f);
+                float4* w = &bins[(size_t)p * nw * nu + u];  // planes of nu words
+                w[0] = make_float4((float)o[0], (float)o[1], (float)o[2], 0.f);
+                if (mode == kH0Corrected) {
+                    // exact edge-ray maps of bin u (FP64): central direction
+                    // c = s - S, n its counter-clockwise normal; the edge ray
+                    // S + t d_e meets the line O + r n at r = (O - S) . (k_e c -
+                    // n), k_e = (d_e . n) / (d_e . c) (the reference's offset
+                    // and sign convention, layers/A_H0.cu:215-241)
+                    const double Sx = f.src[0], Sy = f.src[1];
+                    const double t0 = u - 0.5 * nu + 0.5;
+                    const double cx0 = f.dtv[0] + f.puv[0] * t0, cy0 = f.dtv[1] + f.puv[1] * t0;
+                    const double cx = cx0 - Sx, cy = cy0 - Sy, cl = std::hypot(cx, cy);
+                    const double nx_ = -cy / cl, ny_ = cx / cl;
+                    double al[2][2], be[2];
+                    for (int e = 0; e < 2; ++e) {
+                        const double sgn = e == 0 ? -0.5 : 0.5;
+                        const double dx_ = cx + sgn * f.puv[0], dy_ = cy + sgn * f.puv[1];
+                        const double k = (dx_ * nx_ + dy_ * ny_) / (dx_ * cx + dy_ * cy);
+                        al[e][0] = k * cx - nx_;
+                        al[e][1] = k * cy - ny_;
+                        be[e] = -(al[e][0] * Sx + al[e][1] * Sy);
+                    }
+                    w[0].w = (float)be[0];
+                    w[nu] = make_float4((float)al[0][0], (float)al[0][1], (float)al[1][0], (float)al[1][1]);
+                    w[2 * nu] = make_float4((float)be[1], 0.f, 0.f, 0.f);
+                }
             }
         }
         back_view_ = view;
