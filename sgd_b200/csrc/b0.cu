@@ -30,9 +30,9 @@ struct B0Basis {
     struct View {
         float pm0, pm1, pm3, pm8, pm9, pm11, puvx, singular, srcx, srcy, dtvx, dtvy, puvy, dx, dy, nx2, ny2;
     };
-    // per bin: vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2, 0, 0 (computed in FP64,
-    // stored in FP32: the reference's FP64 arithmetic on them ends in FP32
-    // arguments of the spline)
+    // per bin: vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2, 1/x0, 1/(2 x0 x1) (x0 >= x1
+    // = |vx|, |vy|; computed in FP64, stored in FP32: the reference's FP64
+    // arithmetic on them ends in FP32 arguments of the spline)
     static constexpr int kBinF4 = 2;
     struct Cell {
         float ox, oy, sx, sy;  // pixel centre; centre of the next bin of the walk (FP32 stepped)
@@ -96,7 +96,9 @@ struct B0Basis {
         const float vblur = (b0.z + b0.w) * (-r1);
         const float x1 = sx - px, y1 = sy - py, x2 = c.ox - 0.5f * V.dx - px, y2 = c.oy + 0.5f * V.dy - py;
         const float y = fmaf(b0.z, r1, dot2f(x1, y2, -x2, y1) * b1.x);
-        const float conv = conv1d(-y, b0.x, b0.y, vblur);
+        // the spline as the (vx, vy) trapezoid's CDF differenced over the
+        // blur width (box3_by_cum; within ~1e-7 of the closed form)
+        const float conv = box3_by_cum(-y, b0.x, b0.y, vblur, b1.z, b1.w);
         return (conv > 1e-7f && conv == conv) ? conv : 0.f;
     }
 };
@@ -181,7 +183,12 @@ public:
                 sb0 /= ((bx - px) * (sx - px) + (by - py) * (sy - py)) / (lsp * lsp);
                 float4* o = &bins[(size_t)p * B0Basis::kBinF4 * nu + u];  // planes of nu words
                 o[0] = make_float4((float)vx, (float)vy, (float)a0s, (float)sb0);
-                o[nu] = make_float4((float)(1.0 / lsp), (float)(1.0 / (lsp * lsp)), 0.f, 0.f);
+                // the (vx, vy) trapezoid's 1/x0 and 1/(2 x0 x1), x0 >= x1 the
+                // widths' magnitudes (an infinite second one for a box, whose
+                // ramp is empty)
+                const float fx = std::fabs((float)vx), fy = std::fabs((float)vy);
+                const float fx0 = std::max(fx, fy), fx1 = std::min(fx, fy);
+                o[nu] = make_float4((float)(1.0 / lsp), (float)(1.0 / (lsp * lsp)), 1.0f / fx0, 0.5f / (fx0 * fx1));
             }
         }
         finish_init(view, bins);

@@ -140,6 +140,22 @@ __device__ __forceinline__ float box2_cum_diff(float e1, float e0, float p, floa
     return copysignf(G(fabsf(e1)), e1) - copysignf(G(fabsf(e0)), e0);
 }
 
+// The 3-direction box spline of signed widths p, q, v at y (box3's
+// convention) as the difference of the (p, q) trapezoid's CDF over v:
+// (F2(y) - F2(y - v)) / v, with the trapezoid's 1/x0 and 1/(2 x0 x1) given
+// (per-bin constants of a table).
+__device__ __forceinline__ float box3_by_cum(float y, float p, float q, float v, float ih, float ir) {
+    const float x0 = fmaxf(fabsf(p), fabsf(q)), x1 = fminf(fabsf(p), fabsf(q));
+    const float k0 = (x0 - x1) * 0.5f, k1 = (x0 + x1) * 0.5f, c = (p + q) * 0.5f;
+    auto G = [&](float t) {
+        const float d = k1 - t;
+        const float g = t <= k0 ? t * ih : __fmaf_rn(-ir * d, d, 0.5f);
+        return t >= k1 ? 0.5f : g;
+    };
+    const float e1 = y - c, e0 = (y - v) - c;
+    return __fdividef(copysignf(G(fabsf(e1)), e1) - copysignf(G(fabsf(e0)), e0), v);
+}
+
 // The sum of the three 3-direction box splines (-w, va, vb), (-w, vb, vc),
 // (-w, vc, va) at y (the H0 footprint, layers/A_H0.cu:21-36 with
 // spline_conv.hh:244-293): each is the difference over the blur width w > 0
