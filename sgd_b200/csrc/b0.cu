@@ -85,6 +85,7 @@ struct B0Basis {
         c.sx += V.puvx;
         c.sy += V.puvy;
     }
+    __device__ static void start(const View&, Cell&, int) {}
     __device__ static float value(const View& V, Cell& c, int, BinRef t, const Fan2DParams&) {
         const float sx = c.sx, sy = c.sy;
         skip(V, c);
@@ -142,6 +143,7 @@ struct B0ParBasis {
         return (conv > 1e-7f && conv == conv) ? conv : 0.f;
     }
     __device__ static void skip(const View&, Cell&) {}
+    __device__ static void start(const View&, Cell&, int) {}
 };
 
 namespace {

@@ -87,6 +87,7 @@ struct B1RefBasis {
         c.sx += V.puvx;
         c.sy += V.puvy;
     }
+    __device__ static void start(const View&, Cell&, int) {}
     // Odd cumulative profile G of the unit-area tri(a) * tri(b) convolution
     // (fan_geometry.h: S(x) in closed form, every power a distance to a knot).
     __device__ static float G(float x, const float4& k0, const float4& k1, const float4& k2) {

@@ -20,6 +20,7 @@
 //                           lets a basis step its bin position as the
 //                           reference does
 //   B::skip(V, c)           steps past a bin without evaluating it
+//   B::start(V, c, u)       before the first bin u a walk evaluates
 // The forward's strips and the back's windows come from each cell's true
 // footprint (plan_fan2d, proj2d.h); a bin outside it has footprint exactly 0.
 // So both kernels evaluate every (cell, bin) pair with a non-zero value and
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
             const int ue = min(c.hi, u0 + nb - 1);
             int u = c.lo;
             for (; u < u0; ++u) B::skip(V, c);
+            B::start(V, c, u);
             for (; u <= ue; ++u) {
                 const float v = B::value(V, c, u, BinRef{s_bin + (u - u0), kF2Block}, P);
                 if (v != 0.f) acc[33 * (u - u0)] = fmaf(v, C, acc[33 * (u - u0)]);
@@ -312,6 +314,7 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
             const int ue = min(cl.hi, lh.y);
             int u = cl.lo;
             for (; u < lh.x; ++u) B::skip(V, cl);
+            B::start(V, cl, u);
             for (; u <= ue; ++u) {
                 const float val = B::value(V, cl, u, BinRef{tb + u, P.wcap}, P);
                 if (val != 0.f) kahan_fma(csum, ccmp, val, sb[u]);

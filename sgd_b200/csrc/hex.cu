@@ -169,6 +169,7 @@ struct HexBasis {
         c.sx += V.puvx;
         c.sy += V.puvy;
     }
+    __device__ static void start(const View&, Cell&, int) {}
     __device__ static float value(const View& V, Cell& c, int, BinRef t, const Fan2DParams&) {
         if (M == kH0Corrected) {
             // the exact bin geometry (this mode is held to the FP64 replica,

@@ -59,6 +59,7 @@ struct Fan2DVisit {
         B::load_view(P.view + (size_t)p * B::kViewFloats, V);
         typename B::Cell c;
         B::setup(V, i, j, P, c);
+        B::start(V, c, c.lo);
         for (int u = c.lo; u <= c.hi; ++u) {
             const float v = B::value(V, c, u, BinRef{P.bins + (size_t)p * B::kBinF4 * P.nu + u, P.nu}, P);
             if (v != 0.f) f(u, v * scale);

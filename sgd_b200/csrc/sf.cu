@@ -7,9 +7,13 @@
 // fan_geometry.h) into bin coordinates, sorted into a trapezoid us[0..3]; the
 // footprint in bin u is the trapezoid's integral over [u, u+1] (unit plateau)
 // times dx / max(|sin t|, |cos t|), t the direction of the pixel centre from
-// the source.  The expressions are written as the reference writes them so
-// that the compiler forms the same operations; bins with gamma <= 1e-7 are
-// dropped as the reference drops them.
+// the source; bins with gamma <= 1e-7 are dropped as the reference drops them.
+// The corners' divisions are fast (MUFU) divisions: a range end that one moves
+// by an ulp across a bin edge adds or drops a bin whose integral is about
+// k ulp^2, far below that threshold.  The integral over bin [u, u+1] is F(u +
+// 1) - F(u) with F the trapezoid's cumulative area (the reference sums its
+// three clipped pieces, layers/A_SF.cu:48-84: the same number up to an FP32
+// rounding of F), so a walk over a cell's bins takes one F per bin.
 #include <cmath>
 
 #include "common.h"
@@ -29,6 +33,7 @@ struct SFBasis {
         float us[4];
         float weight;
         float k01, k23;  // the trapezoid's ramp factors 1 / (2 (us1 - us0)), 1 / (2 (us3 - us2))
+        float F;         // the cumulative area left of the walk's next bin
         int lo, hi;
     };
     __device__ static void load_view(const float* v, View& V) {
@@ -49,13 +54,14 @@ struct SFBasis {
     __device__ static void setup(const View& V, int ix, int iy, const Fan2DParams& P, Cell& c) {
         const float signx1 = ix - 0.5f, signx2 = ix + 0.5f, signy1 = iy - 0.5f, signy2 = iy + 0.5f;
         float* us = c.us;
-        us[0] = (V.pm0 * signx1 + V.pm3 + V.pm1 * signy1) / (V.pm8 * signx1 + V.pm11 + V.pm9 * signy1);
-        us[1] = (V.pm0 * signx1 + V.pm3 + V.pm1 * signy2) / (V.pm8 * signx1 + V.pm11 + V.pm9 * signy2);
-        us[2] = (V.pm0 * signx2 + V.pm3 + V.pm1 * signy1) / (V.pm8 * signx2 + V.pm11 + V.pm9 * signy1);
-        us[3] = (V.pm0 * signx2 + V.pm3 + V.pm1 * signy2) / (V.pm8 * signx2 + V.pm11 + V.pm9 * signy2);
+        us[0] = __fdividef(V.pm0 * signx1 + V.pm3 + V.pm1 * signy1, V.pm8 * signx1 + V.pm11 + V.pm9 * signy1);
+        us[1] = __fdividef(V.pm0 * signx1 + V.pm3 + V.pm1 * signy2, V.pm8 * signx1 + V.pm11 + V.pm9 * signy2);
+        us[2] = __fdividef(V.pm0 * signx2 + V.pm3 + V.pm1 * signy1, V.pm8 * signx2 + V.pm11 + V.pm9 * signy1);
+        us[3] = __fdividef(V.pm0 * signx2 + V.pm3 + V.pm1 * signy2, V.pm8 * signx2 + V.pm11 + V.pm9 * signy2);
         if (V.singular != 0.f) {
+            const float r = __fdividef(1.0f, V.puvx);
 #pragma unroll
-            for (int k = 0; k < 4; ++k) us[k] = (us[k] * 1.5f - 1.0f) / V.puvx;
+            for (int k = 0; k < 4; ++k) us[k] = (us[k] * 1.5f - 1.0f) * r;
         }
         sort2(us[0], us[1]);
         sort2(us[2], us[3]);
@@ -67,7 +73,8 @@ struct SFBasis {
         // dx / max(|sin t|, |cos t|) for t = atan2(X, Y) (:174-177) without
         // the trigonometry: |sin t| = |X| / r, |cos t| = |Y| / r
         const float X = V.dx * (ix - V.nx2) - V.srcx, Y = V.dy * (iy - V.ny2) - V.srcy;
-        c.weight = V.dx * sqrtf(dot2f(X, X, Y, Y)) * __fdividef(1.0f, fmaxf(fabsf(X), fabsf(Y)));
+        const float r2 = dot2f(X, X, Y, Y);
+        c.weight = V.dx * __fdividef(r2 * rsqrtf(r2), fmaxf(fabsf(X), fabsf(Y)));
         // per-bin constants of gamma_calculate (:48-84), once per cell and
         // view (fast reciprocals: within an ulp or two of the reference's
         // divisions; a zero-width ramp still gives an infinite factor whose
@@ -75,26 +82,23 @@ struct SFBasis {
         c.k01 = __fdividef(0.5f, us[1] - us[0]);
         c.k23 = __fdividef(0.5f, us[3] - us[2]);
     }
-    // layers/A_SF.cu:48-84
-    __device__ static float gamma(float s1, float s2, const Cell& c) {
+    // the cumulative area at the first bin the walk evaluates
+    __device__ static void start(const View&, Cell& c, int u) { c.F = area(c, (float)u); }
+    // the trapezoid's area left of s: ramp up, plateau, ramp down (a
+    // zero-width ramp contributes nothing; its factor is infinite)
+    __device__ static float area(const Cell& c, float s) {
         const float* us = c.us;
-        float g = 0.0f, tmp, b1, b2;
-        b1 = fmaxf(s1, us[0]);
-        b2 = fminf(s2, us[1]);
-        tmp = (b2 > b1) ? c.k01 * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0])) : 0.0f;
-        if (tmp == tmp) g += tmp;
-        b1 = fmaxf(s1, us[1]);
-        b2 = fminf(s2, us[2]);
-        tmp = (b2 > b1) ? b2 - b1 : 0.0f;
-        if (tmp == tmp) g += tmp;
-        b1 = fmaxf(s1, us[2]);
-        b2 = fminf(s2, us[3]);
-        tmp = (b2 > b1) ? c.k23 * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3])) : 0.0f;
-        if (tmp == tmp) g += tmp;
-        return g;
+        const float a = fminf(fmaxf(s, us[0]), us[1]) - us[0];
+        const float b = fminf(fmaxf(s, us[1]), us[2]) - us[1];
+        const float e = fminf(fmaxf(s, us[2]), us[3]) - us[2];
+        const float up = a > 0.f ? c.k01 * a * a : 0.f;
+        const float down = e > 0.f ? c.k23 * e * __fmaf_rn(2.f, us[3] - us[2], -e) : 0.f;
+        return up + b + down;
     }
     __device__ static float value(const View&, Cell& c, int u, BinRef, const Fan2DParams&) {
-        const float g = gamma((float)u, u + 1.0f, c);
+        const float F1 = area(c, u + 1.0f);
+        const float g = F1 - c.F;
+        c.F = F1;
         const float val = c.weight * g;
         return (g > 1e-7f && val == val) ? val : 0.f;
     }
