@@ -32,8 +32,8 @@ struct SFBasis {
     struct Cell {
         float us[4];
         float weight;
-        float k01, k23;  // the trapezoid's ramp factors 1 / (2 (us1 - us0)), 1 / (2 (us3 - us2))
-        float F;         // the cumulative area left of the walk's next bin
+        float r0, r1, r2;  // reciprocal widths of the ramp up, the plateau and the ramp down
+        float F;           // the cumulative area left of the walk's next bin
         int lo, hi;
     };
     __device__ static void load_view(const float* v, View& V) {
@@ -75,25 +75,26 @@ struct SFBasis {
         const float X = V.dx * (ix - V.nx2) - V.srcx, Y = V.dy * (iy - V.ny2) - V.srcy;
         const float r2 = dot2f(X, X, Y, Y);
         c.weight = V.dx * __fdividef(r2 * rsqrtf(r2), fmaxf(fabsf(X), fabsf(Y)));
-        // per-bin constants of gamma_calculate (:48-84), once per cell and
-        // view (fast reciprocals: within an ulp or two of the reference's
-        // divisions; a zero-width ramp still gives an infinite factor whose
-        // terms the NaN test drops)
-        c.k01 = __fdividef(0.5f, us[1] - us[0]);
-        c.k23 = __fdividef(0.5f, us[3] - us[2]);
+        // the pieces' reciprocal widths, once per cell and view (fast
+        // reciprocals; a zero width gives an infinite one, see area)
+        c.r0 = __fdividef(1.0f, us[1] - us[0]);
+        c.r1 = __fdividef(1.0f, us[2] - us[1]);
+        c.r2 = __fdividef(1.0f, us[3] - us[2]);
     }
     // the cumulative area at the first bin the walk evaluates
     __device__ static void start(const View&, Cell& c, int u) { c.F = area(c, (float)u); }
-    // the trapezoid's area left of s: ramp up, plateau, ramp down (a
-    // zero-width ramp contributes nothing; its factor is infinite)
+    // the trapezoid's area left of s from each piece's covered fraction t
+    // in [0, 1] (saturated products, on the FMA pipe): ramp up w01 t0^2 / 2,
+    // plateau w12 t1, ramp down w23 t2 (2 - t2) / 2.  A zero-width piece has
+    // an infinite reciprocal width; its fraction saturates to 0 or 1 (0 for
+    // the NaN at its own end) and it adds zero width times that.
     __device__ static float area(const Cell& c, float s) {
         const float* us = c.us;
-        const float a = fminf(fmaxf(s, us[0]), us[1]) - us[0];
-        const float b = fminf(fmaxf(s, us[1]), us[2]) - us[1];
-        const float e = fminf(fmaxf(s, us[2]), us[3]) - us[2];
-        const float up = a > 0.f ? c.k01 * a * a : 0.f;
-        const float down = e > 0.f ? c.k23 * e * __fmaf_rn(2.f, us[3] - us[2], -e) : 0.f;
-        return up + b + down;
+        const float t0 = __saturatef((s - us[0]) * c.r0);
+        const float t1 = __saturatef((s - us[1]) * c.r1);
+        const float t2 = __saturatef((s - us[2]) * c.r2);
+        const float h01 = 0.5f * (us[1] - us[0]), w12 = us[2] - us[1], h23 = 0.5f * (us[3] - us[2]);
+        return __fmaf_rn(h01 * t0, t0, __fmaf_rn(w12, t1, h23 * t2 * (2.0f - t2)));
     }
     __device__ static float value(const View&, Cell& c, int u, BinRef, const Fan2DParams&) {
         const float F1 = area(c, u + 1.0f);
