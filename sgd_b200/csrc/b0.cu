@@ -30,7 +30,7 @@ struct B0Basis {
     struct View {
         float pm0, pm1, pm3, pm8, pm9, pm11, puvx, singular, srcx, srcy, dtvx, dtvy, puvy, dx, dy, nx2, ny2;
     };
-    // per bin: vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2, 1/x0, 1/(2 x0 x1) (x0 >= x1
+    // per bin: vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2, 1/x0, 1/x1 (x0 >= x1
     // = |vx|, |vy|; computed in FP64, stored in FP32: the reference's FP64
     // arithmetic on them ends in FP32 arguments of the spline)
     static constexpr int kBinF4 = 2;
@@ -51,29 +51,52 @@ struct B0Basis {
             a = t;
         }
     }
-    // layers/A_B0.cu:152-198
+    // x within 8 ulp (plus 2^-22) of an integer: the fast quotient x and
+    // the IEEE one may lie on either side of it
+    __device__ static bool near_int(float x) {
+        const float f = x - floorf(x), tol = __fmaf_rn(fabsf(x), 0x1p-20f, 0x1p-22f);
+        return f < tol || f > 1.0f - tol;
+    }
+    // layers/A_B0.cu:152-198.  The bin range is the reference's: the floors
+    // of the extreme corner projections under IEEE division.  Fast
+    // quotients (within 2 ulp of the IEEE ones) give the same floors unless an
+    // extreme lies next to an integer; that case, a non-finite projection
+    // and the singular views take the IEEE divisions.
     __device__ static void setup(const View& V, int ix, int iy, const Fan2DParams& P, Cell& c) {
         c.ox = (ix - V.nx2) * V.dx;
         c.oy = (iy - V.ny2) * V.dy;
         const float signx1 = ix - 0.5f, signx2 = ix + 0.5f, signy1 = iy - 0.5f, signy2 = iy + 0.5f;
         const float u1 = V.pm0 * signx1 + V.pm3, u2 = V.pm8 * signx1 + V.pm11;
         const float u3 = V.pm0 * signx2 + V.pm3, u4 = V.pm8 * signx2 + V.pm11;
-        float us[4];
-        us[0] = (u1 + V.pm1 * signy1) / (u2 + V.pm9 * signy1);
-        us[1] = (u1 + V.pm1 * signy2) / (u2 + V.pm9 * signy2);
-        us[2] = (u3 + V.pm1 * signy1) / (u4 + V.pm9 * signy1);
-        us[3] = (u3 + V.pm1 * signy2) / (u4 + V.pm9 * signy2);
-        if (V.singular != 0.f) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) us[k] = (us[k] * 1.5f - 1.0f) / V.puvx;
+        const float n0 = u1 + V.pm1 * signy1, d0 = u2 + V.pm9 * signy1;
+        const float n1 = u1 + V.pm1 * signy2, d1 = u2 + V.pm9 * signy2;
+        const float n2 = u3 + V.pm1 * signy1, d2 = u4 + V.pm9 * signy1;
+        const float n3 = u3 + V.pm1 * signy2, d3 = u4 + V.pm9 * signy2;
+        float lo_u, hi_u;
+        bool ieee = V.singular != 0.f;
+        if (!ieee) {
+            const float q0 = __fdividef(n0, d0), q1 = __fdividef(n1, d1);
+            const float q2 = __fdividef(n2, d2), q3 = __fdividef(n3, d3);
+            lo_u = fminf(fminf(q0, q1), fminf(q2, q3));
+            hi_u = fmaxf(fmaxf(q0, q1), fmaxf(q2, q3));
+            ieee = !(fabsf((q0 + q1) + (q2 + q3)) < 1e30f) || near_int(lo_u) || near_int(hi_u);
         }
-        sort2(us[0], us[1]);
-        sort2(us[2], us[3]);
-        sort2(us[0], us[2]);
-        sort2(us[1], us[3]);
-        sort2(us[1], us[2]);
-        c.lo = min(max(0, (int)floorf(us[0])), P.nu - 1);
-        c.hi = min(max(0, (int)floorf(us[3])), P.nu - 1);
+        if (ieee) {
+            float us[4] = {n0 / d0, n1 / d1, n2 / d2, n3 / d3};
+            if (V.singular != 0.f) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) us[k] = (us[k] * 1.5f - 1.0f) / V.puvx;
+            }
+            sort2(us[0], us[1]);
+            sort2(us[2], us[3]);
+            sort2(us[0], us[2]);
+            sort2(us[1], us[3]);
+            sort2(us[1], us[2]);
+            lo_u = us[0];
+            hi_u = us[3];
+        }
+        c.lo = min(max(0, (int)floorf(lo_u)), P.nu - 1);
+        c.hi = min(max(0, (int)floorf(hi_u)), P.nu - 1);
         const float fl = (float)c.lo;
         c.sx = V.dtvx + V.puvx * (fl - 0.5f * P.nu + 0.5f);
         c.sy = V.dtvy + V.puvy * (fl - 0.5f * P.nu + 0.5f);
@@ -89,7 +112,7 @@ struct B0Basis {
     __device__ static float value(const View& V, Cell& c, int, BinRef t, const Fan2DParams&) {
         const float sx = c.sx, sy = c.sy;
         skip(V, c);
-        const float4 b0 = t[0], b1 = t[1];  // vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2
+        const float4 b0 = t[0], b1 = t[1];  // vx, vy, a0s, sb0 | 1/lsp, 1/lsp^2, 1/x0, 1/x1
         const float px = V.srcx, py = V.srcy;
         // layers/A_B0.cu:207-219: the FP32 products as the reference forms
         // them, its FP64 scalings in FP32
@@ -185,12 +208,12 @@ public:
                 sb0 /= ((bx - px) * (sx - px) + (by - py) * (sy - py)) / (lsp * lsp);
                 float4* o = &bins[(size_t)p * B0Basis::kBinF4 * nu + u];  // planes of nu words
                 o[0] = make_float4((float)vx, (float)vy, (float)a0s, (float)sb0);
-                // the (vx, vy) trapezoid's 1/x0 and 1/(2 x0 x1), x0 >= x1 the
-                // widths' magnitudes (an infinite second one for a box, whose
-                // ramp is empty)
+                // the (vx, vy) trapezoid's 1/x0 and 1/x1, x0 >= x1 the widths'
+                // magnitudes (an infinite second one for a box, whose ramp is
+                // empty)
                 const float fx = std::fabs((float)vx), fy = std::fabs((float)vy);
                 const float fx0 = std::max(fx, fy), fx1 = std::min(fx, fy);
-                o[nu] = make_float4((float)(1.0 / lsp), (float)(1.0 / (lsp * lsp)), 1.0f / fx0, 0.5f / (fx0 * fx1));
+                o[nu] = make_float4((float)(1.0 / lsp), (float)(1.0 / (lsp * lsp)), 1.0f / fx0, 1.0f / fx1);
             }
         }
         finish_init(view, bins);

@@ -30,17 +30,20 @@
 // in a chunk of views (exact products), then in FP64, so the pair is an
 // adjoint pair well below 1e-6 even on heavily cancelling Gaussian inputs.
 //
-//   fan2d_forward_kernel  detector-block driven: a CTA per (view, block of 32
-//                         bins).  The block's ray strip is crossed by the
-//                         lines of the grid's major axis; each lane owns lines
-//                         and walks the few cells of its line inside the strip
+//   fan2d_forward_kernel  detector-block driven: a single-warp CTA per (view,
+//                         block of 32 bins, part of the block's lines).  The
+//                         block's ray strip is crossed by the lines of the
+//                         grid's major axis; each lane owns lines and walks
+//                         the few cells of its line inside the strip
 //                         (host-computed strip records), adding each value to
 //                         its own FP32 shared-memory column of the block's
 //                         bins.  Neighbouring lanes own neighbouring lines and
 //                         read the image (j-major strips) or its transposed
 //                         copy (i-major) at neighbouring addresses.  The
-//                         columns are summed across lanes and warps and every
-//                         bin is written once: no atomics.
+//                         columns are summed across lanes in FP64 and each
+//                         part's sums written once; fan2d_forward_sum_kernel
+//                         adds the parts in order: no atomics, and no warp
+//                         waits for another at a barrier.
 //   fan2d_back_kernel     voxel driven: a CTA per tile of cells, a thread per
 //                         cell.  Per chunk of kF2Views views the CTA stages the
 //                         view constants and the tile's window of the basis
@@ -101,27 +104,30 @@ __device__ __forceinline__ void kahan_fma(float& s, float& c, float a, float b) 
 // at alpha_a + beta_a m and alpha_b + beta_b m; candidate cells lie within
 // `margin` of the span between them.  s0 = (j_major, alpha_a, beta_a,
 // alpha_b), s1 = (beta_b, margin, first line, last line).
+//
+// One warp per (block, view, part): part q takes the block's lines first +
+// 32 q + lane + 32 kF2FwdParts t.  A warp that runs out of lines retires
+// and frees its slot; nothing waits for the other parts, whose FP64 sums
+// fan2d_forward_sum_kernel adds in part order.
 template <class B>
-__global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DParams P, const float* __restrict__ img,
-                                                                         float* __restrict__ sino, float scale) {
+__global__ void __launch_bounds__(32, 32) fan2d_forward_kernel(Fan2DParams P, const float* __restrict__ img) {
     constexpr int kBF4 = B::kBinF4 > 0 ? B::kBinF4 : 1;
     // each lane's FP32 column of the block's bins over its lines (a few terms
-    // per bin), summed across lanes and warps in FP64
-    __shared__ float s_acc[kF2FwdWarps][kF2Block][33];
-    __shared__ double s_red[kF2FwdWarps][kF2Block];
+    // per bin), summed across lanes in FP64
+    __shared__ float s_acc[kF2Block][33];
     __shared__ float4 s_bin[kBF4 * kF2Block];  // [word][bin of the block]
     __shared__ __align__(16) float s_view[B::kViewFloats];
-    const int k = blockIdx.x, p = blockIdx.y;
+    const int k = blockIdx.x, p = blockIdx.y, q = blockIdx.z;
     const int u0 = k * kF2Block, nb = min(kF2Block, P.nu - u0);
-    const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    for (int e = tid; e < B::kViewFloats; e += blockDim.x) s_view[e] = __ldg(P.view + (size_t)p * B::kViewFloats + e);
+    const int l = threadIdx.x;
+    for (int e = l; e < B::kViewFloats; e += 32) s_view[e] = __ldg(P.view + (size_t)p * B::kViewFloats + e);
     if (B::kBinF4 > 0)
-        for (int e = tid; e < nb * B::kBinF4; e += blockDim.x) {
+        for (int e = l; e < nb * B::kBinF4; e += 32) {
             const int k = e / nb, b = e - k * nb;
             s_bin[k * kF2Block + b] = __ldg(P.bins + ((size_t)p * B::kBinF4 + k) * P.nu + u0 + b);
         }
-    for (int e = l; e < kF2Block * 33; e += 32) (&s_acc[w][0][0])[e] = 0.f;
-    __syncthreads();
+    for (int e = l; e < kF2Block * 33; e += 32) (&s_acc[0][0])[e] = 0.f;
+    __syncwarp();
 
     typename B::View V;
     B::load_view(s_view, V);
@@ -134,8 +140,8 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
     // strips read the image and i-major ones its transposed copy coalesced
     const int nmaj = jmaj ? P.nj : P.ni;
     const float* src = jmaj ? img : P.imgT;
-    float* acc = &s_acc[w][0][l];  // bin b at acc[33 b]: this lane's column
-    for (int m = mlo + tid; m <= mhi; m += blockDim.x) {
+    float* acc = &s_acc[0][l];  // bin b at acc[33 b]: this lane's column
+    for (int m = mlo + 32 * q + l; m <= mhi; m += 32 * kF2FwdParts) {
         const float fm = (float)m;
         const float na = fmaf(s0.z, fm, s0.y), nbb = fmaf(s1.x, fm, s0.w);
         const int nlo = max(0, (int)ceilf(fminf(na, nbb) - s1.y));
@@ -153,24 +159,30 @@ __global__ void __launch_bounds__(kF2FwdWarps * 32) fan2d_forward_kernel(Fan2DPa
             for (; u < u0; ++u) B::skip(V, c);
             B::start(V, c, u);
             for (; u <= ue; ++u) {
+                // a dropped bin's value is 0: adding 0 * C leaves the column as
+                // it is (for a finite image value)
                 const float v = B::value(V, c, u, BinRef{s_bin + (u - u0), kF2Block}, P);
-                if (v != 0.f) acc[33 * (u - u0)] = fmaf(v, C, acc[33 * (u - u0)]);
+                acc[33 * (u - u0)] = fmaf(v, C, acc[33 * (u - u0)]);
             }
         }
     }
     __syncwarp();
     if (l < nb) {
         double t = 0.0;
-        for (int q = 0; q < 32; ++q) t += (double)s_acc[w][l][q];
-        s_red[w][l] = t;
+        for (int r = 0; r < 32; ++r) t += (double)s_acc[l][r];
+        P.part[((size_t)q * P.np + p) * P.nu + u0 + l] = t;
     }
-    __syncthreads();
-    if (w == 0 && l < nb) {
+}
+
+// sino (or out64) = scale * the sum of the forward's parts, in part order
+static __global__ void fan2d_forward_sum_kernel(Fan2DParams P, float* __restrict__ sino, float scale) {
+    const size_t n = (size_t)P.np * P.nu;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
         double t = 0.0;
 #pragma unroll
-        for (int q = 0; q < kF2FwdWarps; ++q) t += s_red[q][l];
-        if (P.out64) P.out64[(size_t)p * P.nu + u0 + l] = t * (double)scale;
-        else sino[(size_t)p * P.nu + u0 + l] = (float)t * scale;
+        for (int q = 0; q < kF2FwdParts; ++q) t += P.part[q * n + e];
+        if (P.out64) P.out64[e] = t * (double)scale;
+        else sino[e] = (float)t * scale;
     }
 }
 
@@ -316,8 +328,8 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
             for (; u < lh.x; ++u) B::skip(V, cl);
             B::start(V, cl, u);
             for (; u <= ue; ++u) {
-                const float val = B::value(V, cl, u, BinRef{tb + u, P.wcap}, P);
-                if (val != 0.f) kahan_fma(csum, ccmp, val, sb[u]);
+                // (a dropped bin's 0 adds nothing: s - c stays as it is)
+                kahan_fma(csum, ccmp, B::value(V, cl, u, BinRef{tb + u, P.wcap}, P), sb[u]);
             }
         }
         acc += (double)csum - (double)ccmp;

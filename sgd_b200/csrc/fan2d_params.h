@@ -12,6 +12,7 @@ struct Fan2DParams {
     const float* view = nullptr;     // [np][B::kViewFloats], 16-byte rows
     const float4* bins = nullptr;    // basis-specific per-(view, bin) table [np][B::kBinF4][nu] (planes), or null
     float* imgT = nullptr;           // [nj][ni] transposed copy of the image for i-major strips (forward scratch)
+    double* part = nullptr;          // [kF2FwdParts][np][nu] the forward's partial sums (scratch)
     const float4* strips = nullptr;  // [np][nblk][2] forward block strips (fan2d.cuh)
     int nblk = 0;                    // bin blocks of kF2Block bins per view
     const int2* twin = nullptr;      // [tiles][np] back-projection tile bin windows
@@ -23,8 +24,9 @@ struct Fan2DParams {
     double* out64 = nullptr;         // when set, the kernels write their FP64 sums here instead of the FP32 output
 };
 
-// forward: one CTA per (view, block of kF2Block bins), kF2FwdWarps warps
-constexpr int kF2Block = 32, kF2FwdWarps = 4;
+// forward: one single-warp CTA per (view, block of kF2Block bins, part of
+// the block's lines), kF2FwdParts parts
+constexpr int kF2Block = 32, kF2FwdParts = 4;
 // back: one CTA per kF2TileI x kF2TileJ cells (one per thread), views staged
 // kF2Views at a time
 constexpr int kF2TileI = 8, kF2TileJ = 32, kF2BackThreads = kF2TileI * kF2TileJ, kF2Views = 4;

@@ -190,6 +190,8 @@ void Proj2D::finish_init(const std::vector<float>& view, const std::vector<float
     SGD_CUDA(cudaMalloc(&d_img_, nimg * sizeof(float)));
     SGD_CUDA(cudaMalloc(&d_imgT_, nimg * sizeof(float)));
     P.imgT = d_imgT_;
+    SGD_CUDA(cudaMalloc(&d_part_, kF2FwdParts * nsino * sizeof(double)));
+    P.part = d_part_;
     SGD_CUDA(cudaMalloc(&d_sino_, nsino * sizeof(float)));
     SGD_CUDA(cudaMallocHost(&h_img_, nimg * sizeof(float)));
     SGD_CUDA(cudaMallocHost(&h_sino_, nsino * sizeof(float)));
@@ -204,6 +206,7 @@ Proj2D::~Proj2D() {
     cudaFree(d_err_);
     cudaFree(d_img_);
     cudaFree(d_imgT_);
+    cudaFree(d_part_);
     cudaFree(d_out64_);
     cudaFree(d_sino_);
     cudaFreeHost(h_img_);

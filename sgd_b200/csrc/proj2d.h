@@ -71,6 +71,7 @@ protected:
     int* d_err_ = nullptr;
     float* d_img_ = nullptr;
     float* d_imgT_ = nullptr;  // the forward's line-major image copy
+    double* d_part_ = nullptr;  // the forward's partial sums [kF2FwdParts][np][nu]
     double* d_out64_ = nullptr;  // the FP64 host entry points' output (allocated at their first call)
     void ensure_out64();
     float* d_sino_ = nullptr;

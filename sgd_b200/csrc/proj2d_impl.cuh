@@ -15,8 +15,11 @@ template <class B>
 void fan2d_forward(const Fan2DParams& P, const float* img, float* sino, float scale, cudaStream_t s) {
     fan2d_transpose_kernel<<<dim3((P.nj + 31) / 32, (P.ni + 31) / 32), dim3(32, 8), 0, s>>>(img, P.imgT, P.ni, P.nj);
     SGD_LAUNCH_CHECK();
-    dim3 grid(P.nblk, P.np);
-    fan2d_forward_kernel<B><<<grid, kF2FwdWarps * 32, 0, s>>>(P, img, sino, scale);
+    dim3 grid(P.nblk, P.np, kF2FwdParts);
+    fan2d_forward_kernel<B><<<grid, 32, 0, s>>>(P, img);
+    SGD_LAUNCH_CHECK();
+    const size_t n = (size_t)P.np * P.nu;
+    fan2d_forward_sum_kernel<<<(unsigned)std::min<size_t>((n + 255) / 256, 148 * 16), 256, 0, s>>>(P, sino, scale);
     SGD_LAUNCH_CHECK();
 }
 

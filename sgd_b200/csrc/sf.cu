@@ -73,8 +73,9 @@ struct SFBasis {
         // dx / max(|sin t|, |cos t|) for t = atan2(X, Y) (:174-177) without
         // the trigonometry: |sin t| = |X| / r, |cos t| = |Y| / r
         const float X = V.dx * (ix - V.nx2) - V.srcx, Y = V.dy * (iy - V.ny2) - V.srcy;
+        // (X = Y = 0, a cell centred on the source: atan2(0, 0) = 0, weight dx)
         const float r2 = dot2f(X, X, Y, Y);
-        c.weight = V.dx * __fdividef(r2 * rsqrtf(r2), fmaxf(fabsf(X), fabsf(Y)));
+        c.weight = r2 > 0.f ? V.dx * __fdividef(r2 * rsqrtf(r2), fmaxf(fabsf(X), fabsf(Y))) : V.dx;
         // the pieces' reciprocal widths, once per cell and view (fast
         // reciprocals; a zero width gives an infinite one, see area)
         c.r0 = __fdividef(1.0f, us[1] - us[0]);
@@ -100,8 +101,8 @@ struct SFBasis {
         const float F1 = area(c, u + 1.0f);
         const float g = F1 - c.F;
         c.F = F1;
-        const float val = c.weight * g;
-        return (g > 1e-7f && val == val) ? val : 0.f;
+        // (the amplitude is finite, so the product is a number wherever g is)
+        return g > 1e-7f ? c.weight * g : 0.f;
     }
     __device__ static void skip(const View&, Cell&) {}
 };

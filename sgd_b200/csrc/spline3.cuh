@@ -140,20 +140,30 @@ __device__ __forceinline__ float box2_cum_diff(float e1, float e0, float p, floa
     return copysignf(G(fabsf(e1)), e1) - copysignf(G(fabsf(e0)), e0);
 }
 
+// x0 F2 - x0 / 2 at e (measured from the trapezoid's centre) for the
+// trapezoid of magnitudes x0 >= x1: sgn(e) (min(|e|, k0) + x1 tau (1 - tau /
+// 2)), tau = sat((|e| - k0) / x1) the covered fraction of the ramp, k0 = (x0 -
+// x1) / 2, o = -k0 / x1.  On the plateau this is |e|; on the ramp it is k0 +
+// x1 tau - x1 tau^2 / 2 = x0 / 2 - x1 (1 - tau)^2 / 2; beyond it x0 / 2.  All
+// of it on the FMA pipe (saturated products, a minimum, a sign copy).  For x1
+// = 0 (a box: 1/x1 infinite) tau is 0 or 1 (0 for the NaN at the knot) and
+// the ramp term is 0.
+__device__ __forceinline__ float trap_cum_scaled(float e, float k0, float x1, float rx1, float o) {
+    const float t = fabsf(e);
+    const float tau = __saturatef(__fmaf_rn(t, rx1, o));
+    return copysignf(__fmaf_rn(x1 * tau, __fmaf_rn(-0.5f, tau, 1.0f), fminf(t, k0)), e);
+}
+
 // The 3-direction box spline of signed widths p, q, v at y (box3's
 // convention) as the difference of the (p, q) trapezoid's CDF over v:
-// (F2(y) - F2(y - v)) / v, with the trapezoid's 1/x0 and 1/(2 x0 x1) given
-// (per-bin constants of a table).
-__device__ __forceinline__ float box3_by_cum(float y, float p, float q, float v, float ih, float ir) {
+// (F2(y) - F2(y - v)) / v, with the trapezoid's 1/x0 and 1/x1 given (per-bin
+// constants of a table; x0 >= x1 the widths' magnitudes).
+__device__ __forceinline__ float box3_by_cum(float y, float p, float q, float v, float ih, float rx1) {
     const float x0 = fmaxf(fabsf(p), fabsf(q)), x1 = fminf(fabsf(p), fabsf(q));
-    const float k0 = (x0 - x1) * 0.5f, k1 = (x0 + x1) * 0.5f, c = (p + q) * 0.5f;
-    auto G = [&](float t) {
-        const float d = k1 - t;
-        const float g = t <= k0 ? t * ih : __fmaf_rn(-ir * d, d, 0.5f);
-        return t >= k1 ? 0.5f : g;
-    };
+    const float k0 = (x0 - x1) * 0.5f, c = (p + q) * 0.5f, o = -k0 * rx1;
     const float e1 = y - c, e0 = (y - v) - c;
-    return __fdividef(copysignf(G(fabsf(e1)), e1) - copysignf(G(fabsf(e0)), e0), v);
+    const float d = trap_cum_scaled(e1, k0, x1, rx1, o) - trap_cum_scaled(e0, k0, x1, rx1, o);
+    return __fdividef(d * ih, v);
 }
 
 // The sum of the three 3-direction box splines (-w, va, vb), (-w, vb, vc),

@@ -65,8 +65,8 @@ class FanProjector:
             self.launches_per_step = 3
         else:
             self.kernels = {"forward": "fan2d_forward_kernel", "back": "fan2d_back_kernel"}
-            # image transpose + forward kernel, back kernel
-            self.launches_per_step = 3
+            # image transpose + forward kernel + sum of its parts, back kernel
+            self.launches_per_step = 4
         self._fwd = getattr(L, f"sgd_{kind}_forward_dev")
         self._bwd = getattr(L, f"sgd_{kind}_backward_dev")
         self._destroy = getattr(L, f"{pre}_destroy")
@@ -111,9 +111,9 @@ class _HandleProjector:
 
     # the library's kernels behind each direction, and the launches of one
     # forward + back projection (the generic 2D kernels: the forward's image
-    # transpose and kernel, the back kernel)
+    # transpose, kernel and sum of its parts, the back kernel)
     kernels = {"forward": "fan2d_forward_kernel", "back": "fan2d_back_kernel"}
-    launches_per_step = 3
+    launches_per_step = 4
 
     def _setup(self, handle, fwd, bwd, destroy, image_shape, sino_shape, what):
         if not handle:
