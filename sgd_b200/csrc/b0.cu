@@ -51,12 +51,6 @@ struct B0Basis {
             a = t;
         }
     }
-    // x within 8 ulp (plus 2^-22) of an integer: the fast quotient x and
-    // the IEEE one may lie on either side of it
-    __device__ static bool near_int(float x) {
-        const float f = x - floorf(x), tol = __fmaf_rn(fabsf(x), 0x1p-20f, 0x1p-22f);
-        return f < tol || f > 1.0f - tol;
-    }
     // layers/A_B0.cu:152-198.  The bin range is the reference's: the floors
     // of the extreme corner projections under IEEE division.  Fast
     // quotients (within 2 ulp of the IEEE ones) give the same floors unless an
@@ -79,7 +73,7 @@ struct B0Basis {
             const float q2 = __fdividef(n2, d2), q3 = __fdividef(n3, d3);
             lo_u = fminf(fminf(q0, q1), fminf(q2, q3));
             hi_u = fmaxf(fmaxf(q0, q1), fmaxf(q2, q3));
-            ieee = !(fabsf((q0 + q1) + (q2 + q3)) < 1e30f) || near_int(lo_u) || near_int(hi_u);
+            ieee = !(fabsf((q0 + q1) + (q2 + q3)) < 1e30f) || near_integer(lo_u) || near_integer(hi_u);
         }
         if (ieee) {
             float us[4] = {n0 / d0, n1 / d1, n2 / d2, n3 / d3};

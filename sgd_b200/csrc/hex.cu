@@ -19,10 +19,9 @@
 //   Hl: the 4-direction box spline (vblur, va, vb, vc) (A_Hl.cu:21-46,
 //       FP64 divided differences of truncated cubes there): with all four
 //       directions kept, the difference over the blur width of the
-//       3-direction spline's CDF in closed form, FP32 (box4_by_cum,
-//       spline3.cuh; within 5e-7 of the FP64 form); otherwise, as the
-//       reference, FP64 divided differences with the directions below 1e-8
-//       dropped;
+//       3-direction spline's CDF in closed form, FP32, from per-bin constants
+//       (box4_hex_by_cum, spline3.cuh); otherwise, as the reference, FP64
+//       divided differences with the directions below 1e-8 dropped;
 // va, vb, vc = dt sin(theta + {0, 2pi/3, 4pi/3}) with theta the bin's ray
 // direction (FP64, per view and bin on the host; the reference recomputes them
 // per pair from the stepped FP32 bin centre, a difference far below 1e-6).
@@ -34,6 +33,7 @@
 // and H0's extra skip test in the back projection (A_H0.cu:333-334).
 // "H0 corrected" bounds the true hexagon of each site and has no skip test:
 // the pair is then an exact transpose.
+#include <algorithm>
 #include <cmath>
 
 #include "common.h"
@@ -60,8 +60,10 @@ struct HexBasis {
     // per bin FP32 (va, vb, vc, ...); H0 with the true bounds adds the exact
     // edge-ray maps: (va, vb, vc, beta_a) (alpha_a, alpha_b) (beta_b, 0, 0, 0),
     // the signed offset of edge ray e from site O along the line through O
-    // perpendicular to the bin's central ray being alpha_e . O + beta_e
-    static constexpr int kBinF4 = M == kH0Corrected ? 3 : 1;
+    // perpendicular to the bin's central ray being alpha_e . O + beta_e; Hl
+    // adds its 3-direction spline's constants (box4_hex_by_cum):
+    // (va, vb, vc, GK2) (x1, x2, h, rp6)
+    static constexpr int kBinF4 = M == kH0Corrected ? 3 : (M == kHl ? 2 : 1);
     struct Cell {
         float ox, oy, sx, sy;  // site; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
@@ -77,29 +79,45 @@ struct HexBasis {
 
     // layers/A_H0.cu:47-156 (first stage; the jittered and linearised stages
     // only apply to singular projections, which a source outside the field of
-    // view never produces; a full scan stays as the last resort)
+    // view never produces; a full scan stays as the last resort).  With every
+    // vertex regular, fast quotients give the reference's floors unless an
+    // extreme lies next to an integer (near_integer); that case and any
+    // irregular vertex take the reference's IEEE divisions.
     __device__ static void pmi_bounds(const View& V, int ic, int il, int nu, int& lo, int& hi) {
         const float icc = (float)ic + ((il & 1) ? 0.5f : 0.0f), ilc = (float)il;
         const float offc[6] = {0.0f, +0.5f, +0.5f, 0.0f, -0.5f, -0.5f};
         const float offl[6] = {-2.0f, -1.0f, +1.0f, +2.0f, +1.0f, -1.0f};
+        float num[6], den[6];
         float umin = 1e30f, umax = -1e30f;
-        int nvalid = 0;
+        bool regular = true;
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const float ix = icc + offc[k], iy = ilc + offl[k];
-            const float num = fmaf(V.pm0, ix, fmaf(V.pm1, iy, V.pm3));
-            const float den = fmaf(V.pm8, ix, fmaf(V.pm9, iy, V.pm11));
-            if (!isfinite(num) || !isfinite(den) || fabsf(den) < 1e-8f) continue;
-            const float u = num / den;
-            if (!isfinite(u)) continue;
+            num[k] = fmaf(V.pm0, ix, fmaf(V.pm1, iy, V.pm3));
+            den[k] = fmaf(V.pm8, ix, fmaf(V.pm9, iy, V.pm11));
+            regular = regular && fabsf(num[k]) < 1e30f && fabsf(den[k]) >= 1e-8f && fabsf(den[k]) < 1e30f;
+            const float u = __fdividef(num[k], den[k]);
             umin = fminf(umin, u);
             umax = fmaxf(umax, u);
-            ++nvalid;
         }
-        if (nvalid < 2) {
-            lo = 0;
-            hi = nu - 1;
-            return;
+        if (!regular || !(fabsf(umin) < 1e30f && fabsf(umax) < 1e30f) || near_integer(umin) || near_integer(umax)) {
+            umin = 1e30f;
+            umax = -1e30f;
+            int nvalid = 0;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                if (!isfinite(num[k]) || !isfinite(den[k]) || fabsf(den[k]) < 1e-8f) continue;
+                const float u = num[k] / den[k];
+                if (!isfinite(u)) continue;
+                umin = fminf(umin, u);
+                umax = fmaxf(umax, u);
+                ++nvalid;
+            }
+            if (nvalid < 2) {
+                lo = 0;
+                hi = nu - 1;
+                return;
+            }
         }
         lo = min(max(0, (int)floorf(umin)), nu - 1);
         hi = min(max(0, (int)floorf(umax)), nu - 1);
@@ -214,7 +232,8 @@ struct HexBasis {
             // closed form, FP32; otherwise the reference's FP64 divided
             // differences with the vanishing directions dropped
             if (fabsf(fblur) > 1e-8f && fabsf(va) > 1e-8f && fabsf(vb) > 1e-8f && fabsf(vc) > 1e-8f) {
-                const float conv = box4_by_cum(fy, -fblur, va, vb, vc);
+                const float4 k = t[1];
+                const float conv = box4_hex_by_cum(fy, -fblur, k.x, k.y, k.z, k.w, w.w);
                 return (conv == conv && conv > 0.f) ? conv : 0.f;
             }
             const double conv = conv4((double)fy, (double)fblur, (double)va, (double)vb, (double)vc);
@@ -250,7 +269,9 @@ public:
         const float fdy = fdt * (mode == kHl ? 0.5f : 1.5f);
         constexpr int kVF = HexBasis<kHl>::kViewFloats;
         std::vector<float> view((size_t)np * kVF, 0.f);
-        const int nw = mode == kH0Corrected ? HexBasis<kH0Corrected>::kBinF4 : HexBasis<kHl>::kBinF4;
+        const int nw = mode == kH0Corrected ? HexBasis<kH0Corrected>::kBinF4
+                       : mode == kHl        ? HexBasis<kHl>::kBinF4
+                                            : HexBasis<kH0Reference>::kBinF4;
         std::vector<float4> bins((size_t)np * nu * nw);
         std::vector<BinHomography> hom;
         bin_homographies(geo, hom);
@@ -284,6 +305,16 @@ public:
                 o[2] = (double)fdt * std::sin((double)th + 4.0 * kPi / 3.0);
                 float4* w = &bins[(size_t)p * nw * nu + u];  // planes of nu words
                 w[0] = make_float4((float)o[0], (float)o[1], (float)o[2], 0.f);
+                if (mode == kHl) {
+                    // the 3-direction spline's constants (FP64): magnitudes
+                    // x0 >= x1 >= x2 with x0 = x1 + x2 (the directions sum to 0)
+                    double a[3] = {std::fabs(o[0]), std::fabs(o[1]), std::fabs(o[2])};
+                    std::sort(a, a + 3);
+                    const double x1 = a[1], x2 = a[0], x0 = x1 + x2;
+                    const double rp6 = 1.0 / (6.0 * x0 * x1 * x2);
+                    w[0].w = (float)(0.5 - rp6 * x2 * x2 * x2);
+                    w[nu] = make_float4((float)x1, (float)x2, (float)(1.0 / x0), (float)rp6);
+                }
                 if (mode == kH0Corrected) {
                     // exact edge-ray maps of bin u (FP64): central direction
                     // c = s - S, n its counter-clockwise normal; the edge ray

@@ -52,75 +52,33 @@ __device__ __forceinline__ float box3(float y, float v1, float v2, float v3) {
 
 namespace sgd {
 
-// The cumulative of the symmetric unit-area 3-direction box spline of widths
-// x0 >= x1 >= x2 > 0 from its centre: G(t) = int_0^t M(s) ds for t >= 0, G(0) =
-// 0, G(t >= K3) = 1/2.  Each piece is written with distances to a nearby knot
-// (the ramp down from K2, the top from K3), so FP32 keeps its accuracy.  With
-// F(y) = 1/2 + sgn(y - c) G(|y - c|), c the support's centre, F is the
-// spline's CDF, and the 4-direction box spline of widths (w, x0, x1, x2) is
-// (F(y + w) - F(y)) / w: one blur direction integrated in closed form.
-struct Box3Cum {
-    float K0, K1, K2, K3, h, rp, x2, m, GK2;
-};
-
-__device__ __forceinline__ Box3Cum box3_cum_setup(float x0, float x1, float x2) {
-    Box3Cum b;
-    b.h = __fdividef(1.0f, x0);
-    b.rp = __fdividef(1.0f, x0 * x1 * x2);
-    b.K0 = (x0 - x1 - x2) * 0.5f;
-    b.K1 = (x0 - x1 + x2) * 0.5f;
-    b.K2 = (x0 + x1 - x2) * 0.5f;
-    b.K3 = (x0 + x1 + x2) * 0.5f;
-    b.x2 = x2;
-    b.m = (x0 + x1) * 0.5f;
-    const float d = b.K3 - b.K2;  // = x2
-    b.GK2 = 0.5f - b.rp * (1.0f / 6.0f) * d * d * d;
-    return b;
+// The 4-direction box spline of widths (-w, va, vb, vc) at y for lattice
+// directions with va + vb + vc = 0 (the hexagonal lattice's, dt sin(theta +
+// {0, 2pi/3, 4pi/3})), as the difference over the blur width w > 0 of the
+// 3-direction spline's CDF: (F(y + w) - F(y)) / w (the truncated-power sign
+// convention: support's left end at the sum of the negative widths).  The
+// 3-direction spline's largest magnitude is the sum of the other two, x0 =
+// x1 + x2, and its centre is 0, so F(y) = 1/2 + sgn(y) G(|y|) with the
+// cumulative from the centre G(t) = h t - rp6 t^3 up to x2, GK2 - 3 rp6 x2
+// (x1 - t)(x1 + x2 - t) up to x1, 1/2 - rp6 (x1 + x2 - t)^3 up to x1 + x2,
+// 1/2 beyond (each piece written with distances to a nearby knot, so FP32
+// keeps its accuracy).  Per bin: x1 >= x2 > 0, h = 1/(x1 + x2), rp6 = 1/(6
+// (x1 + x2) x1 x2) and GK2 = 1/2 - rp6 x2^3.
+__device__ __forceinline__ float box4_hex_by_cum(float y, float w, float x1, float x2, float h, float rp6,
+                                                 float GK2) {
+    const float K3 = x1 + x2, r3 = 3.0f * rp6 * x2;
+    auto G = [&](float e) {
+        const float t = fabsf(e);
+        const float d3 = K3 - t, d2 = x1 - t;
+        const float top = __fmaf_rn(-rp6 * d3 * d3, d3, 0.5f);
+        const float ramp = __fmaf_rn(-r3 * d2, d3, GK2);
+        const float inner = __fmaf_rn(h, t, -rp6 * t * t * t);
+        float g = t > x2 ? ramp : inner;
+        g = t >= x1 ? top : g;
+        return copysignf(t >= K3 ? 0.5f : g, e);
+    };
+    return __fdividef(G(y + w) - G(y), w);
 }
-
-__device__ __forceinline__ float box3_cum(const Box3Cum& b, float t) {
-    const float rp6 = b.rp * (1.0f / 6.0f);
-    const float d3 = b.K3 - t;
-    const float top = 0.5f - rp6 * d3 * d3 * d3;                                  // K2 <= t < K3
-    const float d2 = b.K2 - t;
-    const float ramp = b.GK2 - b.x2 * b.rp * d2 * __fmaf_rn(-0.5f, b.K2 + t, b.m);  // K1 < t < K2
-    float inner;                                                                  // t <= K1
-    if (b.K0 >= 0.f) {
-        const float s = t - b.K0;
-        inner = t <= b.K0 ? b.h * t : __fmaf_rn(b.h, t, -rp6 * s * s * s);
-    } else {
-        const float a = -b.K0, hk = __fmaf_rn(-b.rp * b.K0, b.K0, b.h);
-        const float ga = __fmaf_rn(hk, a, -b.rp * (1.0f / 3.0f) * a * a * a);
-        const float s = t - b.K0;
-        const float in_a = __fmaf_rn(hk, t, -b.rp * (1.0f / 3.0f) * t * t * t);
-        const float in_b = ga + b.h * (t - a) - rp6 * __fmaf_rn(s * s, s, 8.0f * b.K0 * b.K0 * b.K0);
-        inner = t <= a ? in_a : in_b;
-    }
-    float g = t > b.K1 ? ramp : inner;
-    g = t >= b.K2 ? top : g;
-    return t >= b.K3 ? 0.5f : g;
-}
-
-// (F(y + w) - F(y)) / w for the 3-direction spline of signed widths v1, v2,
-// v3 (support [sum of the negative ones, sum of the positive ones]) and a
-// blur of width w > 0: the 4-direction box spline of widths (-w, v1, v2, v3)
-// at y, the sign convention of the truncated-power form (support's left end
-// at the sum of the negative widths).
-__device__ __forceinline__ float box4_by_cum(float y, float w, float v1, float v2, float v3) {
-    float x0 = fabsf(v1), x1 = fabsf(v2), x2 = fabsf(v3);
-    order_desc(x1, x2);
-    order_desc(x0, x1);
-    order_desc(x1, x2);
-    const Box3Cum b = box3_cum_setup(x0, x1, x2);
-    const float c = (v1 + v2 + v3) * 0.5f;
-    const float e1 = (y + w) - c, e0 = y - c;
-    const float d = copysignf(box3_cum(b, fabsf(e1)), e1) - copysignf(box3_cum(b, fabsf(e0)), e0);
-    return __fdividef(d, w);
-}
-
-}  // namespace sgd
-
-namespace sgd {
 
 // The 2-direction box spline of signed widths p, q (a trapezoid of unit area
 // on [sum of the negative widths, sum of the positive ones]): its CDF F2 at
