@@ -45,12 +45,14 @@
 //                         adds the parts in order: no atomics, and no warp
 //                         waits for another at a barrier.
 //   fan2d_back_kernel     voxel driven: a CTA per tile of cells, a thread per
-//                         cell.  Per chunk of kF2Views views the CTA stages the
+//                         cell.  Per chunk of kF2Views views warp 0 stages the
 //                         view constants and the tile's window of the basis
-//                         table by bulk asynchronous copies (TMA, completed on
-//                         an mbarrier, double-buffered) and the sinogram
-//                         window by plain loads; each thread accumulates over
-//                         all views in a register and writes its cell once.
+//                         table by bulk asynchronous copies (TMA) into a ring
+//                         of kF2Stages slots, with full/empty mbarriers per
+//                         slot instead of CTA barriers; the sinogram is read
+//                         through the read-only cache.  Each thread
+//                         accumulates over all views in registers and writes
+//                         its cell once.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -211,29 +213,35 @@ static __global__ void fan2d_transpose_kernel(const float* __restrict__ in, floa
     }
 }
 
-// Shared memory of the back kernel: 2 mbarriers | windows [2][VC] int2 |
-// view constants [2][VC][kViewFloats] | tables [2][VC][kBinF4][wcap] float4 |
-// sinogram windows [2][VC][wcap] floats.
-template <class B, int VC>
+// Shared memory of the back kernel: mbarriers full[S], empty[S] | view
+// constants [S][VC][kViewFloats] | tables [S][VC][kBinF4][wcap] float4.
+template <class B, int VC, int S>
 __host__ __device__ constexpr size_t fan2d_back_header() {
-    return 16 + 2 * VC * 8 + (size_t)2 * VC * B::kViewFloats * 4;
+    return (size_t)2 * S * 8 + (size_t)S * VC * B::kViewFloats * 4;
 }
-template <class B, int VC>
+template <class B, int VC, int S>
 __host__ __device__ constexpr size_t fan2d_back_smem(int wcap) {
-    return fan2d_back_header<B, VC>() + (size_t)2 * VC * wcap * (B::kBinF4 * 16 + 4);
+    return fan2d_back_header<B, VC, S>() + (size_t)S * VC * wcap * (B::kBinF4 * 16);
 }
 
-template <class B, int VC>
+// The back projection's staging ring: chunk c (views c VC .. c VC + VC - 1)
+// lives in slot c % S.  Warp 0 stages chunk c + S - 2 when it starts chunk c
+// (after every warp has released that slot's previous chunk, c - 2); each warp
+// waits for its chunk's copies on full[slot] and releases the slot on
+// empty[slot] when done.  No warp waits for the others at a CTA barrier: the
+// warps of a tile drift apart by up to S - 1 chunks, so that a chunk's uneven
+// work (cells' bin counts differ per view) evens out over several chunks.
+template <class B, int VC, int S>
 __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams P, const float* __restrict__ sino,
                                                                     float* __restrict__ img, float scale) {
     static_assert(B::kViewFloats % 4 == 0, "view rows must be whole 16-byte words");
-    static_assert(fan2d_back_header<B, VC>() % 16 == 0, "staged tables must start 16-byte aligned");
+    static_assert(fan2d_back_header<B, VC, S>() % 16 == 0, "staged tables must start 16-byte aligned");
+    static_assert(S >= 3 && VC <= 32, "the ring needs three slots; a lane per view of a chunk");
     extern __shared__ __align__(16) unsigned char f2_smem[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(f2_smem);
-    int2* win = reinterpret_cast<int2*>(f2_smem + 16);                                   // [2][VC]
-    float* sview = reinterpret_cast<float*>(f2_smem + 16 + 2 * VC * 8);                    // [2][VC][kViewFloats]
-    float4* sbin = reinterpret_cast<float4*>(f2_smem + fan2d_back_header<B, VC>());       // [2][VC][wcap * kBinF4]
-    float* ssino = reinterpret_cast<float*>(sbin + (size_t)2 * VC * P.wcap * B::kBinF4);  // [2][VC][wcap]
+    uint64_t* full = reinterpret_cast<uint64_t*>(f2_smem);                          // [S]
+    uint64_t* empty = full + S;                                                       // [S]
+    float* sview = reinterpret_cast<float*>(f2_smem + 2 * S * 8);                     // [S][VC][kViewFloats]
+    float4* sbin = reinterpret_cast<float4*>(f2_smem + fan2d_back_header<B, VC, S>());  // [S][VC][kBinF4][wcap]
     __shared__ int s_abort;
 
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
@@ -244,108 +252,112 @@ __global__ void __launch_bounds__(kF2BackThreads) fan2d_back_kernel(Fan2DParams 
     const int nchunks = (P.np + VC - 1) / VC;
 
     if (tid == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int k = 0; k < S; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&empty[k], kF2TileI);  // one arrival per warp
+        }
         fence_mbar_init();
         s_abort = 0;
     }
     __syncthreads();
 
-    // chunk c: windows (plain stores), view constants and table windows (bulk
-    // copies by lane v of warp 0 for view v), sinogram windows (all threads)
-    auto stage = [&](int c) {
-        const int st = c & 1;
-        if (w == 0) {
-            const int p = c * VC + l;
-            int2 lh = make_int2(0, -1);
-            uint32_t bytes = 0;
-            if (l < VC) {
-                if (p < P.np) {
-                    lh = __ldg(twin + p);
-                    bytes = B::kViewFloats * 4;
-                    if (B::kBinF4 > 0 && lh.y >= lh.x) bytes += (uint32_t)(lh.y - lh.x + 1) * B::kBinF4 * 16;
-                }
-                win[st * VC + l] = lh;
-            }
+    // warp 0: stage chunk n into slot n % S, lane v taking view v (view
+    // constants and table window by bulk copies, completed on full[slot]).
+    // For n >= S the slot's previous chunk n - S must have been released by
+    // every warp first.  Returns false when that wait gives up.
+    auto stage = [&](int n) -> bool {
+        const int slot = n % S;
+        if (n >= S) {
+            // every lane acquires the release itself before its copies overwrite the slot
+            const bool ok = mbar_wait_bounded(&empty[slot], (uint32_t)(n / S - 1) & 1u, P.wait_limit);
+            if (!__all_sync(0xffffffffu, ok)) return false;
+        }
+        const int p = n * VC + l;
+        int2 lh = make_int2(0, -1);
+        uint32_t bytes = 0;
+        if (l < VC && p < P.np) {
+            lh = __ldg(twin + p);
+            bytes = B::kViewFloats * 4;
+            if (B::kBinF4 > 0 && lh.y >= lh.x) bytes += (uint32_t)(lh.y - lh.x + 1) * B::kBinF4 * 16;
+        }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
-            if (l == 0) mbar_arrive_expect_tx(&bars[st], bytes);
-            __syncwarp();
-            if (l < VC && p < P.np) {
-                fence_proxy_async_smem();
-                bulk_copy_g2s(sview + (st * VC + l) * B::kViewFloats, P.view + (size_t)p * B::kViewFloats,
-                              B::kViewFloats * 4, &bars[st]);
-                if (B::kBinF4 > 0 && lh.y >= lh.x)
-                    for (int k = 0; k < B::kBinF4; ++k)
-                        bulk_copy_g2s(sbin + ((size_t)(st * VC + l) * B::kBinF4 + k) * P.wcap,
-                                      P.bins + ((size_t)p * B::kBinF4 + k) * P.nu + lh.x,
-                                      (uint32_t)(lh.y - lh.x + 1) * 16, &bars[st]);
-            }
+        for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
+        if (l == 0) mbar_arrive_expect_tx(&full[slot], bytes);
+        __syncwarp();
+        if (l < VC && p < P.np) {
+            fence_proxy_async_smem();
+            bulk_copy_g2s(sview + (slot * VC + l) * B::kViewFloats, P.view + (size_t)p * B::kViewFloats,
+                          B::kViewFloats * 4, &full[slot]);
+            if (B::kBinF4 > 0 && lh.y >= lh.x)
+                for (int k = 0; k < B::kBinF4; ++k)
+                    bulk_copy_g2s(sbin + ((size_t)(slot * VC + l) * B::kBinF4 + k) * P.wcap,
+                                  P.bins + ((size_t)p * B::kBinF4 + k) * P.nu + lh.x,
+                                  (uint32_t)(lh.y - lh.x + 1) * 16, &full[slot]);
         }
-        for (int v = 0; v < VC; ++v) {
-            const int p = c * VC + v;
-            if (p >= P.np) break;
-            const int2 lh = __ldg(twin + p);
-            const float* sp = sino + (size_t)p * P.nu + lh.x;
-            float* dp = ssino + (st * VC + v) * P.wcap;
-            for (int e = tid; e <= lh.y - lh.x; e += kF2BackThreads) dp[e] = __ldg(sp + e);
-        }
+        return true;
     };
 
-    // chunk f's copies never arrived: wait (bounded) for them and for chunk
-    // f + 1's, which were issued before f's wait, so that no bulk copy is
-    // still landing in this CTA's shared memory when it exits; the tile is
-    // left unwritten
-    auto drain = [&](int f) {
-        if (tid == 0) {
-            mbar_wait_bounded(&bars[f & 1], (uint32_t)(f >> 1) & 1u, kF2WaitLimit);
-            if (f + 1 < nchunks) mbar_wait_bounded(&bars[(f + 1) & 1], (uint32_t)((f + 1) >> 1) & 1u, kF2WaitLimit);
-        }
-    };
-
-    stage(0);
+    int staged = 0;  // warp 0: chunks staged so far
+    if (w == 0)
+        for (; staged < min(S - 2, nchunks); ++staged) stage(staged);
     double acc = 0.0;
     for (int c = 0; c < nchunks; ++c) {
-        __syncthreads();  // chunk c's windows and sinogram visible; chunk c-1 fully consumed
-        if (s_abort) {
-            drain(c - 1);
-            return;
+        if (*(volatile int*)&s_abort) break;
+        if (w == 0 && c + S - 2 < nchunks) {
+            if (!stage(c + S - 2)) {
+                if (l == 0) {
+                    s_abort = 1;
+                    if (P.err) atomicExch(P.err, 1);
+                }
+                break;
+            }
+            staged = c + S - 1;
         }
-        if (c + 1 < nchunks) stage(c + 1);
-        const int st = c & 1;
-        if (!mbar_wait_bounded(&bars[st], (uint32_t)(c >> 1) & 1u, P.wait_limit)) {
+        const int slot = c % S;
+        if (!mbar_wait_bounded(&full[slot], (uint32_t)(c / S) & 1u, P.wait_limit)) {
             s_abort = 1;
             if (P.err) atomicExch(P.err, 1);
-            continue;
+            break;
         }
-        if (!mine) continue;
-        // a compensated FP32 sum within a chunk of views, FP64 across chunks
-        float csum = 0.f, ccmp = 0.f;
+        if (mine) {
+            // a compensated FP32 sum within a chunk of views, FP64 across chunks
+            float csum = 0.f, ccmp = 0.f;
 #pragma unroll 1
-        for (int v = 0; v < VC; ++v) {
-            const int2 lh = win[st * VC + v];
-            if (lh.y < lh.x) continue;
-            typename B::View V;
-            B::load_view(sview + (st * VC + v) * B::kViewFloats, V);
-            typename B::Cell cl;
-            B::setup(V, i, j, P, cl);
-            if (cl.hi < lh.x || cl.lo > lh.y) continue;
-            const float4* tb = sbin + (size_t)(st * VC + v) * P.wcap * B::kBinF4 - lh.x;
-            const float* sb = ssino + (st * VC + v) * P.wcap - lh.x;
-            const int ue = min(cl.hi, lh.y);
-            int u = cl.lo;
-            for (; u < lh.x; ++u) B::skip(V, cl);
-            B::start(V, cl, u);
-            for (; u <= ue; ++u) {
-                // (a dropped bin's 0 adds nothing: s - c stays as it is)
-                kahan_fma(csum, ccmp, B::value(V, cl, u, BinRef{tb + u, P.wcap}, P), sb[u]);
+            for (int v = 0; v < VC; ++v) {
+                const int p = c * VC + v;
+                if (p >= P.np) break;
+                const int2 lh = __ldg(twin + p);
+                if (lh.y < lh.x) continue;
+                typename B::View V;
+                B::load_view(sview + (slot * VC + v) * B::kViewFloats, V);
+                typename B::Cell cl;
+                B::setup(V, i, j, P, cl);
+                if (cl.hi < lh.x || cl.lo > lh.y) continue;
+                const float4* tb = sbin + (size_t)(slot * VC + v) * P.wcap * B::kBinF4 - lh.x;
+                const float* sb = sino + (size_t)p * P.nu;
+                const int ue = min(cl.hi, lh.y);
+                int u = cl.lo;
+                for (; u < lh.x; ++u) B::skip(V, cl);
+                B::start(V, cl, u);
+                for (; u <= ue; ++u) {
+                    // (a dropped bin's 0 adds nothing: s - c stays as it is)
+                    kahan_fma(csum, ccmp, B::value(V, cl, u, BinRef{tb + u, P.wcap}, P), __ldg(sb + u));
+                }
             }
+            acc += (double)csum - (double)ccmp;
         }
-        acc += (double)csum - (double)ccmp;
+        __syncwarp();
+        if (l == 0) mbar_arrive(&empty[slot]);
     }
     __syncthreads();
     if (s_abort) {
-        drain(nchunks - 1);
+        // copies that may still be landing: the last chunk staged into each
+        // slot (a chunk whose phase already completed passes at once).  The
+        // tile is left unwritten.
+        if (w == 0 && l < S) {
+            const int n = staged - 1 - ((staged - 1 - l) % S + S) % S;  // the last staged chunk in slot l
+            if (staged > 0 && n >= 0 && n % S == l) mbar_wait_bounded(&full[l], (uint32_t)(n / S) & 1u, kF2WaitLimit);
+        }
         return;
     }
     if (i < P.ni && j < P.nj) {

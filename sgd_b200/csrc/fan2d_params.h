@@ -28,7 +28,14 @@ struct Fan2DParams {
 // the block's lines), kF2FwdParts parts
 constexpr int kF2Block = 32, kF2FwdParts = 4;
 // back: one CTA per kF2TileI x kF2TileJ cells (one per thread), views staged
-// kF2Views at a time
+// kF2Views at a time in a ring of fan2d_back_stages<B>() slots
 constexpr int kF2TileI = 8, kF2TileJ = 32, kF2BackThreads = kF2TileI * kF2TileJ, kF2Views = 4;
+
+// Ring slots of the back projection: four with no per-bin table, three with
+// one (so that a basis with a two-word table keeps its CTAs per SM)
+template <class B>
+constexpr int fan2d_back_stages() {
+    return B::kBinF4 == 0 ? 4 : 3;
+}
 
 }  // namespace sgd

@@ -57,13 +57,13 @@ struct HexBasis {
         float h0, h1, h2, h3, h4, h5;
         int mode, back;
     };
-    // per bin FP32 (va, vb, vc, ...); H0 with the true bounds adds the exact
-    // edge-ray maps: (va, vb, vc, beta_a) (alpha_a, alpha_b) (beta_b, 0, 0, 0),
-    // the signed offset of edge ray e from site O along the line through O
-    // perpendicular to the bin's central ray being alpha_e . O + beta_e; Hl
-    // adds its 3-direction spline's constants (box4_hex_by_cum):
-    // (va, vb, vc, GK2) (x1, x2, h, rp6)
-    static constexpr int kBinF4 = M == kH0Corrected ? 3 : (M == kHl ? 2 : 1);
+    // per bin FP32 (va, vb, vc, ...); H0 with the true bounds holds (va, vb,
+    // beta_a, beta_b) (alpha_a, alpha_b), vc = -(va + vb) (the three lattice
+    // directions sum to 0) and the exact edge-ray maps, the signed offset of
+    // edge ray e from site O along the line through O perpendicular to the
+    // bin's central ray being alpha_e . O + beta_e; Hl adds its 3-direction
+    // spline's constants (box4_hex_by_cum): (va, vb, vc, GK2) (x1, x2, h, rp6)
+    static constexpr int kBinF4 = M == kH0Reference ? 1 : 2;
     struct Cell {
         float ox, oy, sx, sy;  // site; centre of the next bin of the walk (FP32 stepped)
         int lo, hi;
@@ -193,10 +193,10 @@ struct HexBasis {
             // the exact bin geometry (this mode is held to the FP64 replica,
             // not to the reference's FP32 rounding): two affine maps in place
             // of the edge-ray intersections, divisions and square roots
-            const float4 w0 = t[0], w1 = t[1], w2 = t[2];
-            const float xa = __fmaf_rn(w1.x, c.ox, __fmaf_rn(w1.y, c.oy, w0.w));
-            const float xb = __fmaf_rn(w1.z, c.ox, __fmaf_rn(w1.w, c.oy, w2.x));
-            const float conv = box3_sum3_by_cum(xa, fabsf(xb - xa), w0.x, w0.y, w0.z);
+            const float4 w0 = t[0], w1 = t[1];
+            const float xa = __fmaf_rn(w1.x, c.ox, __fmaf_rn(w1.y, c.oy, w0.z));
+            const float xb = __fmaf_rn(w1.z, c.ox, __fmaf_rn(w1.w, c.oy, w0.w));
+            const float conv = box3_sum3_by_cum(xa, fabsf(xb - xa), w0.x, w0.y, -(w0.x + w0.y));
             return (conv == conv && conv > 0.f) ? conv : 0.f;
         }
         const float sx = c.sx, sy = c.sy;
@@ -335,9 +335,8 @@ public:
                         al[e][1] = k * cy - ny_;
                         be[e] = -(al[e][0] * Sx + al[e][1] * Sy);
                     }
-                    w[0].w = (float)be[0];
+                    w[0] = make_float4((float)o[0], (float)o[1], (float)be[0], (float)be[1]);
                     w[nu] = make_float4((float)al[0][0], (float)al[0][1], (float)al[1][0], (float)al[1][1]);
-                    w[2 * nu] = make_float4((float)be[1], 0.f, 0.f, 0.f);
                 }
             }
         }

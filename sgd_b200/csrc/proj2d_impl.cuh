@@ -25,13 +25,13 @@ void fan2d_forward(const Fan2DParams& P, const float* img, float* sino, float sc
 
 template <class B>
 void fan2d_back(const Fan2DParams& P, const float* sino, float* img, float scale, cudaStream_t s) {
-    const size_t smem = fan2d_back_smem<B, kF2Views>(P.wcap);
+    const size_t smem = fan2d_back_smem<B, kF2Views, fan2d_back_stages<B>()>(P.wcap);
     if (smem > 227 * 1024) fail("back projection: tile window of %d bins does not fit in shared memory", P.wcap);
     if (smem > 48 * 1024)
-        SGD_CUDA(cudaFuncSetAttribute(fan2d_back_kernel<B, kF2Views>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SGD_CUDA(cudaFuncSetAttribute(fan2d_back_kernel<B, kF2Views, fan2d_back_stages<B>()>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
     dim3 grid(P.tiles_j, (P.ni + kF2TileI - 1) / kF2TileI);
-    fan2d_back_kernel<B, kF2Views><<<grid, kF2BackThreads, smem, s>>>(P, sino, img, scale);
+    fan2d_back_kernel<B, kF2Views, fan2d_back_stages<B>()><<<grid, kF2BackThreads, smem, s>>>(P, sino, img, scale);
     SGD_LAUNCH_CHECK();
 }
 
