@@ -73,12 +73,13 @@ constexpr uint32_t kF2WaitLimit = 1u << 22;
 // evaluate identical values.
 __device__ __forceinline__ float dot2f(float a, float b, float c, float d) { return __fmaf_rn(a, b, __fmul_rn(c, d)); }
 
-// x within 8 ulp (plus 2^-22) of an integer: a fast quotient x (within 2 ulp
-// of the IEEE one) and the IEEE quotient may then have different floors.
-// Bases whose bin ranges are the reference's floors of IEEE quotients take
-// fast quotients and fall back to IEEE division where this holds.
+// x within |x| 2^-21 (4 ulp) plus 2^-22 of an integer: a fast quotient x
+// (within 2 ulp of the IEEE one) and the IEEE quotient may then have
+// different floors.  Bases whose bin ranges are the reference's floors of
+// IEEE quotients take fast quotients and fall back to IEEE division where
+// this holds (about one extreme in 2000 at bin indices of a few hundred).
 __device__ __forceinline__ bool near_integer(float x) {
-    const float f = x - floorf(x), tol = __fmaf_rn(fabsf(x), 0x1p-20f, 0x1p-22f);
+    const float f = x - floorf(x), tol = __fmaf_rn(fabsf(x), 0x1p-21f, 0x1p-22f);
     return f < tol || f > 1.0f - tol;
 }
 

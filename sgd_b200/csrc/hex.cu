@@ -218,12 +218,17 @@ struct HexBasis {
                 return 0.f;
         }
         // the edge rays' separation and the site's offset: the reference takes
-        // FP64 square roots of these FP32 differences; their FP32 roots differ
-        // by at most an ulp, far below the FP32 geometry's own rounding
+        // FP64 square roots of these FP32 differences and gives the offset
+        // the sign of the site's side of edge ray a.  Both vectors lie along
+        // the central ray's counter-clockwise normal n = (-(sy - py), sx -
+        // px) / |s - p|, and since edge ray a turns the same way as the
+        // central ray (cross(a - p, n) > 0) the offset's projection on n
+        // carries exactly that sign: the projections are the same lengths
+        // to a few ulp, far below the FP32 geometry's own rounding
         const float dbx = bx1 - ax1, dby = by1 - ay1, dax = ax1 - ox, day = ay1 - oy;
-        const float fblur = -sqrtf(fmaf(dbx, dbx, dby * dby));
-        float fy = sqrtf(fmaf(dax, dax, day * day));
-        if ((ay - py) * (ox - px) < (oy - py) * (ax - px)) fy = -fy;
+        const float cx = sx - px, cy = sy - py, rn = rsqrtf(fmaf(cx, cx, cy * cy));
+        const float fblur = -fabsf(dot2f(dby, cx, -dbx, cy)) * rn;
+        const float fy = dot2f(day, cx, -dax, cy) * rn;
         const float4 w = t[0];
         const float va = w.x, vb = w.y, vc = w.z;
         if (M == kHl) {
