@@ -40,10 +40,11 @@ int sgd_geometry_pmi(int nx, int ny, int nz, int np, int nu, int nv, double dx, 
 
 /* New, host only: the 64-byte B1 footprint record of every (view, bin), as
  * the B1 kernels read them (np*nu*16 floats, layout [view][chunk][bin][4]):
- * the edge offsets xa = i*r0 + (j*r2 + r4), xb = i*r1 + (j*r3 + r5) of pixel
- * (i, j) on the line through its centre across the bin's central ray, and
- * the constants of the closed-form footprint (b, b, a, a, a+b, a+b, 1/a,
- * 1/(2a^2), -b^2/(12a^2), 1/(12a^2b^2)) that replaces the reference's
+ * the edge offsets ya = i*r0 + (j*r2 + r4), yb = i*r1 + (j*r3 + r5) of pixel
+ * (i, j) on the line through its centre across the bin's central ray, in
+ * units of the profile half-width a, and the constants of the closed-form
+ * footprint (beta, beta, 1+beta, 1+beta, -beta^2/12 twice, 1/(12 beta^2)
+ * twice, 1/a, a; beta = b/a) that replaces the reference's
  * linear_convolution_1d (layers/A_B1.cu:182-197, layers/spline_conv.hh:
  * 295-405).  Arguments as b1_init.  0 / -1. */
 int sgd_b1_bin_records(int nx, int ny, int np, int nu, double dx, double dy, double du, double lsd, double lso,

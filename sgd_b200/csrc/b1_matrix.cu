@@ -82,11 +82,15 @@ struct B1GenVisit {
         for (int u = lo; u <= hi; ++u) {
             const B1Bin r = bin_record(rec, p, u, nu);
             const float4 g = __ldg(gen + (size_t)p * nu + u);
-            const float xa = b1_xa(fi, b1_xa_inner(fj, r), r), xb = b1_xb(fi, b1_xb_inner(fj, r), r);
+            // edge offsets in units of a (ya, yb) for the footprint, in mm
+            // (xa, xb) for the window tests
+            const float ya = b1_xa(fi, b1_xa_inner(fj, r), r), yb = b1_xb(fi, b1_xb_inner(fj, r), r);
+            const float a = r.q3.w, xa = ya * a, xb = yb * a;
             const float w = fabsf(xb - xa), m = fminf(fabsf(xa), fabsf(xb));
             if (m * g.x > dx && m * g.y > dy) continue;
             if (fabsf(xa) > g.z + w) continue;
-            const float conv = b1_conv_x(-xa, -xa + w, r);
+            const float wy = fabsf(yb - ya);
+            const float conv = b1_conv_x(-ya, -ya + wy, r);
             if (conv > 0.f) f(u, conv);
         }
     }

@@ -192,6 +192,17 @@ void b1_profile_constants(double a, double b, float* r) {
     r[15] = b > 0 ? (float)(1.0 / (12.0 * a * a * b * b)) : 0.f;
 }
 
+void b1_unit_profile_constants(double a, double b, float* r) {
+    if (b <= 1e-7) b = 0.0;  // single-triangle limit
+    const double beta = b / a;
+    r[6] = r[7] = (float)beta;
+    r[8] = r[9] = (float)(1.0 + beta);
+    r[10] = r[11] = (float)(-beta * beta / 12.0);
+    r[12] = r[13] = beta > 0 ? (float)(1.0 / (12.0 * beta * beta)) : 0.f;
+    r[14] = (float)(1.0 / a);
+    r[15] = (float)a;
+}
+
 void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>& strip) {
     const int np = g.np, nu = g.nu;
     rec.assign((size_t)np * nu * kB1Rec, 0.f);
@@ -216,17 +227,19 @@ void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>
             // x_E(O) = t k_E - q = (O - P).(k_E t - n)
             const double mAx = ka * tx - nxv, mAy = ka * ty - nyv;
             const double mBx = kb * tx - nxv, mBy = kb * ty - nyv;
-            float r[kB1Rec];
-            r[0] = (float)(mAx * g.dx);
-            r[1] = (float)(mBx * g.dx);
-            r[2] = (float)(mAy * g.dy);
-            r[3] = (float)(mBy * g.dy);
-            r[4] = (float)((x0 - px) * mAx + (y0 - py) * mAy);
-            r[5] = (float)((x0 - px) * mBx + (y0 - py) * mBy);
             // profile half-widths (layers/A_B1.cu:429-478): vx = |dx cos(theta)|,
-            // vy = |dy sin(theta)| with theta = atan2(|px - sx|, |py - sy|)
+            // vy = |dy sin(theta)| with theta = atan2(|px - sx|, |py - sy|);
+            // offsets are stored in units of a
             const double vx = std::fabs(g.dx * ty), vy = std::fabs(g.dy * tx);
-            b1_profile_constants(std::max(vx, vy), std::min(vx, vy), r);
+            const double a = std::max(vx, vy);
+            float r[kB1Rec];
+            r[0] = (float)(mAx * g.dx / a);
+            r[1] = (float)(mBx * g.dx / a);
+            r[2] = (float)(mAy * g.dy / a);
+            r[3] = (float)(mBy * g.dy / a);
+            r[4] = (float)(((x0 - px) * mAx + (y0 - py) * mAy) / a);
+            r[5] = (float)(((x0 - px) * mBx + (y0 - py) * mBy) / a);
+            b1_unit_profile_constants(a, std::min(vx, vy), r);
             for (int q = 0; q < 4; ++q)
                 for (int k = 0; k < 4; ++k) rec[(((size_t)p * 4 + q) * nu + u) * 4 + k] = r[4 * q + k];
 

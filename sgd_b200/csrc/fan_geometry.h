@@ -88,23 +88,29 @@ void bin_homographies(const FanGeometry& g, std::vector<BinHomography>& out);
 // centre perpendicular to the bin's central ray, of the bin's two edge rays, and
 // G is the odd extension of the cumulative profile S of the convolution of two
 // unit-area triangles of half-widths a = max(vx, vy), b = min(vx, vy)
-// (conv_2tri_1box_* of layers/spline_conv.hh:295-390).  With
-// w = (b - x)+, p = (a + b - x)+, q = (a - x)+ (x >= 0):
-//     S(x) = x/a - x^2/(2a^2) - b^2/(12a^2) + w^4/(12a^2b^2)   for x <= a - b
-//     S(x) = 1/2 - (p^4 - 2q^4 - 2w^4)/(24a^2b^2)               for x >  a - b
-// Every power is of a distance to a nearby knot, so FP32 keeps its accuracy as
-// b -> 0; b <= 1e-7 uses the single-triangle limit as the reference does
-// (layers/A_B1.cu:52-55).  One 64-byte record per (view, bin), stored as four
-// float4 chunks in the layout [view][chunk][bin] so that consecutive bins of
-// one chunk are consecutive 16-byte words (shared-memory bank groups).  The
-// fields come in the pairs that the packed-FP32 form of the footprint takes as
-// operands (b1_kernels.cuh):
-//   [0] [1]  i coefficients of xa, xb        xa = i*r[0] + (j*r[2] + r[4])
-//   [2] [3]  j coefficients of xa, xb        xb = i*r[1] + (j*r[3] + r[5])
-//   [4] [5]  constant terms of xa, xb
-//   [6] [7]  b, b      [8] [9]  a, a      [10] [11]  a+b, a+b
-//   [12] 1/a   [13] 1/(2a^2)   [14] -b^2/(12a^2)   [15] 1/(12a^2b^2)
-// (a-b and 1/(24a^2b^2) = [15]/2 are formed in the kernels.)
+// (conv_2tri_1box_* of layers/spline_conv.hh:295-390).  The records measure
+// offsets in units of a: y = x / a, beta = b / a <= 1, and then
+//     conv = (G(yb) - G(ya)) / (yb - ya) / a
+// with, for y >= 0, w = (beta - y)+, p = (1 + beta - y)+, q = (1 - y)+:
+//     S(y) = y - y^2/2 - beta^2/12 + w^4/(12 beta^2)          for 1 - y >= beta
+//     S(y) = 1/2 + (q^4 + w^4 - p^4/2)/(12 beta^2)            otherwise
+// (the first piece is the second plus (1 - beta - y)^4/(24 beta^2), which
+// cancels badly as beta -> 0; every power in the pieces used is of a distance
+// to a nearby knot, so FP32 keeps its accuracy).  b <= 1e-7 uses the
+// single-triangle limit as the reference does (layers/A_B1.cu:52-55).  In
+// units of a the polynomial's own coefficients are the constants 1 and -1/2,
+// so a record needs four profile constants, each stored twice.  One 64-byte
+// record per (view, bin), stored as four float4 chunks in the layout
+// [view][chunk][bin] so that consecutive bins of one chunk are consecutive
+// 16-byte words (shared-memory bank groups).  Every field pair is an operand
+// pair of the packed-FP32 form of the footprint (b1_kernels.cuh), so a
+// kernel builds none:
+//   [0] [1]  i coefficients of ya, yb        ya = i*r[0] + (j*r[2] + r[4])
+//   [2] [3]  j coefficients of ya, yb        yb = i*r[1] + (j*r[3] + r[5])
+//   [4] [5]  constant terms of ya, yb
+//   [6] [7]  beta, beta          [8] [9]  1+beta, 1+beta
+//   [10] [11]  -beta^2/12 (twice)    [12] [13]  1/(12 beta^2) (twice; 0 for beta = 0)
+//   [14] 1/a     [15] a (mm)
 // ---------------------------------------------------------------------------
 constexpr int kB1Rec = 16;
 
@@ -114,8 +120,14 @@ constexpr int kB1Rec = 16;
 // [4] = 1 when the major axis is y (rows), 0 when it is x (columns).
 constexpr int kStripRec = 8;
 
-// Fills r[6..15] for profile half-widths a >= b.
+// Fills r[6..15] for profile half-widths a >= b in the original units (the
+// layout of the reference-rounding mode's tables: b, b, a, a, a+b, a+b, 1/a,
+// 1/(2a^2), -b^2/(12a^2), 1/(12a^2b^2)).
 void b1_profile_constants(double a, double b, float* r);
+
+// Fills r[6..15] of a B1 record (offsets in units of a, above) for profile
+// half-widths a >= b.
+void b1_unit_profile_constants(double a, double b, float* r);
 
 void b1_tables(const FanGeometry& g, std::vector<float>& rec, std::vector<float>& strip);
 

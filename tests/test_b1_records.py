@@ -33,18 +33,17 @@ def records(nx, ny, nu, dx, dy, du, lsd, lso, ang, dz=None, drho=None):
     return out.reshape(npv, 4, nu, 4).transpose(0, 2, 1, 3).reshape(npv, nu, 16)
 
 
-def G(x, r):
-    """Odd extension of the cumulative profile, from the record's constants
-    (FP64 evaluation of the FP32 constants)."""
-    b, a, apb = r[..., 6], r[..., 8], r[..., 10]
-    c1, c2, nc3, c4 = r[..., 12], r[..., 13], r[..., 14], r[..., 15]
-    ax = np.abs(x)
-    w = np.maximum(b - ax, 0.0)
-    s_in = ax * (c1 - ax * c2) + nc3 + c4 * w ** 4
-    p = np.maximum(apb - ax, 0.0)
-    q = np.maximum(a - ax, 0.0)
-    s_out = 0.5 - 0.5 * c4 * (p ** 4 - 2 * q ** 4 - 2 * w ** 4)
-    return np.copysign(np.where(ax <= a - b, s_in, s_out), x)
+def G(y, r):
+    """Odd extension of the cumulative profile, y in units of the half-width
+    a, from the record's constants (FP64 evaluation of the FP32 constants)."""
+    beta, opb, nk3, k4 = r[..., 6], r[..., 8], r[..., 10], r[..., 12]
+    ay = np.abs(y)
+    w = np.maximum(beta - ay, 0.0)
+    s_in = ay - 0.5 * ay * ay + nk3 + k4 * w ** 4
+    p = np.maximum(opb - ay, 0.0)
+    q = np.maximum(1.0 - ay, 0.0)
+    s_out = 0.5 + k4 * (q ** 4 + w ** 4 - 0.5 * p ** 4)
+    return np.copysign(np.where(1.0 - ay >= beta, s_in, s_out), y)
 
 
 def forward_from_records(rec, x, nx, ny, dx, dy):
@@ -54,9 +53,9 @@ def forward_from_records(rec, x, nx, ny, dx, dy):
     out = np.empty(rec.shape[:2])
     for p in range(rec.shape[0]):                             # one view at a time
         r = rec[p].astype(np.float64)[:, None, None, :]       # (nu, 1, 1, 16)
-        xa = i * r[..., 0] + (j * r[..., 2] + r[..., 4])
-        xb = i * r[..., 1] + (j * r[..., 3] + r[..., 5])
-        conv = (G(xb, r) - G(xa, r)) / (xb - xa)
+        ya = i * r[..., 0] + (j * r[..., 2] + r[..., 4])
+        yb = i * r[..., 1] + (j * r[..., 3] + r[..., 5])
+        conv = (G(yb, r) - G(ya, r)) / (yb - ya) * r[..., 14]
         conv = np.where(conv > KCONV_EPS, conv, 0.0)
         out[p] = (dx * dy) * np.einsum("uij,ij->u", conv, img)
     return out.ravel()
@@ -89,19 +88,19 @@ def test_records_with_source_offsets(oracle_mod):
 def test_record_fields_are_consistent():
     nx, ny, nu, dx, dy, du, lsd, lso, ang = fan_case("rect")
     r = records(nx, ny, nu, dx, dy, du, lsd, lso, ang).astype(np.float64)
-    b, a = r[..., 6], r[..., 8]
-    assert np.array_equal(r[..., 6], r[..., 7]) and np.array_equal(r[..., 8], r[..., 9])
-    assert np.array_equal(r[..., 10], r[..., 11])
-    assert np.all(a >= b) and np.all(b >= 0) and np.all(a > 0)
-    assert np.allclose(r[..., 10], a + b, rtol=1e-6)
-    assert np.allclose(r[..., 12], 1 / a, rtol=1e-6)
-    assert np.allclose(r[..., 13], 1 / (2 * a * a), rtol=1e-6)
-    assert np.allclose(r[..., 14], -b * b / (12 * a * a), rtol=1e-6)
-    nz = b > 1e-7
-    assert np.allclose(r[..., 15][nz], 1 / (12 * a[nz] ** 2 * b[nz] ** 2), rtol=1e-6)
-    # a and b are the pixel's half-widths across the central ray: a^2 + b^2
-    # lies between min(dx, dy)^2 and max(dx, dy)^2
-    s = a * a + b * b
+    for k in (6, 8, 10, 12):                                  # stored operand pairs
+        assert np.array_equal(r[..., k], r[..., k + 1])
+    beta, a = r[..., 6], r[..., 15]
+    assert np.all(beta <= 1) and np.all(beta >= 0) and np.all(a > 0)
+    assert np.allclose(r[..., 8], 1 + beta, rtol=1e-6)
+    assert np.allclose(r[..., 10], -beta * beta / 12, rtol=1e-6, atol=1e-12)
+    assert np.allclose(r[..., 14], 1 / a, rtol=1e-6)
+    nz = beta * a > 1e-7
+    assert np.allclose(r[..., 12][nz], 1 / (12 * beta[nz] ** 2), rtol=1e-6)
+    assert np.all(r[..., 12][~nz] == 0)
+    # a and b = beta a are the pixel's half-widths across the central ray:
+    # a^2 + b^2 lies between min(dx, dy)^2 and max(dx, dy)^2
+    s = a * a * (1 + beta * beta)
     assert np.all(s >= min(dx, dy) ** 2 * (1 - 1e-6)) and np.all(s <= max(dx, dy) ** 2 * (1 + 1e-6))
 
 
