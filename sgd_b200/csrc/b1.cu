@@ -17,7 +17,6 @@ namespace sgd {
 namespace {
 
 constexpr int kFwdWarps = 8;
-constexpr int kVC = 4;  // views per staged chunk
 
 __global__ void __launch_bounds__(kFwdWarps * 32)
 b1_forward_kernel(const float4* __restrict__ rec, const float* __restrict__ strip, const float* __restrict__ img,
@@ -29,11 +28,15 @@ b1_forward_kernel(const float4* __restrict__ rec, const float* __restrict__ stri
     b1_forward_row(rec, strip, img, imgT, sino, nx, ny, nu, dxdy, gw, lane);
 }
 
-// One CTA per 32x8 tile; wins[tile * np + p] = (lo, hi), the tile's bins in view p.
-__global__ void __launch_bounds__(kBackThreads, 8)
+// One CTA per 32x8 tile; wins[tile * np + p] = (lo, hi), the tile's bins in
+// view p.  Staged planes of WCAP bins (b1_back_tile), four views per chunk up
+// to 320 bins and two beyond.  Seven CTAs of 128 threads per SM (72
+// registers): a 512^2 image's 1024 tiles run in one wave on 148 SMs.
+template <int WCAP>
+__global__ void __launch_bounds__(kBackThreads, 7)
 b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__ hom, const int2* __restrict__ wins,
-               const float* __restrict__ sino, float* __restrict__ img, int nx, int ny, int np, int nu, int wcap,
-               float dxdy, int* __restrict__ err, uint32_t wait_limit) {
+               const float* __restrict__ sino, float* __restrict__ img, int nx, int ny, int np, int nu, float dxdy,
+               int* __restrict__ err, uint32_t wait_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int s_abort;
     if (threadIdx.x == 0) {
@@ -45,8 +48,8 @@ b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__
     }
     uint32_t use0 = 0, use1 = 0;
     const int2* twin = wins + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * np;
-    b1_back_tile<kVC>(rec, hom, twin, sino, img, nx, ny, np, nu, wcap, dxdy, err, wait_limit, blockIdx.y * kBackTI,
-                      blockIdx.x * kBackTJ, smem, s_abort, use0, use1);
+    b1_back_tile<b1_back_vc(WCAP), WCAP>(rec, hom, twin, sino, img, nx, ny, np, nu, dxdy, err, wait_limit,
+                                         blockIdx.y * kBackTI, blockIdx.x * kBackTJ, smem, s_abort, use0, use1);
 }
 
 __global__ void transpose_kernel(const float* __restrict__ in, float* __restrict__ out, int rows, int cols) {
@@ -94,8 +97,7 @@ __global__ void b1_count_kernel(const BinHomography* __restrict__ hom, int nx, i
 int b1_back_windows(const FanGeometry& g, const std::vector<BinHomography>& hom, std::vector<int>& wins) {
     // Per 32x8 tile and view, the bins its pixels' +-1 supports can reach: the
     // kernel's corner rule in double, one extra bin each side so the kernel's
-    // FP32 per-pixel ranges always fall inside.  Returns the largest window,
-    // rounded up to a multiple of 4 (the shared-memory capacity per view).
+    // FP32 per-pixel ranges always fall inside.  Returns the widest window.
     const int gx = (g.ny + kBackTJ - 1) / kBackTJ, gy = (g.nx + kBackTI - 1) / kBackTI;
     wins.assign((size_t)gx * gy * g.np * 2, 0);
     int wmax = 1;
@@ -121,16 +123,47 @@ int b1_back_windows(const FanGeometry& g, const std::vector<BinHomography>& hom,
                 wmax = std::max(wmax, hi - lo + 1);
             }
         }
-    return (wmax + 3) & ~3;
+    return wmax;
 }
 
-size_t b1_back_smem_bytes(int wcap) { return b1_back_smem<kVC>(wcap); }
+int b1_back_plane(int widest) {
+    for (int c : kBackCaps)
+        if (widest + 1 <= c) return c;
+    fail("B1 back projector: a tile's bin window of %d bins does not fit in shared memory (at most %d)", widest,
+         kBackCaps[sizeof(kBackCaps) / sizeof(kBackCaps[0]) - 1] - 1);
+}
 
-void b1_prepare_device() {
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    // the whole unified L1 as shared memory: five CTAs of staged windows per SM
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
+namespace {
+
+// Calls f(kernel, dynamic shared memory bytes) for the back kernel of plane stride wcap.
+template <class F>
+void with_back_kernel(int wcap, F&& f) {
+    switch (wcap) {
+#define SGD_B1_BACK_CASE(W) \
+    case W: f(b1_back_kernel<W>, b1_back_smem<b1_back_vc(W), W>()); break;
+        SGD_B1_BACK_CASE(16) SGD_B1_BACK_CASE(32) SGD_B1_BACK_CASE(48) SGD_B1_BACK_CASE(64)
+        SGD_B1_BACK_CASE(96) SGD_B1_BACK_CASE(128) SGD_B1_BACK_CASE(192) SGD_B1_BACK_CASE(256)
+        SGD_B1_BACK_CASE(320) SGD_B1_BACK_CASE(448) SGD_B1_BACK_CASE(640)
+#undef SGD_B1_BACK_CASE
+        default: fail("B1 back projector: no kernel for a window plane of %d bins", wcap);
+    }
+}
+
+}  // namespace
+
+size_t b1_back_smem_bytes(int wcap) {
+    size_t bytes = 0;
+    with_back_kernel(wcap, [&](auto, size_t smem) { bytes = smem; });
+    return bytes;
+}
+
+void b1_prepare_device(int wcap) {
+    with_back_kernel(wcap, [](auto kern, size_t smem) {
+        SGD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // the whole unified L1 as shared memory: seven CTAs of staged windows per SM
+        SGD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared));
+    });
 }
 
 void b1_forward_launch(const B1Device& d, const float* img, float* imgT, float* sino, cudaStream_t s) {
@@ -146,9 +179,11 @@ void b1_forward_launch(const B1Device& d, const float* img, float* imgT, float* 
 
 void b1_back_launch(const B1Device& d, const float* sino, float* img, cudaStream_t s) {
     dim3 tg((d.ny + kBackTJ - 1) / kBackTJ, (d.nx + kBackTI - 1) / kBackTI);
-    b1_back_kernel<<<tg, kBackThreads, b1_back_smem_bytes(d.wcap), s>>>(
-        reinterpret_cast<const float4*>(d.rec), d.hom, reinterpret_cast<const int2*>(d.wins), sino, img, d.nx, d.ny,
-        d.np, d.nu, d.wcap, d.dxdy, d.err, d.wait_limit);
+    with_back_kernel(d.wcap, [&](auto kern, size_t smem) {
+        kern<<<tg, kBackThreads, smem, s>>>(reinterpret_cast<const float4*>(d.rec), d.hom,
+                                            reinterpret_cast<const int2*>(d.wins), sino, img, d.nx, d.ny, d.np, d.nu,
+                                            d.dxdy, d.err, d.wait_limit);
+    });
     SGD_LAUNCH_CHECK();
 }
 

@@ -17,14 +17,24 @@ struct B1Device {
     const float* strip = nullptr;        // [np][nu][kStripRec]
     const BinHomography* hom = nullptr;  // [np]
     const int* wins = nullptr;           // [tiles][np][2] bin windows of the back kernel's tiles
-    int wcap = 4;                        // bins of a staged view window in the back kernel
+    int wcap = 16;                       // plane stride of the back kernel's staged windows (b1_back_plane)
+    int wmax = 1;                        // widest bin window of a back-projection tile and view
     int* err = nullptr;                  // device flag: a bounded wait in a kernel gave up
     unsigned wait_limit = 1u << 22;      // polls of a back-projection staging wait before it gives up
 };
 
+// Plane strides the back kernel is built for, and its views per chunk at each
+// (two at the widest planes, to stay within shared memory).
+constexpr int kBackCaps[] = {16, 32, 48, 64, 96, 128, 192, 256, 320, 448, 640};
+__host__ __device__ constexpr int b1_back_vc(int wcap) { return wcap <= 320 ? 4 : 2; }
+
+// Tile bin windows of the back kernel; returns the widest.
 int b1_back_windows(const FanGeometry& g, const std::vector<BinHomography>& hom, std::vector<int>& wins);
+// Smallest plane stride that holds a window of `widest` bins and the null bin;
+// fails when none does.
+int b1_back_plane(int widest);
 size_t b1_back_smem_bytes(int wcap);
-void b1_prepare_device();
+void b1_prepare_device(int wcap);
 
 // sino[p * nu + u] = sum_{i,j} A[(p,u),(i,j)] img[i * ny + j]; imgT is scratch of nx*ny floats.
 void b1_forward_launch(const B1Device& d, const float* img, float* imgT, float* sino, cudaStream_t s);

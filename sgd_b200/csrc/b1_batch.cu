@@ -67,8 +67,8 @@ b1_forward_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restr
     }
 }
 
-template <int VC>
-__global__ void __launch_bounds__(kBackThreads, 8)
+template <int VC, int WCAP>
+__global__ void __launch_bounds__(kBackThreads, 7)
 b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict__ start, int ns, long long total,
                      const float* __restrict__ sino, float* __restrict__ img, unsigned long long* __restrict__ counter,
                      int* __restrict__ err, uint32_t wait_limit) {
@@ -93,10 +93,9 @@ b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict
         const B1Slice S = sl[k];
         const int t = (int)(item - start[k]);
         const int bx = t % S.tiles_x, by = t / S.tiles_x;
-        if (!b1_back_tile<VC>(S.rec, S.hom, S.wins + (size_t)t * S.np, sino + S.sino_off, img + S.img_off, S.nx,
-                              S.ny, S.np, S.nu, S.wcap, S.dxdy, err, wait_limit, by * kBackTI, bx * kBackTJ, smem,
-                              s_abort,
-                              use0, use1))
+        if (!b1_back_tile<VC, WCAP>(S.rec, S.hom, S.wins + (size_t)t * S.np, sino + S.sino_off, img + S.img_off,
+                                    S.nx, S.ny, S.np, S.nu, S.dxdy, err, wait_limit, by * kBackTI, bx * kBackTJ,
+                                    smem, s_abort, use0, use1))
             return;
     }
 }
@@ -125,6 +124,36 @@ __global__ void batch_transpose_kernel(const B1Slice* __restrict__ sl, const flo
 
 constexpr int kFWs[3] = {4, 8, 16};
 constexpr int kVCs[3] = {2, 4, 8};
+// Plane strides of the batch's back kernels (staged windows of every slice).
+constexpr int kBatchCaps[] = {48, 64, 96, 128, 256};
+constexpr size_t kSmemMax = 227 * 1024;
+
+// Dynamic shared memory of the back kernel for vc views per chunk and plane
+// stride wcap (b1_back_smem).
+constexpr size_t batch_back_smem(int vc, int wcap) {
+    return (size_t)(16 + 3 * vc * 8 + 3 * vc * 32) + (size_t)2 * vc * kBackPlanes * wcap * 16;
+}
+
+// Calls f(kernel, dynamic shared memory bytes) for views per chunk vc and
+// plane stride wcap; fails for a combination that does not fit in shared
+// memory (eight views of 256-bin windows).
+template <class F>
+void with_batch_back_kernel(int vc, int wcap, F&& f) {
+    if (batch_back_smem(vc, wcap) > kSmemMax)
+        fail("B1 batch: %d views per chunk of %d-bin windows exceed shared memory", vc, wcap);
+#define SGD_B1_BATCH_CASE(V, W)                                                      \
+    if (vc == V && wcap == W) {                                                      \
+        static_assert(b1_back_smem<V, W>() == batch_back_smem(V, W), "smem formula"); \
+        f(b1_back_batch_kernel<V, W>, b1_back_smem<V, W>());                         \
+        return;                                                                      \
+    }
+    SGD_B1_BATCH_CASE(2, 48) SGD_B1_BATCH_CASE(2, 64) SGD_B1_BATCH_CASE(2, 96) SGD_B1_BATCH_CASE(2, 128)
+    SGD_B1_BATCH_CASE(2, 256) SGD_B1_BATCH_CASE(4, 48) SGD_B1_BATCH_CASE(4, 64) SGD_B1_BATCH_CASE(4, 96)
+    SGD_B1_BATCH_CASE(4, 128) SGD_B1_BATCH_CASE(4, 256) SGD_B1_BATCH_CASE(8, 48) SGD_B1_BATCH_CASE(8, 64)
+    SGD_B1_BATCH_CASE(8, 96) SGD_B1_BATCH_CASE(8, 128)
+#undef SGD_B1_BATCH_CASE
+    fail("B1 batch: no back kernel for %d views per chunk and %d-bin windows", vc, wcap);
+}
 
 }  // namespace
 
@@ -183,15 +212,20 @@ B1Batch::B1Batch(int ns, const int* nx, const int* ny, const int* np, const int*
         S.img_off = img_off_[k];
         S.sino_off = sino_off_[k];
         S.nx = d.nx; S.ny = d.ny; S.np = d.np; S.nu = d.nu;
-        S.wcap = d.wcap;
         S.tiles_x = (d.ny + kBackTJ - 1) / kBackTJ;
         S.dxdy = d.dxdy;
-        wcap_max_ = std::max(wcap_max_, d.wcap);
+        wmax_ = std::max(wmax_, d.wmax);
         back_start_[q + 1] = back_start_[q] + (long long)S.tiles_x * ((d.nx + kBackTI - 1) / kBackTI);
         max_nx_ = std::max(max_nx_, d.nx);
         max_ny_ = std::max(max_ny_, d.ny);
     }
-    if (b1_back_smem<8>(wcap_max_) > 200 * 1024) fail("B1 batch: bin window of %d bins too wide", wcap_max_);
+    wcap_ = 0;
+    for (int c : kBatchCaps)
+        if (wmax_ + 1 <= c) {
+            wcap_ = c;
+            break;
+        }
+    if (!wcap_) fail("B1 batch: a tile's bin window of %d bins is too wide (at most %d)", wmax_, kBatchCaps[4] - 1);
     SGD_CUDA(cudaMalloc(&d_slices_, ns * sizeof(B1Slice)));
     SGD_CUDA(cudaMemcpy(d_slices_, host.data(), ns * sizeof(B1Slice), cudaMemcpyHostToDevice));
     SGD_CUDA(cudaMalloc(&d_start_, 2 * (ns + 1) * sizeof(long long)));
@@ -199,15 +233,14 @@ B1Batch::B1Batch(int ns, const int* nx, const int* ny, const int* np, const int*
     SGD_CUDA(cudaMalloc(&d_err_, sizeof(int)));
     SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
     SGD_CUDA(cudaMalloc(&d_imgT_, std::max(1ll, img_off_[ns]) * sizeof(float)));
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<4>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
-    SGD_CUDA(cudaFuncSetAttribute(b1_back_batch_kernel<8>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                  cudaSharedmemCarveoutMaxShared));
+    for (int vc : kVCs) {
+        if (batch_back_smem(vc, wcap_) > kSmemMax) continue;
+        with_batch_back_kernel(vc, wcap_, [](auto kern, size_t smem) {
+            SGD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            SGD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          cudaSharedmemCarveoutMaxShared));
+        });
+    }
     set_variant(8, 4);
 }
 
@@ -225,6 +258,7 @@ B1Batch::~B1Batch() {
 void B1Batch::set_variant(int fw, int vc) {
     if (fw != 4 && fw != 8 && fw != 16) fail("B1 batch: forward warps %d not in {4, 8, 16}", fw);
     if (vc != 2 && vc != 4 && vc != 8) fail("B1 batch: views per chunk %d not in {2, 4, 8}", vc);
+    with_batch_back_kernel(vc, wcap_, [](auto, size_t) {});  // fails when the windows do not fit
     // the start table below is read by persistent kernels that may still be
     // running on the caller's or the batch's stream: let them finish first
     SGD_CUDA(cudaDeviceSynchronize());
@@ -272,9 +306,7 @@ void B1Batch::backward(const float* sino, float* img, cudaStream_t s) {
         kern<<<grid, kBackThreads, smem, s>>>(d_slices_, bstart, ns_, total, sino, img, d_counter_ + 1, d_err_,
                                               wait_limit_);
     };
-    if (vc_ == 2) launch(b1_back_batch_kernel<2>, b1_back_smem<2>(wcap_max_));
-    else if (vc_ == 4) launch(b1_back_batch_kernel<4>, b1_back_smem<4>(wcap_max_));
-    else launch(b1_back_batch_kernel<8>, b1_back_smem<8>(wcap_max_));
+    with_batch_back_kernel(vc_, wcap_, launch);
     SGD_LAUNCH_CHECK();
 }
 
@@ -337,7 +369,7 @@ int B1Batch::tune(const char* cache_path) {
         std::string k;
         int fw = 0, vc = 0;
         while (in >> k >> fw >> vc)
-            if (k == key) {
+            if (k == key && batch_back_smem(vc, wcap_) <= kSmemMax) {  // an entry this build can run
                 set_variant(fw, vc);
                 return 1;
             }
@@ -374,6 +406,7 @@ int B1Batch::tune(const char* cache_path) {
         if (t < tf) { tf = t; best_fw = fw; }
     }
     for (int vc : kVCs) {
+        if (batch_back_smem(vc, wcap_) > kSmemMax) continue;
         set_variant(best_fw, vc);
         const float t = time_ms([&] { backward(sino, img, stream_); });
         if (t < tb) { tb = t; best_vc = vc; }

@@ -20,7 +20,7 @@ struct B1Slice {
     const BinHomography* hom;
     const int2* wins;
     long long img_off, sino_off;  // into the caller's arenas
-    int nx, ny, np, nu, wcap, tiles_x;
+    int nx, ny, np, nu, tiles_x;
     float dxdy;
 };
 
@@ -65,7 +65,8 @@ private:
     std::vector<int> order_, layer_of_;  // processing order; slice -> layer
     std::vector<long long> img_off_, sino_off_, fwd_start_, back_start_;
     std::string signature_, gpu_name_;
-    int ns_ = 0, sms_ = 0, device_ = 0, wcap_max_ = 4, max_nx_ = 0, max_ny_ = 0;
+    int ns_ = 0, sms_ = 0, device_ = 0, max_nx_ = 0, max_ny_ = 0;
+    int wmax_ = 1, wcap_ = 0;  // widest tile window over the slices; plane stride of the back kernel
     int fw_ = 8, vc_ = 4;
     unsigned wait_limit_ = 1u << 22;
     cudaStream_t stream_ = nullptr;

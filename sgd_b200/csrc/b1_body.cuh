@@ -13,11 +13,14 @@
 //                    projects onto in shared memory: the 64-byte footprint
 //                    records by TMA bulk copies completed on an mbarrier
 //                    (double-buffered, the next chunk in flight while this one
-//                    is evaluated), the sinogram values by plain loads.  Each
-//                    thread evaluates a bin's two edges as one packed-FP32
-//                    pair (the constant pairs built from the staged record),
-//                    accumulates over all views in registers and writes its
-//                    pixel once, no atomics.
+//                    is evaluated), the sinogram values by plain loads, as five
+//                    planes of 16-byte words per view whose stride WCAP is a
+//                    compile-time constant (one address per evaluation, the
+//                    five loads at fixed offsets from it), closed by a null
+//                    bin whose footprint is zero.  Each thread evaluates a
+//                    bin's two edges as one packed-FP32 pair (the record's
+//                    operand pairs as staged), accumulates over all views in
+//                    registers and writes its pixel once, no atomics.
 //
 // Reference: layers/A_B1.cu:62-208 (forward, one launch per view, FP64
 // atomics) and :211-353 (backward).
@@ -37,15 +40,22 @@ constexpr int kBackTJ = 32;   // tile extent along j (y): contiguous in memory
 constexpr int kBackThreads = kBackTI * kBackTJ / 2;  // two pixels per thread
 constexpr uint32_t kWaitLimit = 1u << 22;
 
-// 2 mbarriers | 3 x VC windows | 3 x VC homographies, then the staged records
+// 2 mbarriers | 3 x VC windows | 3 x VC homographies, then the staged planes
 template <int VC>
 __host__ __device__ constexpr int b1_header_bytes() {
     return 16 + 3 * VC * 8 + 3 * VC * 32;
 }
 
-template <int VC>
-__host__ __device__ constexpr size_t b1_back_smem(int wcap) {
-    return b1_header_bytes<VC>() + (size_t)2 * VC * wcap * (sizeof(B1Bin) + sizeof(float));
+// Staged planes per view: the four record chunks and the sinogram (the .x of
+// a 16-byte word, so that one address serves all five loads of a bin).
+constexpr int kBackPlanes = 5;
+
+// Shared memory of the back tile: two chunk slots of VC views, each view
+// kBackPlanes planes of WCAP 16-byte words.  A view's window of bins must
+// leave room for the null bin: widest window + 1 <= WCAP.
+template <int VC, int WCAP>
+__host__ __device__ constexpr size_t b1_back_smem() {
+    return b1_header_bytes<VC>() + (size_t)2 * VC * kBackPlanes * WCAP * 16;
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -126,20 +136,20 @@ __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, c
 }
 
 // Back projection of the 32x8 tile at (i0, j0).  twin[p] = (lo, hi): bins of
-// view p the tile's pixels can touch (host-computed, conservative; fits in
-// wcap).  The CTA's two mbarriers (at the start of smem) are initialised by
-// the caller; use0/use1 count the phases barriers 0/1 completed before this
-// tile, so that a persistent CTA can run many tiles on the same barriers.
-// Returns false, with *err set and the tile unwritten, when a staged chunk
-// never arrived (bounded wait); the CTA's barriers are then out of step and it
-// must not run further tiles.
+// view p the tile's pixels can touch (host-computed, conservative; at most
+// WCAP - 1 of them).  The CTA's two mbarriers (at the start of smem) are
+// initialised by the caller; use0/use1 count the phases barriers 0/1
+// completed before this tile, so that a persistent CTA can run many tiles on
+// the same barriers.  Returns false, with *err set and the tile unwritten,
+// when a staged chunk never arrived (bounded wait); the CTA's barriers are
+// then out of step and it must not run further tiles.
 // wait_limit: polls of each staging wait before it gives up (kWaitLimit in
 // production; a test sets 0 to take the failure path).
-template <int VC>
+template <int VC, int WCAP>
 __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, const BinHomography* __restrict__ hom,
                                              const int2* __restrict__ twin, const float* __restrict__ sino,
-                                             float* __restrict__ img, int nx, int ny, int np, int nu, int wcap,
-                                             float dxdy, int* __restrict__ err, uint32_t wait_limit, int i0, int j0,
+                                             float* __restrict__ img, int nx, int ny, int np, int nu, float dxdy,
+                                             int* __restrict__ err, uint32_t wait_limit, int i0, int j0,
                                              unsigned char* smem, volatile int& s_abort, uint32_t& use0,
                                              uint32_t& use1) {
     constexpr int kHeader = b1_header_bytes<VC>();
@@ -147,8 +157,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem);           // [2]
     int* win = reinterpret_cast<int*>(smem + 16);                   // [3][VC][2]
     float* hs = reinterpret_cast<float*>(smem + 16 + 3 * VC * 8);  // [3][VC][8]
-    float4* srec = reinterpret_cast<float4*>(smem + kHeader);      // [2][VC][4 chunks][wcap]
-    float* ssino = reinterpret_cast<float*>(srec + 2 * VC * 4 * wcap);  // [2][VC][wcap]
+    float4* srec = reinterpret_cast<float4*>(smem + kHeader);      // [2][VC][kBackPlanes][WCAP]
 
     // warp w covers columns j0 + 8w .. + 7 of rows i0 .. i0 + 3 (pixel A) and
     // of rows i0 + 4 .. i0 + 7 (pixel B): 8 x 4 blocks whose lanes read few
@@ -160,9 +169,9 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     const int nchunks = (np + VC - 1) / VC;
     auto parity = [&](int c) { return (((c & 1) ? use1 : use0) + (uint32_t)(c >> 1)) & 1u; };
 
-    // stage chunk c: windows and homographies (read after the next barrier)
-    // and footprint records by TMA, lane v of warp 0 taking view v; sinogram
-    // values by all threads
+    // stage chunk c: windows and homographies (read after the next barrier),
+    // the null bin after each window, and footprint records by TMA, lane v of
+    // warp 0 taking view v; sinogram values by all threads
     auto stage = [&](int c) {
         const int st = c & 1, slot = c % 3;
         if (w == 0) {
@@ -179,7 +188,16 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
                 }
                 win[(slot * VC + l) * 2] = lh.x;
                 win[(slot * VC + l) * 2 + 1] = lh.y;
-                if (lh.y >= lh.x) bytes = (uint32_t)(lh.y - lh.x + 1) * sizeof(B1Bin);
+                const int n = lh.y >= lh.x ? lh.y - lh.x + 1 : 0;
+                bytes = (uint32_t)n * sizeof(B1Bin);
+                // the null bin: edges 4 and 5 half-widths from the pixel,
+                // beta = 0 and 1/a = 0, so conv = 0; sinogram 0
+                float4* nb = srec + (st * VC + l) * kBackPlanes * WCAP + n;
+                nb[0] = make_float4(0.f, 0.f, 0.f, 0.f);
+                nb[WCAP] = make_float4(4.f, 5.f, 0.f, 0.f);
+                nb[2 * WCAP] = make_float4(1.f, 1.f, 0.f, 0.f);
+                nb[3 * WCAP] = make_float4(0.f, 0.f, 0.f, 0.f);
+                nb[4 * WCAP] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
@@ -189,8 +207,8 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
                 fence_proxy_async_smem();
                 const uint32_t n = (uint32_t)(lh.y - lh.x + 1) * 16u;
                 for (int q = 0; q < 4; ++q)
-                    bulk_copy_g2s(srec + ((st * VC + l) * 4 + q) * wcap, rec + ((size_t)p * 4 + q) * nu + lh.x, n,
-                                  &bars[st]);
+                    bulk_copy_g2s(srec + ((st * VC + l) * kBackPlanes + q) * WCAP,
+                                  rec + ((size_t)p * 4 + q) * nu + lh.x, n, &bars[st]);
             }
         }
         for (int v = 0; v < VC; ++v) {
@@ -198,8 +216,8 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             if (p >= np) break;
             const int2 lh = __ldg(twin + p);
             const float* sp = sino + (size_t)p * nu + lh.x;
-            float* dp = ssino + (st * VC + v) * wcap;
-            for (int k = tid; k <= lh.y - lh.x; k += kBackThreads) dp[k] = __ldg(sp + k);
+            float* dp = reinterpret_cast<float*>(srec + ((st * VC + v) * kBackPlanes + 4) * WCAP);
+            for (int k = tid; k <= lh.y - lh.x; k += kBackThreads) dp[4 * k] = __ldg(sp + k);
         }
     };
 
@@ -240,30 +258,32 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             int a, b, aB, bB;
             box_bins_bound(hs + (slot * VC + v) * 8, fi, fj, nu, a, b);
             box_bins_bound(hs + (slot * VC + v) * 8, fiB, fj, nu, aB, bB);
-            a = max(a, lo);
-            b = min(b, hi);
-            aB = max(aB, lo);
-            bB = hasB ? min(bB, hi) : aB - 1;
-            const float4* rb = srec + (st * VC + v) * 4 * wcap - lo;
-            const float* sb = ssino + (st * VC + v) * wcap - lo;
+            // window-relative ranges; top is the null bin
+            const int top = hi - lo + 1;
+            a = max(a, lo) - lo;
+            b = min(b, hi) - lo;
+            aB = max(aB, lo) - lo;
+            bB = hasB ? min(bB, hi) - lo : -1;
+            const float4* rb = srec + (st * VC + v) * kBackPlanes * WCAP;
             // per view, each pixel's bins in one loop: trip counts differ by
             // at most one bin between the lanes of a warp.  (A single flat
             // loop over all the chunk's (view, bin) pairs, switching views
             // per lane, measured 1.38x slower at 512^2 x 720 views: the warp
             // ran the switch on most iterations.)  The two pixels' k-th bins
-            // are evaluated side by side, clamped into their ranges with the
-            // surplus evaluation discarded: two independent chains per
-            // iteration (one pixel per thread measured 3.4 % slower).
+            // are evaluated side by side, two independent chains; a pixel
+            // whose bins ran out evaluates the null bin.
             const int n = max(b - a, bB - aB) + 1;
 #pragma unroll 1
             for (int k = 0; k < n; ++k) {
-                const int u = a <= b ? min(a + k, b) : lo, uB = aB <= bB ? min(aB + k, bB) : lo;
-                const B1Pair kA = b1_pair(B1Bin{rb[u], rb[u + wcap], rb[u + 2 * wcap], rb[u + 3 * wcap]});
-                const B1Pair kB = b1_pair(B1Bin{rb[uB], rb[uB + wcap], rb[uB + 2 * wcap], rb[uB + 3 * wcap]});
+                const float4* qA = rb + (a + k <= b ? a + k : top);
+                const float4* qB = rb + (aB + k <= bB ? aB + k : top);
+                const B1Pair kA = b1_pair(B1Bin{qA[0], qA[WCAP], qA[2 * WCAP], qA[3 * WCAP]});
+                const B1Pair kB = b1_pair(B1Bin{qB[0], qB[WCAP], qB[2 * WCAP], qB[3 * WCAP]});
+                const float sA = qA[4 * WCAP].x, sB = qB[4 * WCAP].x;
                 const float convA = b1_conv_pair(b1_edges2(fi2, b1_inner2(fj2, kA), kA), kA);
                 const float convB = b1_conv_pair(b1_edges2(fiB2, b1_inner2(fj2, kB), kB), kB);
-                if (a + k <= b && convA > kConvEps) csum = fmaf(convA, sb[u], csum);
-                if (aB + k <= bB && convB > kConvEps) csumB = fmaf(convB, sb[uB], csumB);
+                if (convA > kConvEps) csum = fmaf(convA, sA, csum);
+                if (convB > kConvEps) csumB = fmaf(convB, sB, csumB);
             }
         }
         acc += (double)csum;

@@ -61,16 +61,15 @@ A_B1::A_B1(int nx, int ny, int np, int nu, double dx, double dy, double du, doub
     dev.dxdy = (float)(dx * dy);
     dev.rec = d_rec_; dev.strip = d_strip_; dev.hom = d_hom_;
     std::vector<int> wins;
-    dev.wcap = b1_back_windows(geo, hom, wins);
+    dev.wmax = b1_back_windows(geo, hom, wins);
+    dev.wcap = b1_back_plane(dev.wmax);
     SGD_CUDA(cudaMalloc(&d_wins_, wins.size() * sizeof(int)));
     SGD_CUDA(cudaMemcpy(d_wins_, wins.data(), wins.size() * sizeof(int), cudaMemcpyHostToDevice));
     dev.wins = d_wins_;
-    if (b1_back_smem_bytes(dev.wcap) > 200 * 1024)
-        fail("B1 back projector: bin window of %d bins does not fit in shared memory", dev.wcap);
     SGD_CUDA(cudaMalloc(&d_err_, sizeof(int)));
     SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
     dev.err = d_err_;
-    b1_prepare_device();
+    b1_prepare_device(dev.wcap);
 
     const size_t nimg = (size_t)nx * ny, nsino = (size_t)np * nu;
     SGD_CUDA(cudaMalloc(&st.d_img, nimg * sizeof(float)));
