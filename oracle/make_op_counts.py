@@ -57,6 +57,23 @@ def main():
         + b1["flops_per_evaluation"] * b1["evaluations_per_pixel_view"],
         "bins_per_cell_view": b1["evaluations_per_pixel_view"], "model": per_view,
         "source": "the b1_fan512 counts (layers/A_B1.cu:96-206)"}
+    # the cone-beam forward formulas at the 256^3 workload (and its half-size
+    # profiling case): every 4th column of voxels (all rows), 4 views
+    cones = {
+        "b1_3d_cone256": ("b1_3d", 256, 360, 384, 1.0, 1.5, "layers/A_B1_3D.cu:82-312"),
+        "sf3d_cone256": ("sf3d", 256, 360, 384, 1.0, 1.5,
+                         "layers/SF_projector.cu:81-234, amplitude and in-detector bins of the corrected pair"),
+        "b1_3d_small": ("b1_3d", 128, 180, 192, 2.0, 3.0, "layers/A_B1_3D.cu:82-312"),
+        "sf3d_small": ("sf3d", 128, 180, 192, 2.0, 3.0,
+                       "layers/SF_projector.cu:81-234, amplitude and in-detector bins of the corrected pair"),
+    }
+    for name, (kind, n, views, nd, d, dd, src) in cones.items():
+        ang = 2 * np.pi * np.arange(views) / views
+        f, nb = oracle.cone_flops(kind, n, nd, d, dd, 1085.6, 595.0, ang, nviews=4, stride=4)
+        out[name] = {"flops_per_cell_view": f, "bins_per_cell_view": nb,
+                     "model": "FLOPs per voxel-view of the reference forward formula (bin ranges, per-voxel "
+                              "terms, every (u, v) bin visited)",
+                     "source": f"oracle/sgd_oracle.cpp oracle_cone_flops: {src}, 4 views, every 4th voxel column"}
     with open(OUT, "w") as fh:
         json.dump(out, fh, indent=1)
     print(json.dumps(out, indent=1))

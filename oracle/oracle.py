@@ -47,6 +47,7 @@ def lib():
         L.oracle_sf_backward.restype = None
         L.oracle_b1_flops.restype = None
         L.oracle_fan2d_flops.restype = None
+        L.oracle_cone_flops.restype = None
     return _LIB
 
 
@@ -117,6 +118,19 @@ def fan2d_flops(kind, nx, ny, nu, dx, dy, du, lsd, lso, angles, nviews=8):
     lib().oracle_fan2d_flops(k, nx, ny, len(angles), nu, ctypes.c_double(dx), ctypes.c_double(dy),
                              ctypes.c_double(du), ctypes.c_double(lsd), ctypes.c_double(lso), _p(angles), nviews,
                              _p(out))
+    return tuple(out)
+
+
+def cone_flops(kind, n, nd, d, dd, lsd, lso, angles, nviews=4, stride=4):
+    """(FLOPs per voxel-view, (u, v) bins per voxel-view) of the reference's
+    cone-beam forward formula of kind "b1_3d" or "sf3d" on an n^3 volume of
+    pitch d and an nd x nd detector of pitch dd."""
+    k = {"b1_3d": 1, "sf3d": 2}[kind]
+    angles = _c(angles)
+    out = np.zeros(2)
+    lib().oracle_cone_flops(k, n, n, n, len(angles), nd, nd, ctypes.c_double(d), ctypes.c_double(d),
+                            ctypes.c_double(d), ctypes.c_double(dd), ctypes.c_double(dd), ctypes.c_double(lsd),
+                            ctypes.c_double(lso), _p(angles), nviews, stride, _p(out))
     return tuple(out)
 
 

@@ -1913,4 +1913,43 @@ void oracle_fan2d_flops(int kind, int nx, int ny, int np, int nu, double dx, dou
     out[1] = cells ? (double)bins / cells : 0.0;
 }
 
+
+// Algorithmic FLOPs of the reference's cone-beam formulas, counted (+, -, *,
+// /, sqrt) on the path taken over `nviews` evenly spread views and the voxels
+// whose ix and iy are multiples of `stride` (every iz): kind 1 the A_B1_3D
+// forward (layers/A_B1_3D.cu:82-312: bin ranges, per-voxel weight and axial
+// trapezoid, per u the edge-ray footprint, per (u, v) the trapezoid
+// integral), kind 2 the SF_projector forward (layers/SF_projector.cu:81-234,
+// its amplitude and in-detector bins as the corrected pair evaluates them).
+// out[0] = FLOPs per voxel-view, out[1] = (u, v) bins visited per voxel-view.
+void oracle_cone_flops(int kind, int nx, int ny, int nz, int np, int nu, int nv, double dx, double dy, double dz,
+                       double du, double dv, double lsd, double lso, const double* angles, int nviews, int stride,
+                       double* out) {
+    Geo g = make_geo(nx, ny, nz, np, nu, nv, dx, dy, dz, du, dv);
+    build_geo(g, lsd, lso, angles, nullptr, nullptr);
+    std::vector<float> vecs;
+    if (kind == 1) b1_vectors(g, vecs);
+    if (kind == 2) exact_pmi_geo(g);
+    long long total = 0, bins = 0, vv = 0;
+    for (int k = 0; k < nviews; ++k) {
+        const int p = (int)((long long)k * np / nviews);
+        for (int iy = 0; iy < ny; iy += stride)
+            for (int ix = 0; ix < nx; ix += stride)
+                for (int iz = 0; iz < nz; ++iz) {
+                    CountedF::flops = 0;
+                    long long n = 0;
+                    if (kind == 1)
+                        b1_3d_voxel_view<CountedF>(g, &vecs[(size_t)p * nu * 2], 0, p, ix, iy, iz,
+                                                   [&](int, int, double) { ++n; });
+                    else
+                        sf3d_voxel_view<CountedF>(g, lsd, 1, true, false, p, ix, iy, iz, [&](int, double) { ++n; });
+                    total += CountedF::flops;
+                    bins += n;
+                    ++vv;
+                }
+    }
+    out[0] = vv ? (double)total / vv : 0.0;
+    out[1] = vv ? (double)bins / vv : 0.0;
+}
+
 }  // extern "C"
