@@ -77,6 +77,7 @@ A_B1::A_B1(int nx, int ny, int np, int nu, double dx, double dy, double du, doub
     SGD_CUDA(cudaMalloc(&st.d_sino, nsino * sizeof(float)));
     SGD_CUDA(cudaMallocHost(&st.h_img, nimg * sizeof(float)));
     SGD_CUDA(cudaMallocHost(&st.h_sino, nsino * sizeof(float)));
+    SGD_CUDA(cudaMallocHost(&st.h_err, sizeof(int)));
     count = b1_count(dev, stream);
 }
 
@@ -92,6 +93,7 @@ A_B1::~A_B1() {
     cudaFree(st.d_sino);
     cudaFreeHost(st.h_img);
     cudaFreeHost(st.h_sino);
+    cudaFreeHost(st.h_err);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -108,8 +110,9 @@ void A_B1::forward_host(double* b, const double* x) {
     SGD_CUDA(cudaMemcpyAsync(st.d_img, st.h_img, nimg * sizeof(float), cudaMemcpyHostToDevice, stream));
     forward_dev(st.d_img, st.d_sino, stream);
     SGD_CUDA(cudaMemcpyAsync(st.h_sino, st.d_sino, nsino * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    SGD_CUDA(cudaMemcpyAsync(st.h_err, d_err_, sizeof(int), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
-    check_device_status(false);
+    raise_device_error(*st.h_err);
 #pragma omp parallel for schedule(static) if (nsino > (1 << 16))
     for (long long e = 0; e < nsino; ++e) b[e] = (double)st.h_sino[e];
 }
@@ -121,8 +124,9 @@ void A_B1::backward_host(const double* b, double* x) {
     SGD_CUDA(cudaMemcpyAsync(st.d_sino, st.h_sino, nsino * sizeof(float), cudaMemcpyHostToDevice, stream));
     backward_dev(st.d_sino, st.d_img, stream);
     SGD_CUDA(cudaMemcpyAsync(st.h_img, st.d_img, nimg * sizeof(float), cudaMemcpyDeviceToHost, stream));
+    SGD_CUDA(cudaMemcpyAsync(st.h_err, d_err_, sizeof(int), cudaMemcpyDeviceToHost, stream));
     SGD_CUDA(cudaStreamSynchronize(stream));
-    check_device_status(false);
+    raise_device_error(*st.h_err);
 #pragma omp parallel for schedule(static) if (nimg > (1 << 16))
     for (long long e = 0; e < nimg; ++e) x[e] = (double)st.h_img[e];
 }
@@ -132,6 +136,10 @@ void A_B1::check_device_status(bool sync_device) {
     // the *_dev calls may have run on any of the caller's streams
     if (sync_device) SGD_CUDA(cudaDeviceSynchronize());
     SGD_CUDA(cudaMemcpy(&e, d_err_, sizeof(int), cudaMemcpyDeviceToHost));
+    raise_device_error(e);
+}
+
+void A_B1::raise_device_error(int e) {
     if (e) {
         SGD_CUDA(cudaMemset(d_err_, 0, sizeof(int)));
         fail("B1 back projector: a shared-memory staging wait timed out; output not written");

@@ -18,6 +18,7 @@ struct Staging {
     float* d_sino = nullptr;
     float* h_img = nullptr;   // pinned
     float* h_sino = nullptr;  // pinned
+    int* h_err = nullptr;     // pinned copy of the device error flag
 };
 
 class A_B1 {
@@ -55,6 +56,9 @@ public:
     void check_device_status(bool sync_device = true);
 
 private:
+    // Raises (and clears) the device error flag whose value e was read.
+    void raise_device_error(int e);
+
     int* d_err_ = nullptr;
     int* d_wins_ = nullptr;
     float* d_rec_ = nullptr;

@@ -91,7 +91,7 @@ class _Fan2DOperator(LinearOperator):
         x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
         if x.size != self.shape[1]:
             raise ValueError(f"expected {self.shape[1]} image values, got {x.size}")
-        y = np.zeros((self.shape[0],), dtype=np.float64)
+        y = np.empty((self.shape[0],), dtype=np.float64)  # every value is written
         if self._fwd(_ptr(y), _ptr(x), self.cpointer) < 0:
             raise _lib.ProjectorError(f"{self._prefix}_forward_projection: {_lib.last_error()}")
         return y.astype(self.dtype, copy=False)
@@ -100,7 +100,7 @@ class _Fan2DOperator(LinearOperator):
         y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
         if y.size != self.shape[0]:
             raise ValueError(f"expected {self.shape[0]} sinogram values, got {y.size}")
-        x = np.zeros((self.shape[1],), dtype=np.float64)
+        x = np.empty((self.shape[1],), dtype=np.float64)  # every value is written
         _lib.check(self._bwd(_ptr(y), _ptr(x), self.cpointer), f"{self._prefix}_backward_projection")
         return x.astype(self.dtype, copy=False)
 
@@ -277,7 +277,7 @@ class A_B1_3D_operator(LinearOperator):
         x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
         if x.size != self.shape[1]:
             raise ValueError(f"expected {self.shape[1]} volume values, got {x.size}")
-        y = np.zeros((self.shape[0],), dtype=np.float64)
+        y = np.empty((self.shape[0],), dtype=np.float64)  # every value is written
         if self._L.b1_3d_forward_projection(_ptr(y), _ptr(x), self.cpointer) == 2 ** 64 - 1:
             raise _lib.ProjectorError(f"b1_3d_forward_projection: {_lib.last_error()}")
         return y.astype(self.dtype, copy=False)
@@ -286,7 +286,7 @@ class A_B1_3D_operator(LinearOperator):
         y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
         if y.size != self.shape[0]:
             raise ValueError(f"expected {self.shape[0]} projection values, got {y.size}")
-        x = np.zeros((self.shape[1],), dtype=np.float64)
+        x = np.empty((self.shape[1],), dtype=np.float64)  # every value is written
         _lib.check(self._L.sgd_b1_3d_backward_projection(_ptr(y), _ptr(x), self.cpointer),
                    "b1_3d_backward_projection")
         return x.astype(self.dtype, copy=False)
@@ -338,7 +338,7 @@ class SF_projector_operator(LinearOperator):
         x = np.ascontiguousarray(np.ravel(x), dtype=np.float64)
         if x.size != self.shape[1]:
             raise ValueError(f"expected {self.shape[1]} volume values, got {x.size}")
-        y = np.zeros((self.shape[0],), dtype=np.float64)
+        y = np.empty((self.shape[0],), dtype=np.float64)  # every value is written
         _lib.check(self._L.sgd_sf3d_forward_projection(_ptr(y), _ptr(x), self.cpointer), "sgd_sf3d_forward_projection")
         return y.astype(self.dtype, copy=False)
 
@@ -346,7 +346,7 @@ class SF_projector_operator(LinearOperator):
         y = np.ascontiguousarray(np.ravel(y), dtype=np.float64)
         if y.size != self.shape[0]:
             raise ValueError(f"expected {self.shape[0]} projection values, got {y.size}")
-        x = np.zeros((self.shape[1],), dtype=np.float64)
+        x = np.empty((self.shape[1],), dtype=np.float64)  # every value is written
         _lib.check(self._L.sgd_sf3d_backward_projection(_ptr(y), _ptr(x), self.cpointer),
                    "sgd_sf3d_backward_projection")
         return x.astype(self.dtype, copy=False)
