@@ -132,18 +132,75 @@ def parse():
 # ---------------------------------------------------------------------------
 # reference arm / CPU baseline: scipy CSR SpMV on a bounded sample of views
 # ---------------------------------------------------------------------------
+class quiet_stdout:
+    """Sends what native code writes to stdout (the reference library prints
+    its launch shapes) to stderr, so that stdout carries the JSON line only."""
+
+    def __enter__(self):
+        import ctypes
+        self._libc = ctypes.CDLL(None)
+        sys.stdout.flush()
+        self._libc.fflush(None)
+        self._saved = os.dup(1)
+        os.dup2(2, 1)
+        return self
+
+    def __exit__(self, *exc):
+        sys.stdout.flush()
+        self._libc.fflush(None)
+        os.dup2(self._saved, 1)
+        os.close(self._saved)
+        return False
+
+
+def reference_matrix_rows(n_views):
+    """Rows of the B1 system matrix for `n_views` uniformly spaced views, as
+    the reference's own generator builds them (bilinear_matrix_generation,
+    layers/A_B1.cu:545-593, from oracle/_ref/libnetwork.so, built from its
+    sources; it runs on the GPU, one dense view at a time), as scipy CSR; None
+    without that library or a GPU, or when the call fails.  Its angles 2 pi p /
+    n_views are the headline's views p * 720 / n_views."""
+    import ctypes
+    import scipy.sparse as sp
+    import torch
+    path = os.path.join(ROOT, "oracle", "_ref", "libnetwork.so")
+    if not os.path.exists(path) or NP % n_views or not torch.cuda.is_available():
+        return None
+    L = ctypes.CDLL(path)
+    f = L.bilinear_matrix_generation
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int] * 4 + [ctypes.c_double] * 5 + [ctypes.c_void_p, ctypes.c_int]
+    # room for 10 entries per pixel-view (the footprint has about 3.4): the
+    # generator aborts the process on a full buffer (assert)
+    cap = n_views * NX * NY * 10
+    buf = np.empty(3 * cap)
+    with quiet_stdout():
+        n = f(n_views, NU, NX, NY, DX, DY, DU, LSD, LSO, buf.ctypes.data, cap)
+    if n <= 0:
+        return None
+    t = buf[:3 * n].reshape(n, 3)
+    return sp.csr_matrix((t[:, 2], (t[:, 0].astype(np.int64), t[:, 1].astype(np.int64))),
+                         shape=(n_views * NU, NX * NY))
+
+
 class CpuSpmv:
     """The reference's CPU path for this operator: its sparse system matrix
     applied as python/operators/operators.py:45-49 does (A @ x, A.T @ y), on
-    the rows of `n_views` evenly spaced views (a bounded sample; the entries
-    come from the oracle's FP64 replica of layers/A_B1.cu).  Built once."""
+    the rows of `n_views` evenly spaced views (a bounded sample).  The entries
+    come from the reference's own generator where its library was built
+    (kind "reference"), else from the oracle's FP64 replica of
+    layers/A_B1.cu (kind "port").  Built once."""
 
-    def __init__(self, n_views=24):
+    def __init__(self, n_views=12):
         import torch
-        from oracle import oracle
         from sgd_b200.phantom import ellipse_phantom
         self.views = np.arange(0, NP, NP // n_views)[:n_views]
-        self.A = oracle.b1_matrix(NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES, self.views)
+        self.A = reference_matrix_rows(n_views)
+        self.kind = "reference"
+        if self.A is None:
+            from oracle import oracle
+            self.A = oracle.b1_matrix(NX, NY, NU, DX, DY, DU, LSD, LSO, ANGLES, self.views)
+            self.kind = "port"
         self.AT = self.A.T.tocsr()
         self.x = ellipse_phantom(NX, NY, DX, DY, seed=0).ravel()
         self.y = self.A @ self.x
@@ -175,12 +232,14 @@ class CpuSpmv:
         return time.perf_counter() - t0
 
     def desc(self, v1, vn):
+        src = ("the reference's own bilinear_matrix_generation (oracle/_ref, built from layers/A_B1.cu)"
+               if self.kind == "reference" else "the FP64 replica of layers/A_B1.cu")
         return (f"CSR SpMV A@x and A.T@y (python/operators/operators.py:45-49 path), FP64, rows of {len(self.views)} "
-                f"of {NP} views (nnz {self.A.nnz}), entries from the FP64 replica of layers/A_B1.cu; "
+                f"of {NP} views (nnz {self.A.nnz}), entries from {src}; "
                 f"scipy 1 thread {v1:.3e}/s, torch CSR (MKL) {self.threads} threads {vn:.3e}/s")
 
 
-def cpu_spmv_sample(n_views=24, reps=3):
+def cpu_spmv_sample(n_views=12, reps=3):
     """Best-of-`reps` updates/s of the sampled CPU path, single-threaded and on
     every host core; the faster is the value."""
     t_all = time.perf_counter()
@@ -190,8 +249,9 @@ def cpu_spmv_sample(n_views=24, reps=3):
     v1, vn = S.units / best1, S.units / bestn
     spent = time.perf_counter() - t_all
     if vn >= v1:
-        return {"value": vn, "cores": S.threads, "single_thread": v1, "desc": S.desc(v1, vn), "spent": spent}
-    return {"value": v1, "cores": 1, "single_thread": v1, "desc": S.desc(v1, vn), "spent": spent}
+        return {"value": vn, "cores": S.threads, "single_thread": v1, "desc": S.desc(v1, vn), "spent": spent,
+                "kind": S.kind}
+    return {"value": v1, "cores": 1, "single_thread": v1, "desc": S.desc(v1, vn), "spent": spent, "kind": S.kind}
 
 
 def run_reference(args, rank, world):
@@ -210,7 +270,7 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": CONFIG, "parallelism": f"host threads x{S.threads}",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": S.threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": S.threads, "kind": S.kind,
                          "sample": S.desc(single, value), "single_thread_value": single},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -239,20 +299,21 @@ def reference_gpu_layer():
     L.ref_b1_kernel_ms.restype = ctypes.c_float
     L.ref_b1_kernel_ms.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     ang = np.ascontiguousarray(ANGLES, dtype=np.float64)
-    h = L.b1_init(NX, NY, NP, NU, DX, DY, DU, LSD, LSO, ang.ctypes.data_as(dp), None, None)
-    back = ctypes.c_float(0.0)
-    fwd = L.ref_b1_kernel_ms(h, 3, ctypes.byref(back))
     from sgd_b200.phantom import ellipse_phantom
     x = np.ascontiguousarray(ellipse_phantom(NX, NY, DX, DY, seed=0).ravel(), dtype=np.float64)
     y = np.zeros(NP * NU)
     xt = np.zeros(NX * NY)
-    L.b1_forward_projection(y.ctypes.data_as(dp), x.ctypes.data_as(dp), h)
-    t0 = time.perf_counter()
     reps = 2
-    for _ in range(reps):
+    with quiet_stdout():
+        h = L.b1_init(NX, NY, NP, NU, DX, DY, DU, LSD, LSO, ang.ctypes.data_as(dp), None, None)
+        back = ctypes.c_float(0.0)
+        fwd = L.ref_b1_kernel_ms(h, 3, ctypes.byref(back))
         L.b1_forward_projection(y.ctypes.data_as(dp), x.ctypes.data_as(dp), h)
-        L.b1_backward_projection(y.ctypes.data_as(dp), xt.ctypes.data_as(dp), h)
-    abi_ms = (time.perf_counter() - t0) / reps * 1e3
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            L.b1_forward_projection(y.ctypes.data_as(dp), x.ctypes.data_as(dp), h)
+            L.b1_backward_projection(y.ctypes.data_as(dp), xt.ctypes.data_as(dp), h)
+        abi_ms = (time.perf_counter() - t0) / reps * 1e3
     units = 2.0 * NX * NY * NP
     return {"kernels_fwd_ms": fwd, "kernels_bwd_ms": back.value,
             "kernels_updates_per_s": units / ((fwd + back.value) * 1e-3),
@@ -436,7 +497,7 @@ def run_ours(args, rank, world, local_rank):
     cpu = ref_gpu = None
     if world == 1:
         r = cpu_spmv_sample(reps=3)
-        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port", "sample": r["desc"],
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": r["desc"],
                "single_thread_value": r["single_thread"], "seconds": round(r["spent"], 2)}
         ref_gpu = reference_gpu_layer()
 
