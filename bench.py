@@ -121,10 +121,12 @@ def parse():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["fan512", "batch48", "asd_c5"] + sorted(FAMILIES), default="fan512",
+    ap.add_argument("--workload", choices=["fan512", "batch48", "asd_c5", "cnn_conv32"] + sorted(FAMILIES),
+                    default="fan512",
                     help="fan512: the headline single-slice workload; batch48: 48 uneven slices in one "
                          "graph-replayed persistent launch per direction; asd_c5: learned vs plain ASD-POCS "
-                         "(several minutes: pair generation and training included); the others: the other "
+                         "(several minutes: pair generation and training included); cnn_conv32: the CNN's "
+                         "32-channel convolution on the tensor cores; the others: the other "
                          "projector families at their configurations (device-resident fwd+adj)")
     return ap.parse_args()
 
@@ -641,6 +643,96 @@ def run_family(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+def run_conv32(args, rank, world, local_rank):
+    """The warm-start CNN's 32-to-32-channel 3x3 convolution (its three middle
+    layers) on 64 images of 256^2: the tensor-core kernel
+    (sgd_conv3x3_forward_tc: tcgen05 MMAs, FP32 activations as three BF16
+    terms) and the FP32 direct kernel beside it, device-resident, L2 flushed
+    between steps.  Roofline: DRAM bytes (the activations read and written
+    once) over the measured HBM copy bandwidth, and the tensor FLOPs of the
+    three passes over the measured BF16 GEMM peak."""
+    import torch
+    from sgd_b200.cnn import _declare, _stream
+    from sgd_b200 import _lib
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    L = _lib.lib()
+    _declare(L)
+    n, h, w = 64, 256, 256
+    g = torch.Generator(device=dev).manual_seed(rank)
+    X = torch.randn((n, 32, h, w), device=dev, generator=g)
+    W16 = (torch.randn((32, 32, 3, 3), device=dev, generator=g) * 0.2).to(torch.bfloat16)
+    B = torch.randn(32, device=dev, generator=g)
+    out_tc, out_fp = torch.empty_like(X), torch.empty_like(X)
+
+    def tc():
+        _lib.check(L.sgd_conv3x3_forward_tc(X.data_ptr(), W16.data_ptr(), B.data_ptr(), out_tc.data_ptr(), n, 32, 32,
+                                            h, w, 1, _stream()), "conv tc")
+
+    def fp():
+        _lib.check(L.sgd_conv3x3_forward(X.data_ptr(), W16.data_ptr(), B.data_ptr(), out_fp.data_ptr(), n, 32, 32, h,
+                                         w, 1, _stream()), "conv fp32")
+
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        tc()
+        fp()
+    torch.cuda.synchronize(dev)
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(K)]
+    uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    sampler = ClockSampler(uuid)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    for k in range(K):
+        flush.fill_(float(k))
+        ev[k][0].record(stream)
+        tc()
+        ev[k][1].record(stream)
+        flush.fill_(float(k) + 0.5)
+        ev[k][2].record(stream)
+        fp()
+        ev[k][3].record(stream)
+    torch.cuda.synchronize(dev)
+    clocks = sampler.stop()
+    _lib.check(L.sgd_conv3x3_tc_status(), "conv tc status")
+    tc_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    fp_times = [e[2].elapsed_time(e[3]) for e in ev]
+    step_ms = max_over_ranks(tc_ms, world, dev)
+    if rank != 0:
+        return
+    pixels = n * h * w
+    bytes_ = 2 * pixels * 32 * 4
+    flops = 3 * 2.0 * pixels * 32 * 288
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    bf16 = peaks.get("bf16_tflops", 1590.0)
+    rel = float((out_tc - out_fp).double().norm() / out_fp.double().norm())
+    line = {
+        "metric": "32-channel 3x3 convolution pixels/s (warm-start CNN middle layer, tensor cores)",
+        "value": world * pixels / (step_ms * 1e-3), "unit": "pixels/s", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16x3 operands, f32 accumulation", "data": "synthetic (normal activations)",
+        "config": {"workload": "3x3 conv 32->32 channels, ReLU, 64 images 256x256, NCHW FP32",
+                   "l2": "flushed between kernels (256 MiB write outside the timed events)"},
+        "fp32_direct_ms": statistics.mean(fp_times),
+        "rel_l2_tc_vs_fp32": rel,
+        "roofline": {"bound": "hbm", "kernel": "conv3x3_c32_tc_kernel", "achieved": bytes_ / (tc_ms * 1e-3) / 1e9,
+                     "peak": hbm, "unit": "GB/s", "frac": bytes_ / (tc_ms * 1e-3) / 1e9 / hbm,
+                     "traffic": load_traffic().get("cnn_conv32:conv3x3_c32_tc_kernel"), "tensor_tflops": flops / (tc_ms * 1e-3) / 1e12, "tensor_peak": bf16,
+                     "tensor_frac": flops / (tc_ms * 1e-3) / 1e12 / bf16,
+                     "peak_source": "MEASURED_PEAKS.json (hbm_gbs, bf16_tflops)" if peaks else "fallback"},
+        "gpu_launches": K, "clocks": clocks,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_asd(args, rank, world, local_rank):
     """Learned warm start vs plain ASD-POCS (64 fan-beam
     phantoms 256^2, 120 views, Poisson I0 = 1e5, the 5-layer 32-channel CNN
@@ -688,6 +780,8 @@ def main():
             run_batch48(args, rank, world, local_rank)
         elif args.workload == "asd_c5":
             run_asd(args, rank, world, local_rank)
+        elif args.workload == "cnn_conv32":
+            run_conv32(args, rank, world, local_rank)
         elif args.workload in FAMILIES:
             run_family(args, rank, world, local_rank)
         else:

@@ -353,6 +353,17 @@ int sgd_relu_backward(float* g, const float* out, long long n, void* stream);
 int sgd_mse_grad(const float* y, const float* t, float* g, long long n, double* d_loss, void* stream);
 int sgd_adam_step(float* w, void* w_bf16, const float* g, float* m, float* v, long long n, float lr, float b1,
                   float b2, float eps, int step, void* stream);
+/* New: sgd_conv3x3_forward for 32 input and 32 output channels (the
+ * network's middle layers) on the sm_100 tensor cores: an implicit GEMM per
+ * 128-pixel row segment issued as tcgen05.mma with the accumulator in tensor
+ * memory; each FP32 activation enters as three BF16 terms, so the products
+ * are exact and the result is an FP32 accumulation as in the direct kernel.
+ * Other channel counts: -1 with a message.  sgd_conv3x3_tc_status
+ * synchronises the device and returns -1 (and clears the flag) if a tile's
+ * MMAs never completed within the kernel's bounded wait. */
+int sgd_conv3x3_forward_tc(const float* in, const void* w_bf16, const float* bias, float* out, int N, int Cin,
+                           int Cout, int H, int W, int relu, void* stream);
+int sgd_conv3x3_tc_status(void);
 
 /* ---- system matrices ------------------------------------------------------ */
 

@@ -27,8 +27,11 @@ def _declare(L):
     L.sgd_relu_backward.argtypes = [_vp, _vp, ll, _vp]
     L.sgd_mse_grad.argtypes = [_vp, _vp, _vp, ll, _vp, _vp]
     L.sgd_adam_step.argtypes = [_vp, _vp, _vp, _vp, _vp, ll, f, f, f, f, i, _vp]
+    L.sgd_conv3x3_forward_tc.argtypes = [_vp, _vp, _vp, _vp, i, i, i, i, i, i, _vp]
+    L.sgd_conv3x3_tc_status.argtypes = []
     for n in ("sgd_conv3x3_forward", "sgd_conv3x3_backward_data", "sgd_conv3x3_backward_weight",
-              "sgd_relu_backward", "sgd_mse_grad", "sgd_adam_step"):
+              "sgd_relu_backward", "sgd_mse_grad", "sgd_adam_step", "sgd_conv3x3_forward_tc",
+              "sgd_conv3x3_tc_status"):
         getattr(L, n).restype = i
     L._cnn_declared = True
 
@@ -39,9 +42,14 @@ def _stream():
 
 class WarmStartCNN:
     """channels: (1, 32, 32, 32, 32, 1) by default; He-initialised, seeded;
-    the last layer starts at zero, so the untrained network is the identity."""
+    the last layer starts at zero, so the untrained network is the identity.
+    tensor_cores: the forward of 32-to-32-channel layers runs on the tensor
+    cores (sgd_conv3x3_forward_tc: exact products, FP32 accumulation in
+    tensor memory); the other layers and the backward pass use the FP32
+    direct kernels."""
 
-    def __init__(self, channels=(1, 32, 32, 32, 32, 1), seed=0, device=None):
+    def __init__(self, channels=(1, 32, 32, 32, 32, 1), seed=0, device=None, tensor_cores=True):
+        self.tensor_cores = bool(tensor_cores)
         self.L = _lib.lib()
         _declare(self.L)
         self.device = device or torch.device("cuda", torch.cuda.current_device())
@@ -66,9 +74,11 @@ class WarmStartCNN:
         N, C, H, W = x.shape
         cout = self.channels[k + 1]
         out = torch.empty((N, cout, H, W), dtype=torch.float32, device=self.device)
-        _lib.check(self.L.sgd_conv3x3_forward(x.data_ptr(), self.w16[k].data_ptr(), self.b[k].data_ptr(),
-                                              out.data_ptr(), N, C, cout, H, W, int(relu), _stream()),
-                   "sgd_conv3x3_forward")
+        f = self.L.sgd_conv3x3_forward
+        if self.tensor_cores and C == 32 and cout == 32:
+            f = self.L.sgd_conv3x3_forward_tc
+        _lib.check(f(x.data_ptr(), self.w16[k].data_ptr(), self.b[k].data_ptr(), out.data_ptr(), N, C, cout, H, W,
+                     int(relu), _stream()), "sgd_conv3x3_forward")
         return out
 
     def forward(self, x, keep=False):
