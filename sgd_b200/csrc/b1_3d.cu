@@ -157,24 +157,6 @@ __device__ float lc1d(float x1, float x2, float a, float b) {  // layers/A_B1_3D
     return (side ? fabsf(s1 - s2) : (s1 + s2)) / fabsf(x2 - x1);
 }
 
-// layers/A_B1_3D.cu:30-66
-__device__ __forceinline__ float gamma_trap(float s1, float s2, const float* us) {
-    float g = 0.0f, tmp, b1, b2;
-    b1 = fmaxf(s1, us[0]);
-    b2 = fminf(s2, us[1]);
-    tmp = (b2 > b1) ? (1 / (2 * (us[1] - us[0]))) * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0])) : 0.0f;
-    if (tmp == tmp) g += tmp;
-    b1 = fmaxf(s1, us[1]);
-    b2 = fminf(s2, us[2]);
-    tmp = (b2 > b1) ? b2 - b1 : 0.0f;
-    if (tmp == tmp) g += tmp;
-    b1 = fmaxf(s1, us[2]);
-    b2 = fminf(s2, us[3]);
-    tmp = (b2 > b1) ? (1 / (2 * (us[3] - us[2]))) * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3])) : 0.0f;
-    if (tmp == tmp) g += tmp;
-    return g;
-}
-
 struct Column {
     float ox, oy, v1, v2, v3, v4;
     int minu, maxu;
@@ -310,30 +292,26 @@ __device__ __forceinline__ bool axial(const View3& V, const Column& c, int iz, i
     if (!(vs[0] < (float)nv)) return false;
     a.minv = min(max(0, (int)floorf(vs[0])), nv - 1);
     a.maxv = min(max(0, (int)floorf(vs[3])), nv - 1);
-    a.k01 = __fdividef(0.5f, vs[1] - vs[0]);
-    a.k23 = __fdividef(0.5f, vs[3] - vs[2]);
+    // a zero-width ramp contributes nothing (the reference drops its NaN)
+    a.k01 = vs[1] > vs[0] ? __fdividef(0.5f, vs[1] - vs[0]) : 0.f;
+    a.k23 = vs[3] > vs[2] ? __fdividef(0.5f, vs[3] - vs[2]) : 0.f;
     a.width2 = __fdividef(2.0f, (vs[3] - vs[0]) + (vs[2] - vs[1]));
     return true;
 }
 
-// layers/A_B1_3D.cu:30-66 over row [s1, s1 + 1]
-__device__ __forceinline__ float row_gamma(const Axial& a, float s1) {
-    const float* us = a.vs;
-    const float s2 = s1 + 1.0f;
-    float g = 0.0f, tmp, b1, b2;
-    b1 = fmaxf(s1, us[0]);
-    b2 = fminf(s2, us[1]);
-    tmp = (b2 > b1) ? a.k01 * ((b2 - us[0]) * (b2 - us[0]) - (b1 - us[0]) * (b1 - us[0])) : 0.0f;
-    if (tmp == tmp) g += tmp;
-    b1 = fmaxf(s1, us[1]);
-    b2 = fminf(s2, us[2]);
-    tmp = (b2 > b1) ? b2 - b1 : 0.0f;
-    if (tmp == tmp) g += tmp;
-    b1 = fmaxf(s1, us[2]);
-    b2 = fminf(s2, us[3]);
-    tmp = (b2 > b1) ? a.k23 * ((b1 - us[3]) * (b1 - us[3]) - (b2 - us[3]) * (b2 - us[3])) : 0.0f;
-    if (tmp == tmp) g += tmp;
-    return g;
+// Cumulative of the axial trapezoid up to s: each of its three pieces'
+// integral over a row [j, j + 1] (layers/A_B1_3D.cu:30-66) is the difference
+// of the piece's terms at the row's ends clamped into the piece, so a row's
+// share is axial_cdf(j + 1) - axial_cdf(j), one evaluation per row boundary.
+// The clamped distances are exact (Sterbenz); written with round-to-nearest
+// intrinsics so that the forward and back kernels form the same bits.
+__device__ __forceinline__ float axial_cdf(const Axial& a, float s) {
+    const float* u = a.vs;
+    const float c01 = __fsub_rn(fminf(fmaxf(s, u[0]), u[1]), u[0]);
+    const float c12 = __fsub_rn(fminf(fmaxf(s, u[1]), u[2]), u[1]);
+    const float d23 = __fsub_rn(u[3], fminf(fmaxf(s, u[2]), u[3]));
+    const float g = __fmaf_rn(__fmul_rn(a.k01, c01), c01, c12);
+    return __fmaf_rn(-__fmul_rn(a.k23, d23), d23, g);
 }
 
 // The reference's amplitude sqrt(r3^2 / r2^2) of a voxel at height oz.
@@ -455,8 +433,11 @@ __global__ void __launch_bounds__(kFW * 32, 3) b1_3d_fwd_kernel(Geo3 G, Plan3 K,
                     if (C0 == 0.f) continue;
                     const float C = C0 * amplitude(ir2, soz[iz] - pz) * a.width2;
                     if (!(C == C)) continue;
+                    float gp = axial_cdf(a, (float)a.minv);
                     for (int j = a.minv; j <= a.maxv; ++j) {
-                        const float g = row_gamma(a, (float)j);
+                        const float gn = axial_cdf(a, (float)(j + 1));
+                        const float g = __fsub_rn(gn, gp);
+                        gp = gn;
                         if (g > kEps) atomicAdd(Aw + j, C * g);
                     }
                 }
@@ -650,8 +631,11 @@ __global__ void __launch_bounds__(kTX * kTY * 32, 3) b1_3d_back_kernel(const __g
                 if (!ok || !chunk_live(beyond, l)) continue;
                 if (mode == 0 && a.minv >= a.maxv) continue;  // :433
                 float val = 0.f;
+                float gp = axial_cdf(a, (float)a.minv);
                 for (int j = a.minv; j <= a.maxv; ++j) {
-                    const float g = row_gamma(a, (float)j);
+                    const float gn = axial_cdf(a, (float)(j + 1));
+                    const float g = __fsub_rn(gn, gp);
+                    gp = gn;
                     if (g > kEps) val = fmaf(g, Bw[j], val);
                 }
                 const float C = mode == 0 ? amplitude(ir2, oz[q] - pz) : amplitude(ir2, oz[q] - pz) * a.width2;
