@@ -46,9 +46,10 @@ __host__ __device__ constexpr int b1_header_bytes() {
     return 16 + 3 * VC * 8 + 3 * VC * 32;
 }
 
-// Staged planes per view: the four record chunks and the sinogram (the .x of
-// a 16-byte word, so that one address serves all five loads of a bin).
-constexpr int kBackPlanes = 5;
+// Staged planes per view: the four record chunks; the sinogram value of a
+// bin replaces the staged copy of its record's last field (a, which the
+// projection does not read), so one 16-byte load brings both.
+constexpr int kBackPlanes = 4;
 
 // Shared memory of the back tile: two chunk slots of VC views, each view
 // kBackPlanes planes of WCAP 16-byte words.  A view's window of bins must
@@ -197,7 +198,6 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
                 nb[WCAP] = make_float4(4.f, 5.f, 0.f, 0.f);
                 nb[2 * WCAP] = make_float4(1.f, 1.f, 0.f, 0.f);
                 nb[3 * WCAP] = make_float4(0.f, 0.f, 0.f, 0.f);
-                nb[4 * WCAP] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) bytes += __shfl_xor_sync(0xffffffffu, bytes, o);
@@ -211,14 +211,34 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
                                   rec + ((size_t)p * 4 + q) * nu + lh.x, n, &bars[st]);
             }
         }
-        for (int v = 0; v < VC; ++v) {
-            const int p = c * VC + v;
-            if (p >= np) break;
-            const int2 lh = __ldg(twin + p);
-            const float* sp = sino + (size_t)p * nu + lh.x;
-            float* dp = reinterpret_cast<float*>(srec + ((st * VC + v) * kBackPlanes + 4) * WCAP);
-            for (int k = tid; k <= lh.y - lh.x; k += kBackThreads) dp[4 * k] = __ldg(sp + k);
+    };
+
+    // sinogram values of chunk c into registers (element e = v * WCAP + k of
+    // the chunk's windows, thread tid taking e = tid + s * kBackThreads), a
+    // chunk ahead of their use so that the loads' latency is hidden
+    constexpr int kSR = (VC * WCAP + kBackThreads - 1) / kBackThreads;
+    auto prefetch = [&](int c, float* r) {
+#pragma unroll
+        for (int s2 = 0; s2 < kSR; ++s2) {
+            const int e = tid + s2 * kBackThreads, v = e / WCAP, k = e - v * WCAP, p = c * VC + v;
+            r[s2] = 0.f;
+            if (v < VC && p < np) {
+                const int2 lh = __ldg(twin + p);
+                if (k <= lh.y - lh.x) r[s2] = __ldg(sino + (size_t)p * nu + lh.x + k);
+            }
         }
+    };
+    // ... and into the .w of the staged records' last chunk once chunk c's
+    // copies have landed (the copies wrote that field)
+    auto place = [&](int c, const float* r) {
+        const int st = c & 1, slot = c % 3;
+#pragma unroll
+        for (int s2 = 0; s2 < kSR; ++s2) {
+            const int e = tid + s2 * kBackThreads, v = e / WCAP, k = e - v * WCAP;
+            if (v < VC && k <= win[(slot * VC + v) * 2 + 1] - win[(slot * VC + v) * 2])
+                reinterpret_cast<float*>(srec + ((st * VC + v) * kBackPlanes + 3) * WCAP + k)[3] = r[s2];
+        }
+        fence_proxy_async_smem();  // before the bulk copies that will overwrite them
     };
 
     // chunk f's copies never arrived: wait (bounded, full limit) for them and
@@ -233,21 +253,30 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
 
     __syncthreads();  // the previous tile's last chunk is fully consumed
     stage(0);
+    float sv[kSR], svn[kSR];
+    prefetch(0, sv);
 
     double acc = 0.0, accB = 0.0;  // FP32 within a chunk (a few tens of terms), FP64 across chunks
     for (int c = 0; c < nchunks; ++c) {
-        __syncthreads();  // chunk c's windows and sinogram visible; chunk c-1 fully consumed
-        if (s_abort) {
-            drain(c - 1);
-            return false;
+        __syncthreads();  // chunk c's windows visible; chunk c-1 fully consumed
+        if (c + 1 < nchunks) {
+            stage(c + 1);
+            prefetch(c + 1, svn);
         }
-        if (c + 1 < nchunks) stage(c + 1);
         const int st = c & 1, slot = c % 3;
-        if (!mbar_wait_bounded(&bars[st], parity(c), wait_limit)) {
+        if (mbar_wait_bounded(&bars[st], parity(c), wait_limit)) {
+            place(c, sv);
+        } else {
             s_abort = 1;
             atomicExch(err, 1);
-            continue;
         }
+        __syncthreads();  // chunk c's sinogram in place
+        if (s_abort) {
+            drain(c);
+            return false;
+        }
+#pragma unroll
+        for (int s2 = 0; s2 < kSR; ++s2) sv[s2] = svn[s2];
         if (j >= ny || i >= nx) continue;
         const bool hasB = iB < nx;
         float csum = 0.f, csumB = 0.f;
@@ -279,7 +308,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
                 const float4* qB = rb + (aB + k <= bB ? aB + k : top);
                 const B1Pair kA = b1_pair(B1Bin{qA[0], qA[WCAP], qA[2 * WCAP], qA[3 * WCAP]});
                 const B1Pair kB = b1_pair(B1Bin{qB[0], qB[WCAP], qB[2 * WCAP], qB[3 * WCAP]});
-                const float sA = qA[4 * WCAP].x, sB = qB[4 * WCAP].x;
+                const float sA = qA[3 * WCAP].w, sB = qB[3 * WCAP].w;
                 const float convA = b1_conv_pair(b1_edges2(fi2, b1_inner2(fj2, kA), kA), kA);
                 const float convB = b1_conv_pair(b1_edges2(fiB2, b1_inner2(fj2, kB), kB), kB);
                 if (convA > kConvEps) csum = fmaf(convA, sA, csum);
@@ -288,11 +317,6 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
         }
         acc += (double)csum;
         accB += (double)csumB;
-    }
-    __syncthreads();
-    if (s_abort) {  // the last chunk's wait gave up
-        drain(nchunks - 1);
-        return false;
     }
     use0 += (uint32_t)((nchunks + 1) >> 1);
     use1 += (uint32_t)(nchunks >> 1);
