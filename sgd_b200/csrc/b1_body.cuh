@@ -111,8 +111,9 @@ __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, c
             float2 fn = pair((float)nlo);
             const float* sp = img + (size_t)nlo * ny + m;
             for (int n = nlo; n <= nhi; ++n, fn = __fadd2_rn(fn, pair(1.0f)), sp += ny) {
+                const float xv = __ldg(sp);  // issued before the footprint math, which hides its latency
                 const float conv = b1_conv_pair(b1_edges2(fn, inner, k), k);
-                if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
+                if (conv > kConvEps) row = fmaf(conv, xv, row);
             }
             acc += (double)row;
         }
@@ -126,8 +127,9 @@ __device__ __forceinline__ void b1_forward_row(const float4* __restrict__ rec, c
             float2 fn = pair((float)nlo);
             const float* sp = imgT + (size_t)nlo * nx + m;
             for (int n = nlo; n <= nhi; ++n, fn = __fadd2_rn(fn, pair(1.0f)), sp += nx) {
+                const float xv = __ldg(sp);
                 const float conv = b1_conv_pair(b1_edges2(fm, b1_inner2(fn, k), k), k);
-                if (conv > kConvEps) row = fmaf(conv, __ldg(sp), row);
+                if (conv > kConvEps) row = fmaf(conv, xv, row);
             }
             acc += (double)row;
         }
