@@ -38,18 +38,16 @@ b1_back_kernel(const float4* __restrict__ rec, const BinHomography* __restrict__
                const float* __restrict__ sino, float* __restrict__ img, int nx, int ny, int np, int nu, float dxdy,
                int* __restrict__ err, uint32_t wait_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_abort;
     if (threadIdx.x == 0) {
         uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         fence_mbar_init();
-        s_abort = 0;
     }
     uint32_t use0 = 0, use1 = 0;
     const int2* twin = wins + (size_t)(blockIdx.y * gridDim.x + blockIdx.x) * np;
     b1_back_tile<b1_back_vc(WCAP), WCAP>(rec, hom, twin, sino, img, nx, ny, np, nu, dxdy, err, wait_limit,
-                                         blockIdx.y * kBackTI, blockIdx.x * kBackTJ, smem, s_abort, use0, use1);
+                                         blockIdx.y * kBackTI, blockIdx.x * kBackTJ, smem, use0, use1);
 }
 
 __global__ void transpose_kernel(const float* __restrict__ in, float* __restrict__ out, int rows, int cols) {

@@ -73,14 +73,12 @@ b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict
                      const float* __restrict__ sino, float* __restrict__ img, unsigned long long* __restrict__ counter,
                      int* __restrict__ err, uint32_t wait_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int s_abort;
     __shared__ long long s_item;
     if (threadIdx.x == 0) {
         uint64_t* bars = reinterpret_cast<uint64_t*>(smem);
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
         fence_mbar_init();
-        s_abort = 0;
     }
     uint32_t use0 = 0, use1 = 0;
     for (;;) {
@@ -95,7 +93,7 @@ b1_back_batch_kernel(const B1Slice* __restrict__ sl, const long long* __restrict
         const int bx = t % S.tiles_x, by = t / S.tiles_x;
         if (!b1_back_tile<VC, WCAP>(S.rec, S.hom, S.wins + (size_t)t * S.np, sino + S.sino_off, img + S.img_off,
                                     S.nx, S.ny, S.np, S.nu, S.dxdy, err, wait_limit, by * kBackTI, bx * kBackTJ,
-                                    smem, s_abort, use0, use1))
+                                    smem, use0, use1))
             return;
     }
 }

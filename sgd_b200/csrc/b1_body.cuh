@@ -153,7 +153,7 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
                                              const int2* __restrict__ twin, const float* __restrict__ sino,
                                              float* __restrict__ img, int nx, int ny, int np, int nu, float dxdy,
                                              int* __restrict__ err, uint32_t wait_limit, int i0, int j0,
-                                             unsigned char* smem, volatile int& s_abort, uint32_t& use0,
+                                             unsigned char* smem, uint32_t& use0,
                                              uint32_t& use1) {
     constexpr int kHeader = b1_header_bytes<VC>();
     static_assert(kHeader % 16 == 0, "staged records must start 16-byte aligned");
@@ -216,8 +216,8 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
     };
 
     // sinogram values of chunk c into registers (element e = v * WCAP + k of
-    // the chunk's windows, thread tid taking e = tid + s * kBackThreads), a
-    // chunk ahead of their use so that the loads' latency is hidden
+    // the chunk's windows, thread tid taking e = tid + s * kBackThreads; 0
+    // beyond a view's window), loaded while the chunk before is evaluated
     constexpr int kSR = (VC * WCAP + kBackThreads - 1) / kBackThreads;
     auto prefetch = [&](int c, float* r) {
 #pragma unroll
@@ -230,95 +230,109 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
             }
         }
     };
-    // ... and into the .w of the staged records' last chunk once chunk c's
-    // copies have landed (the copies wrote that field)
+    // ... and into the .w of the staged records' last plane once chunk c's
+    // copies have landed (the copies wrote that field).  Every element of
+    // the slot is written: past a window's end the value is 0, which is also
+    // the null bin's, and nothing reads that part of the slot.  No element
+    // depends on the staged windows, which warp 0 may still be writing for
+    // this chunk when the other warps get here.
     auto place = [&](int c, const float* r) {
-        const int st = c & 1, slot = c % 3;
+        const int st = c & 1;
 #pragma unroll
         for (int s2 = 0; s2 < kSR; ++s2) {
             const int e = tid + s2 * kBackThreads, v = e / WCAP, k = e - v * WCAP;
-            if (v < VC && k <= win[(slot * VC + v) * 2 + 1] - win[(slot * VC + v) * 2])
-                reinterpret_cast<float*>(srec + ((st * VC + v) * kBackPlanes + 3) * WCAP + k)[3] = r[s2];
+            if (v < VC) reinterpret_cast<float*>(srec + ((st * VC + v) * kBackPlanes + 3) * WCAP + k)[3] = r[s2];
         }
         fence_proxy_async_smem();  // before the bulk copies that will overwrite them
     };
-
-    // chunk f's copies never arrived: wait (bounded, full limit) for them and
-    // for chunk f + 1's, issued before f's wait, so that no bulk copy is still
-    // landing in this CTA's shared memory when it moves on or exits
-    auto drain = [&](int f) {
-        if (tid == 0) {
-            mbar_wait_bounded(&bars[f & 1], parity(f), kWaitLimit);
-            if (f + 1 < nchunks) mbar_wait_bounded(&bars[(f + 1) & 1], parity(f + 1), kWaitLimit);
+    // wait (bounded) for chunk c's copies and place its sinogram; a wait
+    // that gave up sets the device error and this thread's failed flag,
+    // which the next CTA barrier ORs over the threads
+    bool failed = false;
+    auto land = [&](int c, const float* r) {
+        if (mbar_wait_bounded(&bars[c & 1], parity(c), wait_limit)) {
+            place(c, r);
+        } else {
+            failed = true;
+            atomicExch(err, 1);
         }
     };
 
+    // chunk f's copies never arrived: wait for them (bounded, full limit), so
+    // that no bulk copy is still landing in this CTA's shared memory when it
+    // moves on or exits (chunk f + 1 is staged only after f has landed)
+    auto drain = [&](int f) {
+        if (tid == 0) mbar_wait_bounded(&bars[f & 1], parity(f), kWaitLimit);
+    };
+
+    // One CTA barrier per chunk: chunk c + 1 is staged after the barrier that
+    // ends chunk c - 1 (its slot's last reader), and its copies land while
+    // chunk c is evaluated; each thread then waits for them and places its
+    // share of their sinogram before the next barrier, which makes both
+    // visible to chunk c + 1's evaluation.
     __syncthreads();  // the previous tile's last chunk is fully consumed
     stage(0);
-    float sv[kSR], svn[kSR];
+    float sv[kSR];
     prefetch(0, sv);
+    land(0, sv);
 
+    const bool inA = i < nx && j < ny, hasB = iB < nx;
     double acc = 0.0, accB = 0.0;  // FP32 within a chunk (a few tens of terms), FP64 across chunks
     for (int c = 0; c < nchunks; ++c) {
-        __syncthreads();  // chunk c's windows visible; chunk c-1 fully consumed
-        if (c + 1 < nchunks) {
-            stage(c + 1);
-            prefetch(c + 1, svn);
-        }
-        const int st = c & 1, slot = c % 3;
-        if (mbar_wait_bounded(&bars[st], parity(c), wait_limit)) {
-            place(c, sv);
-        } else {
-            s_abort = 1;
-            atomicExch(err, 1);
-        }
-        __syncthreads();  // chunk c's sinogram in place
-        if (s_abort) {
+        // chunk c landed, placed and its windows visible; chunk c-1 fully
+        // consumed.  Every thread leaves on the same barrier's answer (a
+        // flag in shared memory could be set for chunk c + 1 by a fast
+        // thread before a slow one has read it for chunk c).
+        if (__syncthreads_or(failed)) {
             drain(c);
             return false;
         }
-#pragma unroll
-        for (int s2 = 0; s2 < kSR; ++s2) sv[s2] = svn[s2];
-        if (j >= ny || i >= nx) continue;
-        const bool hasB = iB < nx;
-        float csum = 0.f, csumB = 0.f;
-#pragma unroll
-        for (int v = 0; v < VC; ++v) {
-            const int lo = win[(slot * VC + v) * 2], hi = win[(slot * VC + v) * 2 + 1];
-            if (hi < lo) continue;
-            int a, b, aB, bB;
-            box_bins_bound(hs + (slot * VC + v) * 8, fi, fj, nu, a, b);
-            box_bins_bound(hs + (slot * VC + v) * 8, fiB, fj, nu, aB, bB);
-            // window-relative ranges; top is the null bin
-            const int top = hi - lo + 1;
-            a = max(a, lo) - lo;
-            b = min(b, hi) - lo;
-            aB = max(aB, lo) - lo;
-            bB = hasB ? min(bB, hi) - lo : -1;
-            const float4* rb = srec + (st * VC + v) * kBackPlanes * WCAP;
-            // per view, each pixel's bins in one loop: trip counts differ by
-            // at most one bin between the lanes of a warp.  (A single flat
-            // loop over all the chunk's (view, bin) pairs, switching views
-            // per lane, measured 1.38x slower at 512^2 x 720 views: the warp
-            // ran the switch on most iterations.)  The two pixels' k-th bins
-            // are evaluated side by side, two independent chains; a pixel
-            // whose bins ran out evaluates the null bin.
-            const int n = max(b - a, bB - aB) + 1;
-#pragma unroll 1
-            for (int k = 0; k < n; ++k) {
-                const float4* qA = rb + (a + k <= b ? a + k : top);
-                const float4* qB = rb + (aB + k <= bB ? aB + k : top);
-                const B1Pair kA = b1_pair(B1Bin{qA[0], qA[WCAP], qA[2 * WCAP], qA[3 * WCAP]});
-                const B1Pair kB = b1_pair(B1Bin{qB[0], qB[WCAP], qB[2 * WCAP], qB[3 * WCAP]});
-                const float sA = qA[3 * WCAP].w, sB = qB[3 * WCAP].w;
-                const float convA = b1_conv_pair(b1_edges2(fi2, b1_inner2(fj2, kA), kA), kA);
-                const float convB = b1_conv_pair(b1_edges2(fiB2, b1_inner2(fj2, kB), kB), kB);
-                if (convA > kConvEps) csum = fmaf(convA, sA, csum);
-                if (convB > kConvEps) csumB = fmaf(convB, sB, csumB);
-            }
+        if (c + 1 < nchunks) {
+            stage(c + 1);
+            prefetch(c + 1, sv);  // chunk c's values are in place: sv is free
         }
-        acc += (double)csum;
-        accB += (double)csumB;
+        const int st = c & 1, slot = c % 3;
+        if (inA) {
+            float csum = 0.f, csumB = 0.f;
+#pragma unroll
+            for (int v = 0; v < VC; ++v) {
+                const int lo = win[(slot * VC + v) * 2], hi = win[(slot * VC + v) * 2 + 1];
+                if (hi < lo) continue;
+                int a, b, aB, bB;
+                box_bins_bound(hs + (slot * VC + v) * 8, fi, fj, nu, a, b);
+                box_bins_bound(hs + (slot * VC + v) * 8, fiB, fj, nu, aB, bB);
+                // window-relative ranges; top is the null bin
+                const int top = hi - lo + 1;
+                a = max(a, lo) - lo;
+                b = min(b, hi) - lo;
+                aB = max(aB, lo) - lo;
+                bB = hasB ? min(bB, hi) - lo : -1;
+                const float4* rb = srec + (st * VC + v) * kBackPlanes * WCAP;
+                // per view, each pixel's bins in one loop: trip counts differ by
+                // at most one bin between the lanes of a warp.  (A single flat
+                // loop over all the chunk's (view, bin) pairs, switching views
+                // per lane, measured 1.38x slower at 512^2 x 720 views: the warp
+                // ran the switch on most iterations.)  The two pixels' k-th bins
+                // are evaluated side by side, two independent chains; a pixel
+                // whose bins ran out evaluates the null bin.
+                const int n = max(b - a, bB - aB) + 1;
+#pragma unroll 1
+                for (int k = 0; k < n; ++k) {
+                    const float4* qA = rb + (a + k <= b ? a + k : top);
+                    const float4* qB = rb + (aB + k <= bB ? aB + k : top);
+                    const B1Pair kA = b1_pair(B1Bin{qA[0], qA[WCAP], qA[2 * WCAP], qA[3 * WCAP]});
+                    const B1Pair kB = b1_pair(B1Bin{qB[0], qB[WCAP], qB[2 * WCAP], qB[3 * WCAP]});
+                    const float sA = qA[3 * WCAP].w, sB = qB[3 * WCAP].w;
+                    const float convA = b1_conv_pair(b1_edges2(fi2, b1_inner2(fj2, kA), kA), kA);
+                    const float convB = b1_conv_pair(b1_edges2(fiB2, b1_inner2(fj2, kB), kB), kB);
+                    if (convA > kConvEps) csum = fmaf(convA, sA, csum);
+                    if (convB > kConvEps) csumB = fmaf(convB, sB, csumB);
+                }
+            }
+            acc += (double)csum;
+            accB += (double)csumB;
+        }
+        if (c + 1 < nchunks) land(c + 1, sv);
     }
     use0 += (uint32_t)((nchunks + 1) >> 1);
     use1 += (uint32_t)(nchunks >> 1);
