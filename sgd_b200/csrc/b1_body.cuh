@@ -164,9 +164,12 @@ __device__ __forceinline__ bool b1_back_tile(const float4* __restrict__ rec, con
 
     // warp w covers columns j0 + 8w .. + 7 of rows i0 .. i0 + 3 (pixel A) and
     // of rows i0 + 4 .. i0 + 7 (pixel B): 8 x 4 blocks whose lanes read few
-    // distinct bins of a view
+    // distinct bins of a view.  Each quarter-warp (the lanes of one shared
+    // memory wavefront of 16-byte loads) takes a 2 x 4 block of it, whose
+    // bins span fewer 16-byte words than a row of 8 pixels would
     const int tid = threadIdx.x, w = tid >> 5, l = tid & 31;
-    const int i = i0 + (l >> 3), j = j0 + 8 * w + (l & 7), iB = i + 4;
+    const int quarter = l >> 3, r = l & 7;
+    const int i = i0 + 2 * (quarter >> 1) + (r >> 2), j = j0 + 8 * w + 4 * (quarter & 1) + (r & 3), iB = i + 4;
     const float fi = (float)i, fj = (float)j, fiB = (float)iB;
     const float2 fi2 = pair(fi), fj2 = pair(fj), fiB2 = pair(fiB);
     const int nchunks = (np + VC - 1) / VC;
